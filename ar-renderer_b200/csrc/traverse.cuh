@@ -1,0 +1,231 @@
+// BVH traversal for sm_100a: closest-hit and any-hit queries over the caller's binary BVH, with
+// results bit-identical to the reference CPU routines pr::BVH::Intersect / IntersectP
+// (src/geometry/bvh.cpp:137-232) and pr::Triangle::Intersect (src/geometry/shape.cpp:202-222).
+//
+// Layout (built on the device from the v4 node array by convert_nodes in accel.cu):
+//   WNode, 64 B, one per INTERIOR reference node: both children's boxes plus their references,
+//   so one node visit issues four 16-byte loads that bring both child boxes at once. A child
+//   reference >= 0 names an interior WNode; < 0 is a leaf whose first leaf slot is ~ref.
+//   LeafPrim, 48 B per leaf slot (primOrder order): triangle p0 | e1 = p1 - p0 | e2 = p2 - p0 and
+//   the original primitive index; spheres store centre and radius (64-bit test, as the CPU).
+//   The last slot of every leaf carries an end mark, so a stack entry is just (ref, entry t).
+//
+// Parity. The reference pops a node, tests its own box against the CURRENT tMax, and pushes the
+// far child before descending into the near one (near = by the sign of the split axis). Here a
+// parent tests both child boxes at once, but only the tMax-independent part of the far child's
+// test is evaluated early: its entry distance is pushed with it and compared against the tMax
+// current at pop time, exactly the reference's final `tMin < tMax` clause. Every arithmetic step
+// is an explicitly rounded IEEE operation (__fadd_rn/__fmul_rn/__fdiv_rn, never contracted into
+// an FMA), so box decisions, visit order, tMax updates and hits match bit for bit.
+#pragma once
+
+#include "common.cuh"
+
+namespace prb {
+
+struct __align__(16) WNode {
+    float4 a;  // c0.min.x c0.min.y c0.min.z c0.max.x
+    float4 b;  // c0.max.y c0.max.z c1.min.x c1.min.y
+    float4 c;  // c1.min.z c1.max.x c1.max.y c1.max.z
+    int4 r;    // ref0, ref1, axis, unused
+};
+
+struct __align__(16) LeafPrim {
+    float4 v0;  // triangle: p0, prim index (int bits); sphere: centre, prim index
+    float4 v1;  // triangle: e1, kind 0; sphere: radius, 0, 0, kind 1
+    float4 v2;  // triangle: e2, end-of-leaf mark (int bits 1 on a leaf's last slot, else 0)
+};
+
+constexpr int kStackSize = 64;
+// 1 + 2 * 1.2e-7f * 3 evaluated in float, the far-distance widening of bvh.cpp:143-151.
+constexpr float kWiden = 0x1.00000cp+0f;
+
+struct TraceRay {
+    V3 o, d, inv;
+    int neg[3];
+};
+
+__device__ __forceinline__ TraceRay make_trace_ray(V3 o, V3 d) {
+    TraceRay r;
+    r.o = o;
+    r.d = d;
+    r.inv = {__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z)};
+    r.neg[0] = r.inv.x < 0.f;
+    r.neg[1] = r.inv.y < 0.f;
+    r.neg[2] = r.inv.z < 0.f;
+    return r;
+}
+
+// The tMax-independent part of the reference slab test (bvh.cpp:137-156): returns false when the
+// box is rejected for every tMax; otherwise writes the entry distance tMin, and the box is hit
+// iff tMin < tMax. Comparison order follows the reference so NaN cases resolve the same way.
+__device__ __forceinline__ bool box_entry(const TraceRay &r, float lox, float loy, float loz, float hix, float hiy,
+                                          float hiz, float *tEntry) {
+    float nx = r.neg[0] ? hix : lox, fx = r.neg[0] ? lox : hix;
+    float ny = r.neg[1] ? hiy : loy, fy = r.neg[1] ? loy : hiy;
+    float nz = r.neg[2] ? hiz : loz, fz = r.neg[2] ? loz : hiz;
+    float tMin = __fmul_rn(__fsub_rn(nx, r.o.x), r.inv.x);
+    float tMaxX = __fmul_rn(__fsub_rn(fx, r.o.x), r.inv.x);
+    float tyMin = __fmul_rn(__fsub_rn(ny, r.o.y), r.inv.y);
+    float tyMax = __fmul_rn(__fsub_rn(fy, r.o.y), r.inv.y);
+    tMaxX = __fmul_rn(tMaxX, kWiden);
+    tyMax = __fmul_rn(tyMax, kWiden);
+    if (tMin > tyMax || tyMin > tMaxX) return false;
+    if (tyMin > tMin) tMin = tyMin;
+    if (tyMax < tMaxX) tMaxX = tyMax;
+    float tzMin = __fmul_rn(__fsub_rn(nz, r.o.z), r.inv.z);
+    float tzMax = __fmul_rn(__fsub_rn(fz, r.o.z), r.inv.z);
+    tzMax = __fmul_rn(tzMax, kWiden);
+    if (tMin > tzMax || tzMin > tMaxX) return false;
+    if (tzMin > tMin) tMin = tzMin;
+    if (tzMax < tMaxX) tMaxX = tzMax;
+    *tEntry = tMin;
+    return tMaxX > 0.f;
+}
+
+// Möller-Trumbore in the reference's exact operation order (shape.cpp:202-222).
+__device__ __forceinline__ float dot_rn(float ax, float ay, float az, float bx, float by, float bz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+__device__ __forceinline__ bool hit_triangle(const TraceRay &r, float4 v0, float4 v1, float4 v2, float tMax, float *tHit,
+                                             float *bu, float *bv) {
+    // pvec = d x e2
+    float px = __fsub_rn(__fmul_rn(r.d.y, v2.z), __fmul_rn(r.d.z, v2.y));
+    float py = __fsub_rn(__fmul_rn(r.d.z, v2.x), __fmul_rn(r.d.x, v2.z));
+    float pz = __fsub_rn(__fmul_rn(r.d.x, v2.y), __fmul_rn(r.d.y, v2.x));
+    float det = dot_rn(v1.x, v1.y, v1.z, px, py, pz);
+    if (det == 0.f || !isfinite(det)) return false;
+    float inv = __fdiv_rn(1.f, det);
+    float tx = __fsub_rn(r.o.x, v0.x), ty = __fsub_rn(r.o.y, v0.y), tz = __fsub_rn(r.o.z, v0.z);
+    float u = __fmul_rn(dot_rn(tx, ty, tz, px, py, pz), inv);
+    if (u < 0.f || u > 1.f) return false;
+    // qvec = tvec x e1
+    float qx = __fsub_rn(__fmul_rn(ty, v1.z), __fmul_rn(tz, v1.y));
+    float qy = __fsub_rn(__fmul_rn(tz, v1.x), __fmul_rn(tx, v1.z));
+    float qz = __fsub_rn(__fmul_rn(tx, v1.y), __fmul_rn(ty, v1.x));
+    float v = __fmul_rn(dot_rn(r.d.x, r.d.y, r.d.z, qx, qy, qz), inv);
+    if (v < 0.f || __fadd_rn(u, v) > 1.f) return false;
+    float t = __fmul_rn(dot_rn(v2.x, v2.y, v2.z, qx, qy, qz), inv);
+    if (t <= 0.f || t >= tMax) return false;
+    *tHit = t;
+    *bu = u;
+    *bv = v;
+    return true;
+}
+
+// Robust sphere quadratic in double precision, as pr::Sphere::Intersect (shape.cpp:42-61).
+__device__ __forceinline__ bool hit_sphere(const TraceRay &r, float4 v0, float4 v1, float tMax, float *tHit) {
+    // The origin offset is a float subtraction widened afterwards, as in the reference.
+    double ox = __fsub_rn(r.o.x, v0.x), oy = __fsub_rn(r.o.y, v0.y), oz = __fsub_rn(r.o.z, v0.z);
+    double dx = r.d.x, dy = r.d.y, dz = r.d.z;
+    double rad = v1.x;
+    double a = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    double b = __dadd_rn(__dadd_rn(__dmul_rn(ox, dx), __dmul_rn(oy, dy)), __dmul_rn(oz, dz));
+    double c = __dsub_rn(__dadd_rn(__dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)), __dmul_rn(oz, oz)),
+                         __dmul_rn(rad, rad));
+    double k = __ddiv_rn(b, a);
+    double lx = __dsub_rn(ox, __dmul_rn(k, dx)), ly = __dsub_rn(oy, __dmul_rn(k, dy)),
+           lz = __dsub_rn(oz, __dmul_rn(k, dz));
+    double disc = __dsub_rn(__dmul_rn(rad, rad),
+                            __dadd_rn(__dadd_rn(__dmul_rn(lx, lx), __dmul_rn(ly, ly)), __dmul_rn(lz, lz)));
+    if (disc < 0.0) return false;
+    double q = __dsub_rn(-b, copysign(__dsqrt_rn(__dmul_rn(a, disc)), b));
+    double t0 = __ddiv_rn(c, q), t1 = __ddiv_rn(q, a);
+    if (t0 > t1) {
+        double s = t0;
+        t0 = t1;
+        t1 = s;
+    }
+    double t = t0;
+    if (t <= 0.0) t = t1;
+    if (t <= 0.0 || t >= double(tMax)) return false;
+    *tHit = float(t);
+    return true;
+}
+
+struct Hit {
+    float t, u, v;
+    int prim;  // original primitive index, -1 = none
+};
+
+// Closest hit (kAny = false) or any hit (kAny = true) with t in (0, tMax). Spheres are tested only
+// when kSpheres. rootRef describes the root (interior WNode 0, or a single leaf), rootBox its
+// bounds. Sets *overflow (and stops) when the traversal stack would overflow.
+template <bool kAny, bool kSpheres>
+__device__ __forceinline__ bool traverse(const WNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
+                                         const float *__restrict__ rootBox, int rootRef, const TraceRay &r,
+                                         float tMax, Hit *hit, bool *overflow) {
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    int sp = 0;
+    bool found = false;
+    float tEntry;
+    if (!box_entry(r, rootBox[0], rootBox[1], rootBox[2], rootBox[3], rootBox[4], rootBox[5], &tEntry) ||
+        !(tEntry < tMax))
+        return false;
+    int ref = rootRef;
+    while (true) {
+        if (ref >= 0) {
+            const WNode *n = nodes + ref;
+            float4 a = __ldg(&n->a), b = __ldg(&n->b), c = __ldg(&n->c);
+            int4 rr = __ldg(&n->r);
+            float t0, t1;
+            bool h0 = box_entry(r, a.x, a.y, a.z, a.w, b.x, b.y, &t0);
+            bool h1 = box_entry(r, b.z, b.w, c.x, c.y, c.z, c.w, &t1);
+            // Near child by the sign of the split axis (bvh.cpp:184-190): the second child first
+            // when the ray runs towards -axis.
+            bool secondFirst = r.neg[rr.z];
+            int nRef = secondFirst ? rr.y : rr.x, fRef = secondFirst ? rr.x : rr.y;
+            bool nHit = secondFirst ? h1 : h0, fHit = secondFirst ? h0 : h1;
+            float nT = secondFirst ? t1 : t0, fT = secondFirst ? t0 : t1;
+            if (fHit) {
+                if (sp >= kStackSize) {
+                    *overflow = true;
+                    return found;
+                }
+                stackRef[sp] = fRef;
+                stackT[sp] = fT;
+                ++sp;
+            }
+            if (nHit && nT < tMax) {
+                ref = nRef;
+                continue;
+            }
+        } else {
+            const LeafPrim *p = prims + ~ref;
+            for (bool last = false; !last; ++p) {
+                float4 v0 = __ldg(&p->v0), v1 = __ldg(&p->v1), v2 = __ldg(&p->v2);
+                last = __float_as_int(v2.w) != 0;
+                float t, u = 0.f, v = 0.f;
+                bool h;
+                if (kSpheres && __float_as_int(v1.w) == 1)
+                    h = hit_sphere(r, v0, v1, tMax, &t);
+                else
+                    h = hit_triangle(r, v0, v1, v2, tMax, &t, &u, &v);
+                if (h) {
+                    if (kAny) return true;
+                    tMax = t;
+                    hit->t = t;
+                    hit->u = u;
+                    hit->v = v;
+                    hit->prim = __float_as_int(v0.w);
+                    found = true;
+                }
+            }
+        }
+        // Pop: a deferred far child is visited only if its entry is still before tMax.
+        bool next = false;
+        while (sp > 0) {
+            --sp;
+            if (stackT[sp] < tMax) {
+                ref = stackRef[sp];
+                next = true;
+                break;
+            }
+        }
+        if (!next) break;
+    }
+    return found;
+}
+
+} // namespace prb

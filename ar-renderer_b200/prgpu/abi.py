@@ -1,0 +1,201 @@
+"""ctypes/numpy mirror of include/prgpu_api.h and include/prhost_api.h.
+
+Array-valued fields (BVH nodes, primitives, materials, lights, spectra, media, light-BVH nodes)
+are numpy structured arrays with the exact byte layout of the C structs; the fixed-size structs
+(SceneDesc, Camera, Filter, RenderParams, ...) are ctypes Structures. The libraries are loaded
+from the package directory; a missing library raises -- there is no fallback path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GPU_LIB_PATH = os.path.join(PKG, "libprender_gpu.so")
+HOST_LIB_PATH = os.path.join(PKG, "libprender_host.so")
+
+API_VERSION = 4
+EXT_VERSION = 5
+SPECTRUM_SAMPLES = 95
+SPECTRUM_MIN = 360.0
+SPECTRUM_STEP = 5.0
+FILTER_BINS = 64
+SHEEN_MU, SHEEN_ALPHA = 32, 16
+
+PRIM_TRIANGLE, PRIM_SPHERE = 0, 1
+MAT_DIFFUSE, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_BLACK, MAT_INTERFACE, MAT_COATED_DIFFUSE, MAT_COATED_CONDUCTOR = range(7)
+FILTER_BOX, FILTER_GAUSSIAN, FILTER_BLACKMAN_HARRIS = range(3)
+LIGHT_AREA, LIGHT_POINT = range(2)
+
+# ---------------------------------------------------------------------------------------------
+# numpy layouts of the array structs
+
+F3 = ("<f4", (3,))
+BVH_NODE = np.dtype({"names": ["bmin", "bmax", "offset", "nPrims", "axis", "pad"],
+                     "formats": [F3, F3, "<i4", "<u2", "u1", "u1"],
+                     "offsets": [0, 12, 24, 28, 30, 31], "itemsize": 32})
+PRIMITIVE = np.dtype({"names": ["type", "material", "light", "mediumInside", "mediumOutside", "pad",
+                                "p0", "p1", "p2", "n0", "n1", "n2", "uv", "r", "flip"],
+                      "formats": ["<u4", "<i4", "<i4", "<i4", "<i4", "<u4", F3, F3, F3, F3, F3, F3,
+                                  ("<f4", (6,)), "<f4", "<u4"],
+                      "offsets": [0, 4, 8, 12, 16, 20, 24, 36, 48, 60, 72, 84, 96, 120, 124],
+                      "itemsize": 128})
+MATERIAL = np.dtype({"names": ["type", "albedo", "albedoB", "checkerScale", "eta", "k", "alphaX", "alphaY",
+                               "dispersive", "thin", "coatEta", "coatAlpha", "thickness", "coatG", "coatAlbedo",
+                               "coatDispersive", "coatMaxDepth", "coatSamples", "sheenColor", "sheenRoughness",
+                               "sheenWeight", "pad"],
+                     "formats": ["<u4", "<i4", "<i4", "<f4", "<i4", "<i4", "<f4", "<f4", "<u4", "<u4", "<i4",
+                                 "<f4", "<f4", "<f4", "<i4", "<u4", "<i4", "<i4", "<i4", "<f4", "<f4", "<u4"],
+                     "offsets": [4 * i for i in range(22)], "itemsize": 88})
+MEDIUM = np.dtype({"names": ["sigmaA", "sigmaS", "scale", "g"], "formats": ["<i4", "<i4", "<f4", "<f4"],
+                   "offsets": [0, 4, 8, 12], "itemsize": 16})
+LIGHT = np.dtype({"names": ["type", "primitive", "spectrum", "scale", "position", "twoSided", "cosPower", "area",
+                            "pmf", "pad"],
+                  "formats": ["<u4", "<i4", "<i4", "<f4", F3, "<u4", "<f4", "<f4", "<f4", "<u4"],
+                  "offsets": [0, 4, 8, 12, 16, 28, 32, 36, 40, 44], "itemsize": 48})
+SPECTRUM = np.dtype(("<f4", (SPECTRUM_SAMPLES,)))
+LIGHT_BVH_NODE = np.dtype({"names": ["bmin", "bmax", "w", "phi", "cosThetaO", "cosThetaE", "twoSided", "child1",
+                                     "light", "parent", "pad"],
+                           "formats": [F3, F3, F3, "<f4", "<f4", "<f4", "<i4", "<i4", "<i4", "<i4", ("<i4", (2,))],
+                           "offsets": [0, 12, 24, 36, 40, 44, 48, 52, 56, 60, 64], "itemsize": 72})
+RAY = np.dtype({"names": ["o", "tMax", "d", "pad"], "formats": [F3, "<f4", F3, "<f4"],
+                "offsets": [0, 12, 16, 28], "itemsize": 32})
+
+
+# ---------------------------------------------------------------------------------------------
+# ctypes structs
+
+class Float3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("cameraToWorld", C.c_float * 12), ("tanHalfFov", C.c_float), ("aspect", C.c_float),
+                ("lensRadius", C.c_float), ("focalDistance", C.c_float), ("width", C.c_int32),
+                ("height", C.c_int32), ("margin", C.c_int32), ("pad", C.c_uint32)]
+
+
+class Filter(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("radius", C.c_float), ("sigma", C.c_float), ("norm", C.c_float),
+                ("cdf", C.c_float * (FILTER_BINS + 1))]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("apiVersion", C.c_int32), ("nodes", C.c_void_p), ("nodeCount", C.c_int32),
+                ("primOrder", C.c_void_p), ("prims", C.c_void_p), ("primCount", C.c_int32),
+                ("materials", C.c_void_p), ("materialCount", C.c_int32), ("lights", C.c_void_p),
+                ("lightCount", C.c_int32), ("spectra", C.c_void_p), ("spectrumCount", C.c_int32),
+                ("media", C.c_void_p), ("mediumCount", C.c_int32), ("cameraMedium", C.c_int32),
+                ("envSpectrum", C.c_int32), ("envScale", C.c_float), ("envPmf", C.c_float),
+                ("worldCenter", Float3), ("worldRadius", C.c_float), ("camera", Camera), ("filter", Filter),
+                ("sheenAlbedo", C.c_void_p), ("cie", C.c_void_p), ("cieYIntegral", C.c_float)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("spp", C.c_int32), ("firstSample", C.c_int32), ("seed", C.c_uint64), ("maxDepth", C.c_int32),
+                ("clampLuminance", C.c_float)]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("globalMemory", C.c_uint64), ("computeUnits", C.c_int32),
+                ("isGpu", C.c_int32), ("backend", C.c_char * 32)]
+
+
+class SceneExt(C.Structure):
+    _fields_ = [("structSize", C.c_uint32), ("lightBVHNodeCount", C.c_int32), ("lightBVH", C.c_void_p),
+                ("lightBVHProb", C.c_float), ("wavefrontPaths", C.c_int32), ("blockSize", C.c_int32),
+                ("flags", C.c_int32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("pathSamples", C.c_uint64), ("closestRays", C.c_uint64), ("shadowRays", C.c_uint64),
+                ("bounces", C.c_uint64), ("kernelLaunches", C.c_uint64), ("deviceMs", C.c_double),
+                ("traceMs", C.c_double), ("shadowMs", C.c_double), ("shadeMs", C.c_double),
+                ("filmMs", C.c_double)]
+
+
+assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
+assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
+assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512
+
+# ---------------------------------------------------------------------------------------------
+# Library loading
+
+_P = C.c_void_p
+_ERR = [C.c_char_p, C.c_int]
+_gpu = None
+_host = None
+
+
+def _bind(lib, name, argtypes, restype) -> None:
+    """Declare a prototype; symbols the library does not export are left unbound (calling them
+    raises AttributeError), and tests/test_abi.py checks the export list against the headers."""
+    if hasattr(lib, name):
+        f = getattr(lib, name)
+        f.argtypes = argtypes
+        f.restype = restype
+
+
+def gpu_lib() -> C.CDLL:
+    """The CUDA module. Raises if it has not been built."""
+    global _gpu
+    if _gpu is None:
+        if not os.path.exists(GPU_LIB_PATH):
+            raise RuntimeError(f"{GPU_LIB_PATH} is missing: run ar-renderer_b200/build.py")
+        lib = C.CDLL(GPU_LIB_PATH)
+        _bind(lib, "prgpu_api_version", [], C.c_int)
+        _bind(lib, "prgpu_ext_version", [], C.c_int)
+        _bind(lib, "prgpu_launch_count", [], C.c_uint64)
+        _bind(lib, "prgpu_list_devices", [_P, C.c_int], C.c_int)
+        _bind(lib, "prgpu_render", [C.c_int, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_render_ex", [C.c_int, _P, _P, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
+                                        _P, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_accel_create", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, C.POINTER(_P), *_ERR], C.c_int)
+        _bind(lib, "prgpu_accel_trace", [_P, _P, C.c_int64, C.c_int32, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_accel_trace_host", [_P, _P, C.c_int64, C.c_int32, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_accel_status", [_P], C.c_int)
+        _bind(lib, "prgpu_accel_bytes", [_P], C.c_int64)
+        _bind(lib, "prgpu_accel_destroy", [_P], None)
+        _gpu = lib
+    return _gpu
+
+
+def host_lib() -> C.CDLL:
+    global _host
+    if _host is None:
+        if not os.path.exists(HOST_LIB_PATH):
+            raise RuntimeError(f"{HOST_LIB_PATH} is missing: run ar-renderer_b200/build.py")
+        lib = C.CDLL(HOST_LIB_PATH)
+        lib.prhost_build_bvh.argtypes = [_P, _P, C.c_int64, C.c_int32, C.c_int32, _P, _P]
+        lib.prhost_build_bvh.restype = C.c_int64
+        lib.prhost_build_bvh_triangles.argtypes = [_P, C.c_int64, C.c_int32, C.c_int32, _P, _P]
+        lib.prhost_build_bvh_triangles.restype = C.c_int64
+        lib.prhost_build_light_bvh.argtypes = [_P, C.c_int32, _P]
+        lib.prhost_build_light_bvh.restype = C.c_int32
+        _host = lib
+    return _host
+
+
+def ptr(a) -> C.c_void_p | None:
+    """Address of a contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "arrays passed across the C ABI must be contiguous"
+    return C.c_void_p(a.ctypes.data)
+
+
+class PrgpuError(RuntimeError):
+    pass
+
+
+def err_buf():
+    return C.create_string_buffer(1024)
+
+
+def check(rc: int, err, what: str) -> None:
+    if rc != 0:
+        raise PrgpuError(f"{what} failed: {err.value.decode(errors='replace')}")

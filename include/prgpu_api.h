@@ -1,0 +1,292 @@
+// prgpu_api.h -- the C ABI of libprender_gpu.so, the B200 (sm_100a) path-tracing module.
+//
+// The first part restates, layout for layout, the plain-data interface that PRender's host
+// (src/integrators/gpu_path.cpp) hands its GPU module, so that this library is a drop-in for
+// prender_gpu: the reference declares it in src/gpu/gpu_api.h:15-173 and checks
+// prgpu_api_version() == 4 before use (src/integrators/gpu_path.cpp:59-65). Every struct below
+// must stay byte-identical to those layouts; static_asserts in the implementation pin sizes and
+// offsets.
+//
+// The second part (PRGPU extension, version 5) adds entry points the v4 interface cannot
+// express: a ray-query service over a caller BVH, an FP64 film with fixed-order accumulation,
+// light-BVH next-event estimation, device-resident handles for benchmarking, and run
+// statistics. A v4 caller never sees them.
+//
+// All pointers are caller-owned host memory unless the name says "device"; they need only be
+// valid for the duration of the call. Entry points never throw; they return 0 on success and
+// otherwise write a NUL-terminated message into err (when err != nullptr and errLen > 0).
+#pragma once
+
+#include <cstdint>
+
+#if defined(_WIN32)
+#define PRGPU_API extern "C" __declspec(dllexport)
+#else
+#define PRGPU_API extern "C" __attribute__((visibility("default")))
+#endif
+
+namespace prgpu {
+
+// --------------------------------------------------------------------------------------------
+// v4 plain-data layouts (src/gpu/gpu_api.h:17-162)
+
+constexpr int kApiVersion = 4;          // gpu_api.h:17
+constexpr int kExtVersion = 5;          // this library's extension level
+constexpr int kSpectrumSamples = 95;    // 360..830 nm every 5 nm, linear interpolation (gpu_api.h:19-21)
+constexpr float kSpectrumMin = 360.f, kSpectrumStep = 5.f;
+constexpr int kFilterBins = 64;         // pixel-filter CDF bins (gpu_api.h:22-23)
+constexpr int kSheenMu = 32, kSheenAlpha = 16;  // sheen albedo table (gpu_api.h:24-25)
+
+struct Float3 {
+    float x, y, z;
+};
+
+struct Spectrum {
+    float v[kSpectrumSamples];
+};
+
+// Flattened binary BVH node, depth-first: an interior node's first child follows it, `offset`
+// names the second child; a leaf covers primOrder[offset .. offset+nPrims). (gpu_api.h:35-40)
+struct BVHNode {
+    Float3 bmin, bmax;
+    int32_t offset;
+    uint16_t nPrims;  // 0 = interior
+    uint8_t axis, pad;
+};
+
+enum PrimType : uint32_t { PrimTriangle = 0, PrimSphere = 1 };
+
+// One primitive: a triangle (p0..p2, optional vertex normals n0..n2 -- n0 == 0 means flat -- and
+// uvs) or a sphere (centre p0, radius r, flip = inward normals). (gpu_api.h:44-56)
+struct Primitive {
+    uint32_t type;
+    int32_t material;
+    int32_t light;                        // area light index or -1
+    int32_t mediumInside, mediumOutside;  // medium on each side, -1 = vacuum
+    uint32_t pad;
+    Float3 p0, p1, p2;
+    Float3 n0, n1, n2;
+    float u0, v0, u1, v1, u2, v2;
+    float r;
+    uint32_t flip;
+};
+
+enum MaterialType : uint32_t {
+    MatDiffuse = 0, MatConductor = 1, MatDielectric = 2, MatBlack = 3, MatInterface = 4,
+    MatCoatedDiffuse = 5, MatCoatedConductor = 6
+};
+
+// Material parameters; spectra are indices into SceneDesc::spectra, -1 = none. (gpu_api.h:61-81)
+struct Material {
+    uint32_t type;
+    int32_t albedo, albedoB;  // reflectance (diffuse / artist conductor); checker second colour
+    float checkerScale;       // checker frequency in uv, 0 = plain
+    int32_t eta, k;           // conductor n, k; dielectric IOR
+    float alphaX, alphaY;     // GGX alpha (roughness^2); max < 1e-3 = smooth
+    uint32_t dispersive;      // IOR varies with wavelength -> secondary wavelengths terminate
+    uint32_t thin;
+    int32_t coatEta;
+    float coatAlpha, thickness, coatG;
+    int32_t coatAlbedo;
+    uint32_t coatDispersive;
+    int32_t coatMaxDepth, coatSamples;
+    int32_t sheenColor;
+    float sheenRoughness, sheenWeight;
+    uint32_t pad;
+};
+
+// Homogeneous medium: sigma = spectrum * scale, Henyey-Greenstein g. (gpu_api.h:84-87)
+struct Medium {
+    int32_t sigmaA, sigmaS;
+    float scale, g;
+};
+
+enum FilterType : uint32_t { FilterBox = 0, FilterGaussian = 1, FilterBlackmanHarris = 2 };
+
+struct Filter {  // gpu_api.h:91-95
+    uint32_t type;
+    float radius, sigma, norm;
+    float cdf[kFilterBins + 1];
+};
+
+enum LightType : uint32_t { LightArea = 0, LightPoint = 1 };
+
+struct Light {  // gpu_api.h:99-110
+    uint32_t type;
+    int32_t primitive;  // area: emitting primitive
+    int32_t spectrum;   // radiance (area) or intensity (point)
+    float scale;
+    Float3 position;    // point light
+    uint32_t twoSided;
+    float cosPower;
+    float area;
+    float pmf;          // power-based selection probability
+    uint32_t pad;
+};
+
+struct Camera {  // gpu_api.h:112-118
+    float cameraToWorld[12];  // row-major 3x4
+    float tanHalfFov, aspect;
+    float lensRadius, focalDistance;
+    int32_t width, height, margin;
+    uint32_t pad;
+};
+
+struct SceneDesc {  // gpu_api.h:120-146
+    int32_t apiVersion;
+    const BVHNode *nodes;
+    int32_t nodeCount;
+    const int32_t *primOrder;
+    const Primitive *prims;
+    int32_t primCount;
+    const Material *materials;
+    int32_t materialCount;
+    const Light *lights;
+    int32_t lightCount;
+    const Spectrum *spectra;
+    int32_t spectrumCount;
+    const Medium *media;
+    int32_t mediumCount;
+    int32_t cameraMedium;
+    int32_t envSpectrum;
+    float envScale;
+    float envPmf;
+    Float3 worldCenter;
+    float worldRadius;
+    Camera camera;
+    Filter filter;
+    const float *sheenAlbedo;  // kSheenAlpha * kSheenMu
+    const float *cie;          // 3 x kSpectrumSamples
+    float cieYIntegral;
+};
+
+struct RenderParams {  // gpu_api.h:148-154
+    int32_t spp;
+    int32_t firstSample;
+    uint64_t seed;
+    int32_t maxDepth;       // <= 0: unlimited (Russian roulette)
+    float clampLuminance;   // 0 = off
+};
+
+struct DeviceInfo {  // gpu_api.h:156-162
+    char name[256];
+    uint64_t globalMemory;
+    int32_t computeUnits;
+    int32_t isGpu;
+    char backend[32];
+};
+
+// --------------------------------------------------------------------------------------------
+// Extension (v5) plain-data layouts. No counterpart in src/gpu/gpu_api.h.
+
+// A ray for the ray-query service: origin, tMax, direction (32 bytes; 16-byte aligned pairs).
+struct Ray {
+    Float3 o;
+    float tMax;
+    Float3 d;
+    float pad;
+};
+
+// Light-BVH node for importance-based next-event estimation, the flattened form of
+// pr::BVHLightSampler's tree (src/lights/light_bvh.h:23-35, built as in light_bvh.cpp:117-177).
+// Interior nodes: first child follows, child1 names the second; leaves: light >= 0 (index into
+// SceneDesc::lights). parent = -1 at the root.
+struct LightBVHNode {
+    Float3 bmin, bmax;
+    Float3 w;             // emission cone axis
+    float phi;            // power bound
+    float cosThetaO, cosThetaE;
+    int32_t twoSided;
+    int32_t child1, light, parent;
+    int32_t pad[2];
+};
+
+// Optional extras for prgpu_render_ex (zero-initialise, then set structSize = sizeof(SceneExt)).
+struct SceneExt {
+    uint32_t structSize;
+    int32_t lightBVHNodeCount;      // 0 = power-based light selection (the v4 behaviour)
+    const LightBVHNode *lightBVH;
+    float lightBVHProb;             // probability of the BVH branch when envSpectrum >= 0 (1 - pInfinite)
+    int32_t wavefrontPaths;         // paths in flight per wavefront (0 = library default)
+    int32_t blockSize;              // threads per block for the wavefront kernels (0 = default)
+    int32_t flags;                  // bit 0: keep the FP64 film on the device between calls
+};
+
+// Per-call counters and device timings.
+struct RenderStats {
+    uint64_t pathSamples;      // camera samples traced
+    uint64_t closestRays;      // closest-hit queries
+    uint64_t shadowRays;       // shadow (any-hit / transmittance) queries
+    uint64_t bounces;          // wavefront iterations
+    uint64_t kernelLaunches;   // kernels launched by this call
+    double deviceMs;           // device time of the render (CUDA events)
+    double traceMs;            // device time in the closest-hit kernel
+    double shadowMs;           // device time in the shadow kernel
+    double shadeMs;            // device time in the shading kernel
+    double filmMs;             // device time in the film kernel
+};
+
+} // namespace prgpu
+
+// --------------------------------------------------------------------------------------------
+// v4 entry points -- the exact set prender_gpu exports (src/gpu/gpu_api.h:166-173), resolved by
+// name in src/integrators/gpu_path.cpp:59-61.
+
+// Returns prgpu::kApiVersion (4). Replaces prgpu_api_version, gpu_api.h:173.
+PRGPU_API int prgpu_api_version();
+
+// Writes up to max CUDA devices; returns the number written. Replaces prgpu_list_devices,
+// gpu_api.h:166-167 (backend reads "cuda").
+PRGPU_API int prgpu_list_devices(prgpu::DeviceInfo *out, int max);
+
+// Renders params->spp samples per pixel (sample indices firstSample .. firstSample+spp-1) and
+// ADDS the unnormalised per-pixel XYZ sums into outXYZ (3 floats per pixel, raster order).
+// Deterministic in (seed, pixel, sample index). Replaces prgpu_render, gpu_api.h:168-172.
+PRGPU_API int prgpu_render(int deviceIndex, const prgpu::SceneDesc *scene, const prgpu::RenderParams *params,
+                           float *outXYZ, char *err, int errLen);
+
+// --------------------------------------------------------------------------------------------
+// Extension entry points (no counterpart in src/gpu/gpu_api.h)
+
+// Returns prgpu::kExtVersion (5).
+PRGPU_API int prgpu_ext_version();
+
+// Like prgpu_render, but ADDS FP64 sums (each pixel's samples added one at a time in sample-index
+// order, so splitting a render into batches gives bit-identical sums), accepts the optional
+// SceneExt (light BVH, wavefront sizing) and reports RenderStats (either may be null).
+PRGPU_API int prgpu_render_ex(int deviceIndex, const prgpu::SceneDesc *scene, const prgpu::SceneExt *ext,
+                              const prgpu::RenderParams *params, double *outXYZ, prgpu::RenderStats *stats,
+                              char *err, int errLen);
+
+// Ray queries against a caller BVH over a triangle soup (the reference CPU routines are
+// pr::BVH::Intersect / IntersectP, src/geometry/bvh.cpp:158-232; triangle test
+// pr::Triangle::Intersect, src/geometry/shape.cpp:202-222). Triangles are 3 vertices each, indexed
+// by primitive; nodes/primOrder as in SceneDesc. Closest hit (anyHit = 0) writes primOut = the
+// hit primitive (-1 = miss), tOut = its distance, b1Out/b2Out = barycentrics (each may be null).
+// Any hit (anyHit = 1) writes primOut = 1 (occluded) or 0. Inputs and outputs are host memory.
+PRGPU_API int prgpu_trace_rays(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
+                               const int32_t *primOrder, const prgpu::Float3 *triVerts, int32_t primCount,
+                               const prgpu::Ray *rays, int64_t rayCount, int32_t anyHit, int32_t *primOut,
+                               float *tOut, float *b1Out, float *b2Out, char *err, int errLen);
+
+// Device-resident acceleration structure for repeated queries: built once from the same inputs
+// as prgpu_trace_rays, queried with device pointers on a caller stream (cudaStream_t as void*).
+typedef struct prgpu_accel_t *prgpu_accel;
+PRGPU_API int prgpu_accel_create(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
+                                 const int32_t *primOrder, const prgpu::Float3 *triVerts, int32_t primCount,
+                                 prgpu_accel *out, char *err, int errLen);
+PRGPU_API int prgpu_accel_trace(prgpu_accel accel, const prgpu::Ray *deviceRays, int64_t rayCount, int32_t anyHit,
+                                int32_t *devicePrimOut, float *deviceTOut, void *stream, char *err, int errLen);
+// Same query with HOST rays and results: the rays are copied in and the results out inside the
+// call, overlapped chunk by chunk with the traversal.
+PRGPU_API int prgpu_accel_trace_host(prgpu_accel accel, const prgpu::Ray *rays, int64_t rayCount, int32_t anyHit,
+                                     int32_t *primOut, float *tOut, char *err, int errLen);
+// Returns and clears the handle's status word: bit 0 = a traversal stack overflowed (the BVH is
+// deeper than 64 levels along some ray); -1 on a bad handle.
+PRGPU_API int prgpu_accel_status(prgpu_accel accel);
+// Bytes of the converted node and triangle arrays on the device (for roofline accounting).
+PRGPU_API int64_t prgpu_accel_bytes(prgpu_accel accel);
+PRGPU_API void prgpu_accel_destroy(prgpu_accel accel);
+
+// Number of kernel launches this library has issued since load (for launch accounting).
+PRGPU_API uint64_t prgpu_launch_count();

@@ -1,0 +1,141 @@
+"""ctypes access to the oracle: the reference renderer's own CPU code (oracle/_ref/libprref.so,
+built by oracle/Makefile from the reference sources plus oracle/ref_harness.cpp) and the plain-C
+restatement (oracle/_ref/librestate.so, oracle/restate.c).
+
+TEST INFRASTRUCTURE ONLY. tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+reference arm use it as the checker or as the timed CPU reference; the product never imports it.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REF_LIB = os.path.join(REF_DIR, "libprref.so")
+RESTATE_LIB = os.path.join(REF_DIR, "librestate.so")
+
+_P = C.c_void_p
+_ref = None
+_restate = None
+
+
+def available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            raise RuntimeError(f"{REF_LIB} missing: build it with `make -C oracle` where the reference tree exists")
+        lib = C.CDLL(REF_LIB)
+        lib.prref_set_threads.argtypes = [C.c_int]
+        lib.prref_thread_count.restype = C.c_int
+        lib.prref_set_cache_dir.argtypes = [C.c_char_p]
+        lib.prref_soup_new.argtypes = [_P, C.c_int64]
+        lib.prref_soup_new.restype = _P
+        lib.prref_soup_free.argtypes = [_P]
+        lib.prref_soup_node_count.argtypes = [_P]
+        lib.prref_soup_node_count.restype = C.c_int64
+        lib.prref_soup_export.argtypes = [_P, _P, _P]
+        lib.prref_soup_trace.argtypes = [_P, _P, C.c_int64, C.c_int, _P, _P, _P, _P]
+        lib.prref_soup_trace.restype = C.c_double
+        lib.prref_bxdf.argtypes = [C.c_int, _P, C.c_int64, _P, _P]
+        lib.prref_fr_dielectric.argtypes = [C.c_float, C.c_float]
+        lib.prref_fr_dielectric.restype = C.c_float
+        lib.prref_fr_complex.argtypes = [C.c_float, C.c_float, C.c_float]
+        lib.prref_fr_complex.restype = C.c_float
+        lib.prref_hg.argtypes = [C.c_int64, _P, _P]
+        lib.prref_homogeneous.argtypes = [C.c_int64, _P, _P, _P]
+        lib.prref_sample_visible.argtypes = [C.c_int64, _P, _P, _P]
+        lib.prref_cie.argtypes = [C.c_int64, _P, _P]
+        lib.prref_cie_y_integral.restype = C.c_float
+        lib.prref_spectrum.argtypes = [C.c_int, C.c_float, C.c_float, C.c_float, C.c_char_p, C.c_int64, _P, _P]
+        lib.prref_spectrum.restype = C.c_int
+        lib.prref_scene_load.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_char_p, C.c_int]
+        lib.prref_scene_load.restype = _P
+        lib.prref_scene_free.argtypes = [_P]
+        lib.prref_scene_prim_count.argtypes = [_P]
+        lib.prref_scene_prim_count.restype = C.c_int64
+        lib.prref_scene_width.argtypes = [_P]
+        lib.prref_scene_height.argtypes = [_P]
+        lib.prref_scene_export.argtypes = [_P, C.c_char_p, C.c_int]
+        lib.prref_scene_export.restype = _P
+        lib.prref_render.argtypes = [_P, C.c_int, C.c_uint64, C.c_int, C.c_int, _P, C.c_char_p, C.c_int]
+        lib.prref_render.restype = C.c_double
+        lib.prref_light_bvh_sample.argtypes = [_P, C.c_int64, _P, _P, _P]
+        lib.prref_scene_light_count.argtypes = [_P]
+        # The RGB->spectrum table is built once (a few seconds) and cached beside the library.
+        lib.prref_set_cache_dir(REF_DIR.encode())
+        _ref = lib
+    return _ref
+
+
+def restate_lib() -> C.CDLL:
+    global _restate
+    if _restate is None:
+        if not os.path.exists(RESTATE_LIB):
+            raise RuntimeError(f"{RESTATE_LIB} missing: run `make -C oracle restate`")
+        lib = C.CDLL(RESTATE_LIB)
+        lib.rs_trace.argtypes = [_P, C.c_int64, _P, _P, _P, C.c_int64, C.c_int, _P, _P, _P, _P]
+        lib.rs_trace.restype = C.c_int
+        _restate = lib
+    return _restate
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class SoupBVH:
+    """The reference pr::BVH built over a triangle soup ((n, 3, 3) float32)."""
+
+    def __init__(self, verts: np.ndarray):
+        self.lib = ref_lib()
+        self.verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3, 3)
+        self.h = self.lib.prref_soup_new(_p(self.verts), self.verts.shape[0])
+
+    def export(self, node_dtype):
+        n = self.lib.prref_soup_node_count(self.h)
+        nodes = np.zeros(n, dtype=node_dtype)
+        order = np.zeros(self.verts.shape[0], dtype=np.int32)
+        self.lib.prref_soup_export(self.h, _p(nodes), _p(order))
+        return nodes, order
+
+    def trace(self, rays: np.ndarray, any_hit=False):
+        """rays: (n, 8) float32 (o, d, tmax, pad). Returns prim, t, b1, b2 (closest) or occluded flags,
+        and the elapsed seconds."""
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = rays.shape[0]
+        prim = np.empty(n, dtype=np.int32)
+        if any_hit:
+            dt = self.lib.prref_soup_trace(self.h, _p(rays), n, 1, _p(prim), None, None, None)
+            return prim, dt
+        t = np.empty(n, dtype=np.float32)
+        b1 = np.empty(n, dtype=np.float32)
+        b2 = np.empty(n, dtype=np.float32)
+        dt = self.lib.prref_soup_trace(self.h, _p(rays), n, 0, _p(prim), _p(t), _p(b1), _p(b2))
+        return prim, t, b1, b2, dt
+
+    def close(self):
+        if self.h:
+            self.lib.prref_soup_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def set_threads(n: int) -> None:
+    ref_lib().prref_set_threads(n)
+
+
+def thread_count() -> int:
+    return ref_lib().prref_thread_count()
