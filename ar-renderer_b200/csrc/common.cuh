@@ -64,7 +64,7 @@ __device__ __forceinline__ Frame frame_from_z(V3 z) {
 __device__ __forceinline__ Frame frame_from_xz(V3 xin, V3 z) {
     V3 x = xin - z * dot(xin, z);
     float l2 = len2(x);
-    if (!(l2 > 1e-12f) || !isfinite(l2)) return frame_from_z(z);
+    if (l2 < 1e-12f || !isfinite(l2)) return frame_from_z(z);
     x = x * rsqrtf(l2);
     return {x, cross(z, x), z};
 }

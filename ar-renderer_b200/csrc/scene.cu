@@ -1,0 +1,193 @@
+// Scene upload: validation of the caller's SceneDesc (every index a kernel will follow is range-
+// checked on the host, so malformed input is an error return, never a device fault), conversion
+// of the BVH, and a content-keyed cache so progressive batches upload once. The reference keys
+// its cache on the primitive pointer and counts only (src/gpu/prender_gpu.cpp:1653-1670) and so
+// misses an edited scene behind the same pointer; here the key also hashes the small tables in
+// full and a strided sample of the large ones.
+
+#include <algorithm>
+#include <cstring>
+
+#include "scene.cuh"
+
+namespace prb {
+
+namespace {
+
+uint64_t fnv(uint64_t h, const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; ++i) {
+        h ^= b[i];
+        h *= 0x100000001b3ull;
+    }
+    return h;
+}
+template <typename T> uint64_t fnv_v(uint64_t h, const T &v) { return fnv(h, &v, sizeof(T)); }
+
+// Hash of up to `samples` evenly strided elements plus the first and last.
+uint64_t sample_hash(uint64_t h, const void *base, size_t count, size_t elem, size_t samples) {
+    if (!base || count == 0) return fnv_v(h, count);
+    const unsigned char *b = static_cast<const unsigned char *>(base);
+    size_t step = std::max<size_t>(1, count / samples);
+    for (size_t i = 0; i < count; i += step) h = fnv(h, b + i * elem, elem);
+    return fnv(h, b + (count - 1) * elem, elem);
+}
+
+uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
+    uint64_t h = 0xcbf29ce484222325ull;
+    h = fnv_v(h, sd->prims);
+    h = fnv_v(h, sd->nodes);
+    h = fnv_v(h, sd->primCount);
+    h = fnv_v(h, sd->nodeCount);
+    h = sample_hash(h, sd->prims, size_t(sd->primCount), sizeof(prgpu::Primitive), 4096);
+    h = sample_hash(h, sd->nodes, size_t(sd->nodeCount), sizeof(prgpu::BVHNode), 4096);
+    h = sample_hash(h, sd->primOrder, size_t(sd->primCount), sizeof(int32_t), 4096);
+    if (sd->materials) h = fnv(h, sd->materials, size_t(sd->materialCount) * sizeof(prgpu::Material));
+    if (sd->lights) h = fnv(h, sd->lights, size_t(sd->lightCount) * sizeof(prgpu::Light));
+    if (sd->spectra) h = fnv(h, sd->spectra, size_t(sd->spectrumCount) * sizeof(prgpu::Spectrum));
+    if (sd->media) h = fnv(h, sd->media, size_t(sd->mediumCount) * sizeof(prgpu::Medium));
+    h = fnv(h, sd->filter.cdf, sizeof(sd->filter.cdf));
+    if (ext && ext->lightBVH && ext->lightBVHNodeCount > 0)
+        h = fnv(h, ext->lightBVH, size_t(ext->lightBVHNodeCount) * sizeof(prgpu::LightBVHNode));
+    return h;
+}
+
+bool spec_ok(int32_t id, int32_t n) { return id >= -1 && id < n; }
+
+bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::string *err) {
+    auto fail = [&](const std::string &m) {
+        *err = m;
+        return false;
+    };
+    if (sd->primCount < 0 || sd->nodeCount < 0 || sd->materialCount < 0 || sd->lightCount < 0 ||
+        sd->spectrumCount < 0 || sd->mediumCount < 0)
+        return fail("negative array count");
+    if ((sd->primCount > 0 && !sd->prims) || (sd->materialCount > 0 && !sd->materials) ||
+        (sd->lightCount > 0 && !sd->lights) || (sd->spectrumCount > 0 && !sd->spectra) ||
+        (sd->mediumCount > 0 && !sd->media))
+        return fail("null scene array");
+    const prgpu::Camera &c = sd->camera;
+    if (c.width <= 0 || c.height <= 0 || int64_t(c.width) * c.height > (int64_t(1) << 28))
+        return fail("camera resolution out of range");
+    if (!std::isfinite(c.tanHalfFov) || c.tanHalfFov <= 0) return fail("bad camera field of view");
+    const int32_t ns = sd->spectrumCount, nm = sd->mediumCount;
+    if (!spec_ok(sd->envSpectrum, ns)) return fail("envSpectrum out of range");
+    if (sd->cameraMedium < -1 || sd->cameraMedium >= nm) return fail("cameraMedium out of range");
+    for (int32_t i = 0; i < sd->materialCount; ++i) {
+        const prgpu::Material &m = sd->materials[i];
+        if (m.type > prgpu::MatCoatedConductor) return fail("unknown material type");
+        if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor || m.sheenWeight > 0)
+            return fail("coated and sheen materials are not supported by this module yet");
+        if (!spec_ok(m.albedo, ns) || !spec_ok(m.albedoB, ns) || !spec_ok(m.eta, ns) || !spec_ok(m.k, ns))
+            return fail("material spectrum index out of range");
+    }
+    for (int32_t i = 0; i < sd->lightCount; ++i) {
+        const prgpu::Light &l = sd->lights[i];
+        if (l.type > prgpu::LightPoint) return fail("unknown light type");
+        if (!spec_ok(l.spectrum, ns)) return fail("light spectrum index out of range");
+        if (l.type == prgpu::LightArea && (l.primitive < 0 || l.primitive >= sd->primCount))
+            return fail("area light primitive out of range");
+    }
+    for (int32_t i = 0; i < nm; ++i)
+        if (!spec_ok(sd->media[i].sigmaA, ns) || !spec_ok(sd->media[i].sigmaS, ns))
+            return fail("medium spectrum index out of range");
+    for (int32_t i = 0; i < sd->primCount; ++i) {
+        const prgpu::Primitive &p = sd->prims[i];
+        if (p.type > prgpu::PrimSphere) return fail("unknown primitive type");
+        if (p.material < 0 || p.material >= sd->materialCount) return fail("primitive material out of range");
+        if (p.light < -1 || p.light >= sd->lightCount) return fail("primitive light out of range");
+        if (p.mediumInside < -1 || p.mediumInside >= nm || p.mediumOutside < -1 || p.mediumOutside >= nm)
+            return fail("primitive medium out of range");
+    }
+    if (ext && ext->lightBVHNodeCount > 0) {
+        if (!ext->lightBVH) return fail("null light BVH");
+        int32_t n = ext->lightBVHNodeCount;
+        for (int32_t i = 0; i < n; ++i) {
+            const prgpu::LightBVHNode &b = ext->lightBVH[i];
+            if (b.light >= 0) {
+                if (b.light >= sd->lightCount) return fail("light BVH leaf out of range");
+            } else if (b.child1 <= i + 1 || b.child1 >= n || i + 1 >= n) {
+                return fail("malformed light BVH interior node");
+            }
+            if (b.parent >= i || b.parent < -1 || (i > 0 && b.parent < 0)) return fail("malformed light BVH parent link");
+        }
+    }
+    return true;
+}
+
+template <typename T> void put(DevBuf &b, const T *src, size_t n, cudaStream_t s) {
+    b.ensure(std::max<size_t>(1, n) * sizeof(T));
+    if (n) PRB_CUDA(cudaMemcpyAsync(b.ptr, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+} // namespace
+
+bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, SceneCache &cache,
+                  std::string *err) {
+    if (!validate(sd, ext, err)) return false;
+    uint64_t key = scene_key(sd, ext);
+    DevScene &d = cache.ds;
+    if (!cache.valid || cache.key != key) {
+        HostAccel h;
+        if (!convert_bvh(sd->nodes, sd->nodeCount, sd->primOrder, sd->primCount, PrimitiveSource{sd->prims}, &h, err))
+            return false;
+        cudaStream_t s = ds.stream;
+        cache.accel.upload(h, s);
+        put(cache.prims, sd->prims, size_t(sd->primCount), s);
+        put(cache.mats, sd->materials, size_t(sd->materialCount), s);
+        put(cache.lights, sd->lights, size_t(sd->lightCount), s);
+        put(cache.spectra, sd->spectra, size_t(sd->spectrumCount), s);
+        put(cache.media, sd->media, size_t(sd->mediumCount), s);
+        put(cache.filterCdf, sd->filter.cdf, size_t(prgpu::kFilterBins + 1), s);
+        int32_t nb = (ext && ext->lightBVHNodeCount > 0) ? ext->lightBVHNodeCount : 0;
+        std::vector<int> leafOf(size_t(std::max(1, sd->lightCount)), -1);
+        for (int32_t i = 0; i < nb; ++i)
+            if (ext->lightBVH[i].light >= 0) leafOf[size_t(ext->lightBVH[i].light)] = i;
+        if (nb) put(cache.lbvh, ext->lightBVH, size_t(nb), s);
+        put(cache.lightLeaf, leafOf.data(), leafOf.size(), s);
+        PRB_CUDA(cudaStreamSynchronize(s));
+        cache.hasSpheres = false;
+        for (int32_t i = 0; i < sd->primCount; ++i)
+            if (sd->prims[i].type == prgpu::PrimSphere) cache.hasSpheres = true;
+        cache.key = key;
+        cache.valid = true;
+        cache.deviceBytes = cache.accel.bytes + int64_t(sd->primCount) * int64_t(sizeof(prgpu::Primitive));
+        d.nodes = cache.accel.nodes.as<WNode>();
+        d.leaves = cache.accel.prims.as<LeafPrim>();
+        d.root = cache.accel.root;
+        d.prims = cache.prims.as<prgpu::Primitive>();
+        d.mats = cache.mats.as<prgpu::Material>();
+        d.lights = cache.lights.as<prgpu::Light>();
+        d.spectra = cache.spectra.as<float>();
+        d.media = cache.media.as<prgpu::Medium>();
+        d.filterCdf = cache.filterCdf.as<float>();
+        d.lbvh = nb ? cache.lbvh.as<prgpu::LightBVHNode>() : nullptr;
+        d.lightLeaf = cache.lightLeaf.as<int>();
+        d.lbvhCount = nb;
+    }
+    // Per-call scalars (cheap; not part of the device copy).
+    d.lightCount = sd->lightCount;
+    d.cameraMedium = sd->cameraMedium;
+    d.envSpectrum = sd->envSpectrum;
+    d.envScale = sd->envScale;
+    d.worldRadius = sd->worldRadius;
+    d.cam = sd->camera;
+    d.norm = sd->cieYIntegral > 0 ? 1.f / (4.f * sd->cieYIntegral) : 0.f;
+    d.hasInterfaces = 0;
+    for (int32_t i = 0; i < sd->materialCount; ++i)
+        if (sd->materials[i].type == prgpu::MatInterface) d.hasInterfaces = 1;
+    d.filterType = sd->filter.type;
+    d.filterRadius = sd->filter.radius;
+    d.filterSigma = sd->filter.sigma;
+    d.filterNorm = sd->filter.norm;
+    if (d.lbvhCount > 0) {
+        d.lbvhProb = ext->lightBVHProb > 0 && ext->lightBVHProb <= 1 ? ext->lightBVHProb : 1.f;
+        d.envPmf = sd->envSpectrum >= 0 ? 1.f - d.lbvhProb : 0.f;
+    } else {
+        d.lbvhProb = 0.f;
+        d.envPmf = sd->envPmf;
+    }
+    return true;
+}
+
+} // namespace prb

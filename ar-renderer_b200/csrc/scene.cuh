@@ -1,0 +1,72 @@
+// The scene on the device: the caller's SceneDesc (v4 layout, src/gpu/gpu_api.h:120-146) checked,
+// converted and kept resident between calls, plus the optional light BVH of the v5 extension.
+//
+// HBM layout: the traversal arrays of traverse.cuh (64-byte interior nodes, 48-byte leaf
+// records in leaf order), the 128-byte Primitive records for shading (read once per hit), and
+// the small tables (materials, lights, media, 95-sample spectra, filter CDF, light-BVH nodes).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "accel.cuh"
+#include "device.cuh"
+
+namespace prb {
+
+struct DevScene {
+    const WNode *nodes;
+    const LeafPrim *leaves;
+    RootInfo root;
+    const prgpu::Primitive *prims;
+    const prgpu::Material *mats;
+    const prgpu::Light *lights;
+    int lightCount;
+    const float *spectra;
+    const prgpu::Medium *media;
+    int cameraMedium;
+    int envSpectrum;
+    float envScale;
+    float envPmf;         // selection probability of the environment in next-event estimation
+    float worldRadius;
+    prgpu::Camera cam;
+    float norm;           // 1 / (4 * integral of CIE y): XYZ normalisation of one sample
+    int hasInterfaces;
+    uint32_t filterType;
+    float filterRadius, filterSigma, filterNorm;
+    const float *filterCdf;  // kFilterBins + 1
+    // Light BVH (lbvhCount > 0 selects importance sampling of the bounded lights).
+    const prgpu::LightBVHNode *lbvh;
+    int lbvhCount;
+    float lbvhProb;          // probability of the BVH branch (1 - probability of the environment)
+    const int *lightLeaf;    // light index -> leaf node (-1 when the light is not in the tree)
+};
+
+struct SceneCache {
+    uint64_t key = 0;
+    bool valid = false;
+    DeviceAccel accel;
+    DevBuf prims, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf;
+    DevScene ds{};
+    bool hasSpheres = false;
+    int64_t deviceBytes = 0;
+    void release() {
+        accel.release();
+        prims.release();
+        mats.release();
+        lights.release();
+        spectra.release();
+        media.release();
+        filterCdf.release();
+        lbvh.release();
+        lightLeaf.release();
+        valid = false;
+    }
+};
+
+// Validates sd (and ext) and makes the cache hold it on the device. Throws CudaError on device
+// failure; returns false with a message on invalid input.
+bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, SceneCache &cache,
+                  std::string *err);
+
+} // namespace prb

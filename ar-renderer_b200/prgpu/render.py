@@ -1,0 +1,62 @@
+"""Rendering through the C ABI: prgpu_render (v4, float sums added into the caller's film) and
+prgpu_render_ex (FP64 film accumulated in sample order, light BVH, statistics)."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+def _desc_ptr(scene) -> C.c_void_p:
+    """A SceneDesc pointer: an int address, a ctypes SceneDesc, or an object with .desc()."""
+    if isinstance(scene, int):
+        return C.c_void_p(scene)
+    if isinstance(scene, abi.SceneDesc):
+        return C.cast(C.pointer(scene), C.c_void_p)
+    return C.cast(C.pointer(scene.desc()), C.c_void_p)
+
+
+def render_v4(scene, width: int, height: int, spp: int, first_sample: int = 0, seed: int = 0, max_depth: int = 0,
+              clamp: float = 0.0, out: np.ndarray | None = None, device: int = 0) -> np.ndarray:
+    """prgpu_render: returns (adds into) float32 XYZ sums of shape (height, width, 3)."""
+    if out is None:
+        out = np.zeros((height, width, 3), dtype=np.float32)
+    rp = abi.RenderParams(spp, first_sample, seed, max_depth, clamp)
+    err = abi.err_buf()
+    rc = abi.gpu_lib().prgpu_render(device, _desc_ptr(scene), C.cast(C.pointer(rp), C.c_void_p), abi.ptr(out), err,
+                                    len(err))
+    abi.check(rc, err, "prgpu_render")
+    return out
+
+
+def render_ex(scene, width: int, height: int, spp: int, first_sample: int = 0, seed: int = 0, max_depth: int = 0,
+              clamp: float = 0.0, out: np.ndarray | None = None, ext: abi.SceneExt | None = None, device: int = 0,
+              stats: bool = False):
+    """prgpu_render_ex: accumulates FP64 XYZ sums (height, width, 3) in sample order onto `out`."""
+    if out is None:
+        out = np.zeros((height, width, 3), dtype=np.float64)
+    assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"]
+    rp = abi.RenderParams(spp, first_sample, seed, max_depth, clamp)
+    st = abi.RenderStats()
+    err = abi.err_buf()
+    extp = C.cast(C.pointer(ext), C.c_void_p) if ext is not None else None
+    rc = abi.gpu_lib().prgpu_render_ex(device, _desc_ptr(scene), extp, C.cast(C.pointer(rp), C.c_void_p),
+                                       abi.ptr(out), C.cast(C.pointer(st), C.c_void_p), err, len(err))
+    abi.check(rc, err, "prgpu_render_ex")
+    return (out, st) if stats else out
+
+
+def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
+             block_size: int = 0) -> abi.SceneExt:
+    e = abi.SceneExt()
+    e.structSize = C.sizeof(abi.SceneExt)
+    if light_bvh is not None and len(light_bvh):
+        e.lightBVHNodeCount = len(light_bvh)
+        e.lightBVH = light_bvh.ctypes.data
+        e.lightBVHProb = light_bvh_prob
+    e.wavefrontPaths = wavefront_paths
+    e.blockSize = block_size
+    return e

@@ -1,0 +1,190 @@
+"""The box-and-spheres scene family as data, written in PRender's native JSON scene format
+(schemas/prscene.schema.json; loader src/scene/scene_loader.cpp) so the reference CPU renderer and
+this module render the same geometry, materials, lights and camera.
+
+Base scene (the plain path-tracer workload): a closed 2 x 2 x 2 box (6 walls, 12 triangles;
+white 0.75, left wall red (0.63, 0.06, 0.05), right wall green (0.14, 0.45, 0.09)), a 0.5 x 0.5
+ceiling quad light with a 6500 K blackbody emitter, and a 35-sphere pyramid (5 x 5 + 3 x 3 + 1,
+radius 0.12) of subdivision-3 icospheres (1280 triangles each) whose materials are drawn with a
+seeded uniform choice among Lambertian (random RGB albedo in [0.1, 0.9]), rough GGX gold
+(alpha 0.2, i.e. roughness sqrt(0.2)) and smooth dispersive BK7. Options add a homogeneous
+chromatic medium filling the box (the uneven-batch variant) and change resolution, samples and
+path length.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def icosphere(subdiv: int):
+    """Unit icosphere: (vertices (n, 3) float64, faces (m, 3) int32), counter-clockwise outward."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, float) / np.linalg.norm(p) for p in v]
+    faces = list(f)
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts), np.array(faces, dtype=np.int32)
+
+
+@dataclass
+class Sphere:
+    center: tuple
+    radius: float
+    material: str  # "lambert", "gold", "bk7"
+    albedo: tuple = (0.5, 0.5, 0.5)
+
+
+@dataclass
+class BoxScene:
+    width: int = 256
+    height: int = 256
+    spp: int = 64
+    max_depth: int = 8
+    seed: int = 0
+    subdiv: int = 3
+    light_temperature: float = 6500.0
+    light_luminance: float = 30.0
+    fov_y: float = 62.0
+    medium: dict | None = None  # {"sigma_a": [r,g,b], "sigma_s": [r,g,b], "g": 0.6}
+    spheres: list = field(default_factory=list)
+    filter: str = "box"
+
+    def triangle_count(self) -> int:
+        return 12 + 2 + len(self.spheres) * 20 * 4 ** self.subdiv
+
+
+def pyramid_spheres(seed: int, radius: float = 0.12):
+    """35 spheres: 5 x 5 + 3 x 3 + 1, touching, resting on the floor (y = -1) near the back."""
+    rng = np.random.default_rng(seed)
+    out = []
+    layers = [(5, 0.0), (3, 1), (1, 2)]
+    cz = -0.25
+    for count, level in layers:
+        y = -1.0 + radius + level * radius * math.sqrt(2.0)
+        off = (count - 1) / 2.0
+        for i in range(count):
+            for k in range(count):
+                x = (i - off) * 2 * radius
+                z = cz + (k - off) * 2 * radius
+                kind = ("lambert", "gold", "bk7")[int(rng.integers(0, 3))]
+                albedo = tuple(float(a) for a in rng.uniform(0.1, 0.9, 3))
+                out.append(Sphere((x, y, z), radius, kind, albedo))
+    return out
+
+
+def box_scene(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8,
+              medium: bool = False, subdiv: int = 3) -> BoxScene:
+    s = BoxScene(width=width, height=height, spp=spp, max_depth=max_depth, seed=seed, subdiv=subdiv)
+    s.spheres = pyramid_spheres(seed)
+    if medium:
+        rng = np.random.default_rng(1000 + seed)
+        s.medium = {"sigma_s": [float(x) for x in rng.uniform(0.05, 0.5, 3)],
+                    "sigma_a": [float(x) for x in rng.uniform(0.0, 0.1, 3)], "g": 0.6}
+    return s
+
+
+def _f32(a) -> list:
+    """float32 values as Python floats that round-trip exactly through JSON."""
+    return [float(x) for x in np.asarray(a, dtype=np.float32).ravel()]
+
+
+def sphere_mesh(sp: Sphere, subdiv: int):
+    """World-space float32 positions, unit normals and indices of one icosphere."""
+    v, f = icosphere(subdiv)
+    p = (v * sp.radius + np.array(sp.center)).astype(np.float32)
+    return p, v.astype(np.float32), f
+
+
+def wall_quads():
+    """The 6 walls as (name, material, 4 corners counter-clockwise seen from inside)."""
+    return [
+        ("floor", "white", [(-1, -1, -1), (-1, -1, 1), (1, -1, 1), (1, -1, -1)]),
+        ("ceiling", "white", [(-1, 1, -1), (1, 1, -1), (1, 1, 1), (-1, 1, 1)]),
+        ("back", "white", [(-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1)]),
+        ("front", "white", [(-1, -1, 1), (-1, 1, 1), (1, 1, 1), (1, -1, 1)]),
+        ("left", "red", [(-1, -1, -1), (-1, 1, -1), (-1, 1, 1), (-1, -1, 1)]),
+        ("right", "green", [(1, -1, -1), (1, -1, 1), (1, 1, 1), (1, 1, -1)]),
+    ]
+
+
+def to_reference_json(s: BoxScene) -> dict:
+    mats = {
+        "white": {"type": "diffuse", "reflectance": [0.75, 0.75, 0.75]},
+        "red": {"type": "diffuse", "reflectance": [0.63, 0.06, 0.05]},
+        "green": {"type": "diffuse", "reflectance": [0.14, 0.45, 0.09]},
+        "gold": {"type": "conductor", "metal": "Au", "roughness": math.sqrt(0.2)},
+        "bk7": {"type": "dielectric", "ior": "BK7"},
+    }
+    geometry, objects = {}, []
+    for name, mat, quad in wall_quads():
+        geometry[name] = {"type": "mesh", "positions": _f32(quad), "indices": [0, 1, 2, 0, 2, 3]}
+        objects.append({"name": name, "geometry": name, "material": mat})
+    for i, sp in enumerate(s.spheres):
+        p, n, f = sphere_mesh(sp, s.subdiv)
+        gid = f"sphere{i}"
+        geometry[gid] = {"type": "mesh", "positions": _f32(p), "normals": _f32(n),
+                         "indices": [int(x) for x in f.ravel()], "closed": True}
+        if sp.material == "lambert":
+            mid = f"lambert{i}"
+            mats[mid] = {"type": "diffuse", "reflectance": list(sp.albedo)}
+        else:
+            mid = sp.material
+        objects.append({"name": gid, "geometry": gid, "material": mid})
+    media = {}
+    if s.medium is not None:
+        media["fog"] = {"type": "homogeneous", "sigma_a": s.medium["sigma_a"], "sigma_s": s.medium["sigma_s"],
+                        "g": s.medium["g"]}
+        # An invisible closed container slightly larger than the room holds the medium; the loader
+        # gives every object inside it (walls, light, spheres) the medium as exterior, and the
+        # camera inside picks it up too.
+        geometry["fogbox"] = {"type": "box", "size": [2.2, 2.2, 2.2]}
+        mats["boundary"] = {"type": "interface"}
+        objects.append({"name": "fogbox", "geometry": "fogbox", "material": "boundary", "interior": "fog",
+                        "exterior": None})
+    doc = {
+        "materials": mats,
+        "media": media,
+        "geometry": geometry,
+        "objects": objects,
+        "lights": {"ceiling": {"type": "rect", "position": [0, 0.999, -0.1], "size": [0.5, 0.5],
+                               "direction": [0, -1, 0], "temperature": s.light_temperature,
+                               "luminance": s.light_luminance}},
+        "cameras": {"cam": {"type": "pinhole", "position": [0, -0.1, 0.98], "look_at": [0, -0.45, -0.3],
+                            "fov_y": s.fov_y}},
+        "render": {"camera": "cam", "seed": s.seed,
+                   "film": {"width": s.width, "height": s.height, "filter": s.filter},
+                   "integrator": {"type": "path", "spp": s.spp, "max_depth": s.max_depth}},
+    }
+    return doc
+
+
+def write_reference_json(s: BoxScene, path: str) -> str:
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        json.dump(to_reference_json(s), f)
+    return path

@@ -1,0 +1,317 @@
+"""Benchmark of the B200 path-tracing module (one JSON line on stdout, rank 0).
+
+Workload (default): the traversal microbenchmark -- 2^24 rays against a 1,048,576-triangle soup
+(centroids uniform in the unit cube, vertex offsets uniform in [-0.01, 0.01]^3; ray origins
+uniform in [-0.5, 1.5]^3, directions uniform on the sphere), one closest-hit pass (tMax = inf,
+primitive id + distance out) and one any-hit pass (tMax uniform in [0, 2]) per step. Synthetic,
+seeded inputs; the BVH is this library's own SAH build (libprender_host.so).
+
+  value  -- Mrays/s of both passes with rays resident in HBM (device time, CUDA events on the
+            launching stream, max over ranks); inputs are 1 GiB per step, larger than L2.
+  e2e    -- the same through prgpu_accel_trace_host with pinned HOST rays and results: the
+            host->device copy of the rays and device->host copy of the hits are inside the
+            timed region.
+  roofline -- the closest-hit kernel: algorithmic bytes per launch (per-ray node, triangle, ray
+            and hit bytes with per-ray work counts measured once on the CPU oracle) over its
+            CUDA-event duration, against the measured HBM copy bandwidth.
+  cpu_baseline -- the reference's own BVH::Intersect / IntersectP (oracle/_ref, compiled from the
+            reference sources) on a bounded sample of the same rays, all host threads.
+
+--impl reference prints the reference CPU traversal as its own arm (rank 0 only).
+Multi-GPU (torchrun): each rank traces its own 2^24 rays (weak scaling, no data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "ar-renderer_b200"), os.path.join(ROOT, "oracle")]
+
+import numpy as np  # noqa: E402
+
+N_TRIS = 1 << 20
+N_RAYS = 1 << 24
+METRIC = "path samples/s; equal-time relMSE guided vs plain (same B200); Mrays/s"
+
+# Per-ray work of the closest-hit pass on this workload with this library's SAH BVH (max 4
+# primitives per leaf), measured once with the oracle's counting traversal (oracle/restate.c) over
+# 2^18 of the benchmark rays: mean interior-node visits and triangle tests per ray.
+NODES_PER_RAY = 29.38
+TRIS_PER_RAY = 2.21
+# Algorithmic bytes per closest-hit ray: every visited node (32 B in the reference layout) and
+# every tested triangle (36 B) read once, the 32-byte ray read and an 8-byte hit written.
+BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
+# DRAM bytes per closest-hit launch from ncu (profiles/trace_closest_soup1m.md), or None.
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            self.file.flush()
+            rows = [l.split(", ") for l in open(self.file.name).read().splitlines() if l.strip()]
+        except Exception:
+            rows = []
+        rows = [r for r in rows if len(r) >= 9 and r[0].strip() == str(self.gpu)]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_inputs(rank: int):
+    from prgpu import trace, workloads
+
+    verts = workloads.triangle_soup(N_TRIS, seed=1)
+    closest = workloads.soup_rays(N_RAYS, seed=2 + 1000 * rank)
+    anyhit = workloads.soup_rays(N_RAYS, seed=3 + 1000 * rank, any_hit=True)
+    return verts, closest, anyhit, trace
+
+
+def cpu_reference(verts, closest, anyhit, rays_per_pass: int):
+    """Reference CPU traversal (oracle/_ref) on the first rays_per_pass rays of each pass."""
+    import ref
+    from prgpu import workloads
+
+    ref.set_threads(0)
+    b = ref.SoupBVH(verts)
+    c = workloads.rays_as_f8(closest[:rays_per_pass])
+    a = workloads.rays_as_f8(anyhit[:rays_per_pass])
+    b.trace(c[: 1 << 14])  # warm the pool
+    *_, t1 = b.trace(c)
+    _, t2 = b.trace(a, any_hit=True)
+    b.close()
+    return 2 * rays_per_pass / (t1 + t2) / 1e6, ref.thread_count(), t1 + t2
+
+
+def run_reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from prgpu import workloads
+
+    verts = workloads.triangle_soup(N_TRIS, seed=1)
+    per = 1 << 21
+    closest = workloads.soup_rays(per, seed=2)
+    anyhit = workloads.soup_rays(per, seed=3, any_hit=True)
+    import ref
+
+    ref.set_threads(0)
+    b = ref.SoupBVH(verts)
+    c8 = workloads.rays_as_f8(closest)
+    a8 = workloads.rays_as_f8(anyhit)
+    for _ in range(args.warmup):
+        b.trace(c8[: 1 << 16])
+    times = []
+    for _ in range(args.steps):
+        *_, t1 = b.trace(c8)
+        _, t2 = b.trace(a8, any_hit=True)
+        times.append(t1 + t2)
+    b.close()
+    dt = sum(times)
+    value = args.steps * 2 * per / dt / 1e6
+    sample = f"{per} closest-hit + {per} any-hit rays of the benchmark workload per step (reference BVH)"
+    line = {
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
+                   "reference_sample_rays_per_pass": per},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": ref.thread_count(), "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    global N_RAYS
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per pass (smaller for profiling captures)")
+    args = ap.parse_args()
+    N_RAYS = args.rays
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from prgpu import abi
+
+    verts, closest, anyhit, trace = make_inputs(rank)
+    nodes, order = trace.build_bvh_triangles(verts, max_leaf=4)
+    acc = trace.Accel(nodes, order, verts, device=local)
+    lib = abi.gpu_lib()
+
+    dc = torch.from_numpy(closest.view(np.uint8)).cuda()
+    da = torch.from_numpy(anyhit.view(np.uint8)).cuda()
+    prim = torch.empty(N_RAYS, dtype=torch.int32, device="cuda")
+    tdist = torch.empty(N_RAYS, dtype=torch.float32, device="cuda")
+    occ = torch.empty(N_RAYS, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        acc.trace_device(dc.data_ptr(), N_RAYS, prim.data_ptr(), tdist.data_ptr(), False, stream.cuda_stream)
+        if ev is not None:
+            ev[1].record(stream)
+        acc.trace_device(da.data_ptr(), N_RAYS, occ.data_ptr(), 0, True, stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.prgpu_launch_count()
+    with ClockSampler(local) as clocks:
+        barrier()
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t_end.record(stream)
+        barrier()
+    launches = int(lib.prgpu_launch_count() - launches0)
+    ms = t_start.elapsed_time(t_end)
+    closest_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
+    if world > 1:
+        x = torch.tensor([ms, closest_ms], device="cuda")
+        dist.all_reduce(x, op=dist.ReduceOp.MAX)
+        ms, closest_ms = float(x[0]), float(x[1])
+    ms_per_step = ms / args.steps
+    value = world * 2 * N_RAYS / (ms_per_step * 1e3)  # Mrays/s, whole job
+    assert acc.status() == 0, "traversal stack overflow"
+
+    # End to end through the C ABI with pinned host buffers (the copies are inside the region).
+    e2e_value = None
+    if not args.no_e2e:
+        hc = torch.from_numpy(closest.view(np.uint8)).pin_memory().numpy().view(abi.RAY)
+        ha = torch.from_numpy(anyhit.view(np.uint8)).pin_memory().numpy().view(abi.RAY)
+        hprim = torch.empty(N_RAYS, dtype=torch.int32).pin_memory().numpy()
+        ht = torch.empty(N_RAYS, dtype=torch.float32).pin_memory().numpy()
+        hocc = torch.empty(N_RAYS, dtype=torch.int32).pin_memory().numpy()
+        e2e_steps = max(3, min(args.steps, 5))
+        for _ in range(2):
+            acc.trace_host(hc, hprim, ht, False)
+            acc.trace_host(ha, hocc, None, True)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            acc.trace_host(hc, hprim, ht, False)
+            acc.trace_host(ha, hocc, None, True)
+        barrier()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        if world > 1:
+            x = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            e2e_s = float(x[0])
+        e2e_value = world * 2 * N_RAYS / e2e_s / 1e6
+        np.testing.assert_array_equal(hprim, prim.cpu().numpy())
+
+    peak, peak_kind = _peaks()
+    achieved = BYTES_PER_RAY * N_RAYS / (closest_ms * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per = 1 << 22
+        v, cores, secs = cpu_reference(verts, closest, anyhit, per)
+        cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+               "sample": f"{per} closest-hit + {per} any-hit rays of this workload through the reference "
+                         f"BVH::Intersect/IntersectP on its own BVH ({secs:.1f} s)"}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
+                   "rays_per_pass": N_RAYS, "triangles": N_TRIS, "bvh": "own binned SAH, <=4 per leaf",
+                   "l2": "inputs larger than L2 (1 GiB of rays per step)", "parallelism": f"replicas x{world}"},
+        "e2e": None if e2e_value is None else
+        {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(2 * N_RAYS * 32),
+         "d2h_bytes_per_step": int(N_RAYS * 8 + N_RAYS * 4)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "kernel": "k_trace<closest>",
+                     "bytes_per_ray": BYTES_PER_RAY, "launch_ms": closest_ms,
+                     "traffic": NCU_TRAFFIC_PER_LAUNCH},
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+        "closest_hit_mrays": N_RAYS / (closest_ms * 1e3),
+        "any_hit_mrays": N_RAYS / ((ms_per_step - closest_ms) * 1e3),
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -290,3 +290,20 @@ PRGPU_API void prgpu_accel_destroy(prgpu_accel accel);
 
 // Number of kernel launches this library has issued since load (for launch accounting).
 PRGPU_API uint64_t prgpu_launch_count();
+
+// Verification entry points: the path tracer's own device functions evaluated on caller inputs
+// (host arrays), for comparison with the reference implementations on identical inputs.
+// BxDF (kind 0 diffuse, 1 conductor, 2 dielectric, 3 thin dielectric; pr::DiffuseBxDF,
+// ConductorBxDF, DielectricBxDF, ThinDielectricBxDF, src/materials/bxdf.cpp:85-256):
+//   params 16 floats: R[4], eta[4], k[4], etaD, alphaX, alphaY, mode (0 radiance, 1 importance);
+//   in 9 floats per item: wo[3], wi[3], uc, u0, u1;
+//   out 16 floats per item: f[4], pdf, sampled (0/1), sample f[4], pdf, wi[3], flags, eta.
+PRGPU_API int prgpu_eval_bxdf(int deviceIndex, int kind, const float *params, int64_t n, const float *in, float *out,
+                              char *err, int errLen);
+// Henyey-Greenstein (src/materials/bxdf.cpp:64-80): in 7 floats (cosTheta, g, wo[3], u0, u1);
+// out 5 floats (phase value, sampled wi[3], its pdf).
+PRGPU_API int prgpu_eval_phase(int deviceIndex, int64_t n, const float *in, float *out, char *err, int errLen);
+// Homogeneous medium (HomogeneousMedium::Transmittance / SampleDistanceHero,
+// src/media/medium.cpp:15-103): in 10 floats (sigma_a[4], sigma_s[4], tMax, u); out 14 floats
+// (Tr(tMax)[4], scattered, t, weight[4], pdfRatio[4]).
+PRGPU_API int prgpu_eval_homogeneous(int deviceIndex, int64_t n, const float *in, float *out, char *err, int errLen);

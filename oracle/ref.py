@@ -133,6 +133,63 @@ class SoupBVH:
             pass
 
 
+class RefScene:
+    """A scene loaded by the reference loader (LoadScene), exportable as the v4 SceneDesc its host
+    would hand the GPU module, and renderable with the reference PathIntegrator."""
+
+    def __init__(self, path: str, width: int = 0, height: int = 0):
+        self.lib = ref_lib()
+        err = C.create_string_buffer(2048)
+        self.h = self.lib.prref_scene_load(path.encode(), width, height, err, len(err))
+        if not self.h:
+            raise RuntimeError("reference LoadScene failed: " + err.value.decode())
+        self.width = self.lib.prref_scene_width(self.h)
+        self.height = self.lib.prref_scene_height(self.h)
+        self._desc = None
+
+    def export(self) -> int:
+        """Address of the exported prgpu::SceneDesc (valid while this object lives)."""
+        if self._desc is None:
+            err = C.create_string_buffer(2048)
+            p = self.lib.prref_scene_export(self.h, err, len(err))
+            if not p:
+                raise RuntimeError("scene export failed: " + err.value.decode())
+            self.warnings = err.value.decode()
+            self._desc = p
+        return self._desc
+
+    def render(self, spp: int, seed: int, max_depth: int, light_bvh: bool = True):
+        """Per-pixel XYZ sums over spp samples, shape (h, w, 3), and the render seconds."""
+        out = np.zeros((self.height, self.width, 3), dtype=np.float32)
+        err = C.create_string_buffer(2048)
+        dt = self.lib.prref_render(self.h, spp, seed, max_depth, 1 if light_bvh else 0, _p(out), err, len(err))
+        if dt < 0:
+            raise RuntimeError("reference render failed: " + err.value.decode())
+        return out, dt
+
+    def light_count(self) -> int:
+        return self.lib.prref_scene_light_count(self.h)
+
+    def light_bvh_sample(self, pts: np.ndarray, with_pmf: bool = True):
+        """pts: (n, 7) float32 (p, n, u). Returns (light index, pmf) and the per-light PMF table."""
+        pts = np.ascontiguousarray(pts, dtype=np.float32)
+        out = np.zeros((pts.shape[0], 2), dtype=np.float32)
+        pm = np.zeros((pts.shape[0], self.light_count()), dtype=np.float32) if with_pmf else None
+        self.lib.prref_light_bvh_sample(self.h, pts.shape[0], _p(pts), _p(out), _p(pm))
+        return out, pm
+
+    def close(self):
+        if self.h:
+            self.lib.prref_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def set_threads(n: int) -> None:
     ref_lib().prref_set_threads(n)
 
