@@ -52,7 +52,7 @@ struct Ggx {
         V3 t2 = cross(wh, t1);
         float r = sqrtf(u0), phi = 2.f * kPi * u1;
         float sp, cp;
-        sincosf(phi, &sp, &cp);
+        sincos_rn(phi, &sp, &cp);
         float px = r * cp, py = r * sp;
         float h = sqrtf(1.f - px * px);
         float s = (1.f + wh.z) * 0.5f;
@@ -88,12 +88,16 @@ __device__ __forceinline__ Cpx cdiv(Cpx a, Cpx b) {
     return {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
 }
 __device__ __forceinline__ Cpx csqrt(Cpx z) {
-    // Principal root: |z|^(1/2) at half the argument.
-    float m = sqrtf(hypotf(z.re, z.im));
-    float a = 0.5f * atan2f(z.im, z.re);
-    float s, c;
-    sincosf(a, &s, &c);
-    return {m * c, m * s};
+    // Principal root in the algebraic form (no trigonometry): with h = |z|,
+    // re = sqrt((h + x) / 2), im = y / (2 re) for x >= 0, and the mirrored form for x < 0.
+    if (z.re == 0.f && z.im == 0.f) return {0.f, z.im};
+    float h = hypotf(z.re, z.im);
+    if (z.re > 0.f) {
+        float d = sqrtf(0.5f * (h + z.re));
+        return {d, 0.5f * (z.im / d)};
+    }
+    float s = sqrtf(0.5f * (h - z.re));
+    return {fabsf(0.5f * (z.im / s)), copysignf(s, z.im)};
 }
 __device__ __forceinline__ float fr_complex(float cosI, float etaR, float etaI) {
     cosI = clampf(cosI, 0.f, 1.f);
@@ -143,7 +147,7 @@ __device__ __forceinline__ void concentric_disk(float u0, float u1, float *x, fl
         th = kPiOver2 - kPiOver4 * (ox / oy);
     }
     float s, c;
-    sincosf(th, &s, &c);
+    sincos_rn(th, &s, &c);
     *x = r * c;
     *y = r * s;
 }
@@ -393,7 +397,7 @@ __device__ __forceinline__ V3 hg_sample(V3 wo, float g, float u0, float u1, floa
     cosTheta = clampf(cosTheta, -1.f, 1.f);
     float sinTheta = safe_sqrt(1.f - sqr(cosTheta));
     float s, c;
-    sincosf(2.f * kPi * u1, &s, &c);
+    sincos_rn(2.f * kPi * u1, &s, &c);
     Frame f = frame_from_z(wo);
     *pdf = hg_phase(cosTheta, g);
     return f.from_local(mk(sinTheta * c, sinTheta * s, cosTheta));

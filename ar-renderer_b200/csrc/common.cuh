@@ -187,6 +187,17 @@ __device__ __forceinline__ SS tab4(const float *__restrict__ spectra, int id, co
     return {{tab(spectra, id, w.l[0]), tab(spectra, id, w.l[1]), tab(spectra, id, w.l[2]), tab(spectra, id, w.l[3])}};
 }
 
+// sin and cos of a float angle evaluated in double precision and rounded once: the correctly
+// rounded float values in all but vanishingly rare cases, as the host C library returns them.
+// Used where sampled directions feed sharp lobes (microfacet peaks), so that a one-ulp
+// difference in the angle's sine is not amplified.
+__device__ __forceinline__ void sincos_rn(float x, float *s, float *c) {
+    double sd, cd;
+    sincos(double(x), &sd, &cd);
+    *s = float(sd);
+    *c = float(cd);
+}
+
 __device__ __forceinline__ float power_heuristic(float f, float g) {
     float f2 = f * f;
     if (isinf(f2)) return 1.f;
