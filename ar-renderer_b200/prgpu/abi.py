@@ -154,6 +154,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_render_ex", [C.c_int, _P, _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
                                         _P, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_trace_rays_noalloc", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64,
+                                                C.c_int32, _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_accel_create", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, C.POINTER(_P), *_ERR], C.c_int)
         _bind(lib, "prgpu_accel_trace", [_P, _P, C.c_int64, C.c_int32, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_accel_trace_host", [_P, _P, C.c_int64, C.c_int32, _P, _P, *_ERR], C.c_int)

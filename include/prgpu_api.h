@@ -269,6 +269,17 @@ PRGPU_API int prgpu_trace_rays(int deviceIndex, const prgpu::BVHNode *nodes, int
                                const prgpu::Ray *rays, int64_t rayCount, int32_t anyHit, int32_t *primOut,
                                float *tOut, float *b1Out, float *b2Out, char *err, int errLen);
 
+// The same query as prgpu_trace_rays, for callers that cannot allocate device memory while they
+// work (their HBM belongs to another allocator's pool, or they must not trigger the device-wide
+// synchronisation of cudaMalloc / cudaFree). It allocates nothing: every device byte comes from
+// one 32 MiB array the library reserves on each GPU where it is loaded. Limits: at most 131,072
+// triangles and 262,143 BVH nodes per call (larger inputs return 1 with a message); any number of
+// rays. Calls run one after another. No counterpart in the reference (src/gpu/gpu_api.h).
+PRGPU_API int prgpu_trace_rays_noalloc(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
+                                       const int32_t *primOrder, const prgpu::Float3 *triVerts, int32_t primCount,
+                                       const prgpu::Ray *rays, int64_t rayCount, int32_t anyHit, int32_t *primOut,
+                                       float *tOut, float *b1Out, float *b2Out, char *err, int errLen);
+
 // Device-resident acceleration structure for repeated queries: built once from the same inputs
 // as prgpu_trace_rays, queried with device pointers on a caller stream (cudaStream_t as void*).
 typedef struct prgpu_accel_t *prgpu_accel;
