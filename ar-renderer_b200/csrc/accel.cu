@@ -10,49 +10,107 @@
 
 namespace prb {
 
-template <bool kAny, bool kSpheres>
-__global__ void __launch_bounds__(256) k_trace(const WNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
-                                               RootInfo root, const float4 *__restrict__ rays, int64_t n,
-                                               int32_t *__restrict__ primOut, float *__restrict__ tOut,
-                                               float *__restrict__ b1Out, float *__restrict__ b2Out,
-                                               int *__restrict__ status) {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        float4 a = __ldcs(rays + 2 * i), b = __ldcs(rays + 2 * i + 1);
-        TraceRay r = make_trace_ray(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z));
-        Hit h;
-        h.prim = -1;
-        h.t = 0.f;
-        h.u = h.v = 0.f;
-        bool overflow = false;
-        bool found = root.empty ? false
-                                : traverse<kAny, kSpheres>(nodes, prims, root.box, root.ref, r, a.w, &h, &overflow);
-        if (overflow) atomicOr(status, 1);
-        if (kAny) {
-            primOut[i] = found ? 1 : 0;
-        } else {
-            primOut[i] = found ? h.prim : -1;
-            if (tOut) tOut[i] = found ? h.t : 0.f;
-            if (b1Out) b1Out[i] = found ? h.u : 0.f;
-            if (b2Out) b2Out[i] = found ? h.v : 0.f;
+// Persistent warps: every lane that has no ray takes the next one from a global counter (one
+// atomic per warp and refill), then the lanes advance their traversals one node or leaf per
+// iteration. Incoherent rays end after very different numbers of steps; refilling keeps the
+// lanes of a warp busy instead of idling until the warp's longest ray ends.
+template <bool kAny>
+__global__ void __launch_bounds__(256) k_trace_persist(const WNode *__restrict__ nodes,
+                                                       const LeafPrim *__restrict__ prims, RootInfo root,
+                                                       const float4 *__restrict__ rays, int64_t n,
+                                                       int32_t *__restrict__ primOut, float *__restrict__ tOut,
+                                                       float *__restrict__ b1Out, float *__restrict__ b2Out,
+                                                       int *__restrict__ status,
+                                                       unsigned long long *__restrict__ counter) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TraceRay r;
+    TravState s;
+    s.ref = 0;
+    s.sp = 0;
+    s.tMax = 0.f;
+    s.found = false;
+    int64_t idx = 0;
+    bool active = false, exhausted = false, overflow = false;
+    while (true) {
+        unsigned need = __ballot_sync(full, !active && !exhausted);
+        if (need) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(counter, (unsigned long long)__popc(need));
+            base = __shfl_sync(full, base, 0);
+            if (!active && !exhausted) {
+                idx = int64_t(base) + __popc(need & ((1u << lane) - 1u));
+                if (idx >= n) {
+                    exhausted = true;
+                } else {
+                    float4 a = __ldcs(rays + 2 * idx), b = __ldcs(rays + 2 * idx + 1);
+                    r = make_trace_ray(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z));
+                    s.tMax = a.w;
+                    s.sp = 0;
+                    s.found = false;
+                    s.hit.prim = -1;
+                    float te;
+                    active = !root.empty &&
+                             box_entry(r, root.box[0], root.box[1], root.box[2], root.box[3], root.box[4], root.box[5], &te) &&
+                             te < s.tMax;
+                    s.ref = root.ref;
+                    if (!active) {
+                        primOut[idx] = kAny ? 0 : -1;
+                        if (!kAny) {
+                            if (tOut) tOut[idx] = 0.f;
+                            if (b1Out) b1Out[idx] = 0.f;
+                            if (b2Out) b2Out[idx] = 0.f;
+                        }
+                    }
+                }
+            }
+        }
+        if (__all_sync(full, exhausted)) break;
+        if (active && traverse_step<kAny, false>(nodes, prims, r, s, stackRef, stackT, &overflow)) {
+            active = false;
+            if (kAny) {
+                primOut[idx] = s.found ? 1 : 0;
+            } else {
+                primOut[idx] = s.found ? s.hit.prim : -1;
+                if (tOut) tOut[idx] = s.found ? s.hit.t : 0.f;
+                if (b1Out) b1Out[idx] = s.found ? s.hit.u : 0.f;
+                if (b2Out) b2Out[idx] = s.found ? s.hit.v : 0.f;
+            }
         }
     }
+    if (overflow) atomicOr(status, 1);
 }
 
+// Resident blocks per SM of a kernel (cached): the persistent grid is exactly one full wave.
+template <typename K> int resident_blocks(K kernel, int block) {
+    int n = 0;
+    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, block, 0));
+    return std::max(1, n);
+}
+
+// dStatus points at the accel's 16-byte status block: int status at 0, ray counter at 8.
 void launch_trace(const DeviceAccel &acc, const prgpu::Ray *dRays, int64_t n, bool anyHit, int32_t *dPrim,
                   float *dT, float *dB1, float *dB2, int *dStatus, cudaStream_t s, int smCount) {
     if (n <= 0) return;
     const int block = 256;
+    static int residentAny = 0, residentClosest = 0;
+    if (!residentAny) residentAny = resident_blocks(k_trace_persist<true>, block);
+    if (!residentClosest) residentClosest = resident_blocks(k_trace_persist<false>, block);
+    auto *counter = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(dStatus) + 8);
+    PRB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     int64_t blocksNeeded = (n + block - 1) / block;
-    // Enough blocks to fill every SM several times over; the grid-stride loop covers the rest.
-    int64_t cap = int64_t(smCount) * 64;
-    int grid = int(std::min<int64_t>(blocksNeeded, cap));
     const auto *r4 = reinterpret_cast<const float4 *>(dRays);
-    if (anyHit)
-        k_trace<true, false><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4, n,
-                                                    dPrim, nullptr, nullptr, nullptr, dStatus);
-    else
-        k_trace<false, false><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4, n,
-                                                     dPrim, dT, dB1, dB2, dStatus);
+    if (anyHit) {
+        int grid = int(std::min<int64_t>(blocksNeeded, int64_t(smCount) * residentAny));
+        k_trace_persist<true><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4, n,
+                                                     dPrim, nullptr, nullptr, nullptr, dStatus, counter);
+    } else {
+        int grid = int(std::min<int64_t>(blocksNeeded, int64_t(smCount) * residentClosest));
+        k_trace_persist<false><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4,
+                                                      n, dPrim, dT, dB1, dB2, dStatus, counter);
+    }
     count_launch();
     PRB_CUDA(cudaGetLastError());
 }
@@ -81,8 +139,8 @@ bool make_accel(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
     DeviceState &ds = device_state(deviceIndex);
     a->device = ds.device;
     a->acc.upload(h, ds.stream);
-    a->status.ensure(sizeof(int));
-    PRB_CUDA(cudaMemsetAsync(a->status.ptr, 0, sizeof(int), ds.stream));
+    a->status.ensure(16);  // status word at 0, persistent-kernel ray counter at 8
+    PRB_CUDA(cudaMemsetAsync(a->status.ptr, 0, 16, ds.stream));
     PRB_CUDA(cudaStreamSynchronize(ds.stream));
     return true;
 }

@@ -228,4 +228,75 @@ __device__ __forceinline__ bool traverse(const WNode *__restrict__ nodes, const 
     return found;
 }
 
+// The same traversal cut into steps (one interior node or one leaf per call), for persistent
+// warps that hand a finished lane a new ray at once instead of waiting for the warp's longest
+// ray. Visit order, box and triangle arithmetic are those of traverse(), so results are
+// identical. Returns true when the ray's traversal is finished.
+struct TravState {
+    int ref, sp;
+    float tMax;
+    bool found;
+    Hit hit;
+};
+
+template <bool kAny, bool kSpheres>
+__device__ __forceinline__ bool traverse_step(const WNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
+                                              const TraceRay &r, TravState &s, int *stackRef, float *stackT,
+                                              bool *overflow) {
+    if (s.ref >= 0) {
+        const WNode *n = nodes + s.ref;
+        float4 a = __ldg(&n->a), b = __ldg(&n->b), c = __ldg(&n->c);
+        int4 rr = __ldg(&n->r);
+        float t0, t1;
+        bool h0 = box_entry(r, a.x, a.y, a.z, a.w, b.x, b.y, &t0);
+        bool h1 = box_entry(r, b.z, b.w, c.x, c.y, c.z, c.w, &t1);
+        bool secondFirst = r.neg[rr.z];
+        int nRef = secondFirst ? rr.y : rr.x, fRef = secondFirst ? rr.x : rr.y;
+        bool nHit = secondFirst ? h1 : h0, fHit = secondFirst ? h0 : h1;
+        float nT = secondFirst ? t1 : t0, fT = secondFirst ? t0 : t1;
+        if (fHit) {
+            if (s.sp >= kStackSize) {
+                *overflow = true;
+                return true;
+            }
+            stackRef[s.sp] = fRef;
+            stackT[s.sp] = fT;
+            ++s.sp;
+        }
+        if (nHit && nT < s.tMax) {
+            s.ref = nRef;
+            return false;
+        }
+    } else {
+        const LeafPrim *p = prims + ~s.ref;
+        for (bool last = false; !last; ++p) {
+            float4 v0 = __ldg(&p->v0), v1 = __ldg(&p->v1), v2 = __ldg(&p->v2);
+            last = __float_as_int(v2.w) != 0;
+            float t, u = 0.f, v = 0.f;
+            bool h;
+            if (kSpheres && __float_as_int(v1.w) == 1)
+                h = hit_sphere(r, v0, v1, s.tMax, &t);
+            else
+                h = hit_triangle(r, v0, v1, v2, s.tMax, &t, &u, &v);
+            if (h) {
+                s.found = true;
+                if (kAny) return true;
+                s.tMax = t;
+                s.hit.t = t;
+                s.hit.u = u;
+                s.hit.v = v;
+                s.hit.prim = __float_as_int(v0.w);
+            }
+        }
+    }
+    while (s.sp > 0) {
+        --s.sp;
+        if (stackT[s.sp] < s.tMax) {
+            s.ref = stackRef[s.sp];
+            return false;
+        }
+    }
+    return true;
+}
+
 } // namespace prb
