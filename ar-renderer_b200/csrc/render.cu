@@ -51,8 +51,14 @@ struct Shadows {
     float *w;    // spectral MIS scale applied to L
 };
 
-enum { kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntSlots = 8 };
-enum { kStatusBadIndex = 1, kStatusGuard = 2 };
+// Device counters of one wavefront: queue lengths, the persistent kernels' work counters, status.
+enum {
+    kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
+    kCntSlots = 8
+};
+enum { kStatusStack = 1, kStatusGuard = 2 };
+// Device statistics (64-bit): closest-hit rays, shadow rays, non-empty bounces.
+enum { kStatClosest = 0, kStatShadow = 1, kStatBounces = 2, kStatSlots = 4 };
 
 constexpr float kShadowEps = 1e-4f;  // src/scene/interaction.h:21
 
@@ -490,21 +496,58 @@ __global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo c
     }
 }
 
+// Closest hit for every queued path, by persistent warps whose finished lanes take the next
+// queue entry at once (see k_trace_persist in accel.cu): bounce rays are incoherent and end
+// after very different numbers of steps.
 template <bool kSpheres>
-__global__ void __launch_bounds__(256) k_extend(DevScene s, Paths P, const int *counters, const int *queue) {
-    int n = counters[kCntActive];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int j = queue[q];
-        float4 o = P.o[j], d = P.d[j];
-        TraceRay r = make_trace_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
-        Hit h;
-        h.prim = -1;
-        h.t = h.u = h.v = 0.f;
-        bool overflow = false;
-        bool found = s.root.empty ? false
-                                  : traverse<false, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, kInf, &h, &overflow);
-        P.hit[j] = make_float4(h.t, h.u, h.v, __int_as_float(found ? h.prim : -1));
+__global__ void __launch_bounds__(256) k_extend(DevScene s, Paths P, int *counters, const int *queue) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n = counters[kCntActive];
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TraceRay r;
+    TravState st;
+    st.ref = 0;
+    st.sp = 0;
+    st.tMax = kInf;
+    st.found = false;
+    int j = 0;
+    bool active = false, exhausted = n == 0, overflow = false;
+    while (!__all_sync(full, exhausted)) {
+        unsigned need = __ballot_sync(full, !active && !exhausted);
+        if (need) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(counters + kCntExtendWork, __popc(need));
+            base = __shfl_sync(full, base, 0);
+            if (!active && !exhausted) {
+                int q = base + __popc(need & ((1u << lane) - 1u));
+                if (q >= n) {
+                    exhausted = true;
+                } else {
+                    j = queue[q];
+                    float4 o = P.o[j], d = P.d[j];
+                    r = make_trace_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
+                    st.tMax = kInf;
+                    st.sp = 0;
+                    st.found = false;
+                    st.hit.prim = -1;
+                    float te;
+                    active = !s.root.empty &&
+                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
+                                       s.root.box[5], &te) &&
+                             te < kInf;
+                    st.ref = s.root.ref;
+                    if (!active) P.hit[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                }
+            }
+        }
+        if (active && traverse_step<false, kSpheres>(s.nodes, s.leaves, r, st, stackRef, stackT, &overflow)) {
+            active = false;
+            P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
+        }
     }
+    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
 }
 
 struct ShadeArgs {
@@ -741,10 +784,87 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
     }
 }
 
-// Visibility of queued NEE samples: any-hit without interfaces, otherwise a walk through medium
-// boundaries with homogeneous transmittance (src/scene/scene.cpp:41-59).
+// An unoccluded NEE sample: its contribution times the transmittance of the medium it crossed
+// goes to the path's radiance sums (one shadow entry per path and bounce, so no atomics).
+__device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P, const Shadows &S, int q) {
+    float4 o4 = S.o[q], d4 = S.d[q];
+    int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
+    SS c = from_f4(S.c[q]);
+    if (medium >= 0) c = c * medium_tr(s, medium, load_lam(P, j), len(mk(d4.x, d4.y, d4.z)));
+    float w = S.w[q];
+    float4 L = P.L[j], Lh = P.Lhero[j];
+    P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
+    P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
+}
+
+// Visibility of queued NEE samples in scenes without medium interfaces: any-hit queries up to
+// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill.
 template <bool kSpheres>
-__global__ void __launch_bounds__(256) k_shadow(DevScene s, Paths P, Shadows S, const int *counters) {
+__global__ void __launch_bounds__(256) k_shadow_any(DevScene s, Paths P, Shadows S, int *counters) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n = counters[kCntShadow];
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TraceRay r;
+    TravState st;
+    st.ref = 0;
+    st.sp = 0;
+    st.tMax = 1.f - kShadowEps;
+    st.found = false;
+    int q = 0;
+    bool active = false, exhausted = n == 0, overflow = false;
+    while (!__all_sync(full, exhausted)) {
+        unsigned need = __ballot_sync(full, !active && !exhausted);
+        if (need) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(counters + kCntShadowWork, __popc(need));
+            base = __shfl_sync(full, base, 0);
+            if (!active && !exhausted) {
+                q = base + __popc(need & ((1u << lane) - 1u));
+                if (q >= n) {
+                    exhausted = true;
+                } else {
+                    float4 o4 = S.o[q], d4 = S.d[q];
+                    r = make_trace_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
+                    st.tMax = 1.f - kShadowEps;
+                    st.sp = 0;
+                    st.found = false;
+                    float te;
+                    active = !s.root.empty &&
+                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
+                                       s.root.box[5], &te) &&
+                             te < st.tMax;
+                    st.ref = s.root.ref;
+                    if (!active) shadow_accept(s, P, S, q);
+                }
+            }
+        }
+        if (active && traverse_step<true, kSpheres>(s.nodes, s.leaves, r, st, stackRef, stackT, &overflow)) {
+            active = false;
+            if (!st.found) shadow_accept(s, P, S, q);
+        }
+    }
+    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
+}
+
+// Moves the survivors' queue into place for the next bounce and accumulates statistics (one
+// thread; keeps the bounce loop free of host round trips).
+__global__ void k_advance(int *counters, unsigned long long *stats) {
+    stats[kStatClosest] += (unsigned long long)counters[kCntActive];
+    stats[kStatShadow] += (unsigned long long)counters[kCntShadow];
+    stats[kStatBounces] += counters[kCntActive] > 0 ? 1ull : 0ull;
+    counters[kCntActive] = counters[kCntNext];
+    counters[kCntNext] = 0;
+    counters[kCntShadow] = 0;
+    counters[kCntExtendWork] = 0;
+    counters[kCntShadowWork] = 0;
+}
+
+// Visibility of queued NEE samples in scenes with medium interfaces: a walk through the boundary
+// surfaces with homogeneous transmittance (src/scene/scene.cpp:41-59).
+template <bool kSpheres>
+__global__ void __launch_bounds__(256) k_shadow_walk(DevScene s, Paths P, Shadows S, const int *counters) {
     int n = counters[kCntShadow];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
         float4 o4 = S.o[q], d4 = S.d[q];
@@ -831,14 +951,18 @@ __global__ void __launch_bounds__(256) k_film(DevScene s, Paths P, ChunkInfo ci,
 // ---------------------------------------------------------------------------------------------
 // Driver
 
+constexpr int kBouncesPerPoll = 4;  // bounces enqueued between two host reads of the queue length
+
 struct RenderState {
     SceneCache scene;
-    DevBuf pathBuf, shadowBuf, queues, counters, film;
+    DevBuf pathBuf, shadowBuf, queues, counters, stats, film;
     int capacity = 0;
     Paths P{};
     Shadows S{};
-    cudaEvent_t ev[8] = {};
+    int *hostActive = nullptr;          // pinned: the active-queue length, polled between bounce blocks
+    cudaEvent_t ev[4 * kBouncesPerPoll + 2] = {};
     bool events = false;
+    int residentExtend[2] = {0, 0}, residentShadow[2] = {0, 0};
 };
 
 std::unique_ptr<RenderState> gRender[64];
@@ -880,6 +1004,7 @@ void ensure_capacity(RenderState &rs, int cap) {
     rs.S.w = reinterpret_cast<float *>(take(cap * sizeof(float)));
     rs.queues.ensure(size_t(2) * cap * sizeof(int));
     rs.counters.ensure(kCntSlots * sizeof(int));
+    rs.stats.ensure(kStatSlots * sizeof(unsigned long long));
     rs.capacity = cap;
 }
 
@@ -888,8 +1013,16 @@ int grid_for(const DeviceState &ds, int64_t work, int perSm = 8) {
     return int(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(ds.prop.multiProcessorCount) * perSm)));
 }
 
+template <typename K> int resident_blocks_of(K kernel) {
+    int n = 0;
+    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0));
+    return std::max(1, n);
+}
+
 // Renders params->spp samples of every pixel and adds them, in sample order, onto the device
-// FP64 film rs.film (already initialised by the caller).
+// FP64 film rs.film (already initialised by the caller). Bounces are enqueued in blocks of
+// kBouncesPerPoll with the queue advanced on the device; the host reads the queue length once
+// per block to stop.
 bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParams &rp, const prgpu::SceneExt *ext,
                       prgpu::RenderStats *stats, std::string *err) {
     cudaStream_t st = ds.stream;
@@ -905,16 +1038,25 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     ensure_capacity(rs, npixChunk * S);
     if (!rs.events) {
         for (auto &e : rs.ev) PRB_CUDA(cudaEventCreate(&e));
+        PRB_CUDA(cudaMallocHost(&rs.hostActive, sizeof(int)));
+        rs.residentExtend[0] = resident_blocks_of(k_extend<false>);
+        rs.residentExtend[1] = resident_blocks_of(k_extend<true>);
+        rs.residentShadow[0] = resident_blocks_of(k_shadow_any<false>);
+        rs.residentShadow[1] = resident_blocks_of(k_shadow_any<true>);
         rs.events = true;
     }
     int *cnt = rs.counters.as<int>();
+    auto *dstats = rs.stats.as<unsigned long long>();
     int *qa = rs.queues.as<int>(), *qb = qa + rs.capacity;
     double traceMs = 0, shadeMs = 0, shadowMs = 0, filmMs = 0;
-    uint64_t closest = 0, shadow = 0, bounces = 0, launches = 0;
-    const bool spheres = rs.scene.hasSpheres;
+    uint64_t launches = 0;
+    const int sph = rs.scene.hasSpheres ? 1 : 0;
+    const int sms = ds.prop.multiProcessorCount;
+    const int gExtend = sms * rs.residentExtend[sph], gShadow = sms * rs.residentShadow[sph];
+    const int gShade = sms * 8;
     const bool timing = stats != nullptr;
-    int hostCnt[kCntSlots];
-    PRB_CUDA(cudaMemsetAsync(cnt + kCntStatus, 0, sizeof(int), st));
+    PRB_CUDA(cudaMemsetAsync(cnt, 0, kCntSlots * sizeof(int), st));
+    PRB_CUDA(cudaMemsetAsync(dstats, 0, kStatSlots * sizeof(unsigned long long), st));
     for (int64_t pix0 = 0; pix0 < npix; pix0 += npixChunk) {
         int np = int(std::min<int64_t>(npixChunk, npix - pix0));
         for (int s0 = 0; s0 < spp; s0 += S) {
@@ -926,83 +1068,81 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
             ci.seed = rp.seed;
             ci.maxDepth = rp.maxDepth;
             int total = np * ci.samples;
-            PRB_CUDA(cudaMemsetAsync(cnt, 0, 3 * sizeof(int), st));
             k_raygen<<<grid_for(ds, total), 256, 0, st>>>(scene, rs.P, ci, cnt, qa);
             ++launches;
-            PRB_CUDA(cudaMemcpyAsync(hostCnt, cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
-            PRB_CUDA(cudaStreamSynchronize(st));
-            int active = hostCnt[kCntActive];
             int *qin = qa, *qout = qb;
-            while (active > 0) {
-                ++bounces;
-                closest += uint64_t(active);
-                int g = grid_for(ds, active);
-                if (timing) PRB_CUDA(cudaEventRecord(rs.ev[0], st));
-                if (spheres) k_extend<true><<<g, 256, 0, st>>>(scene, rs.P, cnt, qin);
-                else k_extend<false><<<g, 256, 0, st>>>(scene, rs.P, cnt, qin);
-                if (timing) PRB_CUDA(cudaEventRecord(rs.ev[1], st));
-                ShadeArgs sa{scene, rs.P, rs.S, qin, qout, cnt, rp.maxDepth};
-                k_shade<<<g, 256, 0, st>>>(sa);
-                if (timing) PRB_CUDA(cudaEventRecord(rs.ev[2], st));
-                PRB_CUDA(cudaMemcpyAsync(hostCnt, cnt, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            for (;;) {
+                for (int b = 0; b < kBouncesPerPoll; ++b) {
+                    if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b], st));
+                    if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, rs.P, cnt, qin);
+                    else k_extend<false><<<gExtend, 256, 0, st>>>(scene, rs.P, cnt, qin);
+                    if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
+                    ShadeArgs sa{scene, rs.P, rs.S, qin, qout, cnt, rp.maxDepth};
+                    k_shade<<<gShade, 256, 0, st>>>(sa);
+                    if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
+                    if (scene.hasInterfaces) {
+                        if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                        else k_shadow_walk<false><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                    } else {
+                        if (sph) k_shadow_any<true><<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                        else k_shadow_any<false><<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                    }
+                    if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 3], st));
+                    k_advance<<<1, 1, 0, st>>>(cnt, dstats);
+                    launches += 4;
+                    std::swap(qin, qout);
+                }
+                PRB_CUDA(cudaGetLastError());
+                PRB_CUDA(cudaMemcpyAsync(rs.hostActive, cnt + kCntActive, sizeof(int), cudaMemcpyDeviceToHost, st));
                 PRB_CUDA(cudaStreamSynchronize(st));
-                int nsh = hostCnt[kCntShadow];
-                shadow += uint64_t(nsh);
-                launches += 2;
-                if (nsh > 0) {
-                    int gs = grid_for(ds, nsh);
-                    if (spheres) k_shadow<true><<<gs, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
-                    else k_shadow<false><<<gs, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
-                    ++launches;
-                }
                 if (timing) {
-                    PRB_CUDA(cudaEventRecord(rs.ev[3], st));
-                    PRB_CUDA(cudaEventSynchronize(rs.ev[3]));
-                    float a = 0, b = 0, c = 0;
-                    PRB_CUDA(cudaEventElapsedTime(&a, rs.ev[0], rs.ev[1]));
-                    PRB_CUDA(cudaEventElapsedTime(&b, rs.ev[1], rs.ev[2]));
-                    PRB_CUDA(cudaEventElapsedTime(&c, rs.ev[2], rs.ev[3]));
-                    traceMs += a;
-                    shadeMs += b;
-                    shadowMs += c;
+                    for (int b = 0; b < kBouncesPerPoll; ++b) {
+                        float x = 0, y = 0, z = 0;
+                        PRB_CUDA(cudaEventElapsedTime(&x, rs.ev[4 * b], rs.ev[4 * b + 1]));
+                        PRB_CUDA(cudaEventElapsedTime(&y, rs.ev[4 * b + 1], rs.ev[4 * b + 2]));
+                        PRB_CUDA(cudaEventElapsedTime(&z, rs.ev[4 * b + 2], rs.ev[4 * b + 3]));
+                        traceMs += x;
+                        shadeMs += y;
+                        shadowMs += z;
+                    }
                 }
-                active = hostCnt[kCntNext];
-                // Next bounce: the survivors become the active queue.
-                int zero3[3] = {active, 0, 0};
-                PRB_CUDA(cudaMemcpyAsync(cnt, zero3, 3 * sizeof(int), cudaMemcpyHostToDevice, st));
-                std::swap(qin, qout);
+                if (*rs.hostActive == 0) break;
             }
-            if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4], st));
+            if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * kBouncesPerPoll], st));
             k_film<<<grid_for(ds, np), 256, 0, st>>>(scene, rs.P, ci, rp.clampLuminance, rs.film.as<double>());
             ++launches;
             if (timing) {
-                PRB_CUDA(cudaEventRecord(rs.ev[5], st));
-                PRB_CUDA(cudaEventSynchronize(rs.ev[5]));
+                PRB_CUDA(cudaEventRecord(rs.ev[4 * kBouncesPerPoll + 1], st));
+                PRB_CUDA(cudaEventSynchronize(rs.ev[4 * kBouncesPerPoll + 1]));
                 float f = 0;
-                PRB_CUDA(cudaEventElapsedTime(&f, rs.ev[4], rs.ev[5]));
+                PRB_CUDA(cudaEventElapsedTime(&f, rs.ev[4 * kBouncesPerPoll], rs.ev[4 * kBouncesPerPoll + 1]));
                 filmMs += f;
             }
         }
     }
     PRB_CUDA(cudaGetLastError());
     int status = 0;
+    unsigned long long hs[kStatSlots] = {};
     PRB_CUDA(cudaMemcpyAsync(&status, cnt + kCntStatus, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PRB_CUDA(cudaMemcpyAsync(hs, dstats, sizeof(hs), cudaMemcpyDeviceToHost, st));
     PRB_CUDA(cudaStreamSynchronize(st));
     count_launch(launches);
     if (stats) {
         stats->pathSamples += uint64_t(npix) * uint64_t(spp);
-        stats->closestRays += closest;
-        stats->shadowRays += shadow;
-        stats->bounces += bounces;
+        stats->closestRays += hs[kStatClosest];
+        stats->shadowRays += hs[kStatShadow];
+        stats->bounces += hs[kStatBounces];
         stats->kernelLaunches += launches;
         stats->traceMs += traceMs;
         stats->shadeMs += shadeMs;
         stats->shadowMs += shadowMs;
         stats->filmMs += filmMs;
     }
-    if (status & kStatusGuard) {
-        // The 8192-iteration guard of the reference ended some paths; not an error there either.
+    if (status & kStatusStack) {
+        *err = "BVH deeper than the traversal stack (64 entries)";
+        return false;
     }
+    // kStatusGuard: the 8,192-step guard of the reference ended some paths; not an error there either.
     return true;
 }
 

@@ -132,6 +132,59 @@ def cpu_reference(verts, closest, anyhit, rays_per_pass: int):
     return 2 * rays_per_pass / (t1 + t2) / 1e6, ref.thread_count(), t1 + t2
 
 
+def path_tracer_bench(args, device: int, cpu: bool):
+    """The plain path tracer on the box scene (256 x 256, 64 spp, 4 hero wavelengths, max depth 8,
+    44,814 primitives), built by this library's host side (prgpu.hostscene) and rendered through
+    prgpu_render_ex. value = path samples/s of device time; e2e = the v4 prgpu_render call with a
+    host SceneDesc and host film (scene upload cached after the first call, film copied out each
+    step); cpu_baseline = the reference PathIntegrator (oracle/_ref) on the same scene."""
+    from prgpu import abi, hostscene, render, scenes
+
+    s = scenes.box_scene(seed=0, width=256, height=256, spp=64, max_depth=8)
+    h = hostscene.build_box_scene(s)
+    desc = h.desc()
+    w, hh, spp = s.width, s.height, s.spp
+    for _ in range(args.warmup):
+        render.render_ex(desc, w, hh, spp, seed=1, max_depth=8)
+    dev_ms, wall = [], []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        _, st = render.render_ex(desc, w, hh, spp, first_sample=k * spp, seed=1, max_depth=8, stats=True)
+        wall.append(time.perf_counter() - t0)
+        dev_ms.append(st.deviceMs)
+    samples = w * hh * spp
+    film = np.zeros((hh, w, 3), np.float32)
+    render.render_v4(desc, w, hh, spp, seed=1, max_depth=8, out=film)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        render.render_v4(desc, w, hh, spp, first_sample=k * spp, seed=1, max_depth=8, out=film)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    out = {
+        "workload": "plain path tracer, box + 35 icospheres (44,814 triangles), 256x256, 64 spp, depth 8, 4 hero wavelengths",
+        "metric": "path samples/s", "value": samples / (statistics.mean(dev_ms) * 1e-3), "unit": "path samples/s",
+        "ms_per_step": statistics.mean(dev_ms), "steps": args.steps,
+        "kernel_ms": {"closest": st.traceMs, "shade": st.shadeMs, "shadow": st.shadowMs, "film": st.filmMs},
+        "rays_per_step": {"closest": int(st.closestRays), "shadow": int(st.shadowRays)},
+        "e2e": {"value": samples / e2e_s, "unit": "path samples/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(w * hh * 3 * 8)},
+    }
+    if cpu:
+        import ref
+
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import render_util
+
+        ref.set_threads(0)
+        rs = ref.RefScene(render_util.scene_file("bench_c0", seed=0, width=256, height=256))
+        rs.render(1, 0, 8)
+        cspp = 8
+        _, dt = rs.render(cspp, 1, 8)
+        out["cpu_baseline"] = {"value": w * hh * cspp / dt, "unit": "path samples/s", "cores": ref.thread_count(),
+                               "kind": "reference",
+                               "sample": f"reference PathIntegrator, same scene from its JSON form, {cspp} spp at 256x256 ({dt:.1f} s)"}
+    return out
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -180,6 +233,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
+    ap.add_argument("--no-path-tracer", action="store_true", help="skip the path-tracer workload")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per pass (smaller for profiling captures)")
     args = ap.parse_args()
     N_RAYS = args.rays
@@ -286,6 +340,9 @@ def main():
         cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference",
                "sample": f"{per} closest-hit + {per} any-hit rays of this workload through the reference "
                          f"BVH::Intersect/IntersectP on its own BVH ({secs:.1f} s)"}
+    pt = None
+    if world == 1 and not args.no_path_tracer:
+        pt = path_tracer_bench(args, local, cpu=not args.no_cpu_baseline)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -309,6 +366,7 @@ def main():
         "gpu_launches": launches,
         "closest_hit_mrays": N_RAYS / (closest_ms * 1e3),
         "any_hit_mrays": N_RAYS / ((ms_per_step - closest_ms) * 1e3),
+        "path_tracer": pt,
     }
     print(json.dumps(line), flush=True)
 
