@@ -7,6 +7,7 @@
 
 #include "bsdf.cuh"
 #include "device.cuh"
+#include "lights.cuh"
 
 namespace prb {
 
@@ -93,6 +94,22 @@ __global__ void k_eval_homogeneous(int64_t n, const float *__restrict__ in, floa
     }
 }
 
+// Light-BVH selection at shading points: in 7 floats (p[3], n[3], u), out 2 floats (light, pmf),
+// and optionally the pmf of every light at that point.
+__global__ void k_eval_light_bvh(LightTree t, int lightCount, int64_t n, const float *__restrict__ in,
+                                 float *__restrict__ out, float *__restrict__ pmfOut) {
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+        const float *x = in + 7 * j;
+        V3 p = mk(x[0], x[1], x[2]), nn = mk(x[3], x[4], x[5]);
+        float pmf = 0.f;
+        int li = lbvh_sample(t, p, nn, x[6], &pmf);
+        out[2 * j] = float(li);
+        out[2 * j + 1] = li >= 0 ? pmf : 0.f;
+        if (pmfOut)
+            for (int k = 0; k < lightCount; ++k) pmfOut[j * lightCount + k] = lbvh_pmf(t, k, p, nn);
+    }
+}
+
 namespace {
 
 template <typename Launch>
@@ -166,4 +183,64 @@ PRGPU_API int prgpu_eval_homogeneous(int deviceIndex, int64_t n, const float *in
     return run_eval(deviceIndex, n, 10, 14, in, out, err, errLen, [&](int g, cudaStream_t s, const float *i, float *o) {
         k_eval_homogeneous<<<g, 256, 0, s>>>(n, i, o);
     });
+}
+
+PRGPU_API int prgpu_eval_light_bvh(int deviceIndex, const prgpu::LightBVHNode *nodes, int32_t nodeCount,
+                                   int32_t lightCount, float bvhProb, int64_t n, const float *in, float *out,
+                                   float *pmfOut, char *err, int errLen) {
+    std::lock_guard<std::mutex> lock(gApiMutex);
+    if (!nodes || nodeCount <= 0 || lightCount <= 0 || n < 0 || (n > 0 && (!in || !out)) || n > (int64_t(1) << 22)) {
+        set_err(err, errLen, "bad arguments");
+        return 1;
+    }
+    std::vector<int> leafOf(size_t(lightCount), -1);
+    for (int32_t i = 0; i < nodeCount; ++i) {
+        const prgpu::LightBVHNode &b = nodes[i];
+        if (b.light >= 0) {
+            if (b.light >= lightCount) {
+                set_err(err, errLen, "light BVH leaf out of range");
+                return 1;
+            }
+            leafOf[size_t(b.light)] = i;
+        } else if (b.child1 <= i + 1 || b.child1 >= nodeCount) {
+            set_err(err, errLen, "malformed light BVH interior node");
+            return 1;
+        }
+        if (b.parent >= i || b.parent < -1 || (i > 0 && b.parent < 0)) {
+            set_err(err, errLen, "malformed light BVH parent link");
+            return 1;
+        }
+    }
+    if (n == 0) return 0;
+    try {
+        DeviceState &ds = device_state(deviceIndex);
+        DevBuf dn, dl, din, dout, dpmf;
+        dn.ensure(size_t(nodeCount) * sizeof(prgpu::LightBVHNode));
+        dl.ensure(leafOf.size() * sizeof(int));
+        din.ensure(size_t(n) * 7 * sizeof(float));
+        dout.ensure(size_t(n) * 2 * sizeof(float));
+        if (pmfOut) dpmf.ensure(size_t(n) * lightCount * sizeof(float));
+        PRB_CUDA(cudaMemcpyAsync(dn.ptr, nodes, size_t(nodeCount) * sizeof(prgpu::LightBVHNode), cudaMemcpyHostToDevice, ds.stream));
+        PRB_CUDA(cudaMemcpyAsync(dl.ptr, leafOf.data(), leafOf.size() * sizeof(int), cudaMemcpyHostToDevice, ds.stream));
+        PRB_CUDA(cudaMemcpyAsync(din.ptr, in, size_t(n) * 7 * sizeof(float), cudaMemcpyHostToDevice, ds.stream));
+        LightTree t{dn.as<prgpu::LightBVHNode>(), nodeCount, bvhProb, dl.as<int>()};
+        int grid = int(std::min<int64_t>((n + 255) / 256, int64_t(ds.prop.multiProcessorCount) * 8));
+        k_eval_light_bvh<<<grid, 256, 0, ds.stream>>>(t, lightCount, n, din.as<float>(), dout.as<float>(),
+                                                       pmfOut ? dpmf.as<float>() : nullptr);
+        count_launch();
+        PRB_CUDA(cudaGetLastError());
+        PRB_CUDA(cudaMemcpyAsync(out, dout.ptr, size_t(n) * 2 * sizeof(float), cudaMemcpyDeviceToHost, ds.stream));
+        if (pmfOut)
+            PRB_CUDA(cudaMemcpyAsync(pmfOut, dpmf.ptr, size_t(n) * lightCount * sizeof(float), cudaMemcpyDeviceToHost, ds.stream));
+        PRB_CUDA(cudaStreamSynchronize(ds.stream));
+        dn.release();
+        dl.release();
+        din.release();
+        dout.release();
+        dpmf.release();
+        return 0;
+    } catch (const CudaError &e) {
+        set_err(err, errLen, e.msg);
+        return 1;
+    }
 }

@@ -21,6 +21,7 @@
 #include <memory>
 
 #include "bsdf.cuh"
+#include "lights.cuh"
 #include "scene.cuh"
 
 namespace prb {
@@ -246,89 +247,11 @@ __device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
     return d2 / (c * l.area);
 }
 
-// Conty-Kulla importance of a light-BVH node at (p, n) (src/lights/light_bvh.cpp:45-83).
-__device__ float lb_importance(const prgpu::LightBVHNode &b, V3 p, V3 n) {
-    V3 bmin = f3(b.bmin), bmax = f3(b.bmax);
-    V3 pc = (bmin + bmax) * 0.5f;
-    float d2 = len2(p - pc);
-    d2 = fmaxf(d2, len(bmax - bmin) * 0.5f);
-    V3 wi = p - pc;
-    float l = len(wi);
-    wi = l > 0.f ? wi * (1.f / l) : mk(0.f, 0.f, 1.f);
-    float cosW = dot(f3(b.w), wi);
-    if (b.twoSided) cosW = fabsf(cosW);
-    float sinW = safe_sqrt(1.f - sqr(cosW));
-    // Cone subtended by the bounds' bounding sphere.
-    float r = len(bmax - pc);
-    float cosB = -1.f;
-    float dc2 = len2(p - pc);
-    if (dc2 >= r * r) cosB = safe_sqrt(1.f - r * r / dc2);
-    float sinB = safe_sqrt(1.f - sqr(cosB));
-    float sinO = safe_sqrt(1.f - sqr(b.cosThetaO));
-    // cos(max(0, a - b)) and sin(max(0, a - b)) from sines and cosines.
-    auto cosSub = [](float sA, float cA, float sB, float cB) { return cA > cB ? 1.f : cA * cB + sA * sB; };
-    auto sinSub = [](float sA, float cA, float sB, float cB) { return cA > cB ? 0.f : sA * cB - cA * sB; };
-    float cosX = cosSub(sinW, cosW, sinO, b.cosThetaO);
-    float sinX = sinSub(sinW, cosW, sinO, b.cosThetaO);
-    float cosP = cosSub(sinX, cosX, sinB, cosB);
-    if (cosP <= b.cosThetaE) return 0.f;
-    float imp = b.phi * cosP / d2;
-    if (n.x != 0.f || n.y != 0.f || n.z != 0.f) {
-        float cosI = fabsf(dot(wi, n));
-        float sinI = safe_sqrt(1.f - sqr(cosI));
-        imp *= cosSub(sinI, cosI, sinB, cosB);
-    }
-    return fmaxf(imp, 0.f);
-}
-
-// Light-BVH descent (src/lights/light_bvh.cpp:179-214), u already remapped to the BVH branch.
-__device__ int lbvh_sample(const DevScene &s, V3 p, V3 n, float u, float *pmf) {
-    int node = 0;
-    float prob = s.lbvhProb;
-    for (int guard = 0; guard < 64; ++guard) {
-        const prgpu::LightBVHNode &b = s.lbvh[node];
-        if (b.light >= 0) {
-            if (node > 0 || lb_importance(b, p, n) > 0.f) {
-                *pmf = prob;
-                return b.light;
-            }
-            return -1;
-        }
-        float c0 = lb_importance(s.lbvh[node + 1], p, n), c1 = lb_importance(s.lbvh[b.child1], p, n);
-        if (c0 == 0.f && c1 == 0.f) return -1;
-        float p0 = c0 / (c0 + c1);
-        if (u < p0) {
-            prob *= p0;
-            u = fminf(u / p0, kOneMinusEps);
-            node = node + 1;
-        } else {
-            prob *= 1.f - p0;
-            u = fminf((u - p0) / (1.f - p0), kOneMinusEps);
-            node = b.child1;
-        }
-    }
-    return -1;
-}
-
-// Probability that NEE at (p, n) picks light li (src/lights/light_bvh.cpp:216-234 in BVH mode,
-// the power pmf otherwise).
+// Probability that NEE at (p, n) picks light li: the light-BVH pmf when the scene has one (the
+// exact leaf-to-root walk), the power pmf otherwise.
 __device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
     if (s.lbvhCount == 0) return s.lights[li].pmf;
-    int leaf = __ldg(s.lightLeaf + li);
-    if (leaf < 0) return 0.f;
-    if (leaf == 0) return lb_importance(s.lbvh[0], p, n) > 0.f ? s.lbvhProb : 0.f;
-    float pmf = s.lbvhProb;
-    int child = leaf;
-    for (int guard = 0; guard < 64; ++guard) {
-        int parent = s.lbvh[child].parent;
-        if (parent < 0) break;
-        const prgpu::LightBVHNode &b = s.lbvh[parent];
-        float c0 = lb_importance(s.lbvh[parent + 1], p, n), c1 = lb_importance(s.lbvh[b.child1], p, n);
-        if (c0 == 0.f && c1 == 0.f) return 0.f;
-        pmf *= (child == b.child1 ? c1 : c0) / (c0 + c1);
-        child = parent;
-    }
-    return pmf;
+    return lbvh_pmf(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, li, p, n);
 }
 
 struct LightSample {
@@ -358,7 +281,7 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
     float pmf = 0.f;
     if (s.lbvhCount > 0) {
         float u = fminf((ul - s.envPmf) / s.lbvhProb, kOneMinusEps);
-        li = lbvh_sample(s, p, n, u, &pmf);
+        li = lbvh_sample(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, p, n, u, &pmf);
     } else {
         if (s.lightCount == 0) return ls;
         float acc = s.envSpectrum >= 0 ? s.envPmf : 0.f;

@@ -165,6 +165,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_eval_bxdf", [C.c_int, C.c_int, _P, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_phase", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_homogeneous", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_eval_light_bvh", [C.c_int, _P, C.c_int32, C.c_int32, C.c_float, C.c_int64, _P, _P, _P,
+                                            *_ERR], C.c_int)
         _gpu = lib
     return _gpu
 

@@ -77,7 +77,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+                                          "-lms", "50"], stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
         return self
@@ -177,7 +177,7 @@ def path_tracer_bench(args, device: int, cpu: bool):
         ref.set_threads(0)
         rs = ref.RefScene(render_util.scene_file("bench_c0", seed=0, width=256, height=256))
         rs.render(1, 0, 8)
-        cspp = 8
+        cspp = 256
         _, dt = rs.render(cspp, 1, 8)
         out["cpu_baseline"] = {"value": w * hh * cspp / dt, "unit": "path samples/s", "cores": ref.thread_count(),
                                "kind": "reference",
@@ -281,13 +281,14 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        step()
-    barrier()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = lib.prgpu_launch_count()
+    # The clock sampler runs from the warm-up through the timed region (both under full load).
     with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 8)):
+            step()
+        barrier()
+        launches0 = lib.prgpu_launch_count()
         barrier()
         t_start.record(stream)
         for k in range(args.steps):
@@ -335,7 +336,7 @@ def main():
     achieved = BYTES_PER_RAY * N_RAYS / (closest_ms * 1e-3) / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        per = 1 << 22
+        per = 1 << 24
         v, cores, secs = cpu_reference(verts, closest, anyhit, per)
         cpu = {"value": v, "unit": "Mrays/s", "cores": cores, "kind": "reference",
                "sample": f"{per} closest-hit + {per} any-hit rays of this workload through the reference "

@@ -318,3 +318,10 @@ PRGPU_API int prgpu_eval_phase(int deviceIndex, int64_t n, const float *in, floa
 // src/media/medium.cpp:15-103): in 10 floats (sigma_a[4], sigma_s[4], tMax, u); out 14 floats
 // (Tr(tMax)[4], scattered, t, weight[4], pdfRatio[4]).
 PRGPU_API int prgpu_eval_homogeneous(int deviceIndex, int64_t n, const float *in, float *out, char *err, int errLen);
+// Light-BVH next-event selection (pr::BVHLightSampler::Sample / PMF, src/lights/light_bvh.cpp:179-234)
+// over caller nodes: in 7 floats (p[3], n[3], u); out 2 floats (chosen light or -1, its pmf);
+// pmfOut (optional) n x lightCount: the pmf of every light at that point. bvhProb scales the
+// BVH branch (1 when there is no infinite light).
+PRGPU_API int prgpu_eval_light_bvh(int deviceIndex, const prgpu::LightBVHNode *nodes, int32_t nodeCount,
+                                   int32_t lightCount, float bvhProb, int64_t n, const float *in, float *out,
+                                   float *pmfOut, char *err, int errLen);
