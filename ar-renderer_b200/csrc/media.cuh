@@ -1,0 +1,192 @@
+// Participating media on the device: homogeneous transmittance and the heterogeneous (voxel grid)
+// medium of pr::GridMedium -- trilinear cell-centred density (src/media/medium.cpp:117-128),
+// clipping of the segment to the grid bounds in medium space (medium.cpp:182-203), ratio tracking
+// with Russian roulette for shadow transmittance (medium.cpp:205-230) and spectral tracking for
+// free-flight sampling (medium.cpp:232-285), both against the global majorant
+// maxDensity * max(sigma_t).
+#pragma once
+
+#include "scene.cuh"
+
+namespace prb {
+
+__device__ __forceinline__ bool is_grid(const DevScene &s, int medium) { return medium >= s.mediumCount; }
+
+__device__ __forceinline__ SS homogeneous_tr(const DevScene &s, int medium, const Lambda &lam, float dist) {
+    const prgpu::Medium &md = s.media[medium];
+    SS st = (tab4(s.spectra, md.sigmaA, lam) + tab4(s.spectra, md.sigmaS, lam)) * md.scale;
+    SS r;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) r.v[i] = isinf(dist) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * dist);
+    return r;
+}
+
+__device__ __forceinline__ float grid_at(const DevGrid &g, int x, int y, int z) {
+    x = min(max(x, 0), g.nx - 1);
+    y = min(max(y, 0), g.ny - 1);
+    z = min(max(z, 0), g.nz - 1);
+    return __ldg(g.density + (size_t(z) * g.ny + y) * g.nx + x);
+}
+
+__device__ __forceinline__ float lerpf(float t, float a, float b) { return (1.f - t) * a + t * b; }
+
+// Density at a medium-space point: 0 outside the bounds, trilinear between cell centres inside.
+__device__ __forceinline__ float grid_density(const DevGrid &g, V3 p) {
+    if (!(p.x >= g.bmin[0] && p.x <= g.bmax[0] && p.y >= g.bmin[1] && p.y <= g.bmax[1] && p.z >= g.bmin[2] &&
+          p.z <= g.bmax[2]))
+        return 0.f;
+    float ox = p.x - g.bmin[0], oy = p.y - g.bmin[1], oz = p.z - g.bmin[2];
+    if (g.bmax[0] > g.bmin[0]) ox /= g.bmax[0] - g.bmin[0];
+    if (g.bmax[1] > g.bmin[1]) oy /= g.bmax[1] - g.bmin[1];
+    if (g.bmax[2] > g.bmin[2]) oz /= g.bmax[2] - g.bmin[2];
+    float x = ox * g.nx - 0.5f, y = oy * g.ny - 0.5f, z = oz * g.nz - 0.5f;
+    int x0 = int(floorf(x)), y0 = int(floorf(y)), z0 = int(floorf(z));
+    float dx = x - x0, dy = y - y0, dz = z - z0;
+    float c00 = lerpf(dx, grid_at(g, x0, y0, z0), grid_at(g, x0 + 1, y0, z0));
+    float c10 = lerpf(dx, grid_at(g, x0, y0 + 1, z0), grid_at(g, x0 + 1, y0 + 1, z0));
+    float c01 = lerpf(dx, grid_at(g, x0, y0, z0 + 1), grid_at(g, x0 + 1, y0, z0 + 1));
+    float c11 = lerpf(dx, grid_at(g, x0, y0 + 1, z0 + 1), grid_at(g, x0 + 1, y0 + 1, z0 + 1));
+    return lerpf(dz, lerpf(dy, c00, c10), lerpf(dy, c01, c11));
+}
+
+// Medium-space ray of the world segment [0, tMax) clipped to the bounds; false when it misses.
+__device__ __forceinline__ bool grid_clip(const DevGrid &g, V3 o, V3 d, float tMax, V3 *mo, V3 *md, float *t0,
+                                          float *t1) {
+    const float *m = g.w2m;
+    *mo = mk(m[0] * o.x + m[1] * o.y + m[2] * o.z + m[3], m[4] * o.x + m[5] * o.y + m[6] * o.z + m[7],
+             m[8] * o.x + m[9] * o.y + m[10] * o.z + m[11]);
+    *md = mk(m[0] * d.x + m[1] * d.y + m[2] * d.z, m[4] * d.x + m[5] * d.y + m[6] * d.z,
+             m[8] * d.x + m[9] * d.y + m[10] * d.z);
+    *t0 = 0.f;
+    *t1 = tMax;
+    float oo[3] = {mo->x, mo->y, mo->z}, dd[3] = {md->x, md->y, md->z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float inv = 1.f / dd[a];
+        float tn = (g.bmin[a] - oo[a]) * inv, tf = (g.bmax[a] - oo[a]) * inv;
+        if (tn > tf) {
+            float t = tn;
+            tn = tf;
+            tf = t;
+        }
+        if (isnan(tn) || isnan(tf)) {
+            if (oo[a] < g.bmin[a] || oo[a] > g.bmax[a]) return false;
+            continue;
+        }
+        *t0 = fmaxf(*t0, tn);
+        *t1 = fminf(*t1, tf);
+        if (*t0 > *t1) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void grid_sigma(const DevScene &s, const DevGrid &g, const Lambda &lam, SS *sa, SS *ss) {
+    *sa = tab4(s.spectra, g.sigmaA, lam) * g.scale;
+    *ss = tab4(s.spectra, g.sigmaS, lam) * g.scale;
+}
+
+// Ratio-tracking transmittance over [0, dist) along the unit direction d, Russian roulette once
+// the largest channel drops below 0.1 (unbiased). rng: a stream for this segment.
+__device__ SS grid_tr(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float dist, Pcg &rng) {
+    V3 mo, md;
+    float t0, t1;
+    if (!isfinite(dist) || !grid_clip(g, o, d, dist, &mo, &md, &t0, &t1)) return splat(1.f);
+    SS sa, ss;
+    grid_sigma(s, g, lam, &sa, &ss);
+    SS st = sa + ss;
+    float mu = g.maxDensity * max_c(st);
+    if (mu <= 0.f) return splat(1.f);
+    float invMu = 1.f / mu;
+    SS T = splat(1.f);
+    float t = t0;
+    for (int iter = 0; iter < 100000; ++iter) {
+        t -= logf(1.f - rng.uniform()) * invMu;
+        if (t >= t1) break;
+        float den = grid_density(g, mo + md * t);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) T.v[i] *= fmaxf(0.f, 1.f - st.v[i] * (den * invMu));
+        float m = max_c(T);
+        if (m <= 0.f) return splat(0.f);
+        if (m < 0.1f) {
+            if (rng.uniform() < 0.5f) return splat(0.f);
+            T = T * 2.f;
+        }
+    }
+    return T;
+}
+
+// Transmittance of a straight segment of length dist (unit direction d) in medium m.
+__device__ __forceinline__ SS medium_transmittance(const DevScene &s, int m, const Lambda &lam, V3 o, V3 d, float dist,
+                                                   Pcg &rng) {
+    if (!is_grid(s, m)) return homogeneous_tr(s, m, lam, dist);
+    return grid_tr(s, s.grids[m - s.mediumCount], lam, o, d, dist, rng);
+}
+
+// Spectral tracking (wavelength-neutral event probabilities from the channel averages over the
+// live wavelengths, per-wavelength weights sigma_e / (mu P_e)). Returns 1 on a real scattering
+// event at *tOut, 2 on absorption, 0 when the segment [0, tMax) is crossed; *weight multiplies
+// the throughput in every case.
+__device__ int grid_sample(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float tMax, Pcg &rng,
+                           float *tOut, SS *weight) {
+    *weight = splat(1.f);
+    *tOut = tMax;
+    V3 mo, md;
+    float t0, t1;
+    if (!grid_clip(g, o, d, tMax, &mo, &md, &t0, &t1)) return 0;
+    SS sa, ss;
+    grid_sigma(s, g, lam, &sa, &ss);
+    SS st = sa + ss;
+    float mu = g.maxDensity * max_c(st);
+    if (mu <= 0.f) return 0;
+    float invMu = 1.f / mu;
+    auto avg = [&](const SS &v) {
+        float sum = 0.f;
+        int n = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (lam.pdf[i] != 0.f) {
+                sum += fabsf(v.v[i]);
+                ++n;
+            }
+        return n ? sum / n : 0.f;
+    };
+    float t = t0;
+    for (int iter = 0; iter < 100000; ++iter) {
+        t -= logf(1.f - rng.uniform()) * invMu;
+        if (t >= t1) break;
+        float den = grid_density(g, mo + md * t);
+        SS sA = sa * den, sS = ss * den;
+        SS sN = splat(mu) + sA * -1.f + sS * -1.f;
+        float pa = avg(sA), ps = avg(sS), pn = avg(sN);
+        float norm = pa + ps + pn;
+        if (norm <= 0.f) continue;
+        float xi = rng.uniform() * norm;
+        if (xi < ps) {
+            *tOut = t;
+            *weight = *weight * sS * (1.f / (mu * ps / norm));
+            return 1;
+        }
+        if (xi < ps + pa) {
+            *tOut = t;
+            *weight = splat(0.f);
+            return 2;
+        }
+        *weight = *weight * sN * (1.f / (mu * pn / norm));
+        if (!nonzero(*weight)) return 0;
+    }
+    *tOut = tMax;
+    return 0;
+}
+
+// A PCG stream for a shadow segment, from its geometry (ratio tracking needs randomness the path
+// state does not carry in the shadow queue).
+__device__ __forceinline__ Pcg segment_stream(V3 o, V3 d, uint32_t salt) {
+    uint64_t h = mix_bits((uint64_t(__float_as_uint(o.x)) << 32) ^ __float_as_uint(o.y) ^ (uint64_t(salt) << 17));
+    h = mix_bits(h ^ (uint64_t(__float_as_uint(o.z)) << 32) ^ __float_as_uint(d.x));
+    h = mix_bits(h ^ (uint64_t(__float_as_uint(d.y)) << 32) ^ __float_as_uint(d.z));
+    Pcg r;
+    r.seed(h, mix_bits(h + 0x9E3779B97F4A7C15ull));
+    return r;
+}
+
+} // namespace prb

@@ -22,6 +22,7 @@
 
 #include "bsdf.cuh"
 #include "lights.cuh"
+#include "media.cuh"
 #include "scene.cuh"
 
 namespace prb {
@@ -345,13 +346,13 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
     return ls;
 }
 
-__device__ SS medium_tr(const DevScene &s, int medium, const Lambda &lam, float dist) {
-    const prgpu::Medium &md = s.media[medium];
-    SS st = (tab4(s.spectra, md.sigmaA, lam) + tab4(s.spectra, md.sigmaS, lam)) * md.scale;
-    SS r;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) r.v[i] = isinf(dist) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * dist);
-    return r;
+// Transmittance of the shadow segment o -> o + dd (length len(dd)) in the given medium.
+__device__ SS segment_tr(const DevScene &s, int medium, const Lambda &lam, V3 o, V3 dd, float frac) {
+    float l = len(dd);
+    float dist = frac * l;
+    if (!is_grid(s, medium)) return homogeneous_tr(s, medium, lam, dist);
+    Pcg rng = segment_stream(o, dd, uint32_t(medium));
+    return medium_transmittance(s, medium, lam, o, dd * (1.f / l), dist, rng);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -565,59 +566,76 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
         }
         bool handled = !alive;
         bool found = prim >= 0;
-        // Participating medium along the segment (hero-driven free flight, medium.cpp:71-103).
+        // Participating medium along the segment: hero-driven free flight in homogeneous media
+        // (medium.cpp:71-103, with the rPath pdf ratios of path-level spectral MIS), spectral
+        // tracking in grid media (medium.cpp:232-285, wavelength-neutral: rPath unchanged).
         if (!handled && medium >= 0) {
-            const prgpu::Medium &md = s.media[medium];
-            SS ss = tab4(s.spectra, md.sigmaS, lam) * md.scale;
-            SS st = tab4(s.spectra, md.sigmaA, lam) * md.scale + ss;
-            float u = fminf(rng.uniform(), kOneMinusEps);
             float tMax = found ? hit.x : kInf;
-            float t = st.v[0] > 0.f ? -logf(1.f - u) / st.v[0] : kInf;
-            if (t < tMax) {
-                SS T;
+            int event = 0;  // 0: the segment is crossed, 1: real scattering at t, 2: the path ends
+            float t = tMax, g = 0.f;
+            if (!is_grid(s, medium)) {
+                const prgpu::Medium &md = s.media[medium];
+                g = md.g;
+                SS ss = tab4(s.spectra, md.sigmaS, lam) * md.scale;
+                SS st = tab4(s.spectra, md.sigmaA, lam) * md.scale + ss;
+                float u = fminf(rng.uniform(), kOneMinusEps);
+                t = st.v[0] > 0.f ? -logf(1.f - u) / st.v[0] : kInf;
+                if (t < tMax) {
+                    SS T;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) T.v[i] = expf(-st.v[i] * t);
-                float pdf0 = st.v[0] * T.v[0];
-                handled = true;
-                if (!(pdf0 > 0.f)) {
-                    alive = false;
-                } else {
-                    beta = beta * T * ss * (1.f / pdf0);
-                    rpath = rpath * st * T * (1.f / pdf0);
-                    if (!nonzero(beta) || (a.maxDepth > 0 && depth >= a.maxDepth)) {
-                        alive = false;
+                    for (int i = 0; i < 4; ++i) T.v[i] = expf(-st.v[i] * t);
+                    float pdf0 = st.v[0] * T.v[0];
+                    if (!(pdf0 > 0.f)) {
+                        event = 2;
                     } else {
-                        ++depth;
-                        V3 p = o + d * t, wo = -d;
-                        nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, md.g, medium, medium);
-                        float u0 = rng.uniform(), u1 = rng.uniform(), phasePdf;
-                        V3 wi = hg_sample(wo, md.g, u0, u1, &phasePdf);
-                        if (!(phasePdf > 0.f)) {
-                            alive = false;
-                        } else {
-                            prevPdf = phasePdf;
-                            prevP = p;
-                            prevN = mk(0.f, 0.f, 0.f);
-                            specular = false;
-                            o = p;
-                            d = wi;
-                            alive = roulette();
-                        }
+                        beta = beta * T * ss * (1.f / pdf0);
+                        rpath = rpath * st * T * (1.f / pdf0);
+                        event = 1;
+                    }
+                } else {
+                    SS T;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        T.v[i] = isinf(tMax) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * tMax);
+                    if (!(T.v[0] > 0.f)) {
+                        event = 2;
+                    } else {
+                        beta = beta * T * (1.f / T.v[0]);
+                        rpath = rpath * T * (1.f / T.v[0]);
+                        if (!nonzero(beta)) event = 2;
                     }
                 }
             } else {
-                SS T;
-#pragma unroll
-                for (int i = 0; i < 4; ++i) T.v[i] = isinf(tMax) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * tMax);
-                if (!(T.v[0] > 0.f)) {
+                const DevGrid &gr = s.grids[medium - s.mediumCount];
+                g = gr.g;
+                SS wgt;
+                event = grid_sample(s, gr, lam, o, d, tMax, rng, &t, &wgt);
+                beta = beta * wgt;
+                if (event == 0 && !nonzero(beta)) event = 2;
+            }
+            if (event == 2) {
+                alive = false;
+                handled = true;
+            } else if (event == 1) {
+                handled = true;
+                if (!nonzero(beta) || (a.maxDepth > 0 && depth >= a.maxDepth)) {
                     alive = false;
-                    handled = true;
                 } else {
-                    beta = beta * T * (1.f / T.v[0]);
-                    rpath = rpath * T * (1.f / T.v[0]);
-                    if (!nonzero(beta)) {
+                    ++depth;
+                    V3 p = o + d * t, wo = -d;
+                    nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, g, medium, medium);
+                    float u0 = rng.uniform(), u1 = rng.uniform(), phasePdf;
+                    V3 wi = hg_sample(wo, g, u0, u1, &phasePdf);
+                    if (!(phasePdf > 0.f)) {
                         alive = false;
-                        handled = true;
+                    } else {
+                        prevPdf = phasePdf;
+                        prevP = p;
+                        prevN = mk(0.f, 0.f, 0.f);
+                        specular = false;
+                        o = p;
+                        d = wi;
+                        alive = roulette();
                     }
                 }
             }
@@ -709,11 +727,12 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
 
 // An unoccluded NEE sample: its contribution times the transmittance of the medium it crossed
 // goes to the path's radiance sums (one shadow entry per path and bounce, so no atomics).
+template <bool kMedia>
 __device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P, const Shadows &S, int q) {
     float4 o4 = S.o[q], d4 = S.d[q];
     int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
     SS c = from_f4(S.c[q]);
-    if (medium >= 0) c = c * medium_tr(s, medium, load_lam(P, j), len(mk(d4.x, d4.y, d4.z)));
+    if (kMedia && medium >= 0) c = c * segment_tr(s, medium, load_lam(P, j), mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), 1.f);
     float w = S.w[q];
     float4 L = P.L[j], Lh = P.Lhero[j];
     P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
@@ -721,8 +740,10 @@ __device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P,
 }
 
 // Visibility of queued NEE samples in scenes without medium interfaces: any-hit queries up to
-// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill.
-template <bool kSpheres>
+// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill. kMedia: the scene has
+// media, so accepted segments carry a transmittance (kept out of the medium-free variant, whose
+// traversal loop would otherwise pay registers for the ratio-tracking code).
+template <bool kSpheres, bool kMedia>
 __global__ void __launch_bounds__(256) k_shadow_any(DevScene s, Paths P, Shadows S, int *counters) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -759,13 +780,13 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s, Paths P, Shadows
                                        s.root.box[5], &te) &&
                              te < st.tMax;
                     st.ref = s.root.ref;
-                    if (!active) shadow_accept(s, P, S, q);
+                    if (!active) shadow_accept<kMedia>(s, P, S, q);
                 }
             }
         }
         if (active && traverse_step<true, kSpheres>(s.nodes, s.leaves, r, st, stackRef, stackT, &overflow)) {
             active = false;
-            if (!st.found) shadow_accept(s, P, S, q);
+            if (!st.found) shadow_accept<kMedia>(s, P, S, q);
         }
     }
     if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
@@ -805,7 +826,7 @@ __global__ void __launch_bounds__(256) k_shadow_walk(DevScene s, Paths P, Shadow
             bool occ = !s.root.empty &&
                        traverse<true, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
             if (occ) continue;
-            if (medium >= 0) T = medium_tr(s, medium, lam, len(dd));
+            if (medium >= 0) T = segment_tr(s, medium, lam, o, dd, 1.f);
         } else {
             bool blocked = true;
             for (int it = 0; it < 256; ++it) {
@@ -816,7 +837,7 @@ __global__ void __launch_bounds__(256) k_shadow_walk(DevScene s, Paths P, Shadow
                 bool hit = !s.root.empty &&
                            traverse<false, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
                 if (hit && s.mats[s.prims[h.prim].material].type != prgpu::MatInterface) break;
-                if (medium >= 0) T = T * medium_tr(s, medium, lam, (hit ? h.t : 1.f) * len(d));
+                if (medium >= 0) T = T * segment_tr(s, medium, lam, o, d, hit ? h.t : 1.f);
                 if (!hit || !nonzero(T)) {
                     blocked = false;
                     break;
@@ -885,7 +906,7 @@ struct RenderState {
     int *hostActive = nullptr;          // pinned: the active-queue length, polled between bounce blocks
     cudaEvent_t ev[4 * kBouncesPerPoll + 2] = {};
     bool events = false;
-    int residentExtend[2] = {0, 0}, residentShadow[2] = {0, 0};
+    int residentExtend[2] = {0, 0}, residentShadow[4] = {0, 0, 0, 0};
 };
 
 std::unique_ptr<RenderState> gRender[64];
@@ -936,6 +957,18 @@ int grid_for(const DeviceState &ds, int64_t work, int perSm = 8) {
     return int(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(ds.prop.multiProcessorCount) * perSm)));
 }
 
+using ShadowAnyFn = void (*)(DevScene, Paths, Shadows, int *);
+
+// variant bit 0: spheres present, bit 1: media present.
+ShadowAnyFn shadow_any_kernel(int variant) {
+    switch (variant & 3) {
+    case 0: return k_shadow_any<false, false>;
+    case 1: return k_shadow_any<true, false>;
+    case 2: return k_shadow_any<false, true>;
+    default: return k_shadow_any<true, true>;
+    }
+}
+
 template <typename K> int resident_blocks_of(K kernel) {
     int n = 0;
     PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, 256, 0));
@@ -964,8 +997,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
         PRB_CUDA(cudaMallocHost(&rs.hostActive, sizeof(int)));
         rs.residentExtend[0] = resident_blocks_of(k_extend<false>);
         rs.residentExtend[1] = resident_blocks_of(k_extend<true>);
-        rs.residentShadow[0] = resident_blocks_of(k_shadow_any<false>);
-        rs.residentShadow[1] = resident_blocks_of(k_shadow_any<true>);
+        for (int v = 0; v < 4; ++v) rs.residentShadow[v] = resident_blocks_of(shadow_any_kernel(v));
         rs.events = true;
     }
     int *cnt = rs.counters.as<int>();
@@ -975,7 +1007,9 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     uint64_t launches = 0;
     const int sph = rs.scene.hasSpheres ? 1 : 0;
     const int sms = ds.prop.multiProcessorCount;
-    const int gExtend = sms * rs.residentExtend[sph], gShadow = sms * rs.residentShadow[sph];
+    const int shadowVariant = sph | (scene.mediumCount + scene.gridCount > 0 ? 2 : 0);
+    const ShadowAnyFn shadowAny = shadow_any_kernel(shadowVariant);
+    const int gExtend = sms * rs.residentExtend[sph], gShadow = sms * rs.residentShadow[shadowVariant];
     const int gShade = sms * 8;
     const bool timing = stats != nullptr;
     PRB_CUDA(cudaMemsetAsync(cnt, 0, kCntSlots * sizeof(int), st));
@@ -1007,8 +1041,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                         if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
                         else k_shadow_walk<false><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
                     } else {
-                        if (sph) k_shadow_any<true><<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
-                        else k_shadow_any<false><<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                        shadowAny<<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 3], st));
                     k_advance<<<1, 1, 0, st>>>(cnt, dstats);

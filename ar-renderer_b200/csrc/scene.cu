@@ -6,7 +6,9 @@
 // full and a strided sample of the large ones.
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "scene.cuh"
 
@@ -49,6 +51,12 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
     h = fnv(h, sd->filter.cdf, sizeof(sd->filter.cdf));
     if (ext && ext->lightBVH && ext->lightBVHNodeCount > 0)
         h = fnv(h, ext->lightBVH, size_t(ext->lightBVHNodeCount) * sizeof(prgpu::LightBVHNode));
+    if (ext && ext->gridMedia && ext->gridMediumCount > 0)
+        for (int32_t k = 0; k < ext->gridMediumCount; ++k) {
+            const prgpu::GridMediumDesc &g = ext->gridMedia[k];
+            h = fnv_v(h, g);
+            h = sample_hash(h, g.density, size_t(g.nx) * size_t(g.ny) * size_t(g.nz), sizeof(float), 65536);
+        }
     return h;
 }
 
@@ -70,7 +78,18 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
     if (c.width <= 0 || c.height <= 0 || int64_t(c.width) * c.height > (int64_t(1) << 28))
         return fail("camera resolution out of range");
     if (!std::isfinite(c.tanHalfFov) || c.tanHalfFov <= 0) return fail("bad camera field of view");
-    const int32_t ns = sd->spectrumCount, nm = sd->mediumCount;
+    const int32_t ns = sd->spectrumCount;
+    const int32_t ng = (ext && ext->gridMediumCount > 0) ? ext->gridMediumCount : 0;
+    const int32_t nm = sd->mediumCount + ng;  // homogeneous media, then grid media
+    if (ng > 0 && !ext->gridMedia) return fail("null grid media");
+    for (int32_t k = 0; k < ng; ++k) {
+        const prgpu::GridMediumDesc &g = ext->gridMedia[k];
+        if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || int64_t(g.nx) * g.ny * g.nz > (int64_t(1) << 31) || !g.density)
+            return fail("bad grid medium dimensions or data");
+        if (!spec_ok(g.sigmaA, ns) || !spec_ok(g.sigmaS, ns)) return fail("grid medium spectrum index out of range");
+        if (!(g.boundsMin.x <= g.boundsMax.x && g.boundsMin.y <= g.boundsMax.y && g.boundsMin.z <= g.boundsMax.z))
+            return fail("empty grid medium bounds");
+    }
     if (!spec_ok(sd->envSpectrum, ns)) return fail("envSpectrum out of range");
     if (sd->cameraMedium < -1 || sd->cameraMedium >= nm) return fail("cameraMedium out of range");
     for (int32_t i = 0; i < sd->materialCount; ++i) {
@@ -88,7 +107,7 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
         if (l.type == prgpu::LightArea && (l.primitive < 0 || l.primitive >= sd->primCount))
             return fail("area light primitive out of range");
     }
-    for (int32_t i = 0; i < nm; ++i)
+    for (int32_t i = 0; i < sd->mediumCount; ++i)
         if (!spec_ok(sd->media[i].sigmaA, ns) || !spec_ok(sd->media[i].sigmaS, ns))
             return fail("medium spectrum index out of range");
     for (int32_t i = 0; i < sd->primCount; ++i) {
@@ -144,6 +163,43 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         for (int32_t i = 0; i < nb; ++i)
             if (ext->lightBVH[i].light >= 0) leafOf[size_t(ext->lightBVH[i].light)] = i;
         if (nb) put(cache.lbvh, ext->lightBVH, size_t(nb), s);
+        // Grid media: the density grids concatenated in one buffer, plus the descriptor table.
+        int32_t ng = (ext && ext->gridMediumCount > 0) ? ext->gridMediumCount : 0;
+        std::vector<DevGrid> grids(size_t(std::max(1, ng)));
+        size_t total = 0;
+        for (int32_t k = 0; k < ng; ++k)
+            total += size_t(ext->gridMedia[k].nx) * ext->gridMedia[k].ny * ext->gridMedia[k].nz;
+        cache.gridData.ensure(std::max<size_t>(1, total) * sizeof(float));
+        size_t off = 0;
+        for (int32_t k = 0; k < ng; ++k) {
+            const prgpu::GridMediumDesc &g = ext->gridMedia[k];
+            size_t n = size_t(g.nx) * g.ny * g.nz;
+            DevGrid &dg = grids[size_t(k)];
+            std::memcpy(dg.w2m, g.worldToMedium, sizeof(dg.w2m));
+            dg.bmin[0] = g.boundsMin.x, dg.bmin[1] = g.boundsMin.y, dg.bmin[2] = g.boundsMin.z;
+            dg.bmax[0] = g.boundsMax.x, dg.bmax[1] = g.boundsMax.y, dg.bmax[2] = g.boundsMax.z;
+            dg.nx = g.nx, dg.ny = g.ny, dg.nz = g.nz;
+            // Negative or non-finite voxels read as 0, as pr::VoxelGridField does (medium.cpp:108-115).
+            float mx = 0.f;
+            for (size_t i = 0; i < n; ++i)
+                if (std::isfinite(g.density[i]) && g.density[i] > mx) mx = g.density[i];
+            dg.maxDensity = g.maxDensity > mx ? g.maxDensity : mx;
+            dg.scale = g.scale;
+            dg.g = std::min(0.99f, std::max(-0.99f, g.g));
+            dg.sigmaA = g.sigmaA;
+            dg.sigmaS = g.sigmaS;
+            dg.density = cache.gridData.as<float>() + off;
+            std::vector<float> clean(g.density, g.density + n);
+            for (float &v : clean)
+                if (!std::isfinite(v) || v < 0.f) v = 0.f;
+            PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.density), clean.data(), n * sizeof(float),
+                                     cudaMemcpyHostToDevice, s));
+            PRB_CUDA(cudaStreamSynchronize(s));
+            off += n;
+        }
+        put(cache.grids, grids.data(), grids.size(), s);
+        d.grids = cache.grids.as<DevGrid>();
+        d.gridCount = ng;
         put(cache.lightLeaf, leafOf.data(), leafOf.size(), s);
         PRB_CUDA(cudaStreamSynchronize(s));
         cache.hasSpheres = false;
@@ -166,6 +222,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         d.lbvhCount = nb;
     }
     // Per-call scalars (cheap; not part of the device copy).
+    d.mediumCount = sd->mediumCount;
     d.lightCount = sd->lightCount;
     d.cameraMedium = sd->cameraMedium;
     d.envSpectrum = sd->envSpectrum;

@@ -14,6 +14,17 @@
 
 namespace prb {
 
+// A heterogeneous medium on the device (GridMediumDesc with its density grid resident in HBM).
+struct DevGrid {
+    float w2m[12];
+    float bmin[3], bmax[3];
+    int nx, ny, nz;
+    float maxDensity;
+    float scale, g;
+    int sigmaA, sigmaS;
+    const float *density;
+};
+
 struct DevScene {
     const WNode *nodes;
     const LeafPrim *leaves;
@@ -40,13 +51,17 @@ struct DevScene {
     int lbvhCount;
     float lbvhProb;          // probability of the BVH branch (1 - probability of the environment)
     const int *lightLeaf;    // light index -> leaf node (-1 when the light is not in the tree)
+    // Heterogeneous media: medium index m >= mediumCount names grids[m - mediumCount].
+    int mediumCount;
+    const DevGrid *grids;
+    int gridCount;
 };
 
 struct SceneCache {
     uint64_t key = 0;
     bool valid = false;
     DeviceAccel accel;
-    DevBuf prims, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf;
+    DevBuf prims, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData;
     DevScene ds{};
     bool hasSpheres = false;
     int64_t deviceBytes = 0;
@@ -60,6 +75,8 @@ struct SceneCache {
         filterCdf.release();
         lbvh.release();
         lightLeaf.release();
+        grids.release();
+        gridData.release();
         valid = false;
     }
 };

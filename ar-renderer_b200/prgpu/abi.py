@@ -104,10 +104,17 @@ class DeviceInfo(C.Structure):
                 ("isGpu", C.c_int32), ("backend", C.c_char * 32)]
 
 
+class GridMediumDesc(C.Structure):
+    _fields_ = [("sigmaA", C.c_int32), ("sigmaS", C.c_int32), ("scale", C.c_float), ("g", C.c_float),
+                ("worldToMedium", C.c_float * 12), ("boundsMin", C.c_float * 3), ("boundsMax", C.c_float * 3),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("maxDensity", C.c_float),
+                ("density", C.c_void_p)]
+
+
 class SceneExt(C.Structure):
     _fields_ = [("structSize", C.c_uint32), ("lightBVHNodeCount", C.c_int32), ("lightBVH", C.c_void_p),
                 ("lightBVHProb", C.c_float), ("wavefrontPaths", C.c_int32), ("blockSize", C.c_int32),
-                ("flags", C.c_int32)]
+                ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p)]
 
 
 class RenderStats(C.Structure):
@@ -119,6 +126,7 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
+assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 48
 assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512
 
 # ---------------------------------------------------------------------------------------------

@@ -50,7 +50,9 @@ def render_ex(scene, width: int, height: int, spp: int, first_sample: int = 0, s
 
 
 def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
-             block_size: int = 0) -> abi.SceneExt:
+             block_size: int = 0, grid_media=None) -> abi.SceneExt:
+    """SceneExt for prgpu_render_ex. grid_media: GridMediumDesc records (media.grid_desc), indexed
+    after the SceneDesc's homogeneous media. The record keeps the arrays it points at alive."""
     e = abi.SceneExt()
     e.structSize = C.sizeof(abi.SceneExt)
     if light_bvh is not None and len(light_bvh):
@@ -59,4 +61,11 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
         e.lightBVHProb = light_bvh_prob
     e.wavefrontPaths = wavefront_paths
     e.blockSize = block_size
+    e._keep = [light_bvh]
+    if grid_media:
+        from .media import grid_array
+        arr = grid_array(list(grid_media))
+        e.gridMediumCount = len(arr)
+        e.gridMedia = C.cast(arr, C.c_void_p)
+        e._keep.append(arr)
     return e

@@ -71,6 +71,9 @@ class BoxScene:
     light_luminance: float = 30.0
     fov_y: float = 62.0
     medium: dict | None = None  # {"sigma_a": [r,g,b], "sigma_s": [r,g,b], "g": 0.6}
+    # Heterogeneous variant: {"sigma_a", "sigma_s", "g", "scale", "density" (nz, ny, nx) float32,
+    # "bounds" (2, 3) medium space, "matrix" 4x4 medium-to-world}; replaces `medium`.
+    grid: dict | None = None
     spheres: list = field(default_factory=list)
     filter: str = "box"
 
@@ -105,6 +108,41 @@ def box_scene(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64,
         rng = np.random.default_rng(1000 + seed)
         s.medium = {"sigma_s": [float(x) for x in rng.uniform(0.05, 0.5, 3)],
                     "sigma_a": [float(x) for x in rng.uniform(0.0, 0.1, 3)], "g": 0.6}
+    return s
+
+
+def smoke_density(res: int = 24, seed: int = 0) -> np.ndarray:
+    """A smooth cloud on a res^3 grid over [-1, 1]^3 ((nz, ny, nx) float32): a floor layer that
+    thins with height plus a few seeded Gaussian puffs, in [0, ~1.5]."""
+    rng = np.random.default_rng(7000 + seed)
+    c = (np.arange(res) + 0.5) / res * 2.0 - 1.0
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    d = 0.6 * np.exp(-2.5 * (y + 1.0))
+    for _ in range(4):
+        m = rng.uniform(-0.6, 0.6, 3)
+        r = rng.uniform(0.25, 0.45)
+        d += rng.uniform(0.5, 1.0) * np.exp(-((x - m[0]) ** 2 + (y - m[1]) ** 2 + (z - m[2]) ** 2) / (2 * r * r))
+    return d.astype(np.float32)
+
+
+def grid_box_scene(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, max_depth: int = 8,
+                   subdiv: int = 3, res: int = 24, constant: float | None = None, turn_deg: float = 20.0,
+                   scale: float = 1.1) -> BoxScene:
+    """The box scene filled with a heterogeneous chromatic smoke (a voxel grid medium). The grid
+    covers [-1, 1]^3 in medium space, mapped to the world by `scale`, a `turn_deg` turn about y
+    and a 0.05 lift, inside a 2.2 interface box around the room. constant: a uniform density
+    instead of the cloud (with turn_deg 0 and scale >= 1.2 the grid covers the whole interface
+    box, and the medium equals a homogeneous one of sigma * constant)."""
+    s = box_scene(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, subdiv=subdiv)
+    rng = np.random.default_rng(2000 + seed)
+    a = math.radians(turn_deg)
+    m = np.array([[scale * math.cos(a), 0, scale * math.sin(a), 0.0], [0, scale, 0, 0.05],
+                  [-scale * math.sin(a), 0, scale * math.cos(a), 0.0], [0, 0, 0, 1]], dtype=np.float64)
+    dens = smoke_density(res, seed) if constant is None else np.full((res, res, res), constant, np.float32)
+    s.grid = {"sigma_s": [float(x) for x in rng.uniform(0.3, 1.2, 3)],
+              "sigma_a": [float(x) for x in rng.uniform(0.02, 0.2, 3)], "g": 0.4, "scale": 1.0,
+              "density": dens, "bounds": np.array([[-1, -1, -1], [1, 1, 1]], np.float32),
+              "matrix": m.astype(np.float32)}
     return s
 
 
@@ -166,6 +204,15 @@ def to_reference_json(s: BoxScene) -> dict:
         mats["boundary"] = {"type": "interface"}
         objects.append({"name": "fogbox", "geometry": "fogbox", "material": "boundary", "interior": "fog",
                         "exterior": None})
+    if s.grid is not None:
+        gr = s.grid
+        media["smoke"] = {"type": "grid", "file": gr["file"], "sigma_a": gr["sigma_a"], "sigma_s": gr["sigma_s"],
+                          "g": gr["g"], "scale": gr["scale"], "bounds": np.asarray(gr["bounds"]).tolist(),
+                          "transform": {"matrix": _f32(gr["matrix"])}}
+        geometry["smokebox"] = {"type": "box", "size": [2.2, 2.2, 2.2]}
+        mats["boundary"] = {"type": "interface"}
+        objects.append({"name": "smokebox", "geometry": "smokebox", "material": "boundary",
+                        "interior": "smoke", "exterior": None})
     doc = {
         "materials": mats,
         "media": media,
@@ -184,7 +231,11 @@ def to_reference_json(s: BoxScene) -> dict:
 
 
 def write_reference_json(s: BoxScene, path: str) -> str:
+    """Writes the scene (and, for the grid variant, its density as a .vol beside it)."""
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    if s.grid is not None:
+        from .media import write_vol
+        s.grid["file"] = write_vol(os.path.abspath(path) + ".vol", s.grid["density"], s.grid["bounds"])
     with open(path, "w") as f:
         json.dump(to_reference_json(s), f)
     return path

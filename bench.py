@@ -140,7 +140,7 @@ def path_tracer_bench(args, device: int, cpu: bool):
     step); cpu_baseline = the reference PathIntegrator (oracle/_ref) on the same scene."""
     from prgpu import abi, hostscene, render, scenes
 
-    s = scenes.box_scene(seed=0, width=256, height=256, spp=64, max_depth=8)
+    s = scenes.box_scene(seed=0, width=args.pt_res, height=args.pt_res, spp=64, max_depth=8)
     h = hostscene.build_box_scene(s)
     desc = h.desc()
     w, hh, spp = s.width, s.height, s.spp
@@ -169,13 +169,13 @@ def path_tracer_bench(args, device: int, cpu: bool):
                 "d2h_bytes_per_step": int(w * hh * 3 * 8)},
     }
     if cpu:
+        import tempfile
+
         import ref
 
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        import render_util
-
         ref.set_threads(0)
-        rs = ref.RefScene(render_util.scene_file("bench_c0", seed=0, width=256, height=256))
+        jp = os.path.join(tempfile.gettempdir(), "prb_bench", "box_c0.prscene.json")
+        rs = ref.RefScene(scenes.write_reference_json(scenes.box_scene(seed=0, width=256, height=256), jp))
         rs.render(1, 0, 8)
         cspp = 256
         _, dt = rs.render(cspp, 1, 8)
@@ -235,6 +235,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass (profiling runs)")
     ap.add_argument("--no-path-tracer", action="store_true", help="skip the path-tracer workload")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per pass (smaller for profiling captures)")
+    ap.add_argument("--path-tracer-only", action="store_true",
+                    help="run only the path-tracer workload and print its JSON object (profiling captures)")
+    ap.add_argument("--pt-res", type=int, default=256, help="path-tracer image side (256 = the measured workload)")
     args = ap.parse_args()
     N_RAYS = args.rays
     args.warmup = max(args.warmup, 3)
@@ -244,6 +247,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.path_tracer_only:
+        print(json.dumps(path_tracer_bench(args, local, cpu=not args.no_cpu_baseline)))
+        return
 
     import torch
     import torch.distributed as dist

@@ -201,6 +201,22 @@ struct LightBVHNode {
     int32_t pad[2];
 };
 
+// Heterogeneous medium: sigma(p, lambda) = density(p) * spectrum(lambda) * scale, Henyey-Greenstein
+// g, with a voxel density grid sampled trilinearly at cell centres over `bounds` in medium space
+// (pr::GridMedium over a pr::VoxelGridField, src/media/medium.h:93-167, medium.cpp:117-128).
+// Distances are sampled by spectral tracking and shadow transmittance by ratio tracking against a
+// global majorant maxDensity * max(sigma_t) (medium.cpp:205-285). Media are referenced from
+// Primitive::mediumInside/Outside and SceneDesc::cameraMedium with indices mediumCount + k.
+struct GridMediumDesc {
+    int32_t sigmaA, sigmaS;     // spectrum indices
+    float scale, g;
+    float worldToMedium[12];    // affine, row-major 3x4
+    Float3 boundsMin, boundsMax;
+    int32_t nx, ny, nz;
+    float maxDensity;           // >= every voxel; 0 = computed from the data
+    const float *density;       // nx * ny * nz floats, x fastest: index (z * ny + y) * nx + x
+};
+
 // Optional extras for prgpu_render_ex (zero-initialise, then set structSize = sizeof(SceneExt)).
 struct SceneExt {
     uint32_t structSize;
@@ -209,7 +225,9 @@ struct SceneExt {
     float lightBVHProb;             // probability of the BVH branch when envSpectrum >= 0 (1 - pInfinite)
     int32_t wavefrontPaths;         // paths in flight per wavefront (0 = library default)
     int32_t blockSize;              // threads per block for the wavefront kernels (0 = default)
-    int32_t flags;                  // bit 0: keep the FP64 film on the device between calls
+    int32_t flags;                  // reserved, 0
+    int32_t gridMediumCount;
+    const GridMediumDesc *gridMedia;
 };
 
 // Per-call counters and device timings.

@@ -69,6 +69,8 @@ def ref_lib() -> C.CDLL:
         lib.prref_render.restype = C.c_double
         lib.prref_light_bvh_sample.argtypes = [_P, C.c_int64, _P, _P, _P]
         lib.prref_scene_light_count.argtypes = [_P]
+        lib.prref_scene_grid_count.argtypes = [_P]
+        lib.prref_scene_grid_info.argtypes = [_P, C.c_int, C.c_char_p, C.c_int, _P]
         # The RGB->spectrum table is built once (a few seconds) and cached beside the library.
         lib.prref_set_cache_dir(REF_DIR.encode())
         _ref = lib
@@ -169,6 +171,19 @@ class RefScene:
 
     def light_count(self) -> int:
         return self.lib.prref_scene_light_count(self.h)
+
+    def grid_media(self):
+        """Heterogeneous media of the export, in index order (index = mediumCount + k): a list of
+        (name, bounds (2, 3) float32 in medium space as the loader fitted them)."""
+        self.export()
+        out = []
+        for k in range(self.lib.prref_scene_grid_count(self.h)):
+            name = C.create_string_buffer(256)
+            b = np.zeros(6, dtype=np.float32)
+            if self.lib.prref_scene_grid_info(self.h, k, name, len(name), _p(b)) != 0:
+                raise RuntimeError("grid medium %d is not a voxel grid" % k)
+            out.append((name.value.decode(), b.reshape(2, 3)))
+        return out
 
     def light_bvh_sample(self, pts: np.ndarray, with_pmf: bool = True):
         """pts: (n, 7) float32 (p, n, u). Returns (light index, pmf) and the per-light PMF table."""

@@ -337,6 +337,9 @@ struct SceneHandle {
     std::map<const Spectrum *, int> specCache;
     std::map<const Material *, int> matCache;
     std::map<const pr::Medium *, int> medCache;
+    // Heterogeneous media, in first-use order: exported as indices mediumCount + k (the layout of
+    // the GPU module's grid-media extension); their parameters come from the scene file.
+    std::vector<const pr::Medium *> grids;
     int interfaceMat = -1;
 
     int Spec(const Spectrum &s) {
@@ -406,7 +409,9 @@ struct SceneHandle {
             media.push_back(g);
             id = int(media.size() - 1);
         } else {
-            Warn("heterogeneous media not exported");
+            // Placeholder -2 - k, resolved to mediumCount + k once every homogeneous medium is known.
+            grids.push_back(md);
+            id = -2 - int(grids.size() - 1);
         }
         medCache[md] = id;
         return id;
@@ -604,7 +609,12 @@ API const prgpu::SceneDesc *prref_scene_export(void *hp, char *err, int errLen) 
     sd.spectrumCount = int(h->spectra.size());
     sd.media = h->media.data();
     sd.mediumCount = int(h->media.size());
-    sd.cameraMedium = cameraMedium;
+    auto resolve = [&](int32_t id) { return id <= -2 ? sd.mediumCount + (-2 - id) : id; };
+    for (prgpu::Primitive &g : h->prims) {
+        g.mediumInside = resolve(g.mediumInside);
+        g.mediumOutside = resolve(g.mediumOutside);
+    }
+    sd.cameraMedium = resolve(cameraMedium);
     sd.envSpectrum = envSpectrum;
     sd.envScale = envScale;
     sd.envPmf = envPmf;
@@ -723,3 +733,21 @@ API void prref_light_bvh_sample(void *hp, int64_t n, const float *in, float *out
 }
 
 API int prref_scene_light_count(void *hp) { return int(static_cast<SceneHandle *>(hp)->scene->lights.size()); }
+
+// Heterogeneous media of the last export (index mediumCount + k): their names in the scene file and
+// the density-field bounds in medium space after the loader fitted them (scene_loader.cpp:1302-1308).
+API int prref_scene_grid_count(void *hp) { return int(static_cast<SceneHandle *>(hp)->grids.size()); }
+
+API int prref_scene_grid_info(void *hp, int k, char *name, int nameLen, float *bounds6) {
+    auto *h = static_cast<SceneHandle *>(hp);
+    if (k < 0 || k >= int(h->grids.size())) return -1;
+    auto *gm = dynamic_cast<const GridMedium *>(h->grids[size_t(k)]);
+    if (!gm) return -1;
+    std::snprintf(name, size_t(nameLen), "%s", gm->name.c_str());
+    const Bounds3f &b = const_cast<GridMedium *>(gm)->Field().bounds;
+    for (int a = 0; a < 3; ++a) {
+        bounds6[a] = b.pMin[a];
+        bounds6[3 + a] = b.pMax[a];
+    }
+    return 0;
+}
