@@ -1,897 +1,18 @@
-// Wavefront spectral volumetric path tracer (prgpu_render / prgpu_render_ex).
-//
-// The estimator is the reference's pr::PathIntegrator::Li (src/integrators/path.cpp:113-238) as its
-// GPU module restates it (src/gpu/prender_gpu.cpp:1344-1460): 4 hero wavelengths, next-event
-// estimation with power-heuristic MIS, path-level spectral MIS in homogeneous media (rPath, the
-// hero-driven free-flight pdf ratios, with Lhero kept for paths whose secondary wavelengths a
-// dispersive interface terminates), Russian roulette on the MIS-weighted throughput from the
-// third vertex on, no clamping unless the caller asks for it.
-//
-// Instead of one thread looping over a pixel's whole path (the reference megakernel), a batch of
-// paths lives in structure-of-arrays state in HBM and advances one bounce per round of kernels:
-//   raygen  -> closest-hit (k_extend) -> shading (k_shade: media, emission, BSDF, NEE, RR)
-//           -> shadow rays (k_shadow) -> ... until the queue is empty -> film (k_film).
-// Queues are compacted with warp-aggregated atomics (one atomic per warp, slots handed out by
-// ballot + popc), so every kernel reads a dense index list. Each path's final XYZ is added to an
-// FP64 per-pixel film in sample-index order, one sample at a time: a render split into batches
-// produces the same bits as one uninterrupted render.
+// Wavefront spectral volumetric path tracer: the drivers of the kernels in wavefront.cuh.
+//   * prgpu_render / prgpu_render_ex: one scene per call, the host polling the active-queue length
+//     once every few bounces;
+//   * prgpu_render_batch: many scenes in one wavefront, run by one CUDA graph launch whose
+//     device-side loop needs no host round trip, with settings from an autotuner.
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <map>
 #include <memory>
 
-#include "bsdf.cuh"
-#include "lights.cuh"
-#include "media.cuh"
-#include "scene.cuh"
+#include "wavefront.cuh"
 
 namespace prb {
-
-// ---------------------------------------------------------------------------------------------
-// Path state (structure of arrays, 16-byte vector accesses)
-
-struct Paths {
-    float4 *o;       // origin, w: prevPdf
-    float4 *d;       // direction, w: etaScale
-    float4 *beta;    // throughput per wavelength
-    float4 *rpath;   // spectral MIS pdf ratios
-    float4 *L;       // MIS-weighted radiance
-    float4 *Lhero;   // unweighted radiance (valid once secondaries terminate)
-    float4 *lam;     // wavelengths
-    float4 *lpdf;    // wavelength pdfs
-    ulonglong2 *rng; // PCG32 state, increment
-    int4 *meta;      // pixel, depth, medium, flags (bit 0 specular, bits 8..23 interface crossings)
-    float4 *prevP;   // previous scattering vertex, w: filter weight of the camera sample
-    float4 *prevN;   // geometric normal there (0 in media), w: iteration guard (int bits)
-    float4 *hit;     // t, b1, b2, prim (int bits; -1 = miss)
-};
-
-struct Shadows {
-    float4 *o;   // origin, w: medium (int bits)
-    float4 *d;   // target - origin, w: path index (int bits)
-    float4 *c;   // contribution before transmittance
-    float *w;    // spectral MIS scale applied to L
-};
-
-// Device counters of one wavefront: queue lengths, the persistent kernels' work counters, status.
-enum {
-    kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
-    kCntSlots = 8
-};
-enum { kStatusStack = 1, kStatusGuard = 2 };
-// Device statistics (64-bit): closest-hit rays, shadow rays, non-empty bounces.
-enum { kStatClosest = 0, kStatShadow = 1, kStatBounces = 2, kStatSlots = 4 };
-
-constexpr float kShadowEps = 1e-4f;  // src/scene/interaction.h:21
-
-// Warp-aggregated append: one atomicAdd per warp; returns this thread's slot.
-__device__ __forceinline__ int warp_append(int *counter) {
-    unsigned mask = __activemask();
-    int lane = threadIdx.x & 31;
-    int leader = __ffs(mask) - 1;
-    int rank = __popc(mask & ((1u << lane) - 1u));
-    int base = 0;
-    if (lane == leader) base = atomicAdd(counter, __popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    return base + rank;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Pixel filter importance sampling (src/gpu/prender_gpu.cpp:1465-1494; the host builds the CDF
-// as src/integrators/gpu_path.cpp:431-456)
-
-__device__ float filter_eval_1d(const DevScene &s, float x) {
-    x = fabsf(x);
-    if (x > s.filterRadius) return 0.f;
-    switch (s.filterType) {
-    case prgpu::FilterGaussian: {
-        float is2 = 1.f / (2.f * s.filterSigma * s.filterSigma);
-        return fmaxf(0.f, expf(-x * x * is2) - expf(-s.filterRadius * s.filterRadius * is2));
-    }
-    case prgpu::FilterBlackmanHarris: {
-        float t = 0.5f + x / (2.f * s.filterRadius);
-        return 0.35875f - 0.48829f * cosf(2.f * kPi * t) + 0.14128f * cosf(4.f * kPi * t) -
-               0.01168f * cosf(6.f * kPi * t);
-    }
-    default: return 1.f;
-    }
-}
-
-__device__ float filter_sample_1d(const DevScene &s, float u, float *pdf) {
-    int lo = 0, hi = prgpu::kFilterBins;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(s.filterCdf + mid) <= u) lo = mid;
-        else hi = mid;
-    }
-    float c0 = __ldg(s.filterCdf + lo), c1 = __ldg(s.filterCdf + lo + 1);
-    float w = c1 - c0;
-    float t = w > 0.f ? (u - c0) / w : 0.5f;
-    float binW = 2.f * s.filterRadius / prgpu::kFilterBins;
-    *pdf = w / binW;
-    return -s.filterRadius + (float(lo) + t) * binW;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Surface interaction (src/geometry/shape.cpp:63-85, 224-264)
-
-struct Surf {
-    V3 p, n, ns, dpdu;
-    float u, v;
-};
-
-__device__ Surf shade_point(const DevScene &s, const prgpu::Primitive &pr, float t, float b1, float b2, V3 o, V3 d) {
-    Surf sf;
-    if (pr.type == prgpu::PrimSphere) {
-        V3 c = f3(pr.p0);
-        V3 rel = (o + d * t) - c;
-        float l = len(rel);
-        V3 n = l > 0.f ? rel * (1.f / l) : mk(0.f, 1.f, 0.f);
-        sf.p = c + n * pr.r;
-        sf.n = pr.flip ? -n : n;
-        sf.ns = sf.n;
-        float phi = atan2f(n.z, n.x);
-        if (phi < 0.f) phi += 2.f * kPi;
-        sf.u = phi * kInv2Pi;
-        sf.v = acosf(clampf(n.y, -1.f, 1.f)) * kInvPi;
-        sf.dpdu = mk(-rel.z, 0.f, rel.x);
-        if (len2(sf.dpdu) < 1e-12f) sf.dpdu = frame_from_z(n).x;
-        return sf;
-    }
-    V3 p0 = f3(pr.p0), p1 = f3(pr.p1), p2 = f3(pr.p2);
-    float b0 = 1.f - b1 - b2;
-    sf.p = p0 * b0 + p1 * b1 + p2 * b2;
-    V3 n = normalize(cross(p1 - p0, p2 - p0));
-    sf.u = pr.u0 * b0 + pr.u1 * b1 + pr.u2 * b2;
-    sf.v = pr.v0 * b0 + pr.v1 * b1 + pr.v2 * b2;
-    V3 ns = n;
-    V3 n0 = f3(pr.n0);
-    if (len2(n0) > 0.f) {
-        ns = n0 * b0 + f3(pr.n1) * b1 + f3(pr.n2) * b2;
-        float l = len(ns);
-        ns = l > 0.f ? ns * (1.f / l) : n;
-        n = face_forward(n, ns);
-    }
-    sf.n = n;
-    sf.ns = ns;
-    float du02 = pr.u0 - pr.u2, du12 = pr.u1 - pr.u2, dv02 = pr.v0 - pr.v2, dv12 = pr.v1 - pr.v2;
-    float det = du02 * dv12 - dv02 * du12;
-    if (fabsf(det) < 1e-9f) {
-        sf.dpdu = frame_from_z(n).x;
-    } else {
-        sf.dpdu = ((p0 - p2) * dv12 - (p1 - p2) * dv02) * (1.f / det);
-        if (!isfinite(sf.dpdu.x) || len2(cross(sf.dpdu, n)) == 0.f) sf.dpdu = frame_from_z(n).x;
-    }
-    return sf;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Materials (src/materials/material.cpp:73-117; src/gpu/prender_gpu.cpp:1136-1226)
-
-__device__ Ggx make_ggx(float ax, float ay) {
-    Ggx g{ax, ay};
-    if (!g.smooth()) {
-        g.ax = fmaxf(g.ax, 1e-4f);
-        g.ay = fmaxf(g.ay, 1e-4f);
-    }
-    return g;
-}
-
-__device__ SS diffuse_albedo(const DevScene &s, const prgpu::Material &m, float u, float v, const Lambda &lam) {
-    int id = m.albedo;
-    if (m.albedoB >= 0 && m.checkerScale > 0.f) {
-        int odd = (int(floorf(u * m.checkerScale)) + int(floorf(v * m.checkerScale))) & 1;
-        if (odd) id = m.albedoB;
-    }
-    SS R = tab4(s.spectra, id, lam);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) R.v[i] = clampf(R.v[i], 0.f, 1.f);
-    return R;
-}
-
-// Builds the lobe of material m at the hit; may terminate the secondary wavelengths.
-__device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam) {
-    Lobe l;
-    l.kind = kLobeNone;
-    l.etaD = 1.f;
-    l.mf = Ggx{0.f, 0.f};
-    switch (m.type) {
-    case prgpu::MatDiffuse:
-        l.kind = kLobeDiffuse;
-        l.R = diffuse_albedo(s, m, u, v, lam);
-        break;
-    case prgpu::MatConductor:
-        l.kind = kLobeConductor;
-        l.mf = make_ggx(m.alphaX, m.alphaY);
-        if (m.eta >= 0) {
-            l.eta = tab4(s.spectra, m.eta, lam);
-            l.k = tab4(s.spectra, m.k, lam);
-        } else {
-            // Artist reflectance r -> eta 1, k = 2 sqrt(r) / sqrt(1 - r) (exact r at normal incidence).
-            SS r = tab4(s.spectra, m.albedo, lam);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                float ri = clampf(r.v[i], 0.f, 0.9999f);
-                l.eta.v[i] = 1.f;
-                l.k.v[i] = 2.f * sqrtf(ri) / safe_sqrt(1.f - ri);
-            }
-        }
-        break;
-    case prgpu::MatDielectric:
-        l.kind = m.thin ? kLobeThin : kLobeDielectric;
-        l.etaD = tab(s.spectra, m.eta, lam.l[0]);
-        if (m.dispersive) lam.terminate_secondary();
-        if (l.etaD == 0.f) l.etaD = 1.f;
-        l.mf = make_ggx(m.alphaX, m.alphaY);
-        break;
-    default: break;
-    }
-    return l;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Lights
-
-__device__ SS emitted(const DevScene &s, const prgpu::Light &l, V3 n, V3 w, const Lambda &lam) {
-    float c = dot(n, w);
-    if (!l.twoSided && c <= 0.f) return splat(0.f);
-    float prof = l.cosPower > 0.f ? powf(fabsf(c), l.cosPower) : 1.f;
-    return tab4(s.spectra, l.spectrum, lam) * (l.scale * prof);
-}
-
-// Solid-angle density of sampling point p (normal n) on area light l from ref (uniform area).
-__device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
-    V3 d = p - ref;
-    float d2 = len2(d);
-    float c = fabsf(dot(n, d * rsqrtf(d2)));
-    if (c == 0.f) return 0.f;
-    return d2 / (c * l.area);
-}
-
-// Probability that NEE at (p, n) picks light li: the light-BVH pmf when the scene has one (the
-// exact leaf-to-root walk), the power pmf otherwise.
-__device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
-    if (s.lbvhCount == 0) return s.lights[li].pmf;
-    return lbvh_pmf(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, li, p, n);
-}
-
-struct LightSample {
-    V3 wi, target;
-    SS Le;
-    float pdf;   // selection pmf times the solid-angle density (1 for point lights)
-    bool delta;
-    bool ok;
-};
-
-// Chooses a light and a point on it as seen from p (normal n, zero in media).
-__device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
-    LightSample ls;
-    ls.ok = false;
-    ls.delta = false;
-    if (ul < s.envPmf && s.envSpectrum >= 0) {
-        float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
-        sincosf(2.f * kPi * u1, &sp, &cp);
-        ls.wi = mk(r * cp, r * sp, z);
-        ls.target = p + ls.wi * (2.f * s.worldRadius);
-        ls.Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
-        ls.pdf = s.envPmf * kInv4Pi;
-        ls.ok = true;
-        return ls;
-    }
-    int li = -1;
-    float pmf = 0.f;
-    if (s.lbvhCount > 0) {
-        float u = fminf((ul - s.envPmf) / s.lbvhProb, kOneMinusEps);
-        li = lbvh_sample(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, p, n, u, &pmf);
-    } else {
-        if (s.lightCount == 0) return ls;
-        float acc = s.envSpectrum >= 0 ? s.envPmf : 0.f;
-        li = s.lightCount - 1;
-        for (int i = 0; i < s.lightCount; ++i) {
-            acc += s.lights[i].pmf;
-            if (ul < acc) {
-                li = i;
-                break;
-            }
-        }
-        pmf = s.lights[li].pmf;
-    }
-    if (li < 0 || !(pmf > 0.f)) return ls;
-    const prgpu::Light &l = s.lights[li];
-    if (l.type == prgpu::LightPoint) {
-        ls.target = f3(l.position);
-        V3 dd = ls.target - p;
-        float d2 = len2(dd);
-        if (!(d2 > 0.f)) return ls;
-        ls.wi = dd * rsqrtf(d2);
-        ls.Le = tab4(s.spectra, l.spectrum, lam) * (l.scale / d2);
-        ls.pdf = pmf;
-        ls.delta = true;
-        ls.ok = true;
-        return ls;
-    }
-    const prgpu::Primitive &lp = s.prims[l.primitive];
-    V3 pl, nl;
-    if (lp.type == prgpu::PrimSphere) {
-        float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
-        sincosf(2.f * kPi * u1, &sp, &cp);
-        V3 nn = mk(r * cp, r * sp, z);
-        pl = f3(lp.p0) + nn * lp.r;
-        nl = lp.flip ? -nn : nn;
-    } else {
-        float b0, b1;
-        if (u0 < u1) {
-            b0 = u0 * 0.5f;
-            b1 = u1 - b0;
-        } else {
-            b1 = u1 * 0.5f;
-            b0 = u0 - b1;
-        }
-        float b2 = 1.f - b0 - b1;
-        V3 p0 = f3(lp.p0), p1 = f3(lp.p1), p2 = f3(lp.p2);
-        pl = p0 * b0 + p1 * b1 + p2 * b2;
-        nl = normalize(cross(p1 - p0, p2 - p0));
-        V3 n0 = f3(lp.n0);
-        if (len2(n0) > 0.f) nl = face_forward(nl, n0 * b0 + f3(lp.n1) * b1 + f3(lp.n2) * b2);
-    }
-    V3 dd = pl - p;
-    float d2 = len2(dd);
-    if (!(d2 > 0.f)) return ls;
-    ls.wi = dd * rsqrtf(d2);
-    ls.Le = emitted(s, l, nl, -ls.wi, lam);
-    ls.pdf = pmf * area_pdf(l, p, pl, nl);
-    if (!nonzero(ls.Le) || !(ls.pdf > 0.f) || !isfinite(ls.pdf)) return ls;
-    ls.target = pl + (dot(-dd, nl) < 0.f ? -nl : nl) * ray_eps(pl);
-    ls.ok = true;
-    return ls;
-}
-
-// Transmittance of the shadow segment o -> o + dd (length len(dd)) in the given medium.
-__device__ SS segment_tr(const DevScene &s, int medium, const Lambda &lam, V3 o, V3 dd, float frac) {
-    float l = len(dd);
-    float dist = frac * l;
-    if (!is_grid(s, medium)) return homogeneous_tr(s, medium, lam, dist);
-    Pcg rng = segment_stream(o, dd, uint32_t(medium));
-    return medium_transmittance(s, medium, lam, o, dd * (1.f / l), dist, rng);
-}
-
-// ---------------------------------------------------------------------------------------------
-// Kernels
-
-struct ChunkInfo {
-    int pixBegin;      // first pixel of the chunk (raster index)
-    int npix;          // pixels in the chunk
-    int samples;       // samples per pixel in the chunk
-    int firstSample;   // absolute sample index of the chunk's first sample
-    uint64_t seed;
-    int maxDepth;      // <= 0: unlimited
-};
-
-__device__ __forceinline__ Lambda load_lam(const Paths &P, int j) {
-    float4 a = P.lam[j], b = P.lpdf[j];
-    Lambda w;
-    w.l[0] = a.x; w.l[1] = a.y; w.l[2] = a.z; w.l[3] = a.w;
-    w.pdf[0] = b.x; w.pdf[1] = b.y; w.pdf[2] = b.z; w.pdf[3] = b.w;
-    return w;
-}
-
-__global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo ci, int *counters, int *queue) {
-    int total = ci.npix * ci.samples;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
-        int sIdx = j / ci.npix, pl = j - sIdx * ci.npix;
-        int pix = ci.pixBegin + pl;
-        int px = pix % s.cam.width, py = pix / s.cam.width;
-        Pcg rng = pixel_sample_stream(uint32_t(pix), uint64_t(ci.firstSample) + uint64_t(sIdx), ci.seed);
-        Lambda lam = sample_visible(rng.uniform());
-        float pdfX, pdfY;
-        float dx = filter_sample_1d(s, rng.uniform(), &pdfX), dy = filter_sample_1d(s, rng.uniform(), &pdfY);
-        float fw = filter_eval_1d(s, dx) * filter_eval_1d(s, dy) * s.filterNorm / (pdfX * pdfY);
-        float l0 = rng.uniform(), l1 = rng.uniform();
-        const prgpu::Camera &c = s.cam;
-        float fx = float(px) + 0.5f + dx, fy = float(py) + 0.5f + dy;
-        V3 dir = normalize(mk((2.f * fx / c.width - 1.f) * c.tanHalfFov * c.aspect, (1.f - 2.f * fy / c.height) * c.tanHalfFov, 1.f));
-        V3 org = mk(0.f, 0.f, 0.f);
-        if (c.lensRadius > 0.f) {
-            float lx, ly;
-            concentric_disk(l0, l1, &lx, &ly);
-            V3 pf = dir * (c.focalDistance / dir.z);
-            org = mk(lx * c.lensRadius, ly * c.lensRadius, 0.f);
-            dir = normalize(pf - org);
-        }
-        const float *M = c.cameraToWorld;
-        V3 o = mk(M[0] * org.x + M[1] * org.y + M[2] * org.z + M[3], M[4] * org.x + M[5] * org.y + M[6] * org.z + M[7],
-                  M[8] * org.x + M[9] * org.y + M[10] * org.z + M[11]);
-        V3 dw = normalize(mk(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
-                             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z));
-        bool valid = fw != 0.f && isfinite(fw);
-        P.o[j] = make_float4(o.x, o.y, o.z, 1.f);
-        P.d[j] = make_float4(dw.x, dw.y, dw.z, 1.f);
-        P.beta[j] = make_float4(1.f, 1.f, 1.f, 1.f);
-        P.rpath[j] = make_float4(1.f, 1.f, 1.f, 1.f);
-        P.L[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        P.Lhero[j] = make_float4(0.f, 0.f, 0.f, 0.f);
-        P.lam[j] = make_float4(lam.l[0], lam.l[1], lam.l[2], lam.l[3]);
-        P.lpdf[j] = make_float4(lam.pdf[0], lam.pdf[1], lam.pdf[2], lam.pdf[3]);
-        P.rng[j] = make_ulonglong2(rng.state, rng.inc);
-        P.meta[j] = make_int4(pix, 0, s.cameraMedium, 0);
-        P.prevP[j] = make_float4(o.x, o.y, o.z, valid ? fw : 0.f);
-        P.prevN[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
-        if (valid) queue[warp_append(counters + kCntActive)] = j;
-    }
-}
-
-// Closest hit for every queued path, by persistent warps whose finished lanes take the next
-// queue entry at once (see k_trace_persist in accel.cu): bounce rays are incoherent and end
-// after very different numbers of steps.
-template <bool kSpheres>
-__global__ void __launch_bounds__(256) k_extend(DevScene s, Paths P, int *counters, const int *queue) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int n = counters[kCntActive];
-    int stackRef[kStackSize];
-    float stackT[kStackSize];
-    TraceRay r;
-    TravState st;
-    st.ref = 0;
-    st.sp = 0;
-    st.tMax = kInf;
-    st.found = false;
-    int j = 0;
-    bool active = false, exhausted = n == 0, overflow = false;
-    while (!__all_sync(full, exhausted)) {
-        unsigned need = __ballot_sync(full, !active && !exhausted);
-        if (need) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(counters + kCntExtendWork, __popc(need));
-            base = __shfl_sync(full, base, 0);
-            if (!active && !exhausted) {
-                int q = base + __popc(need & ((1u << lane) - 1u));
-                if (q >= n) {
-                    exhausted = true;
-                } else {
-                    j = queue[q];
-                    float4 o = P.o[j], d = P.d[j];
-                    r = make_trace_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
-                    st.tMax = kInf;
-                    st.sp = 0;
-                    st.found = false;
-                    st.hit.prim = -1;
-                    float te;
-                    active = !s.root.empty &&
-                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
-                                       s.root.box[5], &te) &&
-                             te < kInf;
-                    st.ref = s.root.ref;
-                    if (!active) P.hit[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-                }
-            }
-        }
-        if (active && traverse_step<false, kSpheres>(s.nodes, s.leaves, r, st, stackRef, stackT, &overflow)) {
-            active = false;
-            P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
-        }
-    }
-    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
-}
-
-struct ShadeArgs {
-    DevScene s;
-    Paths P;
-    Shadows S;
-    const int *queueIn;
-    int *queueOut;
-    int *counters;
-    int maxDepth;
-};
-
-// One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
-__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
-    const DevScene &s = a.s;
-    const Paths &P = a.P;
-    int n = a.counters[kCntActive];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int j = a.queueIn[q];
-        float4 o4 = P.o[j], d4 = P.d[j], hit = P.hit[j];
-        V3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
-        float prevPdf = o4.w, etaScale = d4.w;
-        SS beta = from_f4(P.beta[j]), rpath = from_f4(P.rpath[j]);
-        SS L = from_f4(P.L[j]), Lhero = from_f4(P.Lhero[j]);
-        Lambda lam = load_lam(P, j);
-        ulonglong2 rs = P.rng[j];
-        Pcg rng{rs.x, rs.y};
-        int4 meta = P.meta[j];
-        int depth = meta.y, medium = meta.z, flags = meta.w;
-        bool specular = flags & 1;
-        int crossings = (flags >> 8) & 0xffff;
-        float4 pp4 = P.prevP[j], pn4 = P.prevN[j];
-        V3 prevP = mk(pp4.x, pp4.y, pp4.z), prevN = mk(pn4.x, pn4.y, pn4.z);
-        int iters = __float_as_int(pn4.w) + 1;
-        int prim = __float_as_int(hit.w);
-        bool alive = true;
-
-        auto misScale = [&]() {
-            float av = 0.25f * (rpath.v[0] + rpath.v[1] + rpath.v[2] + rpath.v[3]);
-            return av > 0.f && isfinite(av) ? 1.f / av : 0.f;
-        };
-        auto add = [&](SS c) {
-            Lhero = Lhero + c;
-            L = L + c * misScale();
-        };
-        // NEE: queue a shadow ray carrying f * Le * w / pdf; the visibility test adds it later.
-        // The shadow ray starts in the medium on the light's side of the vertex (medIn / medOut
-        // for surfaces, the current medium for medium vertices where ng = 0).
-        auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut) {
-            float ul = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-            LightSample ls = sample_light(s, p, ng, lam, ul, u0, u1);
-            if (!ls.ok) return;
-            int med = dot(ls.wi, ng) > 0.f ? medOut : medIn;
-            SS f;
-            float spdf;
-            if (lobe) {
-                V3 wol = fr->to_local(wo), wil = fr->to_local(ls.wi);
-                if (wol.z == 0.f) return;
-                f = lobe_f(*lobe, wol, wil) * fabsf(dot(ls.wi, ns));
-                spdf = lobe_pdf(*lobe, wol, wil);
-            } else {
-                float ph = hg_phase(dot(wo, ls.wi), g);
-                f = splat(ph);
-                spdf = ph;
-            }
-            if (!nonzero(f)) return;
-            float w = ls.delta ? 1.f : power_heuristic(ls.pdf, spdf);
-            SS c = beta * f * ls.Le * (w / ls.pdf);
-            if (!nonzero(c)) return;
-            V3 so = p + (dot(ls.target - p, ng) < 0.f ? -ng : ng) * ray_eps(p);
-            int k = warp_append(a.counters + kCntShadow);
-            a.S.o[k] = make_float4(so.x, so.y, so.z, __int_as_float(med));
-            V3 sd = ls.target - so;
-            a.S.d[k] = make_float4(sd.x, sd.y, sd.z, __int_as_float(j));
-            a.S.c[k] = to_f4(c);
-            a.S.w[k] = misScale();
-        };
-        auto roulette = [&]() {
-            if (depth <= 1) return true;
-            float ms = lam.terminated() ? 1.f : misScale();
-            float mx = max_c(beta) * etaScale * ms;
-            if (mx >= 1.f) return true;
-            float qq = fmaxf(0.f, 1.f - mx);
-            if (rng.uniform() < qq) return false;
-            beta = beta * (1.f / (1.f - qq));
-            return true;
-        };
-
-        if (iters > 8192) {
-            alive = false;
-            atomicOr(a.counters + kCntStatus, kStatusGuard);
-        }
-        bool handled = !alive;
-        bool found = prim >= 0;
-        // Participating medium along the segment: hero-driven free flight in homogeneous media
-        // (medium.cpp:71-103, with the rPath pdf ratios of path-level spectral MIS), spectral
-        // tracking in grid media (medium.cpp:232-285, wavelength-neutral: rPath unchanged).
-        if (!handled && medium >= 0) {
-            float tMax = found ? hit.x : kInf;
-            int event = 0;  // 0: the segment is crossed, 1: real scattering at t, 2: the path ends
-            float t = tMax, g = 0.f;
-            if (!is_grid(s, medium)) {
-                const prgpu::Medium &md = s.media[medium];
-                g = md.g;
-                SS ss = tab4(s.spectra, md.sigmaS, lam) * md.scale;
-                SS st = tab4(s.spectra, md.sigmaA, lam) * md.scale + ss;
-                float u = fminf(rng.uniform(), kOneMinusEps);
-                t = st.v[0] > 0.f ? -logf(1.f - u) / st.v[0] : kInf;
-                if (t < tMax) {
-                    SS T;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) T.v[i] = expf(-st.v[i] * t);
-                    float pdf0 = st.v[0] * T.v[0];
-                    if (!(pdf0 > 0.f)) {
-                        event = 2;
-                    } else {
-                        beta = beta * T * ss * (1.f / pdf0);
-                        rpath = rpath * st * T * (1.f / pdf0);
-                        event = 1;
-                    }
-                } else {
-                    SS T;
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        T.v[i] = isinf(tMax) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * tMax);
-                    if (!(T.v[0] > 0.f)) {
-                        event = 2;
-                    } else {
-                        beta = beta * T * (1.f / T.v[0]);
-                        rpath = rpath * T * (1.f / T.v[0]);
-                        if (!nonzero(beta)) event = 2;
-                    }
-                }
-            } else {
-                const DevGrid &gr = s.grids[medium - s.mediumCount];
-                g = gr.g;
-                SS wgt;
-                event = grid_sample(s, gr, lam, o, d, tMax, rng, &t, &wgt);
-                beta = beta * wgt;
-                if (event == 0 && !nonzero(beta)) event = 2;
-            }
-            if (event == 2) {
-                alive = false;
-                handled = true;
-            } else if (event == 1) {
-                handled = true;
-                if (!nonzero(beta) || (a.maxDepth > 0 && depth >= a.maxDepth)) {
-                    alive = false;
-                } else {
-                    ++depth;
-                    V3 p = o + d * t, wo = -d;
-                    nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, g, medium, medium);
-                    float u0 = rng.uniform(), u1 = rng.uniform(), phasePdf;
-                    V3 wi = hg_sample(wo, g, u0, u1, &phasePdf);
-                    if (!(phasePdf > 0.f)) {
-                        alive = false;
-                    } else {
-                        prevPdf = phasePdf;
-                        prevP = p;
-                        prevN = mk(0.f, 0.f, 0.f);
-                        specular = false;
-                        o = p;
-                        d = wi;
-                        alive = roulette();
-                    }
-                }
-            }
-        }
-        if (!handled && !found) {
-            // Escaped: environment emission with MIS against the previous BSDF / phase sample.
-            if (s.envSpectrum >= 0) {
-                SS Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
-                float w = 1.f;
-                if (depth > 0 && !specular) w = power_heuristic(prevPdf, s.envPmf * kInv4Pi);
-                add(beta * Le * w);
-            }
-            alive = false;
-            handled = true;
-        }
-        if (!handled) {
-            const prgpu::Primitive &pr = s.prims[prim];
-            Surf sf = shade_point(s, pr, hit.x, hit.y, hit.z, o, d);
-            if (pr.light >= 0) {
-                const prgpu::Light &l = s.lights[pr.light];
-                SS Le = emitted(s, l, sf.n, -d, lam);
-                if (nonzero(Le)) {
-                    float w = 1.f;
-                    if (depth > 0 && !specular)
-                        w = power_heuristic(prevPdf, light_pmf(s, pr.light, prevP, prevN) * area_pdf(l, prevP, sf.p, sf.n));
-                    add(beta * Le * w);
-                }
-            }
-            const prgpu::Material &m = s.mats[pr.material];
-            if (m.type == prgpu::MatInterface) {
-                // Invisible medium boundary: switch media and continue straight on.
-                if (++crossings > 1000) {
-                    alive = false;
-                } else {
-                    medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
-                    o = offset_origin(sf.p, sf.n, d);
-                }
-            } else if (m.type == prgpu::MatBlack || (a.maxDepth > 0 && depth >= a.maxDepth)) {
-                alive = false;
-            } else {
-                ++depth;
-                Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
-                Frame fr = frame_from_xz(sf.dpdu, sf.ns);
-                V3 wo = -d;
-                if (lobe.non_specular())
-                    nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside);
-                float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                V3 wol = fr.to_local(wo);
-                BSample bs;
-                bool ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
-                ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
-                     isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
-                if (!ok) {
-                    alive = false;
-                } else {
-                    V3 wi = fr.from_local(bs.wi);
-                    beta = beta * bs.f * (fabsf(dot(wi, sf.ns)) / bs.pdf);
-                    prevPdf = bs.pdf;
-                    specular = (bs.flags & kFlagSpecular) != 0u;
-                    if (bs.flags & kFlagTransmission) etaScale *= sqr(bs.eta);
-                    prevP = sf.p;
-                    prevN = sf.n;
-                    o = offset_origin(sf.p, sf.n, wi);
-                    d = wi;
-                    // Medium on the side the new direction enters.
-                    medium = dot(wi, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
-                    if (!nonzero(beta) || !isfinite(max_c(beta))) alive = false;
-                    else alive = roulette();
-                }
-            }
-        }
-        // Write back (the radiance sums always; the ray state only for survivors).
-        P.L[j] = to_f4(L);
-        P.Lhero[j] = to_f4(Lhero);
-        P.lpdf[j] = make_float4(lam.pdf[0], lam.pdf[1], lam.pdf[2], lam.pdf[3]);
-        if (alive) {
-            P.o[j] = make_float4(o.x, o.y, o.z, prevPdf);
-            P.d[j] = make_float4(d.x, d.y, d.z, etaScale);
-            P.beta[j] = to_f4(beta);
-            P.rpath[j] = to_f4(rpath);
-            P.rng[j] = make_ulonglong2(rng.state, rng.inc);
-            P.meta[j] = make_int4(meta.x, depth, medium, (specular ? 1 : 0) | (min(crossings, 0xffff) << 8));
-            P.prevP[j] = make_float4(prevP.x, prevP.y, prevP.z, pp4.w);
-            P.prevN[j] = make_float4(prevN.x, prevN.y, prevN.z, __int_as_float(iters));
-            a.queueOut[warp_append(a.counters + kCntNext)] = j;
-        }
-    }
-}
-
-// An unoccluded NEE sample: its contribution times the transmittance of the medium it crossed
-// goes to the path's radiance sums (one shadow entry per path and bounce, so no atomics).
-template <bool kMedia>
-__device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P, const Shadows &S, int q) {
-    float4 o4 = S.o[q], d4 = S.d[q];
-    int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
-    SS c = from_f4(S.c[q]);
-    if (kMedia && medium >= 0) c = c * segment_tr(s, medium, load_lam(P, j), mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), 1.f);
-    float w = S.w[q];
-    float4 L = P.L[j], Lh = P.Lhero[j];
-    P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
-    P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
-}
-
-// Visibility of queued NEE samples in scenes without medium interfaces: any-hit queries up to
-// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill. kMedia: the scene has
-// media, so accepted segments carry a transmittance (kept out of the medium-free variant, whose
-// traversal loop would otherwise pay registers for the ratio-tracking code).
-template <bool kSpheres, bool kMedia>
-__global__ void __launch_bounds__(256) k_shadow_any(DevScene s, Paths P, Shadows S, int *counters) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int n = counters[kCntShadow];
-    int stackRef[kStackSize];
-    float stackT[kStackSize];
-    TraceRay r;
-    TravState st;
-    st.ref = 0;
-    st.sp = 0;
-    st.tMax = 1.f - kShadowEps;
-    st.found = false;
-    int q = 0;
-    bool active = false, exhausted = n == 0, overflow = false;
-    while (!__all_sync(full, exhausted)) {
-        unsigned need = __ballot_sync(full, !active && !exhausted);
-        if (need) {
-            int base = 0;
-            if (lane == 0) base = atomicAdd(counters + kCntShadowWork, __popc(need));
-            base = __shfl_sync(full, base, 0);
-            if (!active && !exhausted) {
-                q = base + __popc(need & ((1u << lane) - 1u));
-                if (q >= n) {
-                    exhausted = true;
-                } else {
-                    float4 o4 = S.o[q], d4 = S.d[q];
-                    r = make_trace_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
-                    st.tMax = 1.f - kShadowEps;
-                    st.sp = 0;
-                    st.found = false;
-                    float te;
-                    active = !s.root.empty &&
-                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
-                                       s.root.box[5], &te) &&
-                             te < st.tMax;
-                    st.ref = s.root.ref;
-                    if (!active) shadow_accept<kMedia>(s, P, S, q);
-                }
-            }
-        }
-        if (active && traverse_step<true, kSpheres>(s.nodes, s.leaves, r, st, stackRef, stackT, &overflow)) {
-            active = false;
-            if (!st.found) shadow_accept<kMedia>(s, P, S, q);
-        }
-    }
-    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
-}
-
-// Moves the survivors' queue into place for the next bounce and accumulates statistics (one
-// thread; keeps the bounce loop free of host round trips).
-__global__ void k_advance(int *counters, unsigned long long *stats) {
-    stats[kStatClosest] += (unsigned long long)counters[kCntActive];
-    stats[kStatShadow] += (unsigned long long)counters[kCntShadow];
-    stats[kStatBounces] += counters[kCntActive] > 0 ? 1ull : 0ull;
-    counters[kCntActive] = counters[kCntNext];
-    counters[kCntNext] = 0;
-    counters[kCntShadow] = 0;
-    counters[kCntExtendWork] = 0;
-    counters[kCntShadowWork] = 0;
-}
-
-// Visibility of queued NEE samples in scenes with medium interfaces: a walk through the boundary
-// surfaces with homogeneous transmittance (src/scene/scene.cpp:41-59).
-template <bool kSpheres>
-__global__ void __launch_bounds__(256) k_shadow_walk(DevScene s, Paths P, Shadows S, const int *counters) {
-    int n = counters[kCntShadow];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        float4 o4 = S.o[q], d4 = S.d[q];
-        int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
-        V3 o = mk(o4.x, o4.y, o4.z), dd = mk(d4.x, d4.y, d4.z);
-        V3 target = o + dd;
-        SS T = splat(1.f);
-        bool overflow = false;
-        Lambda lam;
-        bool needLam = medium >= 0 || s.hasInterfaces;
-        if (needLam) lam = load_lam(P, j);
-        if (!s.hasInterfaces) {
-            TraceRay r = make_trace_ray(o, dd);
-            Hit h;
-            bool occ = !s.root.empty &&
-                       traverse<true, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
-            if (occ) continue;
-            if (medium >= 0) T = segment_tr(s, medium, lam, o, dd, 1.f);
-        } else {
-            bool blocked = true;
-            for (int it = 0; it < 256; ++it) {
-                V3 d = target - o;
-                TraceRay r = make_trace_ray(o, d);
-                Hit h;
-                h.prim = -1;
-                bool hit = !s.root.empty &&
-                           traverse<false, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
-                if (hit && s.mats[s.prims[h.prim].material].type != prgpu::MatInterface) break;
-                if (medium >= 0) T = T * segment_tr(s, medium, lam, o, d, hit ? h.t : 1.f);
-                if (!hit || !nonzero(T)) {
-                    blocked = false;
-                    break;
-                }
-                const prgpu::Primitive &pr = s.prims[h.prim];
-                Surf sf = shade_point(s, pr, h.t, h.u, h.v, o, d);
-                medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
-                o = offset_origin(sf.p, sf.n, d);
-            }
-            if (blocked) continue;
-        }
-        SS c = from_f4(S.c[q]) * T;
-        float w = S.w[q];
-        float4 L = P.L[j], Lh = P.Lhero[j];
-        P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
-        P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
-    }
-}
-
-// Adds each sample's XYZ to the FP64 film, one sample at a time in sample-index order
-// (src/gpu/prender_gpu.cpp:1541-1559 for the per-sample conversion and clamp).
-__global__ void __launch_bounds__(256) k_film(DevScene s, Paths P, ChunkInfo ci, float clampY, double *film) {
-    for (int pl = blockIdx.x * blockDim.x + threadIdx.x; pl < ci.npix; pl += gridDim.x * blockDim.x) {
-        int pix = ci.pixBegin + pl;
-        double X = film[3 * size_t(pix)], Y = film[3 * size_t(pix) + 1], Z = film[3 * size_t(pix) + 2];
-        for (int sIdx = 0; sIdx < ci.samples; ++sIdx) {
-            int j = sIdx * ci.npix + pl;
-            float fw = P.prevP[j].w;
-            if (fw == 0.f) continue;
-            Lambda lam = load_lam(P, j);
-            SS L = from_f4(lam.terminated() ? P.Lhero[j] : P.L[j]);
-            if (!isfinite(L.v[0] + L.v[1] + L.v[2] + L.v[3])) continue;
-            float sx = 0.f, sy = 0.f, sz = 0.f;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                if (lam.pdf[i] == 0.f) continue;
-                float v = L.v[i] / lam.pdf[i];
-                sx += cie_x(lam.l[i]) * v;
-                sy += cie_y(lam.l[i]) * v;
-                sz += cie_z(lam.l[i]) * v;
-            }
-            float k = fw;
-            if (clampY > 0.f && sy * s.norm > clampY) k *= clampY / (sy * s.norm);
-            k *= s.norm;
-            X += double(sx * k);
-            Y += double(sy * k);
-            Z += double(sz * k);
-        }
-        film[3 * size_t(pix)] = X;
-        film[3 * size_t(pix) + 1] = Y;
-        film[3 * size_t(pix) + 2] = Z;
-    }
-}
-
 // ---------------------------------------------------------------------------------------------
 // Driver
 
@@ -957,7 +78,7 @@ int grid_for(const DeviceState &ds, int64_t work, int perSm = 8) {
     return int(std::max<int64_t>(1, std::min<int64_t>(blocks, int64_t(ds.prop.multiProcessorCount) * perSm)));
 }
 
-using ShadowAnyFn = void (*)(DevScene, Paths, Shadows, int *);
+using ShadowAnyFn = void (*)(DevScene, const DevScene *, Paths, Shadows, int *);
 
 // variant bit 0: spheres present, bit 1: media present.
 ShadowAnyFn shadow_any_kernel(int variant) {
@@ -1031,17 +152,17 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
             for (;;) {
                 for (int b = 0; b < kBouncesPerPoll; ++b) {
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b], st));
-                    if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, rs.P, cnt, qin);
-                    else k_extend<false><<<gExtend, 256, 0, st>>>(scene, rs.P, cnt, qin);
+                    if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
+                    else k_extend<false><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
-                    ShadeArgs sa{scene, rs.P, rs.S, qin, qout, cnt, rp.maxDepth};
-                    k_shade<<<gShade, 256, 0, st>>>(sa);
+                    ShadeArgs sa{scene, nullptr, rs.P, rs.S, qin, qout, cnt, rp.maxDepth};
+                    k_shade<false><<<gShade, 256, 0, st>>>(sa);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
                     if (scene.hasInterfaces) {
-                        if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
-                        else k_shadow_walk<false><<<gShade, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                        if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
+                        else k_shadow_walk<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                     } else {
-                        shadowAny<<<gShadow, 256, 0, st>>>(scene, rs.P, rs.S, cnt);
+                        shadowAny<<<gShadow, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 3], st));
                     k_advance<<<1, 1, 0, st>>>(cnt, dstats);
@@ -1178,6 +299,542 @@ int render_common(int deviceIndex, const prgpu::SceneDesc *sd, const prgpu::Scen
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Batched renders (prgpu_render_batch): many scenes in one wavefront, one graph launch
+//
+// The host cuts every render into chunks (a pixel range x a sample range) and packs them into
+// waves of at most `wavefrontPaths` paths, at most one chunk per render per wave, so that one film
+// kernel per wave can add each chunk's samples in sample order with no two chunks touching the same
+// pixel. The device runs the waves from a conditional while node: each iteration raygens the next
+// wave if the previous one is done, advances every live path two bounces, films a wave whose queue
+// ran empty and sets the loop condition.
+
+struct BatchChunk {
+    int render, pixBegin, npix, samples;
+    int firstSample, pathBase, pixBase, pad;
+    uint64_t seed;
+};
+struct BatchWave {
+    int firstChunk, nChunks, totalPaths, totalPix;
+};
+struct BatchCtl {
+    int wave, nWaves, phase, iter, maxIter, status;  // phase 1: the next iteration raygens a wave
+};
+
+constexpr int kMaxBatch = 256;  // render index in 8 bits of meta.w
+
+// Largest chunk index i in [lo, lo + n) whose base (path or pixel prefix) is <= key.
+__device__ __forceinline__ int find_chunk(const BatchChunk *c, int lo, int n, int key, bool byPixel) {
+    int a = lo, b = lo + n - 1;
+    while (a < b) {
+        int m = (a + b + 1) >> 1;
+        int v = byPixel ? c[m].pixBase : c[m].pathBase;
+        if (v <= key) a = m;
+        else b = m - 1;
+    }
+    return a;
+}
+
+__global__ void __launch_bounds__(256) k_batch_raygen(const DevScene *scenes, Paths P, const BatchCtl *ctl,
+                                                      const BatchWave *waves, const BatchChunk *chunks, int *counters,
+                                                      int *queue) {
+    if (ctl->phase != 1 || ctl->wave >= ctl->nWaves) return;
+    const BatchWave w = waves[ctl->wave];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < w.totalPaths; j += gridDim.x * blockDim.x) {
+        const BatchChunk &c = chunks[find_chunk(chunks, w.firstChunk, w.nChunks, j, false)];
+        int local = j - c.pathBase, sIdx = local / c.npix, pl = local - sIdx * c.npix;
+        raygen_path(scenes[c.render], P, j, c.pixBegin + pl, uint64_t(c.firstSample) + uint64_t(sIdx), c.seed,
+                    c.render, counters, queue);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_batch_film(const DevScene *scenes, Paths P, const BatchCtl *ctl,
+                                                    const BatchWave *waves, const BatchChunk *chunks,
+                                                    const int *counters) {
+    if (counters[kCntActive] != 0 || ctl->wave >= ctl->nWaves) return;
+    const BatchWave w = waves[ctl->wave];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < w.totalPix; t += gridDim.x * blockDim.x) {
+        const BatchChunk &c = chunks[find_chunk(chunks, w.firstChunk, w.nChunks, t, true)];
+        const DevScene &s = scenes[c.render];
+        int pl = t - c.pixBase;
+        film_pixel(s, P, c.pathBase, c.npix, pl, c.samples, s.clampY, s.film + 3 * size_t(c.pixBegin + pl));
+    }
+}
+
+// Loop control (one thread): next wave once the queue is empty; stop after the last wave, or at
+// the iteration bound (every path ends within 8,192 iterations of the shading guard, so the bound
+// is only reached by a fault in this bookkeeping, reported as status bit 0).
+__global__ void k_batch_ctl(BatchCtl *ctl, const int *counters, cudaGraphConditionalHandle loop) {
+    BatchCtl c = *ctl;
+    ++c.iter;
+    c.phase = 0;
+    if (counters[kCntActive] == 0) {
+        ++c.wave;
+        c.phase = 1;
+    }
+    unsigned more = c.wave < c.nWaves ? 1u : 0u;
+    if (more && c.iter >= c.maxIter) {
+        c.status |= 1;
+        more = 0u;
+    }
+    *ctl = c;
+    cudaGraphSetConditional(loop, more);
+}
+
+__global__ void k_batch_init(BatchCtl *ctl, int nWaves, int maxIter, int *counters, unsigned long long *stats) {
+    int i = threadIdx.x;
+    if (i == 0) *ctl = BatchCtl{0, nWaves, 1, 0, maxIter, 0};
+    if (i < kCntSlots) counters[i] = 0;
+    if (i < kStatSlots) stats[i] = 0ull;
+}
+
+struct BatchGraphKey {
+    int capacity = 0, shadeBlock = 0, variant = -1;
+    const void *ptrs[6] = {};
+    bool operator==(const BatchGraphKey &o) const {
+        if (capacity != o.capacity || shadeBlock != o.shadeBlock || variant != o.variant) return false;
+        for (int i = 0; i < 6; ++i)
+            if (ptrs[i] != o.ptrs[i]) return false;
+        return true;
+    }
+};
+
+struct BatchState {
+    std::vector<std::unique_ptr<SceneCache>> caches;
+    RenderState paths;                  // path / shadow state, queues and counters (its scene unused)
+    DevBuf scenes, chunks, waves, ctl, films;
+    cudaGraphExec_t exec = nullptr;
+    BatchGraphKey key;
+    int64_t launchesPerIteration = 0;
+    std::map<uint64_t, std::pair<int, int>> tuned;  // batch shape -> (wavefrontPaths, shadeBlock)
+    cudaEvent_t ev[2] = {};
+};
+
+std::unique_ptr<BatchState> gBatch[64];
+
+BatchState &batch_state(int device) {
+    auto &p = gBatch[device];
+    if (!p) {
+        p = std::make_unique<BatchState>();
+        PRB_CUDA(cudaEventCreate(&p->ev[0]));
+        PRB_CUDA(cudaEventCreate(&p->ev[1]));
+    }
+    return *p;
+}
+
+// Packs the renders into waves (see the section comment). Chunks of one render follow its sample
+// order: whole frames of S samples while a frame fits the share, else pixel ranges of one sample.
+void schedule_waves(const std::vector<int64_t> &npix, const std::vector<int> &spp, int capacity,
+                    const std::vector<prgpu::RenderParams> &rp, std::vector<BatchChunk> *chunks,
+                    std::vector<BatchWave> *waves) {
+    const int n = int(npix.size());
+    std::vector<int64_t> nextPix(static_cast<size_t>(n), 0);
+    std::vector<int> nextSample(static_cast<size_t>(n), 0);
+    auto remaining = [&](int r) {
+        return (int64_t(spp[size_t(r)]) - nextSample[size_t(r)]) * npix[size_t(r)] - nextPix[size_t(r)];
+    };
+    std::vector<int> order;
+    for (;;) {
+        order.clear();
+        for (int r = 0; r < n; ++r)
+            if (npix[size_t(r)] > 0 && remaining(r) > 0) order.push_back(r);
+        if (order.empty()) break;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return remaining(a) < remaining(b); });
+        BatchWave w{int(chunks->size()), 0, 0, 0};
+        int64_t budget = capacity;
+        for (size_t k = 0; k < order.size() && budget > 0; ++k) {
+            int r = order[k];
+            int64_t share = budget / int64_t(order.size() - k);
+            if (share < 1) continue;
+            BatchChunk c{};
+            c.render = r;
+            c.seed = rp[size_t(r)].seed;
+            const int64_t np = npix[size_t(r)];
+            int64_t &pix = nextPix[size_t(r)];
+            int &smp = nextSample[size_t(r)];
+            if (pix == 0 && np <= share) {
+                int64_t S = std::min<int64_t>(spp[size_t(r)] - smp, share / np);
+                c.pixBegin = 0;
+                c.npix = int(np);
+                c.samples = int(S);
+                c.firstSample = rp[size_t(r)].firstSample + smp;
+                smp += int(S);
+            } else {
+                int64_t take = std::min<int64_t>(share, np - pix);
+                c.pixBegin = int(pix);
+                c.npix = int(take);
+                c.samples = 1;
+                c.firstSample = rp[size_t(r)].firstSample + smp;
+                pix += take;
+                if (pix == np) {
+                    pix = 0;
+                    ++smp;
+                }
+            }
+            c.pathBase = w.totalPaths;
+            c.pixBase = w.totalPix;
+            w.totalPaths += c.npix * c.samples;
+            w.totalPix += c.npix;
+            budget -= int64_t(c.npix) * c.samples;
+            chunks->push_back(c);
+            ++w.nChunks;
+        }
+        waves->push_back(w);
+    }
+}
+
+uint64_t batch_shape_key(int device, int count, const prgpu::BatchItem *items) {
+    uint64_t h = 1469598103934665603ull ^ uint64_t(device);
+    auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+    mix(uint64_t(count));
+    for (int i = 0; i < count; ++i) {
+        const prgpu::SceneDesc *sd = items[i].scene;
+        mix(uint64_t(sd->camera.width) << 32 | uint32_t(sd->camera.height));
+        mix(uint64_t(items[i].params.spp) << 32 | uint32_t(items[i].params.maxDepth));
+        mix(uint64_t(sd->primCount) << 32 | uint32_t(sd->mediumCount + (items[i].ext ? items[i].ext->gridMediumCount : 0)));
+    }
+    return h;
+}
+
+// Captures the loop body into the while node's body graph and instantiates the graph.
+void build_batch_graph(DeviceState &ds, BatchState &bs, const BatchGraphKey &key, int sph, bool media, bool walls) {
+    if (bs.exec) {
+        cudaGraphExecDestroy(bs.exec);
+        bs.exec = nullptr;
+    }
+    RenderState &rs = bs.paths;
+    cudaStream_t st = ds.stream;
+    const int sms = ds.prop.multiProcessorCount;
+    const int cap = key.capacity, sb = key.shadeBlock;
+    const DevScene *scenes = bs.scenes.as<DevScene>();
+    auto *ctl = bs.ctl.as<BatchCtl>();
+    const auto *waves = bs.waves.as<BatchWave>();
+    const auto *chunks = bs.chunks.as<BatchChunk>();
+    int *cnt = rs.counters.as<int>();
+    auto *dstats = rs.stats.as<unsigned long long>();
+    int *qa = rs.queues.as<int>(), *qb = qa + cap;
+    DevScene none{};
+
+    auto extendFn = sph ? k_extend<true, true> : k_extend<false, true>;
+    using ShadowFn = void (*)(DevScene, const DevScene *, Paths, Shadows, int *);
+    ShadowFn anyFn = sph ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
+                         : (media ? k_shadow_any<false, true, true> : k_shadow_any<false, false, true>);
+    auto walkFn = sph ? k_shadow_walk<true, true> : k_shadow_walk<false, true>;
+    const int gExtend = sms * resident_blocks_of(extendFn);
+    const int gShadow = walls ? sms * 8 : sms * resident_blocks_of(anyFn);
+    int perSm = 0;
+    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade<true>, sb, 0));
+    const int gShade = sms * std::max(1, perSm);
+    const int gWide = sms * 8;
+
+    cudaGraph_t g = nullptr;
+    PRB_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle loop;
+    PRB_CUDA(cudaGraphConditionalHandleCreate(&loop, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = loop;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    PRB_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    PRB_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int64_t launches = 0;
+    k_batch_raygen<<<gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt, qa);
+    ++launches;
+    int *qin = qa, *qout = qb;
+    for (int b = 0; b < 2; ++b) {
+        extendFn<<<gExtend, 256, 0, st>>>(none, scenes, rs.P, cnt, qin);
+        ShadeArgs sa{none, scenes, rs.P, rs.S, qin, qout, cnt, 0};
+        k_shade<true><<<gShade, sb, 0, st>>>(sa);
+        if (walls) walkFn<<<gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        else anyFn<<<gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        k_advance<<<1, 1, 0, st>>>(cnt, dstats);
+        launches += 4;
+        std::swap(qin, qout);
+    }
+    k_batch_film<<<gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt);
+    k_batch_ctl<<<1, 1, 0, st>>>(ctl, cnt, loop);
+    launches += 2;
+    cudaGraph_t captured = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(st, &captured);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        check_cuda(ce, "cudaStreamEndCapture");
+    }
+    cudaError_t ie = cudaGraphInstantiate(&bs.exec, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(ie, "cudaGraphInstantiate");
+    bs.key = key;
+    bs.launchesPerIteration = launches;
+}
+
+// One batch render with the given settings. trial: films start at zero on the device and are
+// not copied back (autotuning). Returns false with a message on invalid input.
+bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchItem *items, int capacity, int shadeBlock,
+               bool trial, int sppDivisor, prgpu::BatchStats *stats, std::string *err) {
+    auto tHost0 = std::chrono::steady_clock::now();
+    cudaStream_t st = ds.stream;
+    if (int(bs.caches.size()) < count) bs.caches.resize(size_t(count));
+    std::vector<int64_t> npix(static_cast<size_t>(count));
+    std::vector<int> spp(static_cast<size_t>(count));
+    std::vector<prgpu::RenderParams> rp(static_cast<size_t>(count));
+    std::vector<size_t> filmOff(static_cast<size_t>(count));
+    size_t filmTotal = 0;
+    int sph = 0;
+    bool media = false, walls = false;
+    for (int i = 0; i < count; ++i) {
+        if (!bs.caches[size_t(i)]) bs.caches[size_t(i)] = std::make_unique<SceneCache>();
+        std::string e;
+        if (!upload_scene(ds, items[i].scene, items[i].ext, *bs.caches[size_t(i)], &e)) {
+            *err = "batch item " + std::to_string(i) + ": " + e;
+            return false;
+        }
+        const DevScene &d = bs.caches[size_t(i)]->ds;
+        npix[size_t(i)] = int64_t(d.cam.width) * d.cam.height;
+        rp[size_t(i)] = items[i].params;
+        spp[size_t(i)] = sppDivisor > 1 ? std::max(1, items[i].params.spp / sppDivisor) : items[i].params.spp;
+        if (items[i].params.spp == 0) spp[size_t(i)] = 0;
+        filmOff[size_t(i)] = filmTotal;
+        filmTotal += size_t(npix[size_t(i)]) * 3;
+        if (bs.caches[size_t(i)]->hasSpheres) sph = 1;
+        if (d.mediumCount + d.gridCount > 0) media = true;
+        if (d.hasInterfaces) walls = true;
+    }
+    std::vector<BatchChunk> chunks;
+    std::vector<BatchWave> waves;
+    schedule_waves(npix, spp, capacity, rp, &chunks, &waves);
+    ensure_capacity(bs.paths, capacity);
+    bs.films.ensure(std::max<size_t>(1, filmTotal) * sizeof(double));
+    bs.scenes.ensure(size_t(count) * sizeof(DevScene));
+    bs.chunks.ensure(std::max<size_t>(1, chunks.size()) * sizeof(BatchChunk));
+    bs.waves.ensure(std::max<size_t>(1, waves.size()) * sizeof(BatchWave));
+    bs.ctl.ensure(sizeof(BatchCtl));
+    double *films = bs.films.as<double>();
+    std::vector<DevScene> table(static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i) {
+        DevScene d = bs.caches[size_t(i)]->ds;
+        d.maxDepth = items[i].params.maxDepth;
+        d.clampY = items[i].params.clampLuminance;
+        d.film = films + filmOff[size_t(i)];
+        table[size_t(i)] = d;
+        size_t bytes = size_t(npix[size_t(i)]) * 3 * sizeof(double);
+        if (trial) PRB_CUDA(cudaMemsetAsync(d.film, 0, bytes, st));
+        else PRB_CUDA(cudaMemcpyAsync(d.film, items[i].outXYZ, bytes, cudaMemcpyHostToDevice, st));
+    }
+    PRB_CUDA(cudaMemcpyAsync(bs.scenes.ptr, table.data(), table.size() * sizeof(DevScene), cudaMemcpyHostToDevice, st));
+    if (!chunks.empty())
+        PRB_CUDA(cudaMemcpyAsync(bs.chunks.ptr, chunks.data(), chunks.size() * sizeof(BatchChunk),
+                                 cudaMemcpyHostToDevice, st));
+    if (!waves.empty())
+        PRB_CUDA(cudaMemcpyAsync(bs.waves.ptr, waves.data(), waves.size() * sizeof(BatchWave), cudaMemcpyHostToDevice,
+                                 st));
+    BatchGraphKey key;
+    key.capacity = capacity;
+    key.shadeBlock = shadeBlock;
+    key.variant = sph | (media ? 2 : 0) | (walls ? 4 : 0);
+    key.ptrs[0] = bs.paths.pathBuf.ptr;
+    key.ptrs[1] = bs.paths.shadowBuf.ptr;
+    key.ptrs[2] = bs.scenes.ptr;
+    key.ptrs[3] = bs.chunks.ptr;
+    key.ptrs[4] = bs.waves.ptr;
+    key.ptrs[5] = bs.paths.queues.ptr;
+    bool built = false;
+    if (!bs.exec || !(bs.key == key)) {
+        PRB_CUDA(cudaStreamSynchronize(st));
+        build_batch_graph(ds, bs, key, sph, media, walls);
+        built = true;
+    }
+    const int nWaves = int(waves.size());
+    const int maxIter = int(std::min<int64_t>(int64_t(nWaves) * 4200 + 16, int64_t(1) << 30));
+    float ms = 0.f;
+    int64_t launches = 0;
+    BatchCtl hc{};
+    unsigned long long hs[kStatSlots] = {};
+    if (nWaves > 0) {
+        k_batch_init<<<1, 32, 0, st>>>(bs.ctl.as<BatchCtl>(), nWaves, maxIter, bs.paths.counters.as<int>(),
+                                       bs.paths.stats.as<unsigned long long>());
+        PRB_CUDA(cudaEventRecord(bs.ev[0], st));
+        PRB_CUDA(cudaGraphLaunch(bs.exec, st));
+        PRB_CUDA(cudaEventRecord(bs.ev[1], st));
+        PRB_CUDA(cudaMemcpyAsync(&hc, bs.ctl.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        PRB_CUDA(cudaMemcpyAsync(hs, bs.paths.stats.ptr, sizeof(hs), cudaMemcpyDeviceToHost, st));
+        PRB_CUDA(cudaStreamSynchronize(st));
+        PRB_CUDA(cudaGetLastError());
+        PRB_CUDA(cudaEventElapsedTime(&ms, bs.ev[0], bs.ev[1]));
+        launches = 1 + int64_t(hc.iter) * bs.launchesPerIteration;
+        count_launch(uint64_t(launches));
+    }
+    int status = 0;
+    PRB_CUDA(cudaMemcpy(&status, bs.paths.counters.as<int>() + kCntStatus, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hc.status & 1) {
+        *err = "batch loop reached its iteration bound";
+        return false;
+    }
+    if (status & kStatusStack) {
+        *err = "BVH deeper than the traversal stack (64 entries)";
+        return false;
+    }
+    if (!trial) {
+        for (int i = 0; i < count; ++i)
+            PRB_CUDA(cudaMemcpyAsync(items[i].outXYZ, films + filmOff[size_t(i)],
+                                     size_t(npix[size_t(i)]) * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        PRB_CUDA(cudaStreamSynchronize(st));
+    }
+    if (stats) {
+        uint64_t samples = 0;
+        for (int i = 0; i < count; ++i) samples += uint64_t(npix[size_t(i)]) * uint64_t(spp[size_t(i)]);
+        stats->pathSamples = samples;
+        stats->closestRays = hs[kStatClosest];
+        stats->shadowRays = hs[kStatShadow];
+        stats->waves = uint64_t(nWaves);
+        stats->loopIterations = uint64_t(hc.iter);
+        stats->deviceMs = ms;
+        double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tHost0).count();
+        stats->hostMs = std::max(0.0, wall - ms);
+        stats->wavefrontPaths = capacity;
+        stats->shadeBlock = shadeBlock;
+        stats->graphBuilt = built ? 1 : 0;
+    }
+    return true;
+}
+
+bool check_batch(int count, const prgpu::BatchItem *items, bool needFilms, std::string *err) {
+    if (count < 1 || count > kMaxBatch) {
+        *err = "batch size must be 1.." + std::to_string(kMaxBatch);
+        return false;
+    }
+    if (!items) {
+        *err = "null batch items";
+        return false;
+    }
+    for (int i = 0; i < count; ++i) {
+        const prgpu::BatchItem &it = items[i];
+        std::string at = "batch item " + std::to_string(i) + ": ";
+        if (!it.scene || it.scene->apiVersion != prgpu::kApiVersion) {
+            *err = at + "API version mismatch";
+            return false;
+        }
+        if (it.params.spp < 0 || it.params.firstSample < 0) {
+            *err = at + "bad render parameters";
+            return false;
+        }
+        if (it.ext && it.ext->structSize != sizeof(prgpu::SceneExt)) {
+            *err = at + "SceneExt size mismatch";
+            return false;
+        }
+        if (needFilms && !it.outXYZ) {
+            *err = at + "null output film";
+            return false;
+        }
+    }
+    return true;
+}
+
+// The autotuner: candidate capacities x shading block sizes, each timed (best of two runs after a
+// warm-up run that builds its graph) on the batch with every render's spp divided so the trial
+// traces about 2^24 path samples.
+std::pair<int, int> autotune(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchItem *items,
+                             std::string *err, bool *ok) {
+    *ok = false;
+    uint64_t total = 0;
+    for (int i = 0; i < count; ++i)
+        total += uint64_t(items[i].scene->camera.width) * items[i].scene->camera.height * uint64_t(items[i].params.spp);
+    int div = int(std::max<uint64_t>(1, total / (uint64_t(1) << 24)));
+    size_t freeB = 0, totalB = 0;
+    PRB_CUDA(cudaMemGetInfo(&freeB, &totalB));
+    const int caps[] = {1 << 19, 1 << 20, 1 << 21, 1 << 22};
+    const int blocks[] = {128, 256};
+    double best = 1e300;
+    std::pair<int, int> choice{1 << 21, 256};
+    for (int cap : caps) {
+        if (size_t(cap) * 512 > freeB / 2) continue;
+        for (int sb : blocks) {
+            double t = 1e300;
+            for (int rep = 0; rep < 3; ++rep) {
+                prgpu::BatchStats s{};
+                if (!run_batch(ds, bs, count, items, cap, sb, true, div, &s, err)) return choice;
+                if (rep > 0 && s.pathSamples > 0) t = std::min(t, s.deviceMs / double(s.pathSamples));
+            }
+            if (t < best) {
+                best = t;
+                choice = {cap, sb};
+            }
+        }
+    }
+    *ok = true;
+    return choice;
+}
+
+int batch_common(int deviceIndex, int32_t count, const prgpu::BatchItem *items, const prgpu::BatchConfig *config,
+                 prgpu::BatchConfig *tuneOut, prgpu::BatchStats *stats, char *err, int errLen) {
+    std::lock_guard<std::mutex> lock(gApiMutex);
+    try {
+        std::string e;
+        if (!check_batch(count, items, tuneOut == nullptr, &e)) {
+            set_err(err, errLen, e);
+            return 1;
+        }
+        if (config && config->structSize != sizeof(prgpu::BatchConfig)) {
+            set_err(err, errLen, "BatchConfig size mismatch");
+            return 1;
+        }
+        int cap = config ? config->wavefrontPaths : 0, sb = config ? config->shadeBlock : 0;
+        if (cap != 0 && (cap < 1024 || cap > (1 << 24))) {
+            set_err(err, errLen, "wavefrontPaths out of range (1024 .. 2^24)");
+            return 1;
+        }
+        if (sb != 0 && (sb < 64 || sb > 256 || sb % 64 != 0)) {
+            set_err(err, errLen, "shadeBlock must be 64, 128, 192 or 256");
+            return 1;
+        }
+        if (deviceIndex < 0 || deviceIndex >= 64) {
+            set_err(err, errLen, "no such GPU device");
+            return 1;
+        }
+        DeviceState &ds = device_state(deviceIndex);
+        BatchState &bs = batch_state(deviceIndex);
+        bool tunedNow = false;
+        if (tuneOut || cap == 0 || sb == 0) {
+            uint64_t shape = batch_shape_key(deviceIndex, count, items);
+            auto it = bs.tuned.find(shape);
+            if (it == bs.tuned.end() || tuneOut) {
+                bool ok = false;
+                auto c = autotune(ds, bs, count, items, &e, &ok);
+                if (!ok) {
+                    set_err(err, errLen, e);
+                    return 1;
+                }
+                it = bs.tuned.insert_or_assign(shape, c).first;
+                tunedNow = true;
+            }
+            if (cap == 0) cap = it->second.first;
+            if (sb == 0) sb = it->second.second;
+            if (tuneOut) {
+                tuneOut->structSize = sizeof(prgpu::BatchConfig);
+                tuneOut->wavefrontPaths = it->second.first;
+                tuneOut->shadeBlock = it->second.second;
+                tuneOut->flags = 0;
+                return 0;
+            }
+        }
+        if (stats) *stats = prgpu::BatchStats{};
+        if (!run_batch(ds, bs, count, items, cap, sb, false, 1, stats, &e)) {
+            set_err(err, errLen, e);
+            return 1;
+        }
+        if (stats) stats->tuned = tunedNow ? 1 : 0;
+        return 0;
+    } catch (const CudaError &ex) {
+        set_err(err, errLen, ex.msg);
+        return 1;
+    } catch (const std::exception &ex) {
+        set_err(err, errLen, ex.what());
+        return 1;
+    }
+}
+
 } // namespace prb
 
 using namespace prb;
@@ -1199,4 +856,18 @@ PRGPU_API int prgpu_render_ex(int deviceIndex, const prgpu::SceneDesc *scene, co
         return 1;
     }
     return render_common(deviceIndex, scene, ext, params, nullptr, outXYZ, stats, err, errLen);
+}
+
+PRGPU_API int prgpu_render_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
+                                 const prgpu::BatchConfig *config, prgpu::BatchStats *stats, char *err, int errLen) {
+    return batch_common(deviceIndex, count, items, config, nullptr, stats, err, errLen);
+}
+
+PRGPU_API int prgpu_autotune_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
+                                   prgpu::BatchConfig *out, char *err, int errLen) {
+    if (!out) {
+        set_err(err, errLen, "null output config");
+        return 1;
+    }
+    return batch_common(deviceIndex, count, items, nullptr, out, nullptr, err, errLen);
 }

@@ -55,6 +55,10 @@ struct DevScene {
     int mediumCount;
     const DevGrid *grids;
     int gridCount;
+    // Per-render settings of the batched form (the single-render kernels take them as arguments).
+    int maxDepth;            // <= 0: unlimited
+    float clampY;            // 0: off
+    double *film;            // the render's device FP64 film, 3 doubles per pixel
 };
 
 struct SceneCache {

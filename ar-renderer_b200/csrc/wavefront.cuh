@@ -1,0 +1,944 @@
+// The wavefront path tracer's device side: path state in structure-of-arrays form, the per-bounce
+// kernels and the film kernel, used by the single-render and the batched drivers of render.cu (the
+// one file that includes it: the kernels have external linkage).
+//
+// The estimator is the reference's pr::PathIntegrator::Li (src/integrators/path.cpp:113-238) as its
+// GPU module restates it (src/gpu/prender_gpu.cpp:1344-1460): 4 hero wavelengths, next-event
+// estimation with power-heuristic MIS, path-level spectral MIS in homogeneous media (rPath, the
+// hero-driven free-flight pdf ratios, with Lhero kept for paths whose secondary wavelengths a
+// dispersive interface terminates), Russian roulette on the MIS-weighted throughput from the
+// third vertex on, no clamping unless the caller asks for it.
+//
+// Instead of one thread looping over a pixel's whole path (the reference megakernel), a batch of
+// paths lives in structure-of-arrays state in HBM and advances one bounce per round of kernels:
+//   raygen  -> closest-hit (k_extend) -> shading (k_shade: media, emission, BSDF, NEE, RR)
+//           -> shadow rays (k_shadow) -> ... until the queue is empty -> film (k_film).
+// Queues are compacted with warp-aggregated atomics (one atomic per warp, slots handed out by
+// ballot + popc), so every kernel reads a dense index list. Each path's final XYZ is added to an
+// FP64 per-pixel film in sample-index order, one sample at a time: a render split into batches
+// produces the same bits as one uninterrupted render.
+//
+// Batched form (kBatch): paths of many renders share the queues; each path carries its render's
+// index in bits 24..31 of meta.w and reads that render's DevScene from a device table.
+#pragma once
+
+#include <cmath>
+
+#include "bsdf.cuh"
+#include "lights.cuh"
+#include "media.cuh"
+#include "scene.cuh"
+
+namespace prb {
+// ---------------------------------------------------------------------------------------------
+// Path state (structure of arrays, 16-byte vector accesses)
+
+struct Paths {
+    float4 *o;       // origin, w: prevPdf
+    float4 *d;       // direction, w: etaScale
+    float4 *beta;    // throughput per wavelength
+    float4 *rpath;   // spectral MIS pdf ratios
+    float4 *L;       // MIS-weighted radiance
+    float4 *Lhero;   // unweighted radiance (valid once secondaries terminate)
+    float4 *lam;     // wavelengths
+    float4 *lpdf;    // wavelength pdfs
+    ulonglong2 *rng; // PCG32 state, increment
+    int4 *meta;      // pixel, depth, medium, flags (bit 0 specular, bits 8..23 interface crossings)
+    float4 *prevP;   // previous scattering vertex, w: filter weight of the camera sample
+    float4 *prevN;   // geometric normal there (0 in media), w: iteration guard (int bits)
+    float4 *hit;     // t, b1, b2, prim (int bits; -1 = miss)
+};
+
+struct Shadows {
+    float4 *o;   // origin, w: medium (int bits)
+    float4 *d;   // target - origin, w: path index (int bits)
+    float4 *c;   // contribution before transmittance
+    float *w;    // spectral MIS scale applied to L
+};
+
+// Device counters of one wavefront: queue lengths, the persistent kernels' work counters, status.
+enum {
+    kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
+    kCntSlots = 8
+};
+enum { kStatusStack = 1, kStatusGuard = 2 };
+// Device statistics (64-bit): closest-hit rays, shadow rays, non-empty bounces.
+enum { kStatClosest = 0, kStatShadow = 1, kStatBounces = 2, kStatSlots = 4 };
+
+constexpr float kShadowEps = 1e-4f;  // src/scene/interaction.h:21
+
+// Warp-aggregated append: one atomicAdd per warp; returns this thread's slot.
+__device__ __forceinline__ int warp_append(int *counter) {
+    unsigned mask = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(mask) - 1;
+    int rank = __popc(mask & ((1u << lane) - 1u));
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + rank;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pixel filter importance sampling (src/gpu/prender_gpu.cpp:1465-1494; the host builds the CDF
+// as src/integrators/gpu_path.cpp:431-456)
+
+__device__ float filter_eval_1d(const DevScene &s, float x) {
+    x = fabsf(x);
+    if (x > s.filterRadius) return 0.f;
+    switch (s.filterType) {
+    case prgpu::FilterGaussian: {
+        float is2 = 1.f / (2.f * s.filterSigma * s.filterSigma);
+        return fmaxf(0.f, expf(-x * x * is2) - expf(-s.filterRadius * s.filterRadius * is2));
+    }
+    case prgpu::FilterBlackmanHarris: {
+        float t = 0.5f + x / (2.f * s.filterRadius);
+        return 0.35875f - 0.48829f * cosf(2.f * kPi * t) + 0.14128f * cosf(4.f * kPi * t) -
+               0.01168f * cosf(6.f * kPi * t);
+    }
+    default: return 1.f;
+    }
+}
+
+__device__ float filter_sample_1d(const DevScene &s, float u, float *pdf) {
+    int lo = 0, hi = prgpu::kFilterBins;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(s.filterCdf + mid) <= u) lo = mid;
+        else hi = mid;
+    }
+    float c0 = __ldg(s.filterCdf + lo), c1 = __ldg(s.filterCdf + lo + 1);
+    float w = c1 - c0;
+    float t = w > 0.f ? (u - c0) / w : 0.5f;
+    float binW = 2.f * s.filterRadius / prgpu::kFilterBins;
+    *pdf = w / binW;
+    return -s.filterRadius + (float(lo) + t) * binW;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Surface interaction (src/geometry/shape.cpp:63-85, 224-264)
+
+struct Surf {
+    V3 p, n, ns, dpdu;
+    float u, v;
+};
+
+__device__ Surf shade_point(const DevScene &s, const prgpu::Primitive &pr, float t, float b1, float b2, V3 o, V3 d) {
+    Surf sf;
+    if (pr.type == prgpu::PrimSphere) {
+        V3 c = f3(pr.p0);
+        V3 rel = (o + d * t) - c;
+        float l = len(rel);
+        V3 n = l > 0.f ? rel * (1.f / l) : mk(0.f, 1.f, 0.f);
+        sf.p = c + n * pr.r;
+        sf.n = pr.flip ? -n : n;
+        sf.ns = sf.n;
+        float phi = atan2f(n.z, n.x);
+        if (phi < 0.f) phi += 2.f * kPi;
+        sf.u = phi * kInv2Pi;
+        sf.v = acosf(clampf(n.y, -1.f, 1.f)) * kInvPi;
+        sf.dpdu = mk(-rel.z, 0.f, rel.x);
+        if (len2(sf.dpdu) < 1e-12f) sf.dpdu = frame_from_z(n).x;
+        return sf;
+    }
+    V3 p0 = f3(pr.p0), p1 = f3(pr.p1), p2 = f3(pr.p2);
+    float b0 = 1.f - b1 - b2;
+    sf.p = p0 * b0 + p1 * b1 + p2 * b2;
+    V3 n = normalize(cross(p1 - p0, p2 - p0));
+    sf.u = pr.u0 * b0 + pr.u1 * b1 + pr.u2 * b2;
+    sf.v = pr.v0 * b0 + pr.v1 * b1 + pr.v2 * b2;
+    V3 ns = n;
+    V3 n0 = f3(pr.n0);
+    if (len2(n0) > 0.f) {
+        ns = n0 * b0 + f3(pr.n1) * b1 + f3(pr.n2) * b2;
+        float l = len(ns);
+        ns = l > 0.f ? ns * (1.f / l) : n;
+        n = face_forward(n, ns);
+    }
+    sf.n = n;
+    sf.ns = ns;
+    float du02 = pr.u0 - pr.u2, du12 = pr.u1 - pr.u2, dv02 = pr.v0 - pr.v2, dv12 = pr.v1 - pr.v2;
+    float det = du02 * dv12 - dv02 * du12;
+    if (fabsf(det) < 1e-9f) {
+        sf.dpdu = frame_from_z(n).x;
+    } else {
+        sf.dpdu = ((p0 - p2) * dv12 - (p1 - p2) * dv02) * (1.f / det);
+        if (!isfinite(sf.dpdu.x) || len2(cross(sf.dpdu, n)) == 0.f) sf.dpdu = frame_from_z(n).x;
+    }
+    return sf;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Materials (src/materials/material.cpp:73-117; src/gpu/prender_gpu.cpp:1136-1226)
+
+__device__ Ggx make_ggx(float ax, float ay) {
+    Ggx g{ax, ay};
+    if (!g.smooth()) {
+        g.ax = fmaxf(g.ax, 1e-4f);
+        g.ay = fmaxf(g.ay, 1e-4f);
+    }
+    return g;
+}
+
+__device__ SS diffuse_albedo(const DevScene &s, const prgpu::Material &m, float u, float v, const Lambda &lam) {
+    int id = m.albedo;
+    if (m.albedoB >= 0 && m.checkerScale > 0.f) {
+        int odd = (int(floorf(u * m.checkerScale)) + int(floorf(v * m.checkerScale))) & 1;
+        if (odd) id = m.albedoB;
+    }
+    SS R = tab4(s.spectra, id, lam);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) R.v[i] = clampf(R.v[i], 0.f, 1.f);
+    return R;
+}
+
+// Builds the lobe of material m at the hit; may terminate the secondary wavelengths.
+__device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam) {
+    Lobe l;
+    l.kind = kLobeNone;
+    l.etaD = 1.f;
+    l.mf = Ggx{0.f, 0.f};
+    switch (m.type) {
+    case prgpu::MatDiffuse:
+        l.kind = kLobeDiffuse;
+        l.R = diffuse_albedo(s, m, u, v, lam);
+        break;
+    case prgpu::MatConductor:
+        l.kind = kLobeConductor;
+        l.mf = make_ggx(m.alphaX, m.alphaY);
+        if (m.eta >= 0) {
+            l.eta = tab4(s.spectra, m.eta, lam);
+            l.k = tab4(s.spectra, m.k, lam);
+        } else {
+            // Artist reflectance r -> eta 1, k = 2 sqrt(r) / sqrt(1 - r) (exact r at normal incidence).
+            SS r = tab4(s.spectra, m.albedo, lam);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                float ri = clampf(r.v[i], 0.f, 0.9999f);
+                l.eta.v[i] = 1.f;
+                l.k.v[i] = 2.f * sqrtf(ri) / safe_sqrt(1.f - ri);
+            }
+        }
+        break;
+    case prgpu::MatDielectric:
+        l.kind = m.thin ? kLobeThin : kLobeDielectric;
+        l.etaD = tab(s.spectra, m.eta, lam.l[0]);
+        if (m.dispersive) lam.terminate_secondary();
+        if (l.etaD == 0.f) l.etaD = 1.f;
+        l.mf = make_ggx(m.alphaX, m.alphaY);
+        break;
+    default: break;
+    }
+    return l;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Lights
+
+__device__ SS emitted(const DevScene &s, const prgpu::Light &l, V3 n, V3 w, const Lambda &lam) {
+    float c = dot(n, w);
+    if (!l.twoSided && c <= 0.f) return splat(0.f);
+    float prof = l.cosPower > 0.f ? powf(fabsf(c), l.cosPower) : 1.f;
+    return tab4(s.spectra, l.spectrum, lam) * (l.scale * prof);
+}
+
+// Solid-angle density of sampling point p (normal n) on area light l from ref (uniform area).
+__device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
+    V3 d = p - ref;
+    float d2 = len2(d);
+    float c = fabsf(dot(n, d * rsqrtf(d2)));
+    if (c == 0.f) return 0.f;
+    return d2 / (c * l.area);
+}
+
+// Probability that NEE at (p, n) picks light li: the light-BVH pmf when the scene has one (the
+// exact leaf-to-root walk), the power pmf otherwise.
+__device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
+    if (s.lbvhCount == 0) return s.lights[li].pmf;
+    return lbvh_pmf(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, li, p, n);
+}
+
+struct LightSample {
+    V3 wi, target;
+    SS Le;
+    float pdf;   // selection pmf times the solid-angle density (1 for point lights)
+    bool delta;
+    bool ok;
+};
+
+// Chooses a light and a point on it as seen from p (normal n, zero in media).
+__device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
+    LightSample ls;
+    ls.ok = false;
+    ls.delta = false;
+    if (ul < s.envPmf && s.envSpectrum >= 0) {
+        float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
+        sincosf(2.f * kPi * u1, &sp, &cp);
+        ls.wi = mk(r * cp, r * sp, z);
+        ls.target = p + ls.wi * (2.f * s.worldRadius);
+        ls.Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
+        ls.pdf = s.envPmf * kInv4Pi;
+        ls.ok = true;
+        return ls;
+    }
+    int li = -1;
+    float pmf = 0.f;
+    if (s.lbvhCount > 0) {
+        float u = fminf((ul - s.envPmf) / s.lbvhProb, kOneMinusEps);
+        li = lbvh_sample(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, p, n, u, &pmf);
+    } else {
+        if (s.lightCount == 0) return ls;
+        float acc = s.envSpectrum >= 0 ? s.envPmf : 0.f;
+        li = s.lightCount - 1;
+        for (int i = 0; i < s.lightCount; ++i) {
+            acc += s.lights[i].pmf;
+            if (ul < acc) {
+                li = i;
+                break;
+            }
+        }
+        pmf = s.lights[li].pmf;
+    }
+    if (li < 0 || !(pmf > 0.f)) return ls;
+    const prgpu::Light &l = s.lights[li];
+    if (l.type == prgpu::LightPoint) {
+        ls.target = f3(l.position);
+        V3 dd = ls.target - p;
+        float d2 = len2(dd);
+        if (!(d2 > 0.f)) return ls;
+        ls.wi = dd * rsqrtf(d2);
+        ls.Le = tab4(s.spectra, l.spectrum, lam) * (l.scale / d2);
+        ls.pdf = pmf;
+        ls.delta = true;
+        ls.ok = true;
+        return ls;
+    }
+    const prgpu::Primitive &lp = s.prims[l.primitive];
+    V3 pl, nl;
+    if (lp.type == prgpu::PrimSphere) {
+        float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
+        sincosf(2.f * kPi * u1, &sp, &cp);
+        V3 nn = mk(r * cp, r * sp, z);
+        pl = f3(lp.p0) + nn * lp.r;
+        nl = lp.flip ? -nn : nn;
+    } else {
+        float b0, b1;
+        if (u0 < u1) {
+            b0 = u0 * 0.5f;
+            b1 = u1 - b0;
+        } else {
+            b1 = u1 * 0.5f;
+            b0 = u0 - b1;
+        }
+        float b2 = 1.f - b0 - b1;
+        V3 p0 = f3(lp.p0), p1 = f3(lp.p1), p2 = f3(lp.p2);
+        pl = p0 * b0 + p1 * b1 + p2 * b2;
+        nl = normalize(cross(p1 - p0, p2 - p0));
+        V3 n0 = f3(lp.n0);
+        if (len2(n0) > 0.f) nl = face_forward(nl, n0 * b0 + f3(lp.n1) * b1 + f3(lp.n2) * b2);
+    }
+    V3 dd = pl - p;
+    float d2 = len2(dd);
+    if (!(d2 > 0.f)) return ls;
+    ls.wi = dd * rsqrtf(d2);
+    ls.Le = emitted(s, l, nl, -ls.wi, lam);
+    ls.pdf = pmf * area_pdf(l, p, pl, nl);
+    if (!nonzero(ls.Le) || !(ls.pdf > 0.f) || !isfinite(ls.pdf)) return ls;
+    ls.target = pl + (dot(-dd, nl) < 0.f ? -nl : nl) * ray_eps(pl);
+    ls.ok = true;
+    return ls;
+}
+
+// Transmittance of the shadow segment o -> o + dd (length len(dd)) in the given medium.
+__device__ SS segment_tr(const DevScene &s, int medium, const Lambda &lam, V3 o, V3 dd, float frac) {
+    float l = len(dd);
+    float dist = frac * l;
+    if (!is_grid(s, medium)) return homogeneous_tr(s, medium, lam, dist);
+    Pcg rng = segment_stream(o, dd, uint32_t(medium));
+    return medium_transmittance(s, medium, lam, o, dd * (1.f / l), dist, rng);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Kernels
+
+struct ChunkInfo {
+    int pixBegin;      // first pixel of the chunk (raster index)
+    int npix;          // pixels in the chunk
+    int samples;       // samples per pixel in the chunk
+    int firstSample;   // absolute sample index of the chunk's first sample
+    uint64_t seed;
+    int maxDepth;      // <= 0: unlimited
+};
+
+__device__ __forceinline__ Lambda load_lam(const Paths &P, int j) {
+    float4 a = P.lam[j], b = P.lpdf[j];
+    Lambda w;
+    w.l[0] = a.x; w.l[1] = a.y; w.l[2] = a.z; w.l[3] = a.w;
+    w.pdf[0] = b.x; w.pdf[1] = b.y; w.pdf[2] = b.z; w.pdf[3] = b.w;
+    return w;
+}
+
+// Render index of a path, kept in bits 24..31 of meta.w (0 outside batches).
+constexpr int kRenderShift = 24;
+__device__ __forceinline__ int path_render(int metaw) { return int(unsigned(metaw) >> kRenderShift); }
+
+// The scene of a path: the kernel argument for single renders, the batch table otherwise (kept
+// apart so the single-render form reads its scene from the parameter space).
+template <bool kBatch> struct SceneOf;
+template <> struct SceneOf<false> {
+    static __device__ __forceinline__ const DevScene &get(const DevScene &s0, const DevScene *, int) { return s0; }
+};
+template <> struct SceneOf<true> {
+    static __device__ __forceinline__ const DevScene &get(const DevScene &, const DevScene *t, int rid) { return t[rid]; }
+};
+
+// Camera sample `sample` of pixel `pix` (PerspectiveCamera::GenerateRay, camera.cpp:36-48, with
+// SampleVisible wavelengths and filter importance sampling) into path slot j, queued if valid.
+__device__ __forceinline__ void raygen_path(const DevScene &s, const Paths &P, int j, int pix, uint64_t sample,
+                                            uint64_t seed, int rid, int *counters, int *queue) {
+    {
+        int px = pix % s.cam.width, py = pix / s.cam.width;
+        Pcg rng = pixel_sample_stream(uint32_t(pix), sample, seed);
+        Lambda lam = sample_visible(rng.uniform());
+        float pdfX, pdfY;
+        float dx = filter_sample_1d(s, rng.uniform(), &pdfX), dy = filter_sample_1d(s, rng.uniform(), &pdfY);
+        float fw = filter_eval_1d(s, dx) * filter_eval_1d(s, dy) * s.filterNorm / (pdfX * pdfY);
+        float l0 = rng.uniform(), l1 = rng.uniform();
+        const prgpu::Camera &c = s.cam;
+        float fx = float(px) + 0.5f + dx, fy = float(py) + 0.5f + dy;
+        V3 dir = normalize(mk((2.f * fx / c.width - 1.f) * c.tanHalfFov * c.aspect, (1.f - 2.f * fy / c.height) * c.tanHalfFov, 1.f));
+        V3 org = mk(0.f, 0.f, 0.f);
+        if (c.lensRadius > 0.f) {
+            float lx, ly;
+            concentric_disk(l0, l1, &lx, &ly);
+            V3 pf = dir * (c.focalDistance / dir.z);
+            org = mk(lx * c.lensRadius, ly * c.lensRadius, 0.f);
+            dir = normalize(pf - org);
+        }
+        const float *M = c.cameraToWorld;
+        V3 o = mk(M[0] * org.x + M[1] * org.y + M[2] * org.z + M[3], M[4] * org.x + M[5] * org.y + M[6] * org.z + M[7],
+                  M[8] * org.x + M[9] * org.y + M[10] * org.z + M[11]);
+        V3 dw = normalize(mk(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
+                             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z));
+        bool valid = fw != 0.f && isfinite(fw);
+        P.o[j] = make_float4(o.x, o.y, o.z, 1.f);
+        P.d[j] = make_float4(dw.x, dw.y, dw.z, 1.f);
+        P.beta[j] = make_float4(1.f, 1.f, 1.f, 1.f);
+        P.rpath[j] = make_float4(1.f, 1.f, 1.f, 1.f);
+        P.L[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P.Lhero[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+        P.lam[j] = make_float4(lam.l[0], lam.l[1], lam.l[2], lam.l[3]);
+        P.lpdf[j] = make_float4(lam.pdf[0], lam.pdf[1], lam.pdf[2], lam.pdf[3]);
+        P.rng[j] = make_ulonglong2(rng.state, rng.inc);
+        P.meta[j] = make_int4(pix, 0, s.cameraMedium, rid << kRenderShift);
+        P.prevP[j] = make_float4(o.x, o.y, o.z, valid ? fw : 0.f);
+        P.prevN[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+        if (valid) queue[warp_append(counters + kCntActive)] = j;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo ci, int *counters, int *queue) {
+    int total = ci.npix * ci.samples;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        int sIdx = j / ci.npix, pl = j - sIdx * ci.npix;
+        raygen_path(s, P, j, ci.pixBegin + pl, uint64_t(ci.firstSample) + uint64_t(sIdx), ci.seed, 0, counters, queue);
+    }
+}
+
+// Closest hit for every queued path, by persistent warps whose finished lanes take the next
+// queue entry at once (see k_trace_persist in accel.cu): bounce rays are incoherent and end
+// after very different numbers of steps.
+template <bool kSpheres, bool kBatch = false>
+__global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *scenes, Paths P, int *counters,
+                                                const int *queue) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n = counters[kCntActive];
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TraceRay r;
+    TravState st;
+    st.ref = 0;
+    st.sp = 0;
+    st.tMax = kInf;
+    st.found = false;
+    int j = 0;
+    const WNode *nodes = s0.nodes;
+    const LeafPrim *leaves = s0.leaves;
+    bool active = false, exhausted = n == 0, overflow = false;
+    while (!__all_sync(full, exhausted)) {
+        unsigned need = __ballot_sync(full, !active && !exhausted);
+        if (need) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(counters + kCntExtendWork, __popc(need));
+            base = __shfl_sync(full, base, 0);
+            if (!active && !exhausted) {
+                int q = base + __popc(need & ((1u << lane) - 1u));
+                if (q >= n) {
+                    exhausted = true;
+                } else {
+                    j = queue[q];
+                    const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(P.meta[j].w));
+                    nodes = s.nodes;
+                    leaves = s.leaves;
+                    float4 o = P.o[j], d = P.d[j];
+                    r = make_trace_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
+                    st.tMax = kInf;
+                    st.sp = 0;
+                    st.found = false;
+                    st.hit.prim = -1;
+                    float te;
+                    active = !s.root.empty &&
+                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
+                                       s.root.box[5], &te) &&
+                             te < kInf;
+                    st.ref = s.root.ref;
+                    if (!active) P.hit[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                }
+            }
+        }
+        if (active && traverse_step<false, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+            active = false;
+            P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
+        }
+    }
+    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
+}
+
+struct ShadeArgs {
+    DevScene s;
+    const DevScene *scenes;  // batched form: the renders' scenes, indexed by path_render
+    Paths P;
+    Shadows S;
+    const int *queueIn;
+    int *queueOut;
+    int *counters;
+    int maxDepth;
+};
+
+// One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
+template <bool kBatch = false>
+__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
+    const Paths &P = a.P;
+    int n = a.counters[kCntActive];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int j = a.queueIn[q];
+        int4 meta = P.meta[j];
+        const DevScene &s = SceneOf<kBatch>::get(a.s, a.scenes, path_render(meta.w));
+        const int maxDepth = kBatch ? s.maxDepth : a.maxDepth;
+        float4 o4 = P.o[j], d4 = P.d[j], hit = P.hit[j];
+        V3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
+        float prevPdf = o4.w, etaScale = d4.w;
+        SS beta = from_f4(P.beta[j]), rpath = from_f4(P.rpath[j]);
+        SS L = from_f4(P.L[j]), Lhero = from_f4(P.Lhero[j]);
+        Lambda lam = load_lam(P, j);
+        ulonglong2 rs = P.rng[j];
+        Pcg rng{rs.x, rs.y};
+        int depth = meta.y, medium = meta.z, flags = meta.w;
+        bool specular = flags & 1;
+        int crossings = (flags >> 8) & 0xffff;
+        float4 pp4 = P.prevP[j], pn4 = P.prevN[j];
+        V3 prevP = mk(pp4.x, pp4.y, pp4.z), prevN = mk(pn4.x, pn4.y, pn4.z);
+        int iters = __float_as_int(pn4.w) + 1;
+        int prim = __float_as_int(hit.w);
+        bool alive = true;
+
+        auto misScale = [&]() {
+            float av = 0.25f * (rpath.v[0] + rpath.v[1] + rpath.v[2] + rpath.v[3]);
+            return av > 0.f && isfinite(av) ? 1.f / av : 0.f;
+        };
+        auto add = [&](SS c) {
+            Lhero = Lhero + c;
+            L = L + c * misScale();
+        };
+        // NEE: queue a shadow ray carrying f * Le * w / pdf; the visibility test adds it later.
+        // The shadow ray starts in the medium on the light's side of the vertex (medIn / medOut
+        // for surfaces, the current medium for medium vertices where ng = 0).
+        auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut) {
+            float ul = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+            LightSample ls = sample_light(s, p, ng, lam, ul, u0, u1);
+            if (!ls.ok) return;
+            int med = dot(ls.wi, ng) > 0.f ? medOut : medIn;
+            SS f;
+            float spdf;
+            if (lobe) {
+                V3 wol = fr->to_local(wo), wil = fr->to_local(ls.wi);
+                if (wol.z == 0.f) return;
+                f = lobe_f(*lobe, wol, wil) * fabsf(dot(ls.wi, ns));
+                spdf = lobe_pdf(*lobe, wol, wil);
+            } else {
+                float ph = hg_phase(dot(wo, ls.wi), g);
+                f = splat(ph);
+                spdf = ph;
+            }
+            if (!nonzero(f)) return;
+            float w = ls.delta ? 1.f : power_heuristic(ls.pdf, spdf);
+            SS c = beta * f * ls.Le * (w / ls.pdf);
+            if (!nonzero(c)) return;
+            V3 so = p + (dot(ls.target - p, ng) < 0.f ? -ng : ng) * ray_eps(p);
+            int k = warp_append(a.counters + kCntShadow);
+            a.S.o[k] = make_float4(so.x, so.y, so.z, __int_as_float(med));
+            V3 sd = ls.target - so;
+            a.S.d[k] = make_float4(sd.x, sd.y, sd.z, __int_as_float(j));
+            a.S.c[k] = to_f4(c);
+            a.S.w[k] = misScale();
+        };
+        auto roulette = [&]() {
+            if (depth <= 1) return true;
+            float ms = lam.terminated() ? 1.f : misScale();
+            float mx = max_c(beta) * etaScale * ms;
+            if (mx >= 1.f) return true;
+            float qq = fmaxf(0.f, 1.f - mx);
+            if (rng.uniform() < qq) return false;
+            beta = beta * (1.f / (1.f - qq));
+            return true;
+        };
+
+        if (iters > 8192) {
+            alive = false;
+            atomicOr(a.counters + kCntStatus, kStatusGuard);
+        }
+        bool handled = !alive;
+        bool found = prim >= 0;
+        // Participating medium along the segment: hero-driven free flight in homogeneous media
+        // (medium.cpp:71-103, with the rPath pdf ratios of path-level spectral MIS), spectral
+        // tracking in grid media (medium.cpp:232-285, wavelength-neutral: rPath unchanged).
+        if (!handled && medium >= 0) {
+            float tMax = found ? hit.x : kInf;
+            int event = 0;  // 0: the segment is crossed, 1: real scattering at t, 2: the path ends
+            float t = tMax, g = 0.f;
+            if (!is_grid(s, medium)) {
+                const prgpu::Medium &md = s.media[medium];
+                g = md.g;
+                SS ss = tab4(s.spectra, md.sigmaS, lam) * md.scale;
+                SS st = tab4(s.spectra, md.sigmaA, lam) * md.scale + ss;
+                float u = fminf(rng.uniform(), kOneMinusEps);
+                t = st.v[0] > 0.f ? -logf(1.f - u) / st.v[0] : kInf;
+                if (t < tMax) {
+                    SS T;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) T.v[i] = expf(-st.v[i] * t);
+                    float pdf0 = st.v[0] * T.v[0];
+                    if (!(pdf0 > 0.f)) {
+                        event = 2;
+                    } else {
+                        beta = beta * T * ss * (1.f / pdf0);
+                        rpath = rpath * st * T * (1.f / pdf0);
+                        event = 1;
+                    }
+                } else {
+                    SS T;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        T.v[i] = isinf(tMax) ? (st.v[i] > 0.f ? 0.f : 1.f) : expf(-st.v[i] * tMax);
+                    if (!(T.v[0] > 0.f)) {
+                        event = 2;
+                    } else {
+                        beta = beta * T * (1.f / T.v[0]);
+                        rpath = rpath * T * (1.f / T.v[0]);
+                        if (!nonzero(beta)) event = 2;
+                    }
+                }
+            } else {
+                const DevGrid &gr = s.grids[medium - s.mediumCount];
+                g = gr.g;
+                SS wgt;
+                event = grid_sample(s, gr, lam, o, d, tMax, rng, &t, &wgt);
+                beta = beta * wgt;
+                if (event == 0 && !nonzero(beta)) event = 2;
+            }
+            if (event == 2) {
+                alive = false;
+                handled = true;
+            } else if (event == 1) {
+                handled = true;
+                if (!nonzero(beta) || (maxDepth > 0 && depth >= maxDepth)) {
+                    alive = false;
+                } else {
+                    ++depth;
+                    V3 p = o + d * t, wo = -d;
+                    nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, g, medium, medium);
+                    float u0 = rng.uniform(), u1 = rng.uniform(), phasePdf;
+                    V3 wi = hg_sample(wo, g, u0, u1, &phasePdf);
+                    if (!(phasePdf > 0.f)) {
+                        alive = false;
+                    } else {
+                        prevPdf = phasePdf;
+                        prevP = p;
+                        prevN = mk(0.f, 0.f, 0.f);
+                        specular = false;
+                        o = p;
+                        d = wi;
+                        alive = roulette();
+                    }
+                }
+            }
+        }
+        if (!handled && !found) {
+            // Escaped: environment emission with MIS against the previous BSDF / phase sample.
+            if (s.envSpectrum >= 0) {
+                SS Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
+                float w = 1.f;
+                if (depth > 0 && !specular) w = power_heuristic(prevPdf, s.envPmf * kInv4Pi);
+                add(beta * Le * w);
+            }
+            alive = false;
+            handled = true;
+        }
+        if (!handled) {
+            const prgpu::Primitive &pr = s.prims[prim];
+            Surf sf = shade_point(s, pr, hit.x, hit.y, hit.z, o, d);
+            if (pr.light >= 0) {
+                const prgpu::Light &l = s.lights[pr.light];
+                SS Le = emitted(s, l, sf.n, -d, lam);
+                if (nonzero(Le)) {
+                    float w = 1.f;
+                    if (depth > 0 && !specular)
+                        w = power_heuristic(prevPdf, light_pmf(s, pr.light, prevP, prevN) * area_pdf(l, prevP, sf.p, sf.n));
+                    add(beta * Le * w);
+                }
+            }
+            const prgpu::Material &m = s.mats[pr.material];
+            if (m.type == prgpu::MatInterface) {
+                // Invisible medium boundary: switch media and continue straight on.
+                if (++crossings > 1000) {
+                    alive = false;
+                } else {
+                    medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
+                    o = offset_origin(sf.p, sf.n, d);
+                }
+            } else if (m.type == prgpu::MatBlack || (maxDepth > 0 && depth >= maxDepth)) {
+                alive = false;
+            } else {
+                ++depth;
+                Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
+                Frame fr = frame_from_xz(sf.dpdu, sf.ns);
+                V3 wo = -d;
+                if (lobe.non_specular())
+                    nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside);
+                float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                V3 wol = fr.to_local(wo);
+                BSample bs;
+                bool ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                     isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                if (!ok) {
+                    alive = false;
+                } else {
+                    V3 wi = fr.from_local(bs.wi);
+                    beta = beta * bs.f * (fabsf(dot(wi, sf.ns)) / bs.pdf);
+                    prevPdf = bs.pdf;
+                    specular = (bs.flags & kFlagSpecular) != 0u;
+                    if (bs.flags & kFlagTransmission) etaScale *= sqr(bs.eta);
+                    prevP = sf.p;
+                    prevN = sf.n;
+                    o = offset_origin(sf.p, sf.n, wi);
+                    d = wi;
+                    // Medium on the side the new direction enters.
+                    medium = dot(wi, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
+                    if (!nonzero(beta) || !isfinite(max_c(beta))) alive = false;
+                    else alive = roulette();
+                }
+            }
+        }
+        // Write back (the radiance sums always; the ray state only for survivors).
+        P.L[j] = to_f4(L);
+        P.Lhero[j] = to_f4(Lhero);
+        P.lpdf[j] = make_float4(lam.pdf[0], lam.pdf[1], lam.pdf[2], lam.pdf[3]);
+        if (alive) {
+            P.o[j] = make_float4(o.x, o.y, o.z, prevPdf);
+            P.d[j] = make_float4(d.x, d.y, d.z, etaScale);
+            P.beta[j] = to_f4(beta);
+            P.rpath[j] = to_f4(rpath);
+            P.rng[j] = make_ulonglong2(rng.state, rng.inc);
+            P.meta[j] = make_int4(meta.x, depth, medium,
+                                  (specular ? 1 : 0) | (min(crossings, 0xffff) << 8) | (flags & (0xff << kRenderShift)));
+            P.prevP[j] = make_float4(prevP.x, prevP.y, prevP.z, pp4.w);
+            P.prevN[j] = make_float4(prevN.x, prevN.y, prevN.z, __int_as_float(iters));
+            a.queueOut[warp_append(a.counters + kCntNext)] = j;
+        }
+    }
+}
+
+// An unoccluded NEE sample: its contribution times the transmittance of the medium it crossed
+// goes to the path's radiance sums (one shadow entry per path and bounce, so no atomics).
+template <bool kMedia>
+__device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P, const Shadows &S, int q) {
+    float4 o4 = S.o[q], d4 = S.d[q];
+    int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
+    SS c = from_f4(S.c[q]);
+    if (kMedia && medium >= 0) c = c * segment_tr(s, medium, load_lam(P, j), mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z), 1.f);
+    float w = S.w[q];
+    float4 L = P.L[j], Lh = P.Lhero[j];
+    P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
+    P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
+}
+
+// Visibility of queued NEE samples in scenes without medium interfaces: any-hit queries up to
+// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill. kMedia: the scene has
+// media, so accepted segments carry a transmittance (kept out of the medium-free variant, whose
+// traversal loop would otherwise pay registers for the ratio-tracking code).
+template <bool kSpheres, bool kMedia, bool kBatch = false>
+__global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene *scenes, Paths P, Shadows S,
+                                                    int *counters) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int n = counters[kCntShadow];
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TraceRay r;
+    TravState st;
+    st.ref = 0;
+    st.sp = 0;
+    st.tMax = 1.f - kShadowEps;
+    st.found = false;
+    int q = 0, rid = 0;
+    const WNode *nodes = s0.nodes;
+    const LeafPrim *leaves = s0.leaves;
+    bool active = false, exhausted = n == 0, overflow = false;
+    while (!__all_sync(full, exhausted)) {
+        unsigned need = __ballot_sync(full, !active && !exhausted);
+        if (need) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(counters + kCntShadowWork, __popc(need));
+            base = __shfl_sync(full, base, 0);
+            if (!active && !exhausted) {
+                q = base + __popc(need & ((1u << lane) - 1u));
+                if (q >= n) {
+                    exhausted = true;
+                } else {
+                    float4 o4 = S.o[q], d4 = S.d[q];
+                    if (kBatch) rid = path_render(P.meta[__float_as_int(d4.w)].w);
+                    const DevScene &s = SceneOf<kBatch>::get(s0, scenes, rid);
+                    nodes = s.nodes;
+                    leaves = s.leaves;
+                    r = make_trace_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
+                    st.tMax = 1.f - kShadowEps;
+                    st.sp = 0;
+                    st.found = false;
+                    float te;
+                    active = !s.root.empty &&
+                             box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
+                                       s.root.box[5], &te) &&
+                             te < st.tMax;
+                    st.ref = s.root.ref;
+                    if (!active) shadow_accept<kMedia>(s, P, S, q);
+                }
+            }
+        }
+        if (active && traverse_step<true, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+            active = false;
+            if (!st.found) shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
+        }
+    }
+    if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
+}
+
+// Moves the survivors' queue into place for the next bounce and accumulates statistics (one
+// thread; keeps the bounce loop free of host round trips).
+__global__ void k_advance(int *counters, unsigned long long *stats) {
+    stats[kStatClosest] += (unsigned long long)counters[kCntActive];
+    stats[kStatShadow] += (unsigned long long)counters[kCntShadow];
+    stats[kStatBounces] += counters[kCntActive] > 0 ? 1ull : 0ull;
+    counters[kCntActive] = counters[kCntNext];
+    counters[kCntNext] = 0;
+    counters[kCntShadow] = 0;
+    counters[kCntExtendWork] = 0;
+    counters[kCntShadowWork] = 0;
+}
+
+// Visibility of queued NEE samples in scenes with medium interfaces: a walk through the boundary
+// surfaces with homogeneous transmittance (src/scene/scene.cpp:41-59).
+template <bool kSpheres, bool kBatch = false>
+__global__ void __launch_bounds__(256) k_shadow_walk(DevScene s0, const DevScene *scenes, Paths P, Shadows S,
+                                                     const int *counters) {
+    int n = counters[kCntShadow];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        float4 o4 = S.o[q], d4 = S.d[q];
+        int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
+        const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(P.meta[j].w));
+        V3 o = mk(o4.x, o4.y, o4.z), dd = mk(d4.x, d4.y, d4.z);
+        V3 target = o + dd;
+        SS T = splat(1.f);
+        bool overflow = false;
+        Lambda lam;
+        bool needLam = medium >= 0 || s.hasInterfaces;
+        if (needLam) lam = load_lam(P, j);
+        if (!s.hasInterfaces) {
+            TraceRay r = make_trace_ray(o, dd);
+            Hit h;
+            bool occ = !s.root.empty &&
+                       traverse<true, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
+            if (occ) continue;
+            if (medium >= 0) T = segment_tr(s, medium, lam, o, dd, 1.f);
+        } else {
+            bool blocked = true;
+            for (int it = 0; it < 256; ++it) {
+                V3 d = target - o;
+                TraceRay r = make_trace_ray(o, d);
+                Hit h;
+                h.prim = -1;
+                bool hit = !s.root.empty &&
+                           traverse<false, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
+                if (hit && s.mats[s.prims[h.prim].material].type != prgpu::MatInterface) break;
+                if (medium >= 0) T = T * segment_tr(s, medium, lam, o, d, hit ? h.t : 1.f);
+                if (!hit || !nonzero(T)) {
+                    blocked = false;
+                    break;
+                }
+                const prgpu::Primitive &pr = s.prims[h.prim];
+                Surf sf = shade_point(s, pr, h.t, h.u, h.v, o, d);
+                medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
+                o = offset_origin(sf.p, sf.n, d);
+            }
+            if (blocked) continue;
+        }
+        SS c = from_f4(S.c[q]) * T;
+        float w = S.w[q];
+        float4 L = P.L[j], Lh = P.Lhero[j];
+        P.L[j] = make_float4(L.x + c.v[0] * w, L.y + c.v[1] * w, L.z + c.v[2] * w, L.w + c.v[3] * w);
+        P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
+    }
+}
+
+// Adds each sample's XYZ to the FP64 film, one sample at a time in sample-index order
+// (src/gpu/prender_gpu.cpp:1541-1559 for the per-sample conversion and clamp).
+// Pixel pl of a chunk whose sample k sits in path slot base + k * npix: its samples' XYZ added to
+// film3 (X, Y, Z of that pixel) in sample order.
+__device__ __forceinline__ void film_pixel(const DevScene &s, const Paths &P, int base, int npix, int pl, int samples,
+                                           float clampY, double *film3) {
+    double X = film3[0], Y = film3[1], Z = film3[2];
+    for (int sIdx = 0; sIdx < samples; ++sIdx) {
+        int j = base + sIdx * npix + pl;
+        float fw = P.prevP[j].w;
+        if (fw == 0.f) continue;
+        Lambda lam = load_lam(P, j);
+        SS L = from_f4(lam.terminated() ? P.Lhero[j] : P.L[j]);
+        if (!isfinite(L.v[0] + L.v[1] + L.v[2] + L.v[3])) continue;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (lam.pdf[i] == 0.f) continue;
+            float v = L.v[i] / lam.pdf[i];
+            sx += cie_x(lam.l[i]) * v;
+            sy += cie_y(lam.l[i]) * v;
+            sz += cie_z(lam.l[i]) * v;
+        }
+        float k = fw;
+        if (clampY > 0.f && sy * s.norm > clampY) k *= clampY / (sy * s.norm);
+        k *= s.norm;
+        X += double(sx * k);
+        Y += double(sy * k);
+        Z += double(sz * k);
+    }
+    film3[0] = X;
+    film3[1] = Y;
+    film3[2] = Z;
+}
+
+__global__ void __launch_bounds__(256) k_film(DevScene s, Paths P, ChunkInfo ci, float clampY, double *film) {
+    for (int pl = blockIdx.x * blockDim.x + threadIdx.x; pl < ci.npix; pl += gridDim.x * blockDim.x)
+        film_pixel(s, P, 0, ci.npix, pl, ci.samples, clampY, film + 3 * size_t(ci.pixBegin + pl));
+}
+
+} // namespace prb

@@ -117,6 +117,22 @@ class SceneExt(C.Structure):
                 ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("ext", C.c_void_p), ("params", RenderParams), ("outXYZ", C.c_void_p)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("structSize", C.c_uint32), ("wavefrontPaths", C.c_int32), ("shadeBlock", C.c_int32),
+                ("flags", C.c_int32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("pathSamples", C.c_uint64), ("closestRays", C.c_uint64), ("shadowRays", C.c_uint64),
+                ("waves", C.c_uint64), ("loopIterations", C.c_uint64), ("deviceMs", C.c_double),
+                ("hostMs", C.c_double), ("wavefrontPaths", C.c_int32), ("shadeBlock", C.c_int32),
+                ("graphBuilt", C.c_int32), ("tuned", C.c_int32)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("pathSamples", C.c_uint64), ("closestRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("bounces", C.c_uint64), ("kernelLaunches", C.c_uint64), ("deviceMs", C.c_double),
@@ -127,6 +143,7 @@ class RenderStats(C.Structure):
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
 assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 48
+assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72
 assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512
 
 # ---------------------------------------------------------------------------------------------
@@ -160,6 +177,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_list_devices", [_P, C.c_int], C.c_int)
         _bind(lib, "prgpu_render", [C.c_int, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_render_ex", [C.c_int, _P, _P, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_render_batch", [C.c_int, C.c_int32, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_autotune_batch", [C.c_int, C.c_int32, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
                                         _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays_noalloc", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64,

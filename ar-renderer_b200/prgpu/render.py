@@ -69,3 +69,51 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
         e.gridMedia = C.cast(arr, C.c_void_p)
         e._keep.append(arr)
     return e
+
+
+def render_batch(items, config: abi.BatchConfig | None = None, stats: bool = False, device: int = 0):
+    """prgpu_render_batch. items: sequence of (scene, ext or None, RenderParams-like dict, film)
+    where film is a (height, width, 3) float64 C-contiguous array the samples are ADDED to, and
+    the dict holds spp, first_sample, seed, max_depth, clamp. Returns BatchStats when stats."""
+    arr = (abi.BatchItem * len(items))()
+    keep = []
+    for i, (scene, ext, p, film) in enumerate(items):
+        assert film.dtype == np.float64 and film.flags["C_CONTIGUOUS"]
+        arr[i].scene = _desc_ptr(scene).value
+        arr[i].ext = C.addressof(ext) if ext is not None else None
+        arr[i].params = abi.RenderParams(p.get("spp", 1), p.get("first_sample", 0), p.get("seed", 0),
+                                         p.get("max_depth", 0), p.get("clamp", 0.0))
+        arr[i].outXYZ = film.ctypes.data
+        keep.append((scene, ext, film))
+    st = abi.BatchStats()
+    err = abi.err_buf()
+    cfg = C.cast(C.pointer(config), C.c_void_p) if config is not None else None
+    rc = abi.gpu_lib().prgpu_render_batch(device, len(items), C.cast(arr, C.c_void_p), cfg,
+                                          C.cast(C.pointer(st), C.c_void_p), err, len(err))
+    abi.check(rc, err, "prgpu_render_batch")
+    return st if stats else None
+
+
+def batch_config(wavefront_paths: int = 0, shade_block: int = 0) -> abi.BatchConfig:
+    c = abi.BatchConfig()
+    c.structSize = C.sizeof(abi.BatchConfig)
+    c.wavefrontPaths = wavefront_paths
+    c.shadeBlock = shade_block
+    return c
+
+
+def autotune_batch(items, device: int = 0) -> abi.BatchConfig:
+    """prgpu_autotune_batch over the same item tuples as render_batch (films are not touched)."""
+    arr = (abi.BatchItem * len(items))()
+    for i, (scene, ext, p, film) in enumerate(items):
+        arr[i].scene = _desc_ptr(scene).value
+        arr[i].ext = C.addressof(ext) if ext is not None else None
+        arr[i].params = abi.RenderParams(p.get("spp", 1), p.get("first_sample", 0), p.get("seed", 0),
+                                         p.get("max_depth", 0), p.get("clamp", 0.0))
+        arr[i].outXYZ = film.ctypes.data if film is not None else None
+    out = abi.BatchConfig()
+    err = abi.err_buf()
+    rc = abi.gpu_lib().prgpu_autotune_batch(device, len(items), C.cast(arr, C.c_void_p),
+                                            C.cast(C.pointer(out), C.c_void_p), err, len(err))
+    abi.check(rc, err, "prgpu_autotune_batch")
+    return out

@@ -230,6 +230,38 @@ struct SceneExt {
     const GridMediumDesc *gridMedia;
 };
 
+// One render of a batch (prgpu_render_batch): its scene, optional extension, parameters and film.
+struct BatchItem {
+    const SceneDesc *scene;
+    const SceneExt *ext;            // optional (light BVH, grid media); wavefrontPaths/blockSize unused
+    RenderParams params;            // spp, firstSample, seed, maxDepth, clampLuminance of this render
+    double *outXYZ;                 // host film, width * height * 3: samples ADDED in sample order
+};
+
+// Launch settings of a batch. A zero field is filled in by the autotuner (prgpu_autotune_batch),
+// whose choice is cached per device and batch shape.
+struct BatchConfig {
+    uint32_t structSize;            // sizeof(BatchConfig)
+    int32_t wavefrontPaths;         // paths in flight = queue capacity (1,024 .. 2^24)
+    int32_t shadeBlock;             // threads per block of the shading kernel (64, 128, 192 or 256)
+    int32_t flags;                  // reserved, 0
+};
+
+// Counters of one prgpu_render_batch call.
+struct BatchStats {
+    uint64_t pathSamples;           // camera samples traced over all renders
+    uint64_t closestRays;
+    uint64_t shadowRays;
+    uint64_t waves;                 // wavefronts (each a set of chunks, at most one per render)
+    uint64_t loopIterations;        // iterations of the device-side loop (2 bounces each)
+    double deviceMs;                // the graph launch, CUDA events
+    double hostMs;                  // scene residency, scheduling and film copies (wall clock)
+    int32_t wavefrontPaths;         // the settings used
+    int32_t shadeBlock;
+    int32_t graphBuilt;             // 1 when this call had to (re)build the CUDA graph
+    int32_t tuned;                  // 1 when this call ran the autotuner
+};
+
 // Per-call counters and device timings.
 struct RenderStats {
     uint64_t pathSamples;      // camera samples traced
@@ -316,6 +348,21 @@ PRGPU_API int prgpu_accel_status(prgpu_accel accel);
 // Bytes of the converted node and triangle arrays on the device (for roofline accounting).
 PRGPU_API int64_t prgpu_accel_bytes(prgpu_accel accel);
 PRGPU_API void prgpu_accel_destroy(prgpu_accel accel);
+
+// Renders count (1..256) scenes of any size, sample count and path length together: their paths
+// share one set of per-bounce queues in one wavefront, and the whole batch runs as ONE launch of a
+// CUDA graph whose device-side loop (a conditional while node) raygens, traces, shades and films
+// wave after wave with no host round trip. Each film gets exactly the bits prgpu_render_ex would
+// add for that item alone. config may be null (all settings autotuned). No counterpart in the
+// reference, whose host renders one scene per call (src/integrators/gpu_path.cpp:458-509).
+PRGPU_API int prgpu_render_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
+                                 const prgpu::BatchConfig *config, prgpu::BatchStats *stats, char *err, int errLen);
+
+// Times short trial renders of the batch (about 2^24 path samples, films untouched) for every
+// candidate queue capacity and shading block size, caches the fastest for this device and batch
+// shape, and writes it to out.
+PRGPU_API int prgpu_autotune_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
+                                   prgpu::BatchConfig *out, char *err, int errLen);
 
 // Number of kernel launches this library has issued since load (for launch accounting).
 PRGPU_API uint64_t prgpu_launch_count();

@@ -1,0 +1,98 @@
+"""Batched renders (prgpu_render_batch): renders of uneven resolution, sample count and path length
+in one wavefront, run as one CUDA graph launch with a device-side loop. Every path depends only on
+its own (pixel, sample index, seed) stream and each film adds its samples in sample order, so a
+batch must reproduce, bit for bit, what prgpu_render_ex gives for each render alone -- whatever
+the wave packing (small wavefronts force many waves and pixel-range chunks)."""
+
+import numpy as np
+import pytest
+
+import render_util as ru
+from prgpu import abi, hostscene, render, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_batch(oracle):
+    """(scene, ext, params, w, h) for 6 renders: plain, homogeneous medium, grid smoke; sizes from
+    16x16 to 40x24, 3 to 16 spp, depth 4, 8 and unlimited."""
+    out = []
+    specs = [(0, 16, 16, 8, 8, False), (1, 40, 24, 3, 0, True), (2, 32, 32, 16, 4, False),
+             (3, 24, 40, 5, 8, True), (4, 20, 20, 7, 8, False)]
+    for seed, w, h, spp, depth, medium in specs:
+        rs = oracle.RefScene(ru.scene_file(f"batch_{seed}", seed=seed, width=w, height=h, medium=medium))
+        out.append((rs, None, dict(spp=spp, seed=100 + seed, max_depth=depth), w, h))
+    path, s = ru.grid_scene_file("batch_grid", seed=5, width=24, height=24)
+    rs = oracle.RefScene(path)
+    sd, ext = ru.grid_scene_inputs(rs, s)
+    out.append(((rs, sd), ext, dict(spp=6, seed=105, max_depth=8), 24, 24))
+    return out
+
+
+def _desc(scene):
+    if isinstance(scene, tuple):
+        return scene[1]
+    return scene.export()
+
+
+def _alone(batch):
+    films = []
+    for scene, ext, p, w, h in batch:
+        films.append(render.render_ex(_desc(scene), w, h, p["spp"], seed=p["seed"], max_depth=p["max_depth"], ext=ext))
+    return films
+
+
+@pytest.mark.parametrize("capacity", [1024, 1 << 20])
+def test_batch_matches_single_renders_bit_for_bit(gpu, oracle, capacity):
+    batch = _mixed_batch(oracle)
+    ref = _alone(batch)
+    films = [np.zeros((h, w, 3)) for *_, w, h in batch]
+    st = render.render_batch([(_desc(sc), ext, p, f) for (sc, ext, p, _, _), f in zip(batch, films)],
+                             config=render.batch_config(capacity, 128), stats=True)
+    for k, (a, b) in enumerate(zip(films, ref)):
+        assert np.array_equal(a, b), f"render {k} differs (max |d| {np.abs(a - b).max()})"
+    assert st.pathSamples == sum(w * h * p["spp"] for _, _, p, w, h in batch)
+    assert st.waves >= (8 if capacity == 1024 else 1) and st.loopIterations > 0 and st.closestRays > 0
+
+
+def test_batch_adds_onto_films_and_resumes(gpu, oracle):
+    """Films are accumulated onto (read, added to, written back): 3 + 5 samples equal 8."""
+    batch = _mixed_batch(oracle)[:3]
+    full = [np.zeros((h, w, 3)) for *_, w, h in batch]
+    render.render_batch([(_desc(sc), ext, dict(p, spp=8), f) for (sc, ext, p, _, _), f in zip(batch, full)],
+                        config=render.batch_config(4096, 256))
+    part = [np.zeros((h, w, 3)) for *_, w, h in batch]
+    items = [(_desc(sc), ext, dict(p, spp=3), f) for (sc, ext, p, _, _), f in zip(batch, part)]
+    render.render_batch(items, config=render.batch_config(4096, 256))
+    items = [(_desc(sc), ext, dict(p, spp=5, first_sample=3), f) for (sc, ext, p, _, _), f in zip(batch, part)]
+    render.render_batch(items, config=render.batch_config(8192, 128))
+    for a, b in zip(full, part):
+        assert np.array_equal(a, b)
+
+
+def test_autotuner_picks_a_valid_config_and_caches_it(gpu):
+    """Host-built scenes (no reference loader): the tuner times its candidates once per batch
+    shape; render_batch with no config then reuses the choice."""
+    hs = [hostscene.build_box_scene(scenes.box_scene(seed=k, width=32, height=32, medium=bool(k % 2)))
+          for k in range(4)]
+    items = [(h.desc(), None, dict(spp=16, seed=k, max_depth=8), np.zeros((32, 32, 3))) for k, h in enumerate(hs)]
+    cfg = render.autotune_batch(items)
+    assert cfg.wavefrontPaths in (1 << 19, 1 << 20, 1 << 21, 1 << 22) and cfg.shadeBlock in (128, 256)
+    st = render.render_batch(items, stats=True)
+    assert st.tuned == 0 and st.wavefrontPaths == cfg.wavefrontPaths and st.shadeBlock == cfg.shadeBlock
+    for k, (h, _, p, f) in enumerate(items):
+        alone = render.render_ex(h, 32, 32, 16, seed=k, max_depth=8)
+        assert np.array_equal(f, alone)
+
+
+def test_batch_input_validation(gpu):
+    h = hostscene.build_box_scene(scenes.box_scene(seed=0, width=8, height=8))
+    film = np.zeros((8, 8, 3))
+    item = [(h.desc(), None, dict(spp=1), film)]
+    with pytest.raises(abi.PrgpuError, match="shadeBlock"):
+        render.render_batch(item, config=render.batch_config(4096, 100))
+    with pytest.raises(abi.PrgpuError, match="wavefrontPaths"):
+        render.render_batch(item, config=render.batch_config(100, 128))
+    with pytest.raises(abi.PrgpuError, match="batch size"):
+        render.render_batch([], config=render.batch_config(4096, 128))
+    assert not film.any()

@@ -106,10 +106,13 @@ def test_light_bvh_sampling_and_pmf_match_reference(gpu, lightscene):
     # A different light only where u falls within float rounding of a child-selection boundary.
     assert same.mean() > 0.999, same.mean()
     np.testing.assert_allclose(out[same, 1], ref_out[same, 1], rtol=2e-5)
-    # pmfs sum to 1 over the lights; near-zero ones come from importance terms that cancel
-    # (cosines at the edge of a cone), where float rounding alone moves them by ~1e-6.
+    # Near-zero pmfs come from importance terms that cancel (cosines at the edge of a cone), where
+    # float rounding alone moves them by ~1e-6.
     np.testing.assert_allclose(pmf, ref_pmf, rtol=2e-5, atol=5e-6)
-    np.testing.assert_allclose(pmf.sum(1)[pmf.sum(1) > 0], 1.0, rtol=1e-3)
+    # The pmfs sum to at most 1: the sampler gives up (no light) below a node whose two children
+    # both have zero importance (light_bvh.cpp:179-214), and that probability is missing alike.
+    assert pmf.sum(1).max() < 1.0 + 1e-4
+    np.testing.assert_allclose(pmf.sum(1), ref_pmf.sum(1), rtol=1e-4, atol=1e-4)
     # The pmf of the chosen light is the probability it was chosen with.
     np.testing.assert_allclose(out[same & (out[:, 0] >= 0), 1],
                                pmf[same & (out[:, 0] >= 0), out[same & (out[:, 0] >= 0), 0].astype(int)], rtol=2e-5)
