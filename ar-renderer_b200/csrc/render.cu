@@ -20,7 +20,7 @@ constexpr int kBouncesPerPoll = 4;  // bounces enqueued between two host reads o
 
 struct RenderState {
     SceneCache scene;
-    DevBuf pathBuf, shadowBuf, queues, counters, stats, film;
+    DevBuf pathBuf, shadowBuf, queues, classQueues, counters, stats, film;
     int capacity = 0;
     Paths P{};
     Shadows S{};
@@ -68,6 +68,7 @@ void ensure_capacity(RenderState &rs, int cap) {
     rs.S.c = reinterpret_cast<float4 *>(take(cap * sizeof(float4)));
     rs.S.w = reinterpret_cast<float *>(take(cap * sizeof(float)));
     rs.queues.ensure(size_t(2) * cap * sizeof(int));
+    rs.classQueues.ensure(size_t(kClasses) * cap * sizeof(int));
     rs.counters.ensure(kCntSlots * sizeof(int));
     rs.stats.ensure(kStatSlots * sizeof(unsigned long long));
     rs.capacity = cap;
@@ -124,6 +125,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     int *cnt = rs.counters.as<int>();
     auto *dstats = rs.stats.as<unsigned long long>();
     int *qa = rs.queues.as<int>(), *qb = qa + rs.capacity;
+    int *cq = rs.classQueues.as<int>();
     double traceMs = 0, shadeMs = 0, shadowMs = 0, filmMs = 0;
     uint64_t launches = 0;
     const int sph = rs.scene.hasSpheres ? 1 : 0;
@@ -154,8 +156,9 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b], st));
                     if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     else k_extend<false><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
+                    k_classify<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin, cq, rs.capacity);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
-                    ShadeArgs sa{scene, nullptr, rs.P, rs.S, qin, qout, cnt, rp.maxDepth};
+                    ShadeArgs sa{scene, nullptr, rs.P, rs.S, cq, rs.capacity, qout, cnt, rp.maxDepth, 0};
                     k_shade<false><<<gShade, 256, 0, st>>>(sa);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
                     if (scene.hasInterfaces) {
@@ -166,7 +169,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 3], st));
                     k_advance<<<1, 1, 0, st>>>(cnt, dstats);
-                    launches += 4;
+                    launches += 5;
                     std::swap(qin, qout);
                 }
                 PRB_CUDA(cudaGetLastError());
@@ -303,11 +306,13 @@ int render_common(int deviceIndex, const prgpu::SceneDesc *sd, const prgpu::Scen
 // Batched renders (prgpu_render_batch): many scenes in one wavefront, one graph launch
 //
 // The host cuts every render into chunks (a pixel range x a sample range) and packs them into
-// waves of at most `wavefrontPaths` paths, at most one chunk per render per wave, so that one film
+// waves of at most half the path slots, at most one chunk per render per wave, so that one film
 // kernel per wave can add each chunk's samples in sample order with no two chunks touching the same
-// pixel. The device runs the waves from a conditional while node: each iteration raygens the next
-// wave if the previous one is done, advances every live path two bounces, films a wave whose queue
-// ran empty and sets the loop condition.
+// pixel. The device runs the waves from a conditional while node, two waves in flight: wave w
+// lives in slot half w % 2, and as soon as a half is free the next wave is raygenned into it and
+// joins the shared queues while the other wave's longest paths finish. Each iteration raygens (if
+// a wave was started), advances every live path two bounces, films the oldest wave once its half
+// has no live path left, and sets the loop condition. Waves are filmed strictly in order.
 
 struct BatchChunk {
     int render, pixBegin, npix, samples;
@@ -318,7 +323,10 @@ struct BatchWave {
     int firstChunk, nChunks, totalPaths, totalPix;
 };
 struct BatchCtl {
-    int wave, nWaves, phase, iter, maxIter, status;  // phase 1: the next iteration raygens a wave
+    int nWaves, nextWave, filmWave, iter, maxIter, status;
+    int halfWave[2];      // wave occupying each slot half (-1: free)
+    int rgHalf, rgWave;   // wave to raygen at the start of the next iteration (rgHalf -1: none)
+    int halfSlots, pad;
 };
 
 constexpr int kMaxBatch = 256;  // render index in 8 bits of meta.w
@@ -338,62 +346,98 @@ __device__ __forceinline__ int find_chunk(const BatchChunk *c, int lo, int n, in
 __global__ void __launch_bounds__(256) k_batch_raygen(const DevScene *scenes, Paths P, const BatchCtl *ctl,
                                                       const BatchWave *waves, const BatchChunk *chunks, int *counters,
                                                       int *queue) {
-    if (ctl->phase != 1 || ctl->wave >= ctl->nWaves) return;
-    const BatchWave w = waves[ctl->wave];
+    const int half = ctl->rgHalf;
+    if (half < 0) return;
+    const BatchWave w = waves[ctl->rgWave];
+    const int base = half * ctl->halfSlots;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < w.totalPaths; j += gridDim.x * blockDim.x) {
         const BatchChunk &c = chunks[find_chunk(chunks, w.firstChunk, w.nChunks, j, false)];
         int local = j - c.pathBase, sIdx = local / c.npix, pl = local - sIdx * c.npix;
-        raygen_path(scenes[c.render], P, j, c.pixBegin + pl, uint64_t(c.firstSample) + uint64_t(sIdx), c.seed,
+        raygen_path(scenes[c.render], P, base + j, c.pixBegin + pl, uint64_t(c.firstSample) + uint64_t(sIdx), c.seed,
                     c.render, counters, queue);
     }
+}
+
+// The slot half holding the oldest unfilmed wave if none of its paths is left, else -1. The film
+// kernel and the loop control evaluate it on the same state.
+__device__ __forceinline__ int half_to_film(const BatchCtl &c, const int *counters) {
+    for (int h = 0; h < 2; ++h)
+        if (c.halfWave[h] == c.filmWave && c.filmWave < c.nWaves && counters[kCntLive0 + h] == 0) return h;
+    return -1;
 }
 
 __global__ void __launch_bounds__(256) k_batch_film(const DevScene *scenes, Paths P, const BatchCtl *ctl,
                                                     const BatchWave *waves, const BatchChunk *chunks,
                                                     const int *counters) {
-    if (counters[kCntActive] != 0 || ctl->wave >= ctl->nWaves) return;
-    const BatchWave w = waves[ctl->wave];
+    const BatchCtl c = *ctl;
+    const int h = half_to_film(c, counters);
+    if (h < 0) return;
+    const BatchWave w = waves[c.filmWave];
+    const int base = h * c.halfSlots;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < w.totalPix; t += gridDim.x * blockDim.x) {
-        const BatchChunk &c = chunks[find_chunk(chunks, w.firstChunk, w.nChunks, t, true)];
-        const DevScene &s = scenes[c.render];
-        int pl = t - c.pixBase;
-        film_pixel(s, P, c.pathBase, c.npix, pl, c.samples, s.clampY, s.film + 3 * size_t(c.pixBegin + pl));
+        const BatchChunk &ch = chunks[find_chunk(chunks, w.firstChunk, w.nChunks, t, true)];
+        const DevScene &s = scenes[ch.render];
+        int pl = t - ch.pixBase;
+        film_pixel(s, P, base + ch.pathBase, ch.npix, pl, ch.samples, s.clampY, s.film + 3 * size_t(ch.pixBegin + pl));
     }
 }
 
-// Loop control (one thread): next wave once the queue is empty; stop after the last wave, or at
-// the iteration bound (every path ends within 8,192 iterations of the shading guard, so the bound
-// is only reached by a fault in this bookkeeping, reported as status bit 0).
-__global__ void k_batch_ctl(BatchCtl *ctl, const int *counters, cudaGraphConditionalHandle loop) {
+// Loop control (one thread): retire the filmed wave, start the next wave in a free half, stop once
+// the last wave is filmed -- or at the iteration bound (every path ends within 8,192 iterations of
+// the shading guard, so the bound is only reached by a fault in this bookkeeping; status bit 0).
+__global__ void k_batch_ctl(BatchCtl *ctl, const int *counters, cudaGraphConditionalHandle loop, int inGraph) {
     BatchCtl c = *ctl;
     ++c.iter;
-    c.phase = 0;
-    if (counters[kCntActive] == 0) {
-        ++c.wave;
-        c.phase = 1;
+    c.rgHalf = -1;
+    const int h = half_to_film(c, counters);
+    if (h >= 0) {
+        c.halfWave[h] = -1;
+        ++c.filmWave;
     }
-    unsigned more = c.wave < c.nWaves ? 1u : 0u;
+    if (c.nextWave < c.nWaves) {
+        int freeHalf = c.halfWave[0] < 0 ? 0 : (c.halfWave[1] < 0 ? 1 : -1);
+        if (freeHalf >= 0) {
+            c.halfWave[freeHalf] = c.nextWave;
+            c.rgHalf = freeHalf;
+            c.rgWave = c.nextWave;
+            ++c.nextWave;
+        }
+    }
+    unsigned more = c.filmWave < c.nWaves ? 1u : 0u;
     if (more && c.iter >= c.maxIter) {
         c.status |= 1;
         more = 0u;
     }
     *ctl = c;
-    cudaGraphSetConditional(loop, more);
+    if (inGraph) cudaGraphSetConditional(loop, more);
 }
 
-__global__ void k_batch_init(BatchCtl *ctl, int nWaves, int maxIter, int *counters, unsigned long long *stats) {
+__global__ void k_batch_init(BatchCtl *ctl, int nWaves, int maxIter, int halfSlots, int *counters,
+                             unsigned long long *stats) {
     int i = threadIdx.x;
-    if (i == 0) *ctl = BatchCtl{0, nWaves, 1, 0, maxIter, 0};
+    if (i == 0) {
+        BatchCtl c{};
+        c.nWaves = nWaves;
+        c.nextWave = 1;
+        c.filmWave = 0;
+        c.maxIter = maxIter;
+        c.halfWave[0] = 0;
+        c.halfWave[1] = -1;
+        c.rgHalf = 0;
+        c.rgWave = 0;
+        c.halfSlots = halfSlots;
+        *ctl = c;
+    }
     if (i < kCntSlots) counters[i] = 0;
     if (i < kStatSlots) stats[i] = 0ull;
 }
 
 struct BatchGraphKey {
     int capacity = 0, shadeBlock = 0, variant = -1;
-    const void *ptrs[6] = {};
+    const void *ptrs[7] = {};
     bool operator==(const BatchGraphKey &o) const {
         if (capacity != o.capacity || shadeBlock != o.shadeBlock || variant != o.variant) return false;
-        for (int i = 0; i < 6; ++i)
+        for (int i = 0; i < 7; ++i)
             if (ptrs[i] != o.ptrs[i]) return false;
         return true;
     }
@@ -496,37 +540,77 @@ uint64_t batch_shape_key(int device, int count, const prgpu::BatchItem *items) {
     return h;
 }
 
-// Captures the loop body into the while node's body graph and instantiates the graph.
-void build_batch_graph(DeviceState &ds, BatchState &bs, const BatchGraphKey &key, int sph, bool media, bool walls) {
-    if (bs.exec) {
-        cudaGraphExecDestroy(bs.exec);
-        bs.exec = nullptr;
-    }
-    RenderState &rs = bs.paths;
-    cudaStream_t st = ds.stream;
+// Kernel launch shape of the loop body for one batch configuration.
+struct BatchLaunch {
+    void (*extend)(DevScene, const DevScene *, Paths, int *, const int *);
+    void (*shadowAny)(DevScene, const DevScene *, Paths, Shadows, int *);
+    void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, const int *);
+    bool walls;
+    int gExtend, gShadow, gShade, gWide, shadeBlock, capacity;
+};
+
+BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
+    const bool sph = key.variant & 1, media = key.variant & 2;
+    BatchLaunch L{};
+    L.walls = key.variant & 4;
+    L.extend = sph ? k_extend<true, true> : k_extend<false, true>;
+    L.shadowAny = sph ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
+                      : (media ? k_shadow_any<false, true, true> : k_shadow_any<false, false, true>);
+    L.shadowWalk = sph ? k_shadow_walk<true, true> : k_shadow_walk<false, true>;
     const int sms = ds.prop.multiProcessorCount;
-    const int cap = key.capacity, sb = key.shadeBlock;
+    L.gExtend = sms * resident_blocks_of(L.extend);
+    L.gShadow = L.walls ? sms * 8 : sms * resident_blocks_of(L.shadowAny);
+    int perSm = 0;
+    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade<true>, key.shadeBlock, 0));
+    L.gShade = sms * std::max(1, perSm);
+    L.gWide = sms * 8;
+    L.shadeBlock = key.shadeBlock;
+    L.capacity = key.capacity;
+    return L;
+}
+
+// Enqueues one iteration of the batch loop on st (captured into the graph, or launched directly
+// in the host-driven mode); returns the number of kernels.
+int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &L, cudaGraphConditionalHandle loop,
+                            bool inGraph) {
+    RenderState &rs = bs.paths;
     const DevScene *scenes = bs.scenes.as<DevScene>();
     auto *ctl = bs.ctl.as<BatchCtl>();
     const auto *waves = bs.waves.as<BatchWave>();
     const auto *chunks = bs.chunks.as<BatchChunk>();
     int *cnt = rs.counters.as<int>();
     auto *dstats = rs.stats.as<unsigned long long>();
-    int *qa = rs.queues.as<int>(), *qb = qa + cap;
+    int *qa = rs.queues.as<int>(), *qb = qa + L.capacity;
+    int *cq = rs.classQueues.as<int>();
     DevScene none{};
+    int launches = 0;
+    k_batch_raygen<<<L.gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt, qa);
+    ++launches;
+    int *qin = qa, *qout = qb;
+    for (int b = 0; b < 2; ++b) {
+        L.extend<<<L.gExtend, 256, 0, st>>>(none, scenes, rs.P, cnt, qin);
+        k_classify<true><<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, cnt, qin, cq, rs.capacity);
+        ShadeArgs sa{none, scenes, rs.P, rs.S, cq, rs.capacity, qout, cnt, 0, L.capacity / 2};
+        k_shade<true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+        if (L.walls) L.shadowWalk<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        else L.shadowAny<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        k_advance<<<1, 1, 0, st>>>(cnt, dstats);
+        launches += 5;
+        std::swap(qin, qout);
+    }
+    k_batch_film<<<L.gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt);
+    k_batch_ctl<<<1, 1, 0, st>>>(ctl, cnt, loop, inGraph ? 1 : 0);
+    return launches + 2;
+}
 
-    auto extendFn = sph ? k_extend<true, true> : k_extend<false, true>;
-    using ShadowFn = void (*)(DevScene, const DevScene *, Paths, Shadows, int *);
-    ShadowFn anyFn = sph ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
-                         : (media ? k_shadow_any<false, true, true> : k_shadow_any<false, false, true>);
-    auto walkFn = sph ? k_shadow_walk<true, true> : k_shadow_walk<false, true>;
-    const int gExtend = sms * resident_blocks_of(extendFn);
-    const int gShadow = walls ? sms * 8 : sms * resident_blocks_of(anyFn);
-    int perSm = 0;
-    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade<true>, sb, 0));
-    const int gShade = sms * std::max(1, perSm);
-    const int gWide = sms * 8;
-
+// Captures the loop body into the while node's body graph and instantiates the graph.
+void build_batch_graph(DeviceState &ds, BatchState &bs, const BatchGraphKey &key) {
+    if (bs.exec) {
+        cudaGraphExecDestroy(bs.exec);
+        bs.exec = nullptr;
+    }
+    const BatchLaunch L = batch_launch(ds, key);
+    cudaStream_t st = ds.stream;
     cudaGraph_t g = nullptr;
     PRB_CUDA(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle loop;
@@ -540,23 +624,7 @@ void build_batch_graph(DeviceState &ds, BatchState &bs, const BatchGraphKey &key
     PRB_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &np));
     cudaGraph_t body = np.conditional.phGraph_out[0];
     PRB_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int64_t launches = 0;
-    k_batch_raygen<<<gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt, qa);
-    ++launches;
-    int *qin = qa, *qout = qb;
-    for (int b = 0; b < 2; ++b) {
-        extendFn<<<gExtend, 256, 0, st>>>(none, scenes, rs.P, cnt, qin);
-        ShadeArgs sa{none, scenes, rs.P, rs.S, qin, qout, cnt, 0};
-        k_shade<true><<<gShade, sb, 0, st>>>(sa);
-        if (walls) walkFn<<<gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
-        else anyFn<<<gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
-        k_advance<<<1, 1, 0, st>>>(cnt, dstats);
-        launches += 4;
-        std::swap(qin, qout);
-    }
-    k_batch_film<<<gWide, 256, 0, st>>>(scenes, rs.P, ctl, waves, chunks, cnt);
-    k_batch_ctl<<<1, 1, 0, st>>>(ctl, cnt, loop);
-    launches += 2;
+    int launches = enqueue_batch_iteration(st, bs, L, loop, true);
     cudaGraph_t captured = nullptr;
     cudaError_t ce = cudaStreamEndCapture(st, &captured);
     if (ce != cudaSuccess) {
@@ -573,7 +641,7 @@ void build_batch_graph(DeviceState &ds, BatchState &bs, const BatchGraphKey &key
 // One batch render with the given settings. trial: films start at zero on the device and are
 // not copied back (autotuning). Returns false with a message on invalid input.
 bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchItem *items, int capacity, int shadeBlock,
-               bool trial, int sppDivisor, prgpu::BatchStats *stats, std::string *err) {
+               bool hostLoop, bool trial, int sppDivisor, prgpu::BatchStats *stats, std::string *err) {
     auto tHost0 = std::chrono::steady_clock::now();
     cudaStream_t st = ds.stream;
     if (int(bs.caches.size()) < count) bs.caches.resize(size_t(count));
@@ -604,7 +672,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     }
     std::vector<BatchChunk> chunks;
     std::vector<BatchWave> waves;
-    schedule_waves(npix, spp, capacity, rp, &chunks, &waves);
+    schedule_waves(npix, spp, capacity / 2, rp, &chunks, &waves);
     ensure_capacity(bs.paths, capacity);
     bs.films.ensure(std::max<size_t>(1, filmTotal) * sizeof(double));
     bs.scenes.ensure(size_t(count) * sizeof(DevScene));
@@ -640,23 +708,44 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     key.ptrs[3] = bs.chunks.ptr;
     key.ptrs[4] = bs.waves.ptr;
     key.ptrs[5] = bs.paths.queues.ptr;
+    key.ptrs[6] = bs.paths.classQueues.ptr;
     bool built = false;
-    if (!bs.exec || !(bs.key == key)) {
+    if (!hostLoop && (!bs.exec || !(bs.key == key))) {
         PRB_CUDA(cudaStreamSynchronize(st));
-        build_batch_graph(ds, bs, key, sph, media, walls);
+        build_batch_graph(ds, bs, key);
         built = true;
     }
     const int nWaves = int(waves.size());
     const int maxIter = int(std::min<int64_t>(int64_t(nWaves) * 4200 + 16, int64_t(1) << 30));
+    const int halfSlots = capacity / 2;
     float ms = 0.f;
     int64_t launches = 0;
     BatchCtl hc{};
     unsigned long long hs[kStatSlots] = {};
     if (nWaves > 0) {
-        k_batch_init<<<1, 32, 0, st>>>(bs.ctl.as<BatchCtl>(), nWaves, maxIter, bs.paths.counters.as<int>(),
+        k_batch_init<<<1, 32, 0, st>>>(bs.ctl.as<BatchCtl>(), nWaves, maxIter, halfSlots, bs.paths.counters.as<int>(),
                                        bs.paths.stats.as<unsigned long long>());
         PRB_CUDA(cudaEventRecord(bs.ev[0], st));
-        PRB_CUDA(cudaGraphLaunch(bs.exec, st));
+        if (!hostLoop) {
+            PRB_CUDA(cudaGraphLaunch(bs.exec, st));
+        } else {
+            // Host-driven mode (tools that cannot see inside conditional graphs, e.g. profilers):
+            // the same iteration launched directly, the host reading the loop state each time.
+            const BatchLaunch L = batch_launch(ds, key);
+            BatchCtl *hctl = nullptr;
+            PRB_CUDA(cudaMallocHost(&hctl, sizeof(BatchCtl)));
+            int iters = 0;
+            int perIter = 0;
+            for (;;) {
+                perIter = enqueue_batch_iteration(st, bs, L, 0, false);
+                ++iters;
+                PRB_CUDA(cudaMemcpyAsync(hctl, bs.ctl.ptr, sizeof(BatchCtl), cudaMemcpyDeviceToHost, st));
+                PRB_CUDA(cudaStreamSynchronize(st));
+                if (hctl->filmWave >= hctl->nWaves || (hctl->status & 1) || iters >= maxIter) break;
+            }
+            cudaFreeHost(hctl);
+            bs.launchesPerIteration = perIter;
+        }
         PRB_CUDA(cudaEventRecord(bs.ev[1], st));
         PRB_CUDA(cudaMemcpyAsync(&hc, bs.ctl.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
         PRB_CUDA(cudaMemcpyAsync(hs, bs.paths.stats.ptr, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -744,17 +833,17 @@ std::pair<int, int> autotune(DeviceState &ds, BatchState &bs, int count, const p
     int div = int(std::max<uint64_t>(1, total / (uint64_t(1) << 24)));
     size_t freeB = 0, totalB = 0;
     PRB_CUDA(cudaMemGetInfo(&freeB, &totalB));
-    const int caps[] = {1 << 19, 1 << 20, 1 << 21, 1 << 22};
+    const int caps[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
     const int blocks[] = {128, 256};
     double best = 1e300;
-    std::pair<int, int> choice{1 << 21, 256};
+    std::pair<int, int> choice{1 << 22, 256};
     for (int cap : caps) {
         if (size_t(cap) * 512 > freeB / 2) continue;
         for (int sb : blocks) {
             double t = 1e300;
             for (int rep = 0; rep < 3; ++rep) {
                 prgpu::BatchStats s{};
-                if (!run_batch(ds, bs, count, items, cap, sb, true, div, &s, err)) return choice;
+                if (!run_batch(ds, bs, count, items, cap, sb, false, true, div, &s, err)) return choice;
                 if (rep > 0 && s.pathSamples > 0) t = std::min(t, s.deviceMs / double(s.pathSamples));
             }
             if (t < best) {
@@ -778,6 +867,10 @@ int batch_common(int deviceIndex, int32_t count, const prgpu::BatchItem *items, 
         }
         if (config && config->structSize != sizeof(prgpu::BatchConfig)) {
             set_err(err, errLen, "BatchConfig size mismatch");
+            return 1;
+        }
+        if (config && (config->flags & ~1)) {
+            set_err(err, errLen, "unknown BatchConfig flags");
             return 1;
         }
         int cap = config ? config->wavefrontPaths : 0, sb = config ? config->shadeBlock : 0;
@@ -820,7 +913,7 @@ int batch_common(int deviceIndex, int32_t count, const prgpu::BatchItem *items, 
             }
         }
         if (stats) *stats = prgpu::BatchStats{};
-        if (!run_batch(ds, bs, count, items, cap, sb, false, 1, stats, &e)) {
+        if (!run_batch(ds, bs, count, items, cap, sb, config && (config->flags & 1), false, 1, stats, &e)) {
             set_err(err, errLen, e);
             return 1;
         }

@@ -153,6 +153,15 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         cudaStream_t s = ds.stream;
         cache.accel.upload(h, s);
         put(cache.prims, sd->prims, size_t(sd->primCount), s);
+        std::vector<uint8_t> cls(size_t(std::max(1, sd->primCount)), uint8_t(kClassOther));
+        for (int32_t i = 0; i < sd->primCount; ++i) {
+            uint32_t t = sd->materials[sd->prims[i].material].type;
+            cls[size_t(i)] = uint8_t(t == prgpu::MatDiffuse      ? kClassDiffuse
+                                     : t == prgpu::MatConductor  ? kClassConductor
+                                     : t == prgpu::MatDielectric ? kClassDielectric
+                                                                 : kClassOther);
+        }
+        put(cache.primClass, cls.data(), cls.size(), s);
         put(cache.mats, sd->materials, size_t(sd->materialCount), s);
         put(cache.lights, sd->lights, size_t(sd->lightCount), s);
         put(cache.spectra, sd->spectra, size_t(sd->spectrumCount), s);
@@ -212,6 +221,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         d.leaves = cache.accel.prims.as<LeafPrim>();
         d.root = cache.accel.root;
         d.prims = cache.prims.as<prgpu::Primitive>();
+        d.primClass = cache.primClass.as<uint8_t>();
         d.mats = cache.mats.as<prgpu::Material>();
         d.lights = cache.lights.as<prgpu::Light>();
         d.spectra = cache.spectra.as<float>();

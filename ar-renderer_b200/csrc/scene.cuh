@@ -25,11 +25,24 @@ struct DevGrid {
     const float *density;
 };
 
+// Shading classes: the closest-hit kernel files every finished path under one of these, and the
+// shading kernel walks the classes in order, so a warp mostly runs one material's code.
+enum ShadeClass : int {
+    kClassMiss = 0,        // escaped, not in a medium
+    kClassDiffuse = 1,
+    kClassConductor = 2,
+    kClassDielectric = 3,  // smooth, rough or thin
+    kClassOther = 4,       // interfaces, black and anything else
+    kClassMedium = 5,      // the path is inside a medium (free flight first)
+    kClasses = 6
+};
+
 struct DevScene {
     const WNode *nodes;
     const LeafPrim *leaves;
     RootInfo root;
     const prgpu::Primitive *prims;
+    const uint8_t *primClass;    // shading class of each primitive's material (ShadeClass)
     const prgpu::Material *mats;
     const prgpu::Light *lights;
     int lightCount;
@@ -65,13 +78,14 @@ struct SceneCache {
     uint64_t key = 0;
     bool valid = false;
     DeviceAccel accel;
-    DevBuf prims, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData;
+    DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData;
     DevScene ds{};
     bool hasSpheres = false;
     int64_t deviceBytes = 0;
     void release() {
         accel.release();
         prims.release();
+        primClass.release();
         mats.release();
         lights.release();
         spectra.release();

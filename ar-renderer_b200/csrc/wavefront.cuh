@@ -59,7 +59,12 @@ struct Shadows {
 // Device counters of one wavefront: queue lengths, the persistent kernels' work counters, status.
 enum {
     kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
-    kCntSlots = 8
+    // Batched form: live paths per half of the path slots after the last bounce, and the
+    // survivors being counted during the current one.
+    kCntLive0 = 8, kCntLive1 = 9, kCntNextLive0 = 10, kCntNextLive1 = 11,
+    // Paths filed per shading class by the closest-hit kernel (kClasses entries).
+    kCntClass0 = 16,
+    kCntSlots = 24
 };
 enum { kStatusStack = 1, kStatusGuard = 2 };
 // Device statistics (64-bit): closest-hit rays, shadow rays, non-empty bounces.
@@ -445,6 +450,37 @@ __global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo c
     }
 }
 
+// Material sort: files every queued path under its shading class (ShadeClass), 256 paths per block
+// step: ranks from shared-memory counters, one global atomic per class and block for the block's
+// slots, so the shading kernel can walk the classes in order. The order within a class does not
+// matter: every path's update depends on its own state only.
+template <bool kBatch = false>
+__global__ void __launch_bounds__(256) k_classify(DevScene s0, const DevScene *scenes, Paths P, int *counters,
+                                                  const int *queue, int *classQ, int classCap) {
+    __shared__ int hist[kClasses], base[kClasses];
+    const int n = counters[kCntActive];
+    for (int q0 = blockIdx.x * blockDim.x; q0 < n; q0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < kClasses) hist[threadIdx.x] = 0;
+        __syncthreads();
+        const int q = q0 + threadIdx.x;
+        int c = -1, j = 0, rank = 0;
+        if (q < n) {
+            j = queue[q];
+            const int4 mt = P.meta[j];
+            const int prim = __float_as_int(P.hit[j].w);
+            const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(mt.w));
+            c = mt.z >= 0 ? kClassMedium : (prim < 0 ? kClassMiss : int(__ldg(s.primClass + prim)));
+            rank = atomicAdd(&hist[c], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < kClasses)
+            base[threadIdx.x] = hist[threadIdx.x] ? atomicAdd(counters + kCntClass0 + threadIdx.x, hist[threadIdx.x]) : 0;
+        __syncthreads();
+        if (c >= 0) classQ[size_t(c) * classCap + base[c] + rank] = j;
+        __syncthreads();
+    }
+}
+
 // Closest hit for every queued path, by persistent warps whose finished lanes take the next
 // queue entry at once (see k_trace_persist in accel.cu): bounce rays are incoherent and end
 // after very different numbers of steps.
@@ -510,19 +546,33 @@ struct ShadeArgs {
     const DevScene *scenes;  // batched form: the renders' scenes, indexed by path_render
     Paths P;
     Shadows S;
-    const int *queueIn;
+    const int *classQ;       // the closest-hit kernel's per-class queues (kClasses x classCap)
+    int classCap;
     int *queueOut;
     int *counters;
     int maxDepth;
+    int halfSlots;           // batched form: slots [0, halfSlots) are half 0, the rest half 1
 };
 
 // One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
 template <bool kBatch = false>
 __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
-    int n = a.counters[kCntActive];
+    // The classes laid end to end: entry q belongs to the class whose prefix range holds it.
+    int start[kClasses + 1];
+    start[0] = 0;
+#pragma unroll
+    for (int c = 0; c < kClasses; ++c) start[c + 1] = start[c] + a.counters[kCntClass0 + c];
+    const int n = start[kClasses];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int j = a.queueIn[q];
+        int c = 0, first = 0;
+#pragma unroll
+        for (int k = 1; k < kClasses; ++k)
+            if (q >= start[k]) {
+                c = k;
+                first = start[k];
+            }
+        int j = a.classQ[size_t(c) * a.classCap + (q - first)];
         int4 meta = P.meta[j];
         const DevScene &s = SceneOf<kBatch>::get(a.s, a.scenes, path_render(meta.w));
         const int maxDepth = kBatch ? s.maxDepth : a.maxDepth;
@@ -756,6 +806,15 @@ __global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
             P.prevP[j] = make_float4(prevP.x, prevP.y, prevP.z, pp4.w);
             P.prevN[j] = make_float4(prevN.x, prevN.y, prevN.z, __int_as_float(iters));
             a.queueOut[warp_append(a.counters + kCntNext)] = j;
+            if (kBatch) {
+                // Survivors per slot half (warp-aggregated): the batch loop films a wave once its
+                // half has none left.
+                unsigned m = __activemask(), m1 = __ballot_sync(m, j >= a.halfSlots);
+                if ((threadIdx.x & 31) == __ffs(m) - 1) {
+                    if (m1) atomicAdd(a.counters + kCntNextLive1, __popc(m1));
+                    if (m & ~m1) atomicAdd(a.counters + kCntNextLive0, __popc(m & ~m1));
+                }
+            }
         }
     }
 }
@@ -842,9 +901,15 @@ __global__ void k_advance(int *counters, unsigned long long *stats) {
     stats[kStatBounces] += counters[kCntActive] > 0 ? 1ull : 0ull;
     counters[kCntActive] = counters[kCntNext];
     counters[kCntNext] = 0;
+    counters[kCntLive0] = counters[kCntNextLive0];
+    counters[kCntLive1] = counters[kCntNextLive1];
+    counters[kCntNextLive0] = 0;
+    counters[kCntNextLive1] = 0;
     counters[kCntShadow] = 0;
     counters[kCntExtendWork] = 0;
     counters[kCntShadowWork] = 0;
+#pragma unroll
+    for (int c = 0; c < kClasses; ++c) counters[kCntClass0 + c] = 0;
 }
 
 // Visibility of queued NEE samples in scenes with medium interfaces: a walk through the boundary

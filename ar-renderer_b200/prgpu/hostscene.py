@@ -18,7 +18,8 @@ from . import abi, scenes, spectra, trace
 
 class HostScene:
     def __init__(self):
-        self.prims = []
+        self.prims = []  # per-mesh Primitive arrays
+        self._prim_count = 0
         self.materials = []
         self.lights = []
         self.spectra = []
@@ -57,31 +58,34 @@ class HostScene:
              medium_inside=-1, medium_outside=-1):
         p = np.asarray(positions, np.float32).reshape(-1, 3)
         n = None if normals is None else np.asarray(normals, np.float32).reshape(-1, 3)
-        for tri in np.asarray(indices, np.int64).reshape(-1, 3):
-            r = np.zeros(1, abi.PRIMITIVE)[0]
-            r["type"] = abi.PRIM_TRIANGLE
-            r["material"] = material
-            r["light"] = -1
-            r["mediumInside"], r["mediumOutside"] = medium_inside, medium_outside
-            r["p0"], r["p1"], r["p2"] = p[tri[0]], p[tri[1]], p[tri[2]]
-            if n is not None:
-                r["n0"], r["n1"], r["n2"] = n[tri[0]], n[tri[1]], n[tri[2]]
-            r["uv"] = [0, 0, 1, 0, 1, 1]
-            if light_spectrum >= 0:
-                area = 0.5 * np.linalg.norm(np.cross(p[tri[1]] - p[tri[0]], p[tri[2]] - p[tri[0]]))
+        tri = np.asarray(indices, np.int64).reshape(-1, 3)
+        base = self._prim_count
+        r = np.zeros(len(tri), abi.PRIMITIVE)
+        r["type"] = abi.PRIM_TRIANGLE
+        r["material"] = material
+        r["light"] = -1
+        r["mediumInside"], r["mediumOutside"] = medium_inside, medium_outside
+        r["p0"], r["p1"], r["p2"] = p[tri[:, 0]], p[tri[:, 1]], p[tri[:, 2]]
+        if n is not None:
+            r["n0"], r["n1"], r["n2"] = n[tri[:, 0]], n[tri[:, 1]], n[tri[:, 2]]
+        r["uv"] = [0, 0, 1, 0, 1, 1]
+        if light_spectrum >= 0:
+            for k in range(len(tri)):
+                a, b_, c = p[tri[k, 0]], p[tri[k, 1]], p[tri[k, 2]]
                 l = np.zeros(1, abi.LIGHT)[0]
                 l["type"] = abi.LIGHT_AREA
-                l["primitive"] = len(self.prims)
+                l["primitive"] = base + k
                 l["spectrum"] = light_spectrum
                 l["scale"] = light_scale
-                l["area"] = area
-                r["light"] = len(self.lights)
+                l["area"] = 0.5 * np.linalg.norm(np.cross(b_ - a, c - a))
+                r[k]["light"] = len(self.lights)
                 self.lights.append(l)
-            self.prims.append(r)
+        self.prims.append(r)
+        self._prim_count += len(tri)
 
     # -- finalisation ---------------------------------------------------------------------
     def finish(self, cam_pos, cam_target, fov_y, width, height, max_leaf=2):
-        self.prim_array = np.array(self.prims, dtype=abi.PRIMITIVE)
+        self.prim_array = np.concatenate(self.prims) if self.prims else np.zeros(0, abi.PRIMITIVE)
         self.mat_array = np.array(self.materials, dtype=abi.MATERIAL)
         self.spec_array = np.ascontiguousarray(np.stack(self.spectra).astype(np.float32))
         self.media_array = np.array(self.media, dtype=abi.MEDIUM) if self.media else np.zeros(1, abi.MEDIUM)

@@ -94,11 +94,13 @@ def render_batch(items, config: abi.BatchConfig | None = None, stats: bool = Fal
     return st if stats else None
 
 
-def batch_config(wavefront_paths: int = 0, shade_block: int = 0) -> abi.BatchConfig:
+def batch_config(wavefront_paths: int = 0, shade_block: int = 0, host_loop: bool = False) -> abi.BatchConfig:
+    """BatchConfig; zero settings are autotuned. host_loop: the loop driven from the host (profiling)."""
     c = abi.BatchConfig()
     c.structSize = C.sizeof(abi.BatchConfig)
     c.wavefrontPaths = wavefront_paths
     c.shadeBlock = shade_block
+    c.flags = 1 if host_loop else 0
     return c
 
 

@@ -14,6 +14,7 @@ path length.
 
 from __future__ import annotations
 
+import functools
 import json
 import math
 import os
@@ -22,8 +23,21 @@ from dataclasses import dataclass, field
 import numpy as np
 
 
+@functools.lru_cache(maxsize=8)
+def _icosphere(subdiv: int):
+    v, f = _icosphere_build(subdiv)
+    v.setflags(write=False)
+    f.setflags(write=False)
+    return v, f
+
+
 def icosphere(subdiv: int):
     """Unit icosphere: (vertices (n, 3) float64, faces (m, 3) int32), counter-clockwise outward."""
+    v, f = _icosphere(subdiv)
+    return v.copy(), f.copy()
+
+
+def _icosphere_build(subdiv: int):
     t = (1.0 + 5 ** 0.5) / 2.0
     v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
          (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
@@ -109,6 +123,21 @@ def box_scene(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64,
         s.medium = {"sigma_s": [float(x) for x in rng.uniform(0.05, 0.5, 3)],
                     "sigma_a": [float(x) for x in rng.uniform(0.0, 0.1, 3)], "g": 0.6}
     return s
+
+
+def uneven_batch(count: int = 48, seed: int = 4242) -> list:
+    """The uneven batch: `count` renders of the box family, scene seeds 0..count-1, each with a
+    resolution drawn uniformly from {128, 256, 512, 1024}^2, spp from {16, 64, 256} and max depth
+    from {8, 16, 32} (seeded draws); even scene seeds fill the box with the homogeneous chromatic
+    medium of box_scene(medium=True)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = int(rng.choice([16, 64, 256]))
+        depth = int(rng.choice([8, 16, 32]))
+        out.append(box_scene(seed=k, width=res, height=res, spp=spp, max_depth=depth, medium=(k % 2 == 0)))
+    return out
 
 
 def smoke_density(res: int = 24, seed: int = 0) -> np.ndarray:

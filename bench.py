@@ -185,6 +185,70 @@ def path_tracer_bench(args, device: int, cpu: bool):
     return out
 
 
+def batch_bench(args, device: int, cpu: bool):
+    """The uneven batch: 48 renders of the box family (scene seeds 0..47; resolution uniform over
+    {128,256,512,1024}^2, spp over {16,64,256}, depth over {8,16,32}; even seeds with the chromatic
+    homogeneous medium) rendered by ONE prgpu_render_batch call -- one CUDA graph launch whose
+    device-side loop runs every wave -- with the autotuner's queue capacity and shading block.
+    value = path samples/s of the graph's device time; e2e = the same over the whole call (film
+    copies in and out, scene residency checks, scheduling)."""
+    from prgpu import hostscene, render, scenes
+
+    specs = scenes.uneven_batch(48)
+    t0 = time.perf_counter()
+    hosts = [hostscene.build_box_scene(s) for s in specs]
+    build_s = time.perf_counter() - t0
+    films = [np.zeros((s.height, s.width, 3)) for s in specs]
+    div = max(1, args.batch_spp_div)
+    items = [(h.desc(), None, dict(spp=max(1, s.spp // div), seed=1, max_depth=s.max_depth), f)
+             for h, s, f in zip(hosts, specs, films)]
+    t0 = time.perf_counter()
+    cfg = render.autotune_batch(items)
+    tune_s = time.perf_counter() - t0
+    bcfg = render.batch_config(cfg.wavefrontPaths, cfg.shadeBlock, host_loop=args.batch_host_loop)
+    for _ in range(args.batch_warmup):
+        render.render_batch(items, config=bcfg)
+    dev, wall, st = [], [], None
+    for k in range(args.batch_steps):
+        step = [(d, e, dict(p, first_sample=(k + 1) * p["spp"]), f) for d, e, p, f in items]
+        t0 = time.perf_counter()
+        st = render.render_batch(step, config=bcfg, stats=True)
+        wall.append(time.perf_counter() - t0)
+        dev.append(st.deviceMs)
+    samples = int(st.pathSamples)
+    film_bytes = int(sum(f.nbytes for f in films))
+    out = {
+        "workload": "uneven batch: 48 box-family renders, 128^2..1024^2, 16..256 spp, depth 8..32, half with media",
+        "metric": "path samples/s", "value": samples / (statistics.mean(dev) * 1e-3), "unit": "path samples/s",
+        "ms_per_step": statistics.mean(dev), "steps": args.batch_steps, "warmup": args.batch_warmup,
+        "path_samples_per_step": samples, "spp_divided_by": div, "waves": int(st.waves), "loop_iterations": int(st.loopIterations),
+        "graph_launches_per_step": 0 if args.batch_host_loop else 1, "kernel_nodes_per_iteration": 14,
+        "autotuned": {"wavefrontPaths": cfg.wavefrontPaths, "shadeBlock": cfg.shadeBlock, "seconds": tune_s},
+        "host_scene_build_s": build_s,
+        "rays_per_step": {"closest": int(st.closestRays), "shadow": int(st.shadowRays)},
+        "e2e": {"value": samples / statistics.mean(wall), "unit": "path samples/s",
+                "h2d_bytes_per_step": film_bytes, "d2h_bytes_per_step": film_bytes},
+    }
+    if cpu:
+        import ref
+
+        ref.set_threads(0)
+        tot, secs = 0, 0.0
+        for k in (0, 1):
+            s = specs[k]
+            jp = os.path.join(tempfile.gettempdir(), "prb_bench", f"batch_{k}.prscene.json")
+            rs = ref.RefScene(scenes.write_reference_json(s, jp))
+            cspp = 2
+            _, dt = rs.render(cspp, 1, s.max_depth)
+            tot += s.width * s.height * cspp
+            secs += dt
+        out["cpu_baseline"] = {"value": tot / secs, "unit": "path samples/s", "cores": ref.thread_count(),
+                               "kind": "reference",
+                               "sample": f"reference PathIntegrator on batch scenes 0 (medium) and 1 (plain) at their "
+                                         f"resolutions, 2 spp each ({secs:.1f} s)"}
+    return out
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -238,6 +302,15 @@ def main():
     ap.add_argument("--path-tracer-only", action="store_true",
                     help="run only the path-tracer workload and print its JSON object (profiling captures)")
     ap.add_argument("--pt-res", type=int, default=256, help="path-tracer image side (256 = the measured workload)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the uneven-batch workload")
+    ap.add_argument("--batch-only", action="store_true", help="run only the uneven batch and print its JSON object")
+    ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--batch-warmup", type=int, default=1)
+    ap.add_argument("--batch-host-loop", action="store_true",
+                    help="drive the batch loop from the host (profiling captures: ncu cannot see inside "
+                         "conditional graphs)")
+    ap.add_argument("--batch-spp-div", type=int, default=1,
+                    help="divide every render's spp (profiling captures only; the JSON says so)")
     args = ap.parse_args()
     N_RAYS = args.rays
     args.warmup = max(args.warmup, 3)
@@ -249,6 +322,9 @@ def main():
         return run_reference_arm(args, rank, world)
     if args.path_tracer_only:
         print(json.dumps(path_tracer_bench(args, local, cpu=not args.no_cpu_baseline)))
+        return
+    if args.batch_only:
+        print(json.dumps(batch_bench(args, local, cpu=not args.no_cpu_baseline)))
         return
 
     import torch
@@ -350,6 +426,9 @@ def main():
     pt = None
     if world == 1 and not args.no_path_tracer:
         pt = path_tracer_bench(args, local, cpu=not args.no_cpu_baseline)
+    bt = None
+    if world == 1 and not args.no_batch:
+        bt = batch_bench(args, local, cpu=not args.no_cpu_baseline)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -374,6 +453,7 @@ def main():
         "closest_hit_mrays": N_RAYS / (closest_ms * 1e3),
         "any_hit_mrays": N_RAYS / ((ms_per_step - closest_ms) * 1e3),
         "path_tracer": pt,
+        "uneven_batch": bt,
     }
     print(json.dumps(line), flush=True)
 

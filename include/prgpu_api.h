@@ -244,7 +244,9 @@ struct BatchConfig {
     uint32_t structSize;            // sizeof(BatchConfig)
     int32_t wavefrontPaths;         // paths in flight = queue capacity (1,024 .. 2^24)
     int32_t shadeBlock;             // threads per block of the shading kernel (64, 128, 192 or 256)
-    int32_t flags;                  // reserved, 0
+    int32_t flags;                  // bit 0: drive the loop from the host, one synchronisation per
+                                    // iteration, instead of the graph (for profilers, which cannot
+                                    // see inside conditional graphs); other bits 0
 };
 
 // Counters of one prgpu_render_batch call.

@@ -55,6 +55,18 @@ def test_batch_matches_single_renders_bit_for_bit(gpu, oracle, capacity):
     assert st.waves >= (8 if capacity == 1024 else 1) and st.loopIterations > 0 and st.closestRays > 0
 
 
+def test_host_driven_loop_gives_the_same_films(gpu, oracle):
+    """The host-driven mode (no graph; for profilers) runs the same iteration kernels."""
+    batch = _mixed_batch(oracle)[:4]
+    ref = _alone(batch)
+    films = [np.zeros((h, w, 3)) for *_, w, h in batch]
+    st = render.render_batch([(_desc(sc), ext, p, f) for (sc, ext, p, _, _), f in zip(batch, films)],
+                             config=render.batch_config(2048, 256, host_loop=True), stats=True)
+    assert st.graphBuilt == 0
+    for a, b in zip(films, ref):
+        assert np.array_equal(a, b)
+
+
 def test_batch_adds_onto_films_and_resumes(gpu, oracle):
     """Films are accumulated onto (read, added to, written back): 3 + 5 samples equal 8."""
     batch = _mixed_batch(oracle)[:3]
@@ -77,7 +89,7 @@ def test_autotuner_picks_a_valid_config_and_caches_it(gpu):
           for k in range(4)]
     items = [(h.desc(), None, dict(spp=16, seed=k, max_depth=8), np.zeros((32, 32, 3))) for k, h in enumerate(hs)]
     cfg = render.autotune_batch(items)
-    assert cfg.wavefrontPaths in (1 << 19, 1 << 20, 1 << 21, 1 << 22) and cfg.shadeBlock in (128, 256)
+    assert cfg.wavefrontPaths in (1 << 20, 1 << 21, 1 << 22, 1 << 23) and cfg.shadeBlock in (128, 256)
     st = render.render_batch(items, stats=True)
     assert st.tuned == 0 and st.wavefrontPaths == cfg.wavefrontPaths and st.shadeBlock == cfg.shadeBlock
     for k, (h, _, p, f) in enumerate(items):
