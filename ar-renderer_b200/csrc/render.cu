@@ -466,8 +466,10 @@ BatchState &batch_state(int device) {
     return *p;
 }
 
-// Packs the renders into waves (see the section comment). Chunks of one render follow its sample
-// order: whole frames of S samples while a frame fits the share, else pixel ranges of one sample.
+// Packs the renders into waves (see the section comment), render-major: a wave takes the renders
+// in index order, each as much as the remaining budget allows, so a wave touches few scenes and
+// their BVHs stay in L2. Chunks of one render follow its sample order: whole frames of S samples
+// while a frame fits the budget, else pixel ranges of one sample.
 void schedule_waves(const std::vector<int64_t> &npix, const std::vector<int> &spp, int capacity,
                     const std::vector<prgpu::RenderParams> &rp, std::vector<BatchChunk> *chunks,
                     std::vector<BatchWave> *waves) {
@@ -477,34 +479,29 @@ void schedule_waves(const std::vector<int64_t> &npix, const std::vector<int> &sp
     auto remaining = [&](int r) {
         return (int64_t(spp[size_t(r)]) - nextSample[size_t(r)]) * npix[size_t(r)] - nextPix[size_t(r)];
     };
-    std::vector<int> order;
+    int first = 0;
     for (;;) {
-        order.clear();
-        for (int r = 0; r < n; ++r)
-            if (npix[size_t(r)] > 0 && remaining(r) > 0) order.push_back(r);
-        if (order.empty()) break;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return remaining(a) < remaining(b); });
+        while (first < n && remaining(first) <= 0) ++first;
+        if (first >= n) break;
         BatchWave w{int(chunks->size()), 0, 0, 0};
         int64_t budget = capacity;
-        for (size_t k = 0; k < order.size() && budget > 0; ++k) {
-            int r = order[k];
-            int64_t share = budget / int64_t(order.size() - k);
-            if (share < 1) continue;
+        for (int r = first; r < n && budget > 0; ++r) {
+            if (remaining(r) <= 0) continue;
             BatchChunk c{};
             c.render = r;
             c.seed = rp[size_t(r)].seed;
             const int64_t np = npix[size_t(r)];
             int64_t &pix = nextPix[size_t(r)];
             int &smp = nextSample[size_t(r)];
-            if (pix == 0 && np <= share) {
-                int64_t S = std::min<int64_t>(spp[size_t(r)] - smp, share / np);
+            if (pix == 0 && np <= budget) {
+                int64_t S = std::min<int64_t>(spp[size_t(r)] - smp, budget / np);
                 c.pixBegin = 0;
                 c.npix = int(np);
                 c.samples = int(S);
                 c.firstSample = rp[size_t(r)].firstSample + smp;
                 smp += int(S);
             } else {
-                int64_t take = std::min<int64_t>(share, np - pix);
+                int64_t take = std::min<int64_t>(budget, np - pix);
                 c.pixBegin = int(pix);
                 c.npix = int(take);
                 c.samples = 1;

@@ -556,7 +556,7 @@ struct ShadeArgs {
 
 // One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
 template <bool kBatch = false>
-__global__ void __launch_bounds__(256) k_shade(ShadeArgs a) {
+__global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
     // The classes laid end to end: entry q belongs to the class whose prefix range holds it.
     int start[kClasses + 1];
