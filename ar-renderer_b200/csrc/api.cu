@@ -7,6 +7,7 @@
 
 #include "device.cuh"
 #include "../../include/prgpu_api.h"
+#include "guide.cuh"
 
 namespace prb {
 
@@ -61,6 +62,7 @@ static_assert(sizeof(prgpu::Light) == 48 && offsetof(prgpu::Light, position) == 
 static_assert(sizeof(prgpu::Camera) == 80 && offsetof(prgpu::Camera, width) == 64);
 static_assert(sizeof(prgpu::GridMediumDesc) == 112 && offsetof(prgpu::GridMediumDesc, density) == 104);
 static_assert(sizeof(prgpu::SceneExt) == 48 && offsetof(prgpu::SceneExt, gridMedia) == 40);
+static_assert(prgpu::kGuideParams == prb::kGuideParams);
 static_assert(sizeof(prgpu::BatchItem) == 48 && offsetof(prgpu::BatchItem, outXYZ) == 40 &&
               sizeof(prgpu::BatchConfig) == 16 && sizeof(prgpu::BatchStats) == 72);
 static_assert(sizeof(prgpu::RenderParams) == 24 && offsetof(prgpu::RenderParams, seed) == 8);

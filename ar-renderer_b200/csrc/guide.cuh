@@ -1,0 +1,180 @@
+// Path-guiding network: the parts shared by the tensor-core kernels (guide.cu) and the shading
+// kernel -- input encoding, decoding of the network output into a von Mises-Fisher mixture plus
+// a selection probability, the mixture's sampling and pdf, and the gradient of the training loss.
+// No counterpart in the reference renderer (its PathIntegrator samples the BSDF only,
+// src/integrators/path.cpp:215-224, the site where this guide is combined with it).
+//
+// Network: 128 inputs -> 4 hidden layers of 64 (ReLU) -> 48 outputs, FP16 weights and
+// activations, FP32 accumulation. Biases are folded into the weights: input 81 and hidden unit 63
+// of every hidden layer are held at 1, so the weight column of that unit is the next layer's bias.
+//   inputs: x in [0,1]^3 (position normalised to the scene bounds), sin / cos(2^b pi x) for 12
+//           bands b (72), shading normal (3), outgoing direction (3), 1, zeros to 128.
+//   outputs: per lobe k < 8: direction (3, normalised), log kappa (clamped to [-4, 8]), weight
+//           logit (softmax over the 8); output 40: selection logit, c = 0.9 sigmoid; 41..47 unused.
+// One-sample MIS with the BSDF: wi ~ c q + (1 - c) p_bsdf, the pdf of both computed in FP32 from the
+// same decoded parameters, so the estimator stays unbiased for any weights.
+// Loss per training sample (x, n, wo, wi, p_bsdf(wi), weight w >= 0):
+//   -w log(c q(wi) + (1 - c) p_bsdf(wi)),
+// w = f cos Li / pdf_used: the KL divergence from the product of BSDF and incident light.
+#pragma once
+
+#include "common.cuh"
+
+namespace prb {
+
+constexpr int kGuideIn = 128, kGuideHid = 64, kGuideOut = 48, kGuideLayers = 5, kGuideLobes = 8;
+constexpr int kGuideBands = 12, kGuideConstIn = 81, kGuideConstHid = 63;
+// Weight matrix l is [out_l x in_l]; the flattened FP32 master array keeps them in order, row-major.
+__host__ __device__ constexpr int guide_layer_in(int l) { return l == 0 ? kGuideIn : kGuideHid; }
+__host__ __device__ constexpr int guide_layer_out(int l) { return l == kGuideLayers - 1 ? kGuideOut : kGuideHid; }
+constexpr int kGuideParams = kGuideHid * kGuideIn + 3 * kGuideHid * kGuideHid + kGuideOut * kGuideHid;  // 23,552
+constexpr float kGuideMaxSelect = 0.9f;
+
+__host__ __device__ constexpr int guide_weight_offset(int l) {
+    return l == 0 ? 0 : kGuideHid * kGuideIn + (l - 1) * kGuideHid * kGuideHid;
+}
+
+// Input features (FP32) of a shading point; bmin / bext: scene bounds and extent.
+__device__ __forceinline__ void guide_features(V3 x, V3 n, V3 wo, const float *bmin, const float *bext, float *f) {
+    float xn[3] = {(x.x - bmin[0]) / bext[0], (x.y - bmin[1]) / bext[1], (x.z - bmin[2]) / bext[2]};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        xn[a] = fminf(fmaxf(xn[a], 0.f), 1.f);
+        f[a] = xn[a];
+    }
+#pragma unroll
+    for (int b = 0; b < kGuideBands; ++b)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float s, c;
+            sincospif(xn[a] * float(1 << b), &s, &c);
+            f[3 + 6 * b + 2 * a] = s;
+            f[3 + 6 * b + 2 * a + 1] = c;
+        }
+    f[75] = n.x, f[76] = n.y, f[77] = n.z;
+    f[78] = wo.x, f[79] = wo.y, f[80] = wo.z;
+    f[kGuideConstIn] = 1.f;
+}
+
+struct GuideMix {
+    V3 mu[kGuideLobes];
+    float kappa[kGuideLobes];
+    float pi[kGuideLobes];
+    float c;
+};
+
+__device__ __forceinline__ float guide_sigmoid(float x) { return 1.f / (1.f + expf(-x)); }
+
+__device__ __forceinline__ GuideMix guide_decode(const float *o) {
+    GuideMix m;
+    float mx = -1e30f;
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) mx = fmaxf(mx, o[5 * k + 4]);
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) {
+        V3 v = mk(o[5 * k], o[5 * k + 1], o[5 * k + 2]);
+        float l = sqrtf(dot(v, v));
+        m.mu[k] = l > 1e-6f ? v * (1.f / l) : mk(0.f, 0.f, 1.f);
+        m.kappa[k] = expf(fminf(fmaxf(o[5 * k + 3], -4.f), 8.f));
+        m.pi[k] = expf(o[5 * k + 4] - mx);
+        sum += m.pi[k];
+    }
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) m.pi[k] /= sum;
+    m.c = kGuideMaxSelect * guide_sigmoid(o[40]);
+    return m;
+}
+
+// vMF density kappa / (2 pi (1 - exp(-2 kappa))) exp(kappa (mu.w - 1)) (normalised on the sphere).
+__device__ __forceinline__ float vmf_pdf(V3 mu, float kappa, V3 w) {
+    float t = dot(mu, w) - 1.f;
+    if (kappa < 1e-4f) return kInv4Pi;
+    return kappa / (2.f * kPi * -expm1f(-2.f * kappa)) * expf(kappa * t);
+}
+
+__device__ __forceinline__ float guide_pdf(const GuideMix &m, V3 w) {
+    float q = 0.f;
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) q += m.pi[k] * vmf_pdf(m.mu[k], m.kappa[k], w);
+    return q;
+}
+
+// Lobe by u0 over the weights, then the vMF sample of W. Jakob, "Numerically stable sampling of
+// the von Mises-Fisher distribution on S^2" (2012): cos theta = 1 + log(u + (1 - u) e^{-2 kappa}) / kappa.
+__device__ __forceinline__ V3 guide_sample(const GuideMix &m, float u0, float u1, float u2) {
+    int k = kGuideLobes - 1;
+    float acc = 0.f;
+#pragma unroll
+    for (int i = 0; i < kGuideLobes; ++i) {
+        acc += m.pi[i];
+        if (u0 < acc) {
+            k = i;
+            break;
+        }
+    }
+    float kap = m.kappa[k];
+    float ct = kap < 1e-4f ? 1.f - 2.f * u1 : 1.f + logf(u1 + (1.f - u1) * expf(-2.f * kap)) / kap;
+    ct = fminf(fmaxf(ct, -1.f), 1.f);
+    float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
+    float sp, cp;
+    sincospif(2.f * u2, &sp, &cp);
+    V3 t, b;
+    V3 mu = m.mu[k];
+    // Orthonormal basis around mu (Duff et al. 2017, "Building an orthonormal basis, revisited").
+    float sgn = copysignf(1.f, mu.z);
+    float a = -1.f / (sgn + mu.z), bb = mu.x * mu.y * a;
+    t = mk(1.f + sgn * mu.x * mu.x * a, sgn * bb, -sgn * mu.x);
+    b = mk(bb, sgn + mu.y * mu.y * a, -mu.y);
+    return t * (st * cp) + b * (st * sp) + mu * ct;
+}
+
+// Gradient of -w log(c q(wi) + (1 - c) pb) with respect to the 48 raw outputs (FP32).
+// Returns the loss; g receives the gradient (zero for the unused outputs 41..47).
+__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pb, float w, float *g) {
+#pragma unroll
+    for (int i = 0; i < kGuideOut; ++i) g[i] = 0.f;
+    GuideMix m = guide_decode(o);
+    float vk[kGuideLobes];
+    float q = 0.f;
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) {
+        vk[k] = vmf_pdf(m.mu[k], m.kappa[k], wi);
+        q += m.pi[k] * vk[k];
+    }
+    float p = m.c * q + (1.f - m.c) * pb;
+    if (!(p > 0.f) || !(w > 0.f)) return 0.f;
+    float loss = -w * logf(p);
+    float dq = -w * m.c / p;                       // dL/dq
+    float dc = -w * (q - pb) / p;                  // dL/dc
+    float s = guide_sigmoid(o[40]);
+    g[40] = dc * kGuideMaxSelect * s * (1.f - s);
+    float sumPiG = 0.f;
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) sumPiG += m.pi[k] * dq * vk[k];
+#pragma unroll
+    for (int k = 0; k < kGuideLobes; ++k) {
+        // softmax weights
+        g[5 * k + 4] = m.pi[k] * (dq * vk[k]) - m.pi[k] * sumPiG;
+        float dv = dq * m.pi[k] * vk[k];  // dL/d(log vmf_k)
+        float kap = m.kappa[k];
+        float raw = o[5 * k + 3];
+        if (raw > -4.f && raw < 8.f) {
+            // d log vmf / d kappa = 1/kappa - 2 e^{-2k} / (1 - e^{-2k}) + (mu.w - 1); d kappa / d raw = kappa
+            float e = expf(-2.f * kap);
+            float dlog = (kap < 1e-4f) ? 0.f : 1.f / kap - 2.f * e / (-expm1f(-2.f * kap)) + (dot(m.mu[k], wi) - 1.f);
+            g[5 * k + 3] = dv * dlog * kap;
+        }
+        // d log vmf / d mu = kappa wi; mu = v / |v|: dmu/dv = (I - mu mu^T) / |v|
+        V3 v = mk(o[5 * k], o[5 * k + 1], o[5 * k + 2]);
+        float l = sqrtf(dot(v, v));
+        if (l > 1e-6f) {
+            V3 gm = wi * (dv * kap);
+            V3 gv = (gm - m.mu[k] * dot(m.mu[k], gm)) * (1.f / l);
+            g[5 * k] = gv.x, g[5 * k + 1] = gv.y, g[5 * k + 2] = gv.z;
+        }
+    }
+    return loss;
+}
+
+} // namespace prb

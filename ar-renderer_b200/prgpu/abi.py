@@ -179,6 +179,11 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_render_ex", [C.c_int, _P, _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_render_batch", [C.c_int, C.c_int32, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_autotune_batch", [C.c_int, C.c_int32, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_set_weights", [C.c_int, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_get_weights", [C.c_int, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_infer", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_gradient", [C.c_int, C.c_int64, _P, _P, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_adam_step", [C.c_int, C.c_float, C.c_float, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
                                         _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays_noalloc", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64,

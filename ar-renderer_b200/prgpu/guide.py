@@ -1,0 +1,54 @@
+"""The path-guiding network through the C ABI (weights, inference, one training pass, Adam)."""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+N_PARAMS = 23552
+N_IN, N_OUT = 128, 48
+
+
+def set_weights(w: np.ndarray, device: int = 0) -> None:
+    w = np.ascontiguousarray(w, np.float32)
+    assert w.size == N_PARAMS
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_set_weights(device, abi.ptr(w), err, len(err)), err, "prgpu_guide_set_weights")
+
+
+def get_weights(device: int = 0) -> np.ndarray:
+    w = np.zeros(N_PARAMS, np.float32)
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_get_weights(device, abi.ptr(w), err, len(err)), err, "prgpu_guide_get_weights")
+    return w
+
+
+def infer(features: np.ndarray, device: int = 0) -> np.ndarray:
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, N_IN)
+    out = np.zeros((f.shape[0], N_OUT), np.float32)
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_infer(device, f.shape[0], abi.ptr(f), abi.ptr(out), err, len(err)), err,
+              "prgpu_guide_infer")
+    return out
+
+
+def gradient(features: np.ndarray, wi: np.ndarray, pb: np.ndarray, w: np.ndarray, device: int = 0):
+    """(summed loss, gradient of the summed loss) from one GPU training pass."""
+    f = np.ascontiguousarray(features, np.float32).reshape(-1, N_IN)
+    s = np.ascontiguousarray(np.concatenate([np.asarray(wi, np.float32).reshape(-1, 3),
+                                             np.asarray(pb, np.float32).reshape(-1, 1),
+                                             np.asarray(w, np.float32).reshape(-1, 1)], 1))
+    g = np.zeros(N_PARAMS, np.float32)
+    loss = C.c_float(0.0)
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_gradient(device, f.shape[0], abi.ptr(f), abi.ptr(s), C.byref(loss), abi.ptr(g),
+                                                 err, len(err)), err, "prgpu_guide_gradient")
+    return float(loss.value), g
+
+
+def adam_step(grad_scale: float, lr: float = 1e-3, device: int = 0) -> None:
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_adam_step(device, grad_scale, lr, err, len(err)), err, "prgpu_guide_adam_step")

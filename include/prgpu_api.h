@@ -32,6 +32,7 @@ namespace prgpu {
 
 constexpr int kApiVersion = 4;          // gpu_api.h:17
 constexpr int kExtVersion = 5;          // this library's extension level
+constexpr int kGuideParams = 23552;     // weights of the path-guiding network
 constexpr int kSpectrumSamples = 95;    // 360..830 nm every 5 nm, linear interpolation (gpu_api.h:19-21)
 constexpr float kSpectrumMin = 360.f, kSpectrumStep = 5.f;
 constexpr int kFilterBins = 64;         // pixel-filter CDF bins (gpu_api.h:22-23)
@@ -365,6 +366,23 @@ PRGPU_API int prgpu_render_batch(int deviceIndex, int32_t count, const prgpu::Ba
 // shape, and writes it to out.
 PRGPU_API int prgpu_autotune_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
                                    prgpu::BatchConfig *out, char *err, int errLen);
+
+// Path-guiding network (no counterpart in the reference renderer, whose PathIntegrator samples
+// the BSDF only, src/integrators/path.cpp:215-224). 128 inputs (guide features: position in the
+// scene bounds with 12 sin/cos bands, normal, outgoing direction, a constant 1), 4 hidden ReLU
+// layers of 64 (unit 63 held at 1), 48 outputs (8 von Mises-Fisher lobes + a selection
+// probability); FP16 weights on the tensor cores, FP32 master weights and Adam state per device.
+// Weights are prgpu::kGuideParams floats, layer by layer, each layer [out x in] row-major.
+PRGPU_API int prgpu_guide_set_weights(int deviceIndex, const float *weights, char *err, int errLen);
+PRGPU_API int prgpu_guide_get_weights(int deviceIndex, float *weights, char *err, int errLen);
+// Network outputs (n x 48 floats) for n feature rows (n x 128 floats, rounded to FP16 on the device).
+PRGPU_API int prgpu_guide_infer(int deviceIndex, int64_t n, const float *features, float *out, char *err, int errLen);
+// One training pass: samples are n x 5 floats (wi[3], BSDF pdf of wi, weight w); writes the summed
+// loss -sum w log(c q(wi) + (1 - c) pdf) and its gradient w.r.t. the weights (kGuideParams floats).
+PRGPU_API int prgpu_guide_gradient(int deviceIndex, int64_t n, const float *features, const float *samples,
+                                   float *lossSum, float *grad, char *err, int errLen);
+// Adam step (beta 0.9 / 0.999, eps 1e-8) on the last gradient times gradScale.
+PRGPU_API int prgpu_guide_adam_step(int deviceIndex, float gradScale, float learningRate, char *err, int errLen);
 
 // Number of kernel launches this library has issued since load (for launch accounting).
 PRGPU_API uint64_t prgpu_launch_count();
