@@ -25,12 +25,14 @@
 #include <cuda_fp16.h>
 
 #include <cmath>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "device.cuh"
 #include "guide.cuh"
+#include "guide_host.h"
 #include "../../include/prgpu_api.h"
 
 namespace prb {
@@ -260,6 +262,7 @@ struct GuideSample {
     float wi[3];
     float pb;
     float w;
+    float n[3];   // shading normal (the folding plane)
 };
 
 struct GuideSmemTrain {
@@ -280,7 +283,7 @@ __host__ __device__ constexpr uint32_t dw_col(int l) { return 64 + 64 * uint32_t
 __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict__ features,
                                                         const GuideSample *__restrict__ samples, const int *count,
                                                         const __half *__restrict__ packed, float *grad,
-                                                        float *lossSum, int *status) {
+                                                        float *lossSum, int *status, const float *wnorm) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     GuideSmemTrain &S = *reinterpret_cast<GuideSmemTrain *>(smraw);
     const int n = *count;
@@ -300,6 +303,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict
     uint32_t phase = 0;
     bool ok = true, firstTile = true;
     const int r = threadIdx.x;
+    const float wscale = wnorm ? *wnorm : 1.f;
     float z[kGuideHid], lossAcc = 0.f;
     for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const int row = t * kTileRows + r;
@@ -324,7 +328,8 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict
                 float gout[kGuideOut];
                 if (valid) {
                     const GuideSample sm = samples[row];
-                    lossAcc += guide_loss_grad(z, mk(sm.wi[0], sm.wi[1], sm.wi[2]), sm.pb, sm.w, gout);
+                    lossAcc += guide_loss_grad(z, mk(sm.wi[0], sm.wi[1], sm.wi[2]), mk(sm.n[0], sm.n[1], sm.n[2]),
+                                               sm.pb, sm.w * wscale, gout);
                 } else {
 #pragma unroll
                     for (int k = 0; k < kGuideOut; ++k) gout[k] = 0.f;
@@ -405,9 +410,13 @@ __global__ void k_guide_pack(const float *master, __half *packed) {
     }
 }
 
-__global__ void k_guide_adam(float *master, float *m, float *v, const float *grad, float scale, float lr, float b1,
-                             float b2, float eps, int step) {
+__global__ void k_guide_adam(float *master, float *m, float *v, const float *grad, float scale, const float *scaleDev,
+                             float lr, float b1, float b2, float eps, int step) {
     const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
+    if (scaleDev) {
+        scale = *scaleDev;
+        if (scale == 0.f) return;  // empty online batch: no step
+    }
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGuideParams; i += gridDim.x * blockDim.x) {
         float g = grad[i] * scale;
         float mi = b1 * m[i] + (1.f - b1) * g;
@@ -426,10 +435,11 @@ __global__ void k_guide_to_half(const float *in, __half *out, int n) {
 // Host side: per-device guide state and launchers.
 
 struct GuideState {
-    DevBuf master, m, v, grad, packed, scratch, loss, status;
+    DevBuf master, m, v, grad, packed, scratch, loss, status, train;
     int step = 0;
     bool ready = false;
     int sms = 0;
+    float lr = 1e-3f;      // online learning rate (Adam)
 };
 
 GuideState gGuide[64];
@@ -480,16 +490,44 @@ void guide_train(cudaStream_t st, GuideState &g, const __half *features, const G
     PRB_CUDA(cudaMemsetAsync(g.grad.ptr, 0, kGuideParams * sizeof(float), st));
     PRB_CUDA(cudaMemsetAsync(g.loss.ptr, 0, sizeof(float), st));
     k_guide_train<<<grid, 128, train_smem(), st>>>(features, samples, dcount, g.packed.as<__half>(), g.grad.as<float>(),
-                                                   g.loss.as<float>(), g.status.as<int>());
+                                                   g.loss.as<float>(), g.status.as<int>(), nullptr);
     count_launch();
 }
 
 void guide_adam(cudaStream_t st, GuideState &g, float scale, float lr) {
     ++g.step;
     k_guide_adam<<<64, 256, 0, st>>>(g.master.as<float>(), g.m.as<float>(), g.v.as<float>(), g.grad.as<float>(), scale,
-                                     lr, 0.9f, 0.999f, 1e-8f, g.step);
+                                     nullptr, lr, 0.9f, 0.999f, 1e-8f, g.step);
     k_guide_pack<<<64, 256, 0, st>>>(g.master.as<float>(), g.packed.as<__half>());
     count_launch(2);
+}
+
+// Online training: recorded samples -> FP16 features and loss inputs for up to maxRows rows, the
+// batch's weight sum, then the normalisation (weights to mean 1) and the Adam scale (1 / rows).
+__global__ void k_guide_prep(const GuideTrainRec *recs, const int *count, int offset, int maxRows, __half *features,
+                             GuideSample *samples, int *rows, float *wsum) {
+    const int n = max(0, min(*count - offset, maxRows));
+    recs += offset;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *rows = n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const GuideTrainRec r = recs[i];
+        float f[kGuideIn];
+#pragma unroll
+        for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
+        guide_features_n(r.xn, mk(r.n[0], r.n[1], r.n[2]), mk(r.wo[0], r.wo[1], r.wo[2]), f);
+        __half2 *dst = reinterpret_cast<__half2 *>(features + size_t(i) * kGuideIn);
+#pragma unroll
+        for (int k = 0; k < kGuideIn / 2; ++k) dst[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
+        samples[i] = GuideSample{{r.wi[0], r.wi[1], r.wi[2]}, r.pb, r.w, {r.n[0], r.n[1], r.n[2]}};
+        atomicAdd(wsum, r.w);
+    }
+}
+
+__global__ void k_guide_norm(const int *rows, const float *wsum, float *wnorm, float *scale) {
+    const int n = *rows;
+    const float s = *wsum;
+    *wnorm = (n > 0 && s > 0.f) ? float(n) / s : 0.f;
+    *scale = n > 0 ? 1.f / float(n) : 0.f;
 }
 
 int guide_status(DeviceState &ds, GuideState &g) {
@@ -497,6 +535,80 @@ int guide_status(DeviceState &ds, GuideState &g) {
     PRB_CUDA(cudaMemcpyAsync(&s, g.status.ptr, sizeof(int), cudaMemcpyDeviceToHost, ds.stream));
     PRB_CUDA(cudaStreamSynchronize(ds.stream));
     return s;
+}
+
+// Fresh weights: He-uniform, the constant units' outgoing columns (biases) and the rows that
+// produce a constant unit (or an unused output) zero.
+std::vector<float> guide_init_weights(uint64_t seed) {
+    std::vector<float> w(kGuideParams, 0.f);
+    uint64_t st = seed * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    auto uni = [&]() {
+        st ^= st >> 12;
+        st ^= st << 25;
+        st ^= st >> 27;
+        return double((st * 0x2545F4914F6CDD1Dull) >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (int l = 0; l < kGuideLayers; ++l) {
+        const int K = guide_layer_in(l), N = guide_layer_out(l);
+        const double lim = std::sqrt(6.0 / double(l == 0 ? kGuideConstIn + 1 : K));
+        for (int o = 0; o < N; ++o)
+            for (int k = 0; k < K; ++k) {
+                bool zero = (l == 0 && k >= kGuideConstIn) || (l > 0 && k == kGuideConstHid) ||
+                            (l < kGuideLayers - 1 && o == kGuideConstHid) || (l == kGuideLayers - 1 && o > 40);
+                w[size_t(guide_weight_offset(l)) + size_t(o) * K + k] = zero ? 0.f : float((2.0 * uni() - 1.0) * lim);
+            }
+    }
+    return w;
+}
+
+void guide_prepare(DeviceState &ds, int device, bool reset, uint64_t seed) {
+    GuideState &g = gGuide[device];
+    const bool fresh = !g.ready;
+    guide_setup(ds, g);
+    if (fresh || reset) {
+        std::vector<float> w = guide_init_weights(seed);
+        guide_set_weights(ds, g, w.data());
+        PRB_CUDA(cudaStreamSynchronize(ds.stream));
+    }
+}
+
+bool guide_failed(DeviceState &ds, int device) {
+    GuideState &g = gGuide[device];
+    if (!g.ready) return false;
+    int s = guide_status(ds, g);
+    if (s) PRB_CUDA(cudaMemsetAsync(g.status.ptr, 0, sizeof(int), ds.stream));
+    return s != 0;
+}
+
+void guide_infer_rows(cudaStream_t st, int device, const __half *features, const int *dcount, int maxRows, float *out) {
+    guide_forward(st, gGuide[device], features, dcount, maxRows, out);
+}
+
+void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs, const int *dcount, int offset,
+                         int maxRows, float lr) {
+    GuideState &g = gGuide[device];
+    if (lr <= 0.f) lr = g.lr;
+    const size_t fb = size_t(maxRows) * kGuideIn * sizeof(__half), sb = size_t(maxRows) * sizeof(GuideSample);
+    g.train.ensure(((fb + 255) & ~size_t(255)) + ((sb + 255) & ~size_t(255)) + 256);
+    auto *feat = g.train.as<__half>();
+    auto *smp = reinterpret_cast<GuideSample *>(g.train.as<unsigned char>() + ((fb + 255) & ~size_t(255)));
+    auto *stats = reinterpret_cast<float *>(g.train.as<unsigned char>() + ((fb + 255) & ~size_t(255)) +
+                                            ((sb + 255) & ~size_t(255)));
+    int *rows = reinterpret_cast<int *>(stats);
+    float *wsum = stats + 1, *wnorm = stats + 2, *scale = stats + 3;
+    PRB_CUDA(cudaMemsetAsync(stats, 0, 16, st));
+    k_guide_prep<<<g.sms * 4, 128, 0, st>>>(recs, dcount, offset, maxRows, feat, smp, rows, wsum);
+    k_guide_norm<<<1, 1, 0, st>>>(rows, wsum, wnorm, scale);
+    const int tiles = (maxRows + kTileRows - 1) / kTileRows;
+    PRB_CUDA(cudaMemsetAsync(g.grad.ptr, 0, kGuideParams * sizeof(float), st));
+    PRB_CUDA(cudaMemsetAsync(g.loss.ptr, 0, sizeof(float), st));
+    k_guide_train<<<std::max(1, std::min(tiles, g.sms)), 128, train_smem(), st>>>(
+        feat, smp, rows, g.packed.as<__half>(), g.grad.as<float>(), g.loss.as<float>(), g.status.as<int>(), wnorm);
+    ++g.step;
+    k_guide_adam<<<64, 256, 0, st>>>(g.master.as<float>(), g.m.as<float>(), g.v.as<float>(), g.grad.as<float>(), 0.f,
+                                     scale, lr, 0.9f, 0.999f, 1e-8f, g.step);
+    k_guide_pack<<<64, 256, 0, st>>>(g.master.as<float>(), g.packed.as<__half>());
+    count_launch(5);
 }
 
 } // namespace prb
@@ -630,6 +742,46 @@ PRGPU_API int prgpu_guide_gradient(int deviceIndex, int64_t n, const float *feat
             set_err(err, errLen, "guide kernel timed out waiting for the tensor cores");
             return 1;
         }
+        return 0;
+    });
+}
+
+PRGPU_API int prgpu_guide_set_learning_rate(int deviceIndex, float learningRate, char *err, int errLen) {
+    return guarded(err, errLen, [&]() {
+        if (deviceIndex < 0 || deviceIndex >= 64 || !(learningRate > 0.f) || learningRate > 1.f) {
+            set_err(err, errLen, "bad device or learning rate");
+            return 1;
+        }
+        gGuide[deviceIndex].lr = learningRate;
+        return 0;
+    });
+}
+
+PRGPU_API int prgpu_guide_stats(int deviceIndex, float *out4, char *err, int errLen) {
+    return guarded(err, errLen, [&]() {
+        if (!out4 || deviceIndex < 0 || deviceIndex >= 64 || !gGuide[deviceIndex].ready) {
+            set_err(err, errLen, "no guide weights on this device");
+            return 1;
+        }
+        DeviceState &ds = device_state(deviceIndex);
+        GuideState &g = gGuide[deviceIndex];
+        float loss = 0.f, tr[4] = {0.f, 0.f, 0.f, 0.f};
+        PRB_CUDA(cudaMemcpyAsync(&loss, g.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, ds.stream));
+        if (g.train.ptr) {
+            // rows (int bits), weight sum of the last online batch: the stats block after the samples
+            const size_t fb = size_t(1 << 16) * kGuideIn * sizeof(__half), sb = size_t(1 << 16) * sizeof(GuideSample);
+            if (g.train.bytes >= ((fb + 255) & ~size_t(255)) + ((sb + 255) & ~size_t(255)) + 16)
+                PRB_CUDA(cudaMemcpyAsync(tr, g.train.as<unsigned char>() + ((fb + 255) & ~size_t(255)) +
+                                                 ((sb + 255) & ~size_t(255)),
+                                         sizeof(tr), cudaMemcpyDeviceToHost, ds.stream));
+        }
+        PRB_CUDA(cudaStreamSynchronize(ds.stream));
+        int rows;
+        std::memcpy(&rows, &tr[0], sizeof(int));
+        out4[0] = loss;
+        out4[1] = float(rows);
+        out4[2] = tr[1];
+        out4[3] = float(g.step);
         return 0;
     });
 }

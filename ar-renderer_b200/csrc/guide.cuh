@@ -11,11 +11,17 @@
 //           bands b (72), shading normal (3), outgoing direction (3), 1, zeros to 128.
 //   outputs: per lobe k < 8: direction (3, normalised), log kappa (clamped to [-4, 8]), weight
 //           logit (softmax over the 8); output 40: selection logit, c = 0.9 sigmoid; 41..47 unused.
-// One-sample MIS with the BSDF: wi ~ c q + (1 - c) p_bsdf, the pdf of both computed in FP32 from the
-// same decoded parameters, so the estimator stays unbiased for any weights.
-// Loss per training sample (x, n, wo, wi, p_bsdf(wi), weight w >= 0):
-//   -w log(c q(wi) + (1 - c) p_bsdf(wi)),
-// w = f cos Li / pdf_used: the KL divergence from the product of BSDF and incident light.
+// One-sample MIS with the BSDF: wi ~ c q_n + (1 - c) p_bsdf, the pdf of both computed in FP32 from
+// the same decoded parameters, so the estimator stays unbiased for any weights. q_n is the mixture
+// folded onto the hemisphere of the shading normal n that holds wo (a sample below is mirrored
+// across the tangent plane): q_n(w) = q(w) + q(w - 2 (w.n) n) there, 0 on the other side, so no
+// guided sample is wasted below a reflecting surface.
+// Loss per training sample (x, n, wo, wi, p_bsdf(wi), weight w >= 0), w = f cos Li / pdf_used:
+//   -w log q_n(wi)                               (the lobes: KL divergence from the product of
+//                                                 BSDF and incident light)
+//   -w log(c q_n(wi) + (1 - c) p_bsdf(wi))       (the selection probability only: q_n held fixed)
+// Training c through the mixture alone would let it collapse to 0 while the lobes are still poor,
+// after which the lobes' gradient (proportional to c) vanishes.
 #pragma once
 
 #include "common.cuh"
@@ -29,6 +35,7 @@ __host__ __device__ constexpr int guide_layer_in(int l) { return l == 0 ? kGuide
 __host__ __device__ constexpr int guide_layer_out(int l) { return l == kGuideLayers - 1 ? kGuideOut : kGuideHid; }
 constexpr int kGuideParams = kGuideHid * kGuideIn + 3 * kGuideHid * kGuideHid + kGuideOut * kGuideHid;  // 23,552
 constexpr float kGuideMaxSelect = 0.9f;
+constexpr int kGuideVertices = 4;  // diffuse vertices per path that are guided and recorded
 
 __host__ __device__ constexpr int guide_weight_offset(int l) {
     return l == 0 ? 0 : kGuideHid * kGuideIn + (l - 1) * kGuideHid * kGuideHid;
@@ -100,6 +107,14 @@ __device__ __forceinline__ float guide_pdf(const GuideMix &m, V3 w) {
     return q;
 }
 
+__device__ __forceinline__ V3 guide_mirror(V3 w, V3 n) { return w - n * (2.f * dot(w, n)); }
+
+// The folded mixture pdf q_n(w); side: +1 / -1 = the hemisphere of n that holds wo.
+__device__ __forceinline__ float guide_pdf_folded(const GuideMix &m, V3 w, V3 n, float side) {
+    if (dot(w, n) * side <= 0.f) return 0.f;
+    return guide_pdf(m, w) + guide_pdf(m, guide_mirror(w, n));
+}
+
 // Lobe by u0 over the weights, then the vMF sample of W. Jakob, "Numerically stable sampling of
 // the von Mises-Fisher distribution on S^2" (2012): cos theta = 1 + log(u + (1 - u) e^{-2 kappa}) / kappa.
 __device__ __forceinline__ V3 guide_sample(const GuideMix &m, float u0, float u1, float u2) {
@@ -129,47 +144,63 @@ __device__ __forceinline__ V3 guide_sample(const GuideMix &m, float u0, float u1
     return t * (st * cp) + b * (st * sp) + mu * ct;
 }
 
-// Gradient of -w log(c q(wi) + (1 - c) pb) with respect to the 48 raw outputs (FP32).
-// Returns the loss; g receives the gradient (zero for the unused outputs 41..47).
-__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, float pb, float w, float *g) {
+// A training sample recorded by the renderer: normalised position, shading normal, outgoing and
+// sampled directions, the BSDF pdf of wi and the weight w = f cos Li / pdf_used (luminance-free:
+// the average over the hero wavelengths).
+struct GuideTrainRec {
+    float xn[3], n[3], wo[3], wi[3], pb, w;
+};
+
+// Input features from a normalised position (x already in [0,1]^3).
+__device__ __forceinline__ void guide_features_n(const float *xn, V3 n, V3 wo, float *f) {
+    const float zero[3] = {0.f, 0.f, 0.f}, one[3] = {1.f, 1.f, 1.f};
+    guide_features(mk(xn[0], xn[1], xn[2]), n, wo, zero, one, f);
+}
+
+// Gradient of the two-part loss above with respect to the 48 raw outputs (FP32): lobe outputs
+// from -w log q_n, the selection output from -w log(c q_n + (1 - c) pb) with q_n fixed. wi lies on
+// the side of n the sample came from, so q_n(wi) = q(wi) + q(mirror(wi)). Returns the sum of both
+// parts; g receives the gradient (zero for the unused outputs 41..47).
+__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, V3 n, float pb, float w, float *g) {
 #pragma unroll
     for (int i = 0; i < kGuideOut; ++i) g[i] = 0.f;
     GuideMix m = guide_decode(o);
-    float vk[kGuideLobes];
+    const V3 wr = guide_mirror(wi, n);
+    float v1[kGuideLobes], v2[kGuideLobes];
     float q = 0.f;
 #pragma unroll
     for (int k = 0; k < kGuideLobes; ++k) {
-        vk[k] = vmf_pdf(m.mu[k], m.kappa[k], wi);
-        q += m.pi[k] * vk[k];
+        v1[k] = vmf_pdf(m.mu[k], m.kappa[k], wi);
+        v2[k] = vmf_pdf(m.mu[k], m.kappa[k], wr);
+        q += m.pi[k] * (v1[k] + v2[k]);
     }
     float p = m.c * q + (1.f - m.c) * pb;
-    if (!(p > 0.f) || !(w > 0.f)) return 0.f;
-    float loss = -w * logf(p);
-    float dq = -w * m.c / p;                       // dL/dq
-    float dc = -w * (q - pb) / p;                  // dL/dc
+    if (!(p > 0.f) || !(q > 0.f) || !(w > 0.f)) return 0.f;
+    float loss = -w * logf(q) - w * logf(p);
+    float dq = -w / q;                             // d(-w log q_n)/dq_n
+    float dc = -w * (q - pb) / p;                  // d(-w log p)/dc at fixed q_n
     float s = guide_sigmoid(o[40]);
     g[40] = dc * kGuideMaxSelect * s * (1.f - s);
     float sumPiG = 0.f;
 #pragma unroll
-    for (int k = 0; k < kGuideLobes; ++k) sumPiG += m.pi[k] * dq * vk[k];
+    for (int k = 0; k < kGuideLobes; ++k) sumPiG += m.pi[k] * dq * (v1[k] + v2[k]);
 #pragma unroll
     for (int k = 0; k < kGuideLobes; ++k) {
         // softmax weights
-        g[5 * k + 4] = m.pi[k] * (dq * vk[k]) - m.pi[k] * sumPiG;
-        float dv = dq * m.pi[k] * vk[k];  // dL/d(log vmf_k)
-        float kap = m.kappa[k];
-        float raw = o[5 * k + 3];
-        if (raw > -4.f && raw < 8.f) {
+        g[5 * k + 4] = m.pi[k] * dq * (v1[k] + v2[k]) - m.pi[k] * sumPiG;
+        const float d1 = dq * m.pi[k] * v1[k], d2 = dq * m.pi[k] * v2[k];  // dL/d(log vmf_k) at wi, wr
+        const float kap = m.kappa[k];
+        const float raw = o[5 * k + 3];
+        if (raw > -4.f && raw < 8.f && kap >= 1e-4f) {
             // d log vmf / d kappa = 1/kappa - 2 e^{-2k} / (1 - e^{-2k}) + (mu.w - 1); d kappa / d raw = kappa
-            float e = expf(-2.f * kap);
-            float dlog = (kap < 1e-4f) ? 0.f : 1.f / kap - 2.f * e / (-expm1f(-2.f * kap)) + (dot(m.mu[k], wi) - 1.f);
-            g[5 * k + 3] = dv * dlog * kap;
+            const float base = 1.f / kap - 2.f * expf(-2.f * kap) / (-expm1f(-2.f * kap));
+            g[5 * k + 3] = (d1 * (base + dot(m.mu[k], wi) - 1.f) + d2 * (base + dot(m.mu[k], wr) - 1.f)) * kap;
         }
-        // d log vmf / d mu = kappa wi; mu = v / |v|: dmu/dv = (I - mu mu^T) / |v|
+        // d log vmf / d mu = kappa w; mu = v / |v|: dmu/dv = (I - mu mu^T) / |v|
         V3 v = mk(o[5 * k], o[5 * k + 1], o[5 * k + 2]);
         float l = sqrtf(dot(v, v));
         if (l > 1e-6f) {
-            V3 gm = wi * (dv * kap);
+            V3 gm = (wi * d1 + wr * d2) * kap;
             V3 gv = (gm - m.mu[k] * dot(m.mu[k], gm)) * (1.f / l);
             g[5 * k] = gv.x, g[5 * k + 1] = gv.y, g[5 * k + 2] = gv.z;
         }

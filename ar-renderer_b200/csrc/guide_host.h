@@ -1,0 +1,27 @@
+// Host-side interface of the guide network's kernels (guide.cu) for the path tracer's driver.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "guide.cuh"
+
+namespace prb {
+
+// Makes the device's guide state ready; reset (or a first use) draws fresh weights from `seed`.
+void guide_prepare(DeviceState &ds, int device, bool reset, uint64_t seed);
+// Inference over the rows of `features` (FP16, [n x 128]); n is read from dcount on the device,
+// maxRows bounds it. out: FP32 [n x 48].
+void guide_infer_rows(cudaStream_t st, int device, const __half *features, const int *dcount, int maxRows, float *out);
+// One online training step (forward, backward, Adam at learning rate lr, or the device's setting
+// when lr <= 0) on records [offset, offset + maxRows) of the
+// recorded samples (count on the device); weights are normalised to mean 1 within the batch.
+void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs, const int *dcount, int offset,
+                         int maxRows, float lr);
+// True (and cleared) when a guide kernel gave up waiting for its tensor-core work.
+bool guide_failed(DeviceState &ds, int device);
+// Launch bookkeeping: kernels per inference / training step.
+constexpr int kGuideInferLaunches = 1, kGuideTrainLaunches = 5;
+
+} // namespace prb

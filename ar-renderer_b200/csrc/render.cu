@@ -10,17 +10,75 @@
 #include <map>
 #include <memory>
 
+#include "guide_host.h"
 #include "wavefront.cuh"
 
 namespace prb {
 // ---------------------------------------------------------------------------------------------
 // Driver
 
+// Guide inputs for every path filed as diffuse: shading point, shading normal and outgoing
+// direction (the same quantities the shading kernel records for training), FP16 rows in the
+// order of the diffuse class queue.
+__global__ void __launch_bounds__(256) k_guide_features(DevScene s, Paths P, const int *counters, const int *classQ,
+                                                        int classCap, __half *feat) {
+    const int n = counters[kCntClass0 + kClassDiffuse];
+    const float *bmin = s.root.box, *bmax = s.root.box + 3;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int j = classQ[size_t(kClassDiffuse) * classCap + i];
+        float4 o4 = P.o[j], d4 = P.d[j], hit = P.hit[j];
+        V3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
+        const prgpu::Primitive &pr = s.prims[__float_as_int(hit.w)];
+        Surf sf = shade_point(s, pr, hit.x, hit.y, hit.z, o, d);
+        float xn[3] = {(sf.p.x - bmin[0]) / fmaxf(bmax[0] - bmin[0], 1e-20f),
+                       (sf.p.y - bmin[1]) / fmaxf(bmax[1] - bmin[1], 1e-20f),
+                       (sf.p.z - bmin[2]) / fmaxf(bmax[2] - bmin[2], 1e-20f)};
+        float f[kGuideIn];
+#pragma unroll
+        for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
+        guide_features_n(xn, sf.ns, -d, f);
+        __half2 *dst = reinterpret_cast<__half2 *>(feat + size_t(i) * kGuideIn);
+#pragma unroll
+        for (int k = 0; k < kGuideIn / 2; ++k) dst[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
+    }
+}
+
+// After a chunk's film: every complete training record of the chunk's paths becomes a sample
+// (weight = (final mean radiance - snapshot) / mean throughput before the vertex), up to cap;
+// every record is cleared for the next chunk.
+__global__ void __launch_bounds__(256) k_guide_collect(Paths P, float4 *rec, int total, GuideTrainRec *out,
+                                                       int *count, int cap) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
+        const float4 L = P.L[j];
+        const float Lavg = 0.25f * (L.x + L.y + L.z + L.w);
+        for (int v = 0; v < kGuideVertices; ++v) {
+            float4 *r = rec + 4 * (size_t(j) * kGuideVertices + v);
+            float4 r3 = r[3];
+            if (__float_as_int(r3.w) == 0) break;
+            if (__float_as_int(r3.w) == 2) {
+                float4 r0 = r[0], r1 = r[1], r2 = r[2];
+                float w = r0.w > 0.f ? (Lavg - r2.w) / r0.w : 0.f;
+                if (w > 0.f && isfinite(w)) {
+                    int k = atomicAdd(count, 1);
+                    if (k < cap) out[k] = GuideTrainRec{{r0.x, r0.y, r0.z}, {r1.x, r1.y, r1.z}, {r2.x, r2.y, r2.z},
+                                                         {r3.x, r3.y, r3.z}, r1.w, w};
+                }
+            }
+            r[3] = make_float4(0.f, 0.f, 0.f, __int_as_float(0));
+        }
+    }
+}
+
+constexpr int kGuideBatch = 1 << 16;    // training samples per online step
+constexpr int kGuideRecords = 1 << 18;  // samples kept per chunk: up to 4 steps
+
 constexpr int kBouncesPerPoll = 4;  // bounces enqueued between two host reads of the queue length
 
 struct RenderState {
     SceneCache scene;
     DevBuf pathBuf, shadowBuf, queues, classQueues, counters, stats, film;
+    DevBuf guideFeat, guideOut, guideRec, guideTrain;  // guided form (allocated on first use)
+    int guideCap = 0;
     int capacity = 0;
     Paths P{};
     Shadows S{};
@@ -135,6 +193,27 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     const int gExtend = sms * rs.residentExtend[sph], gShadow = sms * rs.residentShadow[shadowVariant];
     const int gShade = sms * 8;
     const bool timing = stats != nullptr;
+    // Guided form: SceneExt::flags bit 0 samples diffuse vertices with the guide network, bit 1
+    // trains it online (one Adam step per chunk on the chunk's recorded samples), bit 2 starts
+    // from fresh weights.
+    const int gflags = ext ? ext->flags : 0;
+    const int guideMode = gflags & 3;
+    GuideTrainRec *trainRecs = nullptr;
+    int *trainCount = nullptr;
+    if (guideMode) {
+        guide_prepare(ds, ds.device, (gflags & 4) != 0, rp.seed);
+        if (rs.guideCap < rs.capacity) {
+            rs.guideFeat.ensure(size_t(rs.capacity) * kGuideIn * sizeof(__half));
+            rs.guideOut.ensure(size_t(rs.capacity) * kGuideOut * sizeof(float));
+            const size_t recBytes = size_t(rs.capacity) * kGuideVertices * 4 * sizeof(float4);
+            rs.guideRec.ensure(recBytes);
+            PRB_CUDA(cudaMemsetAsync(rs.guideRec.ptr, 0, recBytes, st));
+            rs.guideTrain.ensure(size_t(kGuideRecords) * sizeof(GuideTrainRec) + 256);
+            rs.guideCap = rs.capacity;
+        }
+        trainRecs = rs.guideTrain.as<GuideTrainRec>();
+        trainCount = reinterpret_cast<int *>(rs.guideTrain.as<unsigned char>() + size_t(kGuideRecords) * sizeof(GuideTrainRec));
+    }
     PRB_CUDA(cudaMemsetAsync(cnt, 0, kCntSlots * sizeof(int), st));
     PRB_CUDA(cudaMemsetAsync(dstats, 0, kStatSlots * sizeof(unsigned long long), st));
     for (int64_t pix0 = 0; pix0 < npix; pix0 += npixChunk) {
@@ -157,9 +236,18 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     else k_extend<false><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     k_classify<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin, cq, rs.capacity);
+                    if (guideMode & 1) {
+                        k_guide_features<<<gShade, 256, 0, st>>>(scene, rs.P, cnt, cq, rs.capacity,
+                                                                 rs.guideFeat.as<__half>());
+                        guide_infer_rows(st, ds.device, rs.guideFeat.as<__half>(), cnt + kCntClass0 + kClassDiffuse,
+                                         rs.capacity, rs.guideOut.as<float>());
+                        launches += 1 + kGuideInferLaunches;
+                    }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
-                    ShadeArgs sa{scene, nullptr, rs.P, rs.S, cq, rs.capacity, qout, cnt, rp.maxDepth, 0};
-                    k_shade<false><<<gShade, 256, 0, st>>>(sa);
+                    ShadeArgs sa{scene,       nullptr, rs.P, rs.S, cq, rs.capacity, qout, cnt, rp.maxDepth, 0,
+                                 rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode};
+                    if (guideMode) k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
+                    else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
                     if (scene.hasInterfaces) {
                         if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
@@ -191,6 +279,14 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
             if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * kBouncesPerPoll], st));
             k_film<<<grid_for(ds, np), 256, 0, st>>>(scene, rs.P, ci, rp.clampLuminance, rs.film.as<double>());
             ++launches;
+            if (guideMode & 2) {
+                PRB_CUDA(cudaMemsetAsync(trainCount, 0, sizeof(int), st));
+                k_guide_collect<<<grid_for(ds, total), 256, 0, st>>>(rs.P, rs.guideRec.as<float4>(), total, trainRecs,
+                                                                     trainCount, kGuideRecords);
+                for (int k = 0; k < kGuideRecords / kGuideBatch; ++k)
+                    guide_train_records(st, ds.device, trainRecs, trainCount, k * kGuideBatch, kGuideBatch, 0.f);
+                launches += 1 + (kGuideRecords / kGuideBatch) * kGuideTrainLaunches;
+            }
             if (timing) {
                 PRB_CUDA(cudaEventRecord(rs.ev[4 * kBouncesPerPoll + 1], st));
                 PRB_CUDA(cudaEventSynchronize(rs.ev[4 * kBouncesPerPoll + 1]));
@@ -220,6 +316,10 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     }
     if (status & kStatusStack) {
         *err = "BVH deeper than the traversal stack (64 entries)";
+        return false;
+    }
+    if (guideMode && guide_failed(ds, ds.device)) {
+        *err = "guide kernel timed out waiting for the tensor cores";
         return false;
     }
     // kStatusGuard: the 8,192-step guard of the reference ended some paths; not an error there either.

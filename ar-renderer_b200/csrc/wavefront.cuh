@@ -25,6 +25,7 @@
 #include <cmath>
 
 #include "bsdf.cuh"
+#include "guide.cuh"
 #include "lights.cuh"
 #include "media.cuh"
 #include "scene.cuh"
@@ -552,10 +553,16 @@ struct ShadeArgs {
     int *counters;
     int maxDepth;
     int halfSlots;           // batched form: slots [0, halfSlots) are half 0, the rest half 1
+    // Guided form: network outputs by position in the diffuse class queue, the per-path training
+    // records (kGuideVertices of 4 float4 each: xn + mean beta, n + BSDF pdf, wo + radiance
+    // snapshot, wi + state), and the mode (bit 0 sample with the guide, bit 1 record samples).
+    const float *guideOut;
+    float4 *guideRec;
+    int guideMode;
 };
 
 // One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
-template <bool kBatch = false>
+template <bool kBatch = false, bool kGuide = false>
 __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
     // The classes laid end to end: entry q belongs to the class whose prefix range holds it.
@@ -586,12 +593,28 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         Pcg rng{rs.x, rs.y};
         int depth = meta.y, medium = meta.z, flags = meta.w;
         bool specular = flags & 1;
+        int gcount = (flags >> 2) & 7;  // guided form: diffuse vertices passed (capped at kGuideVertices)
         int crossings = (flags >> 8) & 0xffff;
         float4 pp4 = P.prevP[j], pn4 = P.prevN[j];
         V3 prevP = mk(pp4.x, pp4.y, pp4.z), prevN = mk(pn4.x, pn4.y, pn4.z);
         int iters = __float_as_int(pn4.w) + 1;
         int prim = __float_as_int(hit.w);
         bool alive = true;
+        if constexpr (kGuide) if (a.guideMode & 2) {
+            // A record taken at this path's previous vertex: its radiance snapshot is the sum so far
+            // (that vertex's NEE included, nothing from here on), so the final sum minus it is the
+            // light that came along the sampled direction.
+            if (gcount > 0) {
+                float4 *rec = a.guideRec + 4 * (size_t(j) * kGuideVertices + gcount - 1);
+                float4 r3 = rec[3];
+                if (__float_as_int(r3.w) == 1) {
+                    float4 r2 = rec[2];
+                    r2.w = 0.25f * (L.v[0] + L.v[1] + L.v[2] + L.v[3]);
+                    rec[2] = r2;
+                    rec[3] = make_float4(r3.x, r3.y, r3.z, __int_as_float(2));
+                }
+            }
+        }
 
         auto misScale = [&]() {
             float av = 0.25f * (rpath.v[0] + rpath.v[1] + rpath.v[2] + rpath.v[3]);
@@ -604,7 +627,8 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         // NEE: queue a shadow ray carrying f * Le * w / pdf; the visibility test adds it later.
         // The shadow ray starts in the medium on the light's side of the vertex (medIn / medOut
         // for surfaces, the current medium for medium vertices where ng = 0).
-        auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut) {
+        auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut,
+                       const GuideMix *gmix) {
             float ul = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
             LightSample ls = sample_light(s, p, ng, lam, ul, u0, u1);
             if (!ls.ok) return;
@@ -616,6 +640,11 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 if (wol.z == 0.f) return;
                 f = lobe_f(*lobe, wol, wil) * fabsf(dot(ls.wi, ns));
                 spdf = lobe_pdf(*lobe, wol, wil);
+                // Guided vertices sample from the one-sample mixture: MIS against its pdf.
+                if constexpr (kGuide)
+                    if (gmix)
+                        spdf = gmix->c * guide_pdf_folded(*gmix, ls.wi, ns, dot(wo, ns) > 0.f ? 1.f : -1.f) +
+                               (1.f - gmix->c) * spdf;
             } else {
                 float ph = hg_phase(dot(wo, ls.wi), g);
                 f = splat(ph);
@@ -707,7 +736,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 } else {
                     ++depth;
                     V3 p = o + d * t, wo = -d;
-                    nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, g, medium, medium);
+                    nee(p, mk(0.f, 0.f, 0.f), nullptr, nullptr, mk(0.f, 0.f, 0.f), wo, g, medium, medium, nullptr);
                     float u0 = rng.uniform(), u1 = rng.uniform(), phasePdf;
                     V3 wi = hg_sample(wo, g, u0, u1, &phasePdf);
                     if (!(phasePdf > 0.f)) {
@@ -764,14 +793,73 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
                 Frame fr = frame_from_xz(sf.dpdu, sf.ns);
                 V3 wo = -d;
-                if (lobe.non_specular())
-                    nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside);
-                float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
                 V3 wol = fr.to_local(wo);
                 BSample bs;
-                bool ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
-                ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
-                     isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                bool ok;
+                if constexpr (kGuide) {
+                    GuideMix gm;
+                    // The guide is trained on, and applied at, the first kGuideVertices diffuse
+                    // vertices of each path.
+                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse;
+                    const bool inRange = diffuseVertex && gcount < kGuideVertices;
+                    const bool guided = (a.guideMode & 1) && inRange;
+                    const int recIndex = gcount;
+                    if (inRange) ++gcount;
+                    if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut);
+                    if (lobe.non_specular())
+                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
+                            guided ? &gm : nullptr);
+                    float pbGuide = 0.f;
+                    if (guided) {
+                        // One-sample MIS of the guide and the BSDF: wi ~ c q + (1 - c) p_bsdf.
+                        float us = rng.uniform(), uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                        V3 wiw;
+                        ok = wol.z != 0.f;
+                        const float side = dot(wo, sf.ns) > 0.f ? 1.f : -1.f;
+                        if (us < gm.c) {
+                            wiw = guide_sample(gm, uc, u0, u1);
+                            if (dot(wiw, sf.ns) * side < 0.f) wiw = guide_mirror(wiw, sf.ns);
+                        } else {
+                            BSample b2;
+                            ok = ok && lobe_sample(lobe, wol, uc, u0, u1, &b2);
+                            wiw = fr.from_local(b2.wi);
+                        }
+                        V3 wil = fr.to_local(wiw);
+                        pbGuide = lobe_pdf(lobe, wol, wil);
+                        bs.f = lobe_f(lobe, wol, wil);
+                        bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
+                        bs.wi = wil;
+                        bs.flags = kFlagReflection | kFlagDiffuse;
+                        bs.eta = 1.f;
+                    } else {
+                        float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                        ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                    }
+                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                    float4 *rec = a.guideRec + 4 * (size_t(j) * kGuideVertices + recIndex);
+                    if (ok && (a.guideMode & 2) && inRange) {
+                        // First diffuse vertex of the path: record (x, n, wo, wi, p_bsdf, mean beta).
+                        const float *bmin = s.root.box, *bmax = s.root.box + 3;
+                        V3 xn = mk((sf.p.x - bmin[0]) / fmaxf(bmax[0] - bmin[0], 1e-20f),
+                                   (sf.p.y - bmin[1]) / fmaxf(bmax[1] - bmin[1], 1e-20f),
+                                   (sf.p.z - bmin[2]) / fmaxf(bmax[2] - bmin[2], 1e-20f));
+                        V3 wiw = fr.from_local(bs.wi);
+                        float pbr = guided ? pbGuide : lobe_pdf(lobe, wol, bs.wi);
+                        float bavg = 0.25f * (beta.v[0] + beta.v[1] + beta.v[2] + beta.v[3]);
+                        rec[0] = make_float4(xn.x, xn.y, xn.z, bavg);
+                        rec[1] = make_float4(sf.ns.x, sf.ns.y, sf.ns.z, pbr);
+                        rec[2] = make_float4(wo.x, wo.y, wo.z, 0.f);
+                        rec[3] = make_float4(wiw.x, wiw.y, wiw.z, __int_as_float(1));
+                    }
+                } else {
+                    if (lobe.non_specular())
+                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr);
+                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                }
                 if (!ok) {
                     alive = false;
                 } else {
@@ -802,7 +890,8 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
             P.rpath[j] = to_f4(rpath);
             P.rng[j] = make_ulonglong2(rng.state, rng.inc);
             P.meta[j] = make_int4(meta.x, depth, medium,
-                                  (specular ? 1 : 0) | (min(crossings, 0xffff) << 8) | (flags & (0xff << kRenderShift)));
+                                  (specular ? 1 : 0) | (gcount << 2) | (min(crossings, 0xffff) << 8) |
+                                      (flags & (0xff << kRenderShift)));
             P.prevP[j] = make_float4(prevP.x, prevP.y, prevP.z, pp4.w);
             P.prevN[j] = make_float4(prevN.x, prevN.y, prevN.z, __int_as_float(iters));
             a.queueOut[warp_append(a.counters + kCntNext)] = j;

@@ -184,6 +184,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_guide_infer", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_guide_gradient", [C.c_int, C.c_int64, _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_guide_adam_step", [C.c_int, C.c_float, C.c_float, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_stats", [C.c_int, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_set_learning_rate", [C.c_int, C.c_float, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
                                         _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays_noalloc", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64,

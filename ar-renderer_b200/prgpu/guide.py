@@ -35,12 +35,17 @@ def infer(features: np.ndarray, device: int = 0) -> np.ndarray:
     return out
 
 
-def gradient(features: np.ndarray, wi: np.ndarray, pb: np.ndarray, w: np.ndarray, device: int = 0):
-    """(summed loss, gradient of the summed loss) from one GPU training pass."""
+def gradient(features: np.ndarray, wi: np.ndarray, pb: np.ndarray, w: np.ndarray, n: np.ndarray | None = None,
+             device: int = 0):
+    """(summed loss, gradient of the summed loss) from one GPU training pass. n: shading normals
+    (the folding planes; default: features[:, 75:78])."""
     f = np.ascontiguousarray(features, np.float32).reshape(-1, N_IN)
+    if n is None:
+        n = f[:, 75:78]
     s = np.ascontiguousarray(np.concatenate([np.asarray(wi, np.float32).reshape(-1, 3),
                                              np.asarray(pb, np.float32).reshape(-1, 1),
-                                             np.asarray(w, np.float32).reshape(-1, 1)], 1))
+                                             np.asarray(w, np.float32).reshape(-1, 1),
+                                             np.asarray(n, np.float32).reshape(-1, 3)], 1))
     g = np.zeros(N_PARAMS, np.float32)
     loss = C.c_float(0.0)
     err = abi.err_buf()
@@ -52,3 +57,17 @@ def gradient(features: np.ndarray, wi: np.ndarray, pb: np.ndarray, w: np.ndarray
 def adam_step(grad_scale: float, lr: float = 1e-3, device: int = 0) -> None:
     err = abi.err_buf()
     abi.check(abi.gpu_lib().prgpu_guide_adam_step(device, grad_scale, lr, err, len(err)), err, "prgpu_guide_adam_step")
+
+
+def stats(device: int = 0) -> dict:
+    """Last training pass: summed loss, online batch rows and weight sum, Adam steps taken."""
+    out = np.zeros(4, np.float32)
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_stats(device, abi.ptr(out), err, len(err)), err, "prgpu_guide_stats")
+    return {"loss_sum": float(out[0]), "rows": int(out[1]), "weight_sum": float(out[2]), "steps": int(out[3])}
+
+
+def set_learning_rate(lr: float, device: int = 0) -> None:
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_set_learning_rate(device, lr, err, len(err)), err,
+              "prgpu_guide_set_learning_rate")

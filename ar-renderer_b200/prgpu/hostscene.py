@@ -159,6 +159,8 @@ class HostScene:
             sd.camera = self.camera
             sd.filter = self.filter
             sd.cieYIntegral = spectra.cie_y_integral()
+            # The descriptor points into this object's arrays: keep them alive with it.
+            sd._owner = self
             self._desc = sd
         return self._desc
 
@@ -183,12 +185,17 @@ def build_box_scene(s: scenes.BoxScene) -> HostScene:
     for name, mat, quad in scenes.wall_quads():
         h.mesh(np.asarray(quad, np.float32), [0, 1, 2, 0, 2, 3], mats[mat], medium_inside=fog, medium_outside=fog)
     # Ceiling light: a 0.5 x 0.5 quad at (0, 0.999, -0.1) facing down (the "rect" light of the JSON form).
-    c, hs = np.array([0.0, 0.999, -0.1]), 0.25
+    c, hs = np.array([0.0, s.light_y, -0.1]), 0.25
     quad = np.array([[-hs, 0, -hs], [hs, 0, -hs], [hs, 0, hs], [-hs, 0, hs]])
     world = np.stack([quad[:, 2], -quad[:, 1], quad[:, 0]], axis=1) + c
-    h.mesh(world.astype(np.float32), [0, 2, 1, 0, 3, 2], black, normals=np.tile([0.0, -1.0, 0.0], (4, 1)),
-           light_spectrum=h.spectrum(spectra.blackbody(s.light_temperature)), light_scale=s.light_luminance,
-           medium_inside=fog, medium_outside=fog)
+    if s.light_up:  # facing the ceiling: the winding and normal flipped
+        h.mesh(world.astype(np.float32), [0, 1, 2, 0, 2, 3], black, normals=np.tile([0.0, 1.0, 0.0], (4, 1)),
+               light_spectrum=h.spectrum(spectra.blackbody(s.light_temperature)), light_scale=s.light_luminance,
+               medium_inside=fog, medium_outside=fog)
+    else:
+        h.mesh(world.astype(np.float32), [0, 2, 1, 0, 3, 2], black, normals=np.tile([0.0, -1.0, 0.0], (4, 1)),
+               light_spectrum=h.spectrum(spectra.blackbody(s.light_temperature)), light_scale=s.light_luminance,
+               medium_inside=fog, medium_outside=fog)
     for sp in s.spheres:
         p, n, f = scenes.sphere_mesh(sp, s.subdiv)
         if sp.material == "lambert":
@@ -196,5 +203,14 @@ def build_box_scene(s: scenes.BoxScene) -> HostScene:
         else:
             m = mats[sp.material]
         h.mesh(p, f, m, normals=n, medium_inside=fog, medium_outside=fog)
+    if s.slit > 0:
+        for quad in scenes.occluder_quads(s):
+            h.mesh(np.asarray(quad, np.float32), [0, 1, 2, 0, 2, 3], mats["white"], medium_inside=fog,
+                   medium_outside=fog)
+    for c_, r_, st in s.sss:
+        p, n, f = scenes.sphere_mesh(scenes.Sphere(c_, r_, "bk7"), s.subdiv)
+        med = h.medium(spectra.rgb_albedo(np.asarray(st) / max(st)) * 0.2 * max(st),
+                       spectra.rgb_albedo(np.asarray(st) / max(st)) * 0.8 * max(st), 0.0)
+        h.mesh(p, f, mats["bk7"], normals=n, medium_inside=med, medium_outside=fog)
     return h.finish(cam_pos=(0.0, -0.1, 0.98), cam_target=(0.0, -0.45, -0.3), fov_y=s.fov_y, width=s.width,
                     height=s.height)

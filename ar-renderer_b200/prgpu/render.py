@@ -49,10 +49,15 @@ def render_ex(scene, width: int, height: int, spp: int, first_sample: int = 0, s
     return (out, st) if stats else out
 
 
+GUIDE_SAMPLE, GUIDE_TRAIN, GUIDE_RESET = 1, 2, 4
+
+
 def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
-             block_size: int = 0, grid_media=None) -> abi.SceneExt:
+             block_size: int = 0, grid_media=None, guide: int = 0) -> abi.SceneExt:
     """SceneExt for prgpu_render_ex. grid_media: GridMediumDesc records (media.grid_desc), indexed
-    after the SceneDesc's homogeneous media. The record keeps the arrays it points at alive."""
+    after the SceneDesc's homogeneous media. guide: GUIDE_SAMPLE (sample diffuse vertices with the
+    guide network), GUIDE_TRAIN (train it online, one Adam step per wavefront chunk), GUIDE_RESET
+    (fresh weights first). The record keeps the arrays it points at alive."""
     e = abi.SceneExt()
     e.structSize = C.sizeof(abi.SceneExt)
     if light_bvh is not None and len(light_bvh):
@@ -61,6 +66,7 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
         e.lightBVHProb = light_bvh_prob
     e.wavefrontPaths = wavefront_paths
     e.blockSize = block_size
+    e.flags = guide
     e._keep = [light_bvh]
     if grid_media:
         from .media import grid_array

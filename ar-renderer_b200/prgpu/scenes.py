@@ -85,6 +85,17 @@ class BoxScene:
     light_luminance: float = 30.0
     fov_y: float = 62.0
     medium: dict | None = None  # {"sigma_a": [r,g,b], "sigma_s": [r,g,b], "g": 0.6}
+    # Slit variant: the ceiling light above a horizontal occluder at y = occluder_y with a slit of
+    # this width along z through its middle (0 = no occluder).
+    slit: float = 0.0
+    occluder_y: float = 0.8
+    # Subsurface spheres: (centre, radius, sigma_t rgb); BK7 surface, homogeneous interior with
+    # albedo 0.8 (sigma_s = 0.8 sigma_t).
+    sss: list = field(default_factory=list)
+    # Indirect variant: the ceiling light turned to face up (lowered to y = light_y), so the room
+    # is lit only by the bright patch it makes on the ceiling (next-event estimation finds no light).
+    light_up: bool = False
+    light_y: float = 0.999
     # Heterogeneous variant: {"sigma_a", "sigma_s", "g", "scale", "density" (nz, ny, nx) float32,
     # "bounds" (2, 3) medium space, "matrix" 4x4 medium-to-world}; replaces `medium`.
     grid: dict | None = None
@@ -122,6 +133,40 @@ def box_scene(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64,
         rng = np.random.default_rng(1000 + seed)
         s.medium = {"sigma_s": [float(x) for x in rng.uniform(0.05, 0.5, 3)],
                     "sigma_a": [float(x) for x in rng.uniform(0.0, 0.1, 3)], "g": 0.6}
+    return s
+
+
+def slit_scene(seed: int = 0, width: int = 1024, height: int = 1024, spp: int = 64, max_depth: int = 32,
+               subdiv: int = 3, sss_count: int = 12) -> BoxScene:
+    """The guided-vs-plain scene: the box of box_scene, its ceiling light hidden behind a
+    horizontal occluder at y = 0.8 so that light enters only through a 0.1-wide slit, plus
+    `sss_count` subsurface BK7 spheres (interior sigma_t RGB uniform in [1, 20]) in place of the
+    pyramid."""
+    s = BoxScene(width=width, height=height, spp=spp, max_depth=max_depth, seed=seed, subdiv=subdiv)
+    s.slit = 0.1
+    rng = np.random.default_rng(5000 + seed)
+    r = 0.14
+    for k in range(sss_count):
+        x = -0.75 + 0.3 * (k % 6)
+        z = -0.55 + 0.45 * (k // 6)
+        s.sss.append(((x, -1.0 + r, z), r, [float(v) for v in rng.uniform(1.0, 20.0, 3)]))
+    return s
+
+
+def occluder_quads(s: BoxScene):
+    """The two occluder quads (corners counter-clockwise seen from below) leaving the slit open."""
+    y, h = s.occluder_y, s.slit / 2
+    return [[(-1, y, -1), (-1, y, 1), (-h, y, 1), (-h, y, -1)],
+            [(h, y, -1), (h, y, 1), (1, y, 1), (1, y, -1)]]
+
+
+def indirect_scene(seed: int = 0, width: int = 64, height: int = 64, spp: int = 64, max_depth: int = 16,
+                   subdiv: int = 2) -> BoxScene:
+    """The box-and-spheres scene lit only indirectly: its light faces the ceiling from y = 0.9."""
+    s = box_scene(seed=seed, width=width, height=height, spp=spp, max_depth=max_depth, subdiv=subdiv)
+    s.light_up = True
+    s.light_y = 0.9
+    s.light_luminance = 300.0
     return s
 
 
@@ -223,6 +268,19 @@ def to_reference_json(s: BoxScene) -> dict:
             mid = sp.material
         objects.append({"name": gid, "geometry": gid, "material": mid})
     media = {}
+    if s.slit > 0:
+        for k, quad in enumerate(occluder_quads(s)):
+            gid = f"occluder{k}"
+            geometry[gid] = {"type": "mesh", "positions": _f32(quad), "indices": [0, 1, 2, 0, 2, 3]}
+            objects.append({"name": gid, "geometry": gid, "material": "white"})
+    for k, (c, r, st) in enumerate(s.sss):
+        p, n, f = sphere_mesh(Sphere(c, r, "bk7"), s.subdiv)
+        gid = f"sss{k}"
+        geometry[gid] = {"type": "mesh", "positions": _f32(p), "normals": _f32(n),
+                         "indices": [int(x) for x in f.ravel()], "closed": True}
+        media[gid] = {"type": "homogeneous", "sigma_s": [0.8 * v for v in st], "sigma_a": [0.2 * v for v in st],
+                      "g": 0.0}
+        objects.append({"name": gid, "geometry": gid, "material": "bk7", "interior": gid})
     if s.medium is not None:
         media["fog"] = {"type": "homogeneous", "sigma_a": s.medium["sigma_a"], "sigma_s": s.medium["sigma_s"],
                         "g": s.medium["g"]}

@@ -226,7 +226,9 @@ struct SceneExt {
     float lightBVHProb;             // probability of the BVH branch when envSpectrum >= 0 (1 - pInfinite)
     int32_t wavefrontPaths;         // paths in flight per wavefront (0 = library default)
     int32_t blockSize;              // threads per block for the wavefront kernels (0 = default)
-    int32_t flags;                  // reserved, 0
+    int32_t flags;                  // path guiding: bit 0 sample diffuse vertices with the guide
+                                    // network (one-sample MIS with the BSDF), bit 1 train it online
+                                    // (one Adam step per wavefront chunk), bit 2 fresh weights first
     int32_t gridMediumCount;
     const GridMediumDesc *gridMedia;
 };
@@ -377,10 +379,18 @@ PRGPU_API int prgpu_guide_set_weights(int deviceIndex, const float *weights, cha
 PRGPU_API int prgpu_guide_get_weights(int deviceIndex, float *weights, char *err, int errLen);
 // Network outputs (n x 48 floats) for n feature rows (n x 128 floats, rounded to FP16 on the device).
 PRGPU_API int prgpu_guide_infer(int deviceIndex, int64_t n, const float *features, float *out, char *err, int errLen);
-// One training pass: samples are n x 5 floats (wi[3], BSDF pdf of wi, weight w); writes the summed
-// loss -sum w log(c q(wi) + (1 - c) pdf) and its gradient w.r.t. the weights (kGuideParams floats).
+// One training pass: samples are n x 8 floats (wi[3], BSDF pdf of wi, weight w, shading normal[3]);
+// writes the summed loss -sum w (log q_n(wi) + log(c q_n(wi) + (1 - c) pdf)) (q_n: the mixture
+// folded onto the normal's hemisphere holding wi) and its gradient w.r.t. the weights
+// (kGuideParams floats; the selection term's gradient taken at fixed q_n).
 PRGPU_API int prgpu_guide_gradient(int deviceIndex, int64_t n, const float *features, const float *samples,
                                    float *lossSum, float *grad, char *err, int errLen);
+// Learning rate of online training (default 1e-3), per device.
+PRGPU_API int prgpu_guide_set_learning_rate(int deviceIndex, float learningRate, char *err, int errLen);
+// Training state: out4 = {summed loss of the last training pass (with the batch's weights
+// normalised to mean 1 in online training), rows of the last online batch, their weight sum,
+// Adam steps taken}.
+PRGPU_API int prgpu_guide_stats(int deviceIndex, float *out4, char *err, int errLen);
 // Adam step (beta 0.9 / 0.999, eps 1e-8) on the last gradient times gradScale.
 PRGPU_API int prgpu_guide_adam_step(int deviceIndex, float gradScale, float learningRate, char *err, int errLen);
 

@@ -13,7 +13,10 @@ FP32 accumulation order.
 Outputs, per lobe k < 8: direction (3, normalised), log kappa (clamped to [-4, 8]), weight
 logit; output 40 the selection logit, c = 0.9 sigmoid. Mixture pdf of a unit direction w:
 q(w) = sum_k pi_k kappa_k / (2 pi (1 - e^{-2 kappa_k})) exp(kappa_k (mu_k . w - 1)).
-Loss per sample: -w log(c q(wi) + (1 - c) pb).
+The renderer folds the mixture onto the hemisphere of the shading normal n that holds the sample:
+q_n(w) = q(w) + q(w - 2 (w.n) n). Loss per sample, two parts: -w log q_n(wi) trains the lobes,
+-w log(c q_n(wi) + (1 - c) pb) trains the selection output with q_n held fixed (its gradient is
+taken as if q_n were a constant).
 """
 
 from __future__ import annotations
@@ -120,33 +123,46 @@ def mixture_pdf(o, w):
     return (pi * vmf(mu, kappa, w)).sum(1), c
 
 
-def loss_and_grad_out(o, wi, pb, wgt):
-    """Loss per sample and its gradient w.r.t. the 48 outputs (FP64, analytic)."""
+def mirror(w, n):
+    return w - 2.0 * (w * n).sum(1, keepdims=True) * n
+
+
+def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None):
+    """Loss per sample and its gradient w.r.t. the 48 outputs (FP64, analytic); n: the shading
+    normals (folding planes). The mixture part uses q_fixed when given (the value whose gradient
+    is stopped), else the current q_n."""
     o = np.asarray(o, np.float64)
     mu, kappa, pi, c = decode(o)
-    vk = vmf(mu, kappa, wi)
+    wr = mirror(wi, n)
+    v1 = vmf(mu, kappa, wi)
+    v2 = vmf(mu, kappa, wr)
+    vk = v1 + v2
     q = (pi * vk).sum(1)
-    p = c * q + (1 - c) * pb
-    ok = (p > 0) & (wgt > 0)
+    qm = q if q_fixed is None else q_fixed
+    p = c * qm + (1 - c) * pb
+    ok = (p > 0) & (q > 0) & (wgt > 0)
     ps = np.where(ok, p, 1.0)
-    loss = np.where(ok, -wgt * np.log(ps), 0.0)
-    dq = np.where(ok, -wgt * c / ps, 0.0)
-    dc = np.where(ok, -wgt * (q - pb) / ps, 0.0)
+    qs = np.where(ok, q, 1.0)
+    loss = np.where(ok, -wgt * np.log(qs) - wgt * np.log(ps), 0.0)
+    dq = np.where(ok, -wgt / qs, 0.0)
+    dc = np.where(ok, -wgt * (qm - pb) / ps, 0.0)
     g = np.zeros_like(o)
     s = 1.0 / (1.0 + np.exp(-o[:, 40]))
     g[:, 40] = dc * MAX_SELECT * s * (1 - s)
     gpi = dq[:, None] * vk
     sum_pig = (pi * gpi).sum(1, keepdims=True)
     ga = pi * gpi - pi * sum_pig
-    dv = dq[:, None] * pi * vk
+    d1 = dq[:, None] * pi * v1
+    d2 = dq[:, None] * pi * v2
     raw = o[:, :40].reshape(-1, LOBES, 5)[:, :, 3]
     e = np.exp(-2 * kappa)
-    dlog = np.where(kappa < 1e-4, 0.0, 1.0 / kappa - 2 * e / -np.expm1(-2 * kappa)
-                    + (np.einsum("nkc,nc->nk", mu, wi) - 1.0))
-    gk = np.where((raw > -4) & (raw < 8), dv * dlog * kappa, 0.0)
+    base = 1.0 / kappa - 2 * e / -np.expm1(-2 * kappa)
+    t1 = np.einsum("nkc,nc->nk", mu, wi) - 1.0
+    t2 = np.einsum("nkc,nc->nk", mu, wr) - 1.0
+    gk = np.where((raw > -4) & (raw < 8) & (kappa >= 1e-4), (d1 * (base + t1) + d2 * (base + t2)) * kappa, 0.0)
     d = o[:, :40].reshape(-1, LOBES, 5)[:, :, 0:3]
     l = np.linalg.norm(d, axis=2, keepdims=True)
-    gm = wi[:, None, :] * (dv * kappa)[:, :, None]
+    gm = (wi[:, None, :] * d1[:, :, None] + wr[:, None, :] * d2[:, :, None]) * kappa[:, :, None]
     gv = (gm - mu * np.einsum("nkc,nkc->nk", mu, gm)[:, :, None]) / np.maximum(l, 1e-300)
     gv = np.where(l > 1e-6, gv, 0.0)
     G = g[:, :40].reshape(-1, LOBES, 5)
@@ -157,10 +173,19 @@ def loss_and_grad_out(o, wi, pb, wgt):
     return loss, g
 
 
-def backward(params, X, wi, pb, wgt, round16=True):
-    """Mean loss over the batch and the gradient of the SUMMED loss w.r.t. the flat weights."""
+def mixture_q(o, wi, n):
+    """The folded mixture density q_n(wi) (wi on the side of n it was sampled on)."""
+    mu, kappa, pi, _ = decode(np.asarray(o, np.float64))
+    return (pi * (vmf(mu, kappa, wi) + vmf(mu, kappa, mirror(wi, n)))).sum(1)
+
+
+def backward(params, X, wi, pb, wgt, round16=True, n=None):
+    """Mean loss over the batch and the gradient of the SUMMED loss w.r.t. the flat weights
+    (n: folding normals, by default the normal inputs X[:, 75:78])."""
     out, (W, acts, zs) = forward(params, X, round16)
-    loss, g = loss_and_grad_out(out, wi, pb, wgt)
+    if n is None:
+        n = np.asarray(X, np.float64)[:, 75:78]
+    loss, g = loss_and_grad_out(out, wi, pb, wgt, n)
     grads = [None] * 5
     dZ = _r16(g, round16)
     for l in range(4, -1, -1):

@@ -43,14 +43,18 @@ def test_output_gradient_matches_finite_differences():
     rng = np.random.default_rng(1)
     n = 6
     o = rng.normal(0, 1.0, (n, 48))
-    _, wi, pb, w = _batch(n, 2)
-    _, g = G.loss_and_grad_out(o, wi, pb, w)
+    X, wi, pb, w = _batch(n, 2)
+    nrm = X[:, 75:78]
+    wi = np.where((wi * nrm).sum(1, keepdims=True) < 0, G.mirror(wi, nrm), wi)
+    # The gradient is that of the surrogate whose mixture term holds q_n at its current value.
+    q0 = G.mixture_q(o, wi, nrm)
+    _, g = G.loss_and_grad_out(o, wi, pb, w, nrm, q_fixed=q0)
     h = 1e-6
     for i in list(range(0, 41)):
         d = np.zeros_like(o)
         d[:, i] = h
-        lp, _ = G.loss_and_grad_out(o + d, wi, pb, w)
-        lm, _ = G.loss_and_grad_out(o - d, wi, pb, w)
+        lp, _ = G.loss_and_grad_out(o + d, wi, pb, w, nrm, q_fixed=q0)
+        lm, _ = G.loss_and_grad_out(o - d, wi, pb, w, nrm, q_fixed=q0)
         np.testing.assert_allclose(g[:, i], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-7)
 
 
@@ -61,11 +65,13 @@ def test_weight_gradient_matches_finite_differences():
     rng = np.random.default_rng(7)
     idx = np.concatenate([rng.choice(np.flatnonzero(p != 0), 40, replace=False), [81, 8192 + 64 * 5 + 63]])
     h = 1e-4  # the loss carries ~1e-12 of rounding noise, so smaller steps lose digits
+    nrm = X[:, 75:78]
+    q0 = G.mixture_q(G.forward(p, X, False)[0], wi, nrm)
     for i in idx:
         d = np.zeros_like(p)
         d[i] = h
-        lp = G.loss_and_grad_out(G.forward(p + d, X, False)[0], wi, pb, w)[0].sum()
-        lm = G.loss_and_grad_out(G.forward(p - d, X, False)[0], wi, pb, w)[0].sum()
+        lp = G.loss_and_grad_out(G.forward(p + d, X, False)[0], wi, pb, w, nrm, q_fixed=q0)[0].sum()
+        lm = G.loss_and_grad_out(G.forward(p - d, X, False)[0], wi, pb, w, nrm, q_fixed=q0)[0].sum()
         assert abs(grad[i] - (lp - lm) / (2 * h)) <= 1e-3 * max(0.1, abs(grad[i])), i
 
 
