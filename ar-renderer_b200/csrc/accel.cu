@@ -14,8 +14,8 @@ namespace prb {
 // atomic per warp and refill), then the lanes advance their traversals one node or leaf per
 // iteration. Incoherent rays end after very different numbers of steps; refilling keeps the
 // lanes of a warp busy instead of idling until the warp's longest ray ends.
-template <bool kAny>
-__global__ void __launch_bounds__(256) k_trace_persist(const WNode *__restrict__ nodes,
+template <bool kAny, bool kWide>
+__global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ nodes,
                                                        const LeafPrim *__restrict__ prims, RootInfo root,
                                                        const float4 *__restrict__ rays, int64_t n,
                                                        int32_t *__restrict__ primOut, float *__restrict__ tOut,
@@ -68,7 +68,16 @@ __global__ void __launch_bounds__(256) k_trace_persist(const WNode *__restrict__
             }
         }
         if (__all_sync(full, exhausted)) break;
-        if (active && traverse_step<kAny, false>(nodes, prims, r, s, stackRef, stackT, &overflow)) {
+        bool done = false;
+        if (active) {
+            if (kWide)
+                done = traverse4_step<kAny, false>(static_cast<const QNode *>(nodes), prims, r, s, stackRef, stackT,
+                                                   &overflow);
+            else
+                done = traverse_step<kAny, false>(static_cast<const WNode *>(nodes), prims, r, s, stackRef, stackT,
+                                                  &overflow);
+        }
+        if (done) {
             active = false;
             if (kAny) {
                 primOut[idx] = s.found ? 1 : 0;
@@ -91,25 +100,41 @@ template <typename K> int resident_blocks(K kernel, int block) {
 }
 
 // dStatus points at the accel's 16-byte status block: int status at 0, ray counter at 8.
+// wide: the 4-wide tree (fast; hits identical up to the order among exactly equal distances);
+// otherwise the binary tree in the reference's visit order (bvh.cpp:184-190).
 void launch_trace(const DeviceAccel &acc, const prgpu::Ray *dRays, int64_t n, bool anyHit, int32_t *dPrim,
-                  float *dT, float *dB1, float *dB2, int *dStatus, cudaStream_t s, int smCount) {
+                  float *dT, float *dB1, float *dB2, int *dStatus, cudaStream_t s, int smCount, bool wide) {
     if (n <= 0) return;
     const int block = 256;
-    static int residentAny = 0, residentClosest = 0;
-    if (!residentAny) residentAny = resident_blocks(k_trace_persist<true>, block);
-    if (!residentClosest) residentClosest = resident_blocks(k_trace_persist<false>, block);
+    static int resident[2][2] = {{0, 0}, {0, 0}};
+    if (!resident[0][0]) {
+        resident[0][0] = resident_blocks(k_trace_persist<false, false>, block);
+        resident[0][1] = resident_blocks(k_trace_persist<false, true>, block);
+        resident[1][0] = resident_blocks(k_trace_persist<true, false>, block);
+        resident[1][1] = resident_blocks(k_trace_persist<true, true>, block);
+    }
+    const void *nodes = wide ? acc.qnodes.ptr : acc.nodes.ptr;
+    const int residentAny = resident[1][wide ? 1 : 0], residentClosest = resident[0][wide ? 1 : 0];
     auto *counter = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(dStatus) + 8);
     PRB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
     int64_t blocksNeeded = (n + block - 1) / block;
     const auto *r4 = reinterpret_cast<const float4 *>(dRays);
     if (anyHit) {
         int grid = int(std::min<int64_t>(blocksNeeded, int64_t(smCount) * residentAny));
-        k_trace_persist<true><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4, n,
-                                                     dPrim, nullptr, nullptr, nullptr, dStatus, counter);
+        if (wide)
+            k_trace_persist<true, true><<<grid, block, 0, s>>>(nodes, acc.prims.as<LeafPrim>(), acc.root, r4, n, dPrim,
+                                                               nullptr, nullptr, nullptr, dStatus, counter);
+        else
+            k_trace_persist<true, false><<<grid, block, 0, s>>>(nodes, acc.prims.as<LeafPrim>(), acc.root, r4, n, dPrim,
+                                                                nullptr, nullptr, nullptr, dStatus, counter);
     } else {
         int grid = int(std::min<int64_t>(blocksNeeded, int64_t(smCount) * residentClosest));
-        k_trace_persist<false><<<grid, block, 0, s>>>(acc.nodes.as<WNode>(), acc.prims.as<LeafPrim>(), acc.root, r4,
-                                                      n, dPrim, dT, dB1, dB2, dStatus, counter);
+        if (wide)
+            k_trace_persist<false, true><<<grid, block, 0, s>>>(nodes, acc.prims.as<LeafPrim>(), acc.root, r4, n, dPrim,
+                                                                dT, dB1, dB2, dStatus, counter);
+        else
+            k_trace_persist<false, false><<<grid, block, 0, s>>>(nodes, acc.prims.as<LeafPrim>(), acc.root, r4, n,
+                                                                 dPrim, dT, dB1, dB2, dStatus, counter);
     }
     count_launch();
     PRB_CUDA(cudaGetLastError());
@@ -148,7 +173,7 @@ bool make_accel(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
 // Host-buffer query: rays are copied in chunks on the copy stream while the previous chunk is
 // traced on the compute stream; results are copied back per chunk.
 bool trace_host(prgpu_accel_t *a, const prgpu::Ray *rays, int64_t n, int anyHit, int32_t *primOut, float *tOut,
-                float *b1Out, float *b2Out, std::string *err) {
+                float *b1Out, float *b2Out, bool wide, std::string *err) {
     DeviceState &ds = device_state(a->device);
     const int64_t chunk = int64_t(1) << 22;
     int64_t cap = std::min<int64_t>(n, 2 * chunk);
@@ -177,7 +202,7 @@ bool trace_host(prgpu_accel_t *a, const prgpu::Ray *rays, int64_t n, int anyHit,
         launch_trace(a->acc, a->rays.as<prgpu::Ray>() + base, cnt, anyHit != 0, a->prim.as<int32_t>() + base,
                      tOut ? a->t.as<float>() + base : nullptr, b1Out ? a->b1.as<float>() + base : nullptr,
                      b2Out ? a->b2.as<float>() + base : nullptr, a->status.as<int>(), ds.stream,
-                     ds.prop.multiProcessorCount);
+                     ds.prop.multiProcessorCount, wide);
         PRB_CUDA(cudaMemcpyAsync(primOut + off, a->prim.as<int32_t>() + base, size_t(cnt) * sizeof(int32_t),
                                  cudaMemcpyDeviceToHost, ds.stream));
         if (tOut)
@@ -221,7 +246,7 @@ PRGPU_API int prgpu_trace_rays(int deviceIndex, const prgpu::BVHNode *nodes, int
         prgpu_accel_t a;
         std::string e;
         bool ok = make_accel(deviceIndex, nodes, nodeCount, primOrder, triVerts, primCount, &a, &e) &&
-                  trace_host(&a, rays, rayCount, anyHit, primOut, tOut, b1Out, b2Out, &e);
+                  trace_host(&a, rays, rayCount, anyHit, primOut, tOut, b1Out, b2Out, false, &e);
         a.acc.release();
         a.status.release();
         a.rays.release();
@@ -279,7 +304,7 @@ PRGPU_API int prgpu_accel_trace(prgpu_accel accel, const prgpu::Ray *deviceRays,
     try {
         DeviceState &ds = device_state(accel->device);
         launch_trace(accel->acc, deviceRays, rayCount, anyHit != 0, devicePrimOut, deviceTOut, nullptr, nullptr,
-                     accel->status.as<int>(), static_cast<cudaStream_t>(stream), ds.prop.multiProcessorCount);
+                     accel->status.as<int>(), static_cast<cudaStream_t>(stream), ds.prop.multiProcessorCount, true);
         return 0;
     } catch (const CudaError &e) {
         set_err(err, errLen, e.msg);
@@ -298,7 +323,7 @@ PRGPU_API int prgpu_accel_trace_host(prgpu_accel accel, const prgpu::Ray *rays, 
     }
     try {
         std::string e;
-        if (!trace_host(accel, rays, rayCount, anyHit, primOut, tOut, nullptr, nullptr, &e)) {
+        if (!trace_host(accel, rays, rayCount, anyHit, primOut, tOut, nullptr, nullptr, true, &e)) {
             set_err(err, errLen, e);
             return 1;
         }

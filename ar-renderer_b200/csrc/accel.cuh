@@ -4,6 +4,8 @@
 // kernel read out of bounds or loop.
 #pragma once
 
+#include <limits>
+
 #include <string>
 #include <vector>
 
@@ -21,8 +23,67 @@ struct RootInfo {
 struct HostAccel {
     std::vector<WNode> nodes;
     std::vector<LeafPrim> prims;
+    std::vector<QNode> qnodes;  // the same tree collapsed to 4-wide nodes (root = QNode 0 when interior)
     RootInfo root{};
 };
+
+// Collapses the binary tree under interior WNode w into 4-wide nodes: a node takes its two
+// children and, while it has fewer than four, opens the interior child of largest surface area.
+inline int collapse4(const HostAccel &b, int w, std::vector<QNode> *out) {
+    struct Kid {
+        int ref;
+        float lo[3], hi[3];
+    };
+    auto kidsOf = [&](int wi, Kid *k) {
+        const WNode &n = b.nodes[size_t(wi)];
+        k[0] = Kid{n.r.x, {n.a.x, n.a.y, n.a.z}, {n.a.w, n.b.x, n.b.y}};
+        k[1] = Kid{n.r.y, {n.b.z, n.b.w, n.c.x}, {n.c.y, n.c.z, n.c.w}};
+    };
+    auto area = [](const Kid &k) {
+        float dx = k.hi[0] - k.lo[0], dy = k.hi[1] - k.lo[1], dz = k.hi[2] - k.lo[2];
+        return dx * dy + dy * dz + dz * dx;
+    };
+    Kid kids[4];
+    int nk = 2;
+    kidsOf(w, kids);
+    while (nk < 4) {
+        int best = -1;
+        float bestA = -1.f;
+        for (int i = 0; i < nk; ++i)
+            if (kids[i].ref >= 0 && area(kids[i]) > bestA) {
+                bestA = area(kids[i]);
+                best = i;
+            }
+        if (best < 0) break;
+        Kid two[2];
+        kidsOf(kids[best].ref, two);
+        kids[best] = two[0];
+        kids[nk++] = two[1];
+    }
+    const int idx = int(out->size());
+    out->push_back(QNode{});
+    float lo[3][4], hi[3][4];
+    int ch[4];
+    const float inf = std::numeric_limits<float>::infinity();
+    for (int i = 0; i < 4; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a][i] = i < nk ? kids[i].lo[a] : inf;
+            hi[a][i] = i < nk ? kids[i].hi[a] : -inf;
+        }
+        ch[i] = 0;
+    }
+    for (int i = 0; i < nk; ++i) ch[i] = kids[i].ref >= 0 ? collapse4(b, kids[i].ref, out) : kids[i].ref;
+    QNode &q = (*out)[size_t(idx)];
+    q.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    q.loy = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    q.loz = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    q.hix = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    q.hiy = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    q.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    q.child = make_int4(ch[0], ch[1], ch[2], ch[3]);
+    q.pad = make_int4(0, 0, 0, 0);
+    return idx;
+}
 
 // Per-primitive geometry accessor for the conversion: fills the leaf record of primitive `prim`.
 struct TriangleSoupSource {
@@ -148,12 +209,17 @@ bool convert_bvh(const prgpu::BVHNode *nodes, int32_t nodeCount, const int32_t *
     out->root.box[5] = r.bmax.z;
     out->root.ref = childRef(0);
     out->root.empty = 0;
+    out->qnodes.clear();
+    if (out->root.ref >= 0) {
+        out->qnodes.reserve(out->nodes.size() / 2 + 1);
+        collapse4(*out, out->root.ref, &out->qnodes);
+    }
     return true;
 }
 
 // Device copy of a converted BVH.
 struct DeviceAccel {
-    DevBuf nodes, prims;
+    DevBuf nodes, prims, qnodes;
     RootInfo root{};
     int device = -1;
     int64_t bytes = 0;
@@ -166,12 +232,18 @@ struct DeviceAccel {
             PRB_CUDA(cudaMemcpyAsync(nodes.ptr, h.nodes.data(), h.nodes.size() * sizeof(WNode), cudaMemcpyHostToDevice, s));
         if (!h.prims.empty())
             PRB_CUDA(cudaMemcpyAsync(prims.ptr, h.prims.data(), h.prims.size() * sizeof(LeafPrim), cudaMemcpyHostToDevice, s));
+        size_t qb = std::max<size_t>(1, h.qnodes.size()) * sizeof(QNode);
+        qnodes.ensure(qb);
+        if (!h.qnodes.empty())
+            PRB_CUDA(cudaMemcpyAsync(qnodes.ptr, h.qnodes.data(), h.qnodes.size() * sizeof(QNode),
+                                     cudaMemcpyHostToDevice, s));
         root = h.root;
-        bytes = int64_t(h.nodes.size() * sizeof(WNode) + h.prims.size() * sizeof(LeafPrim));
+        bytes = int64_t(h.qnodes.size() * sizeof(QNode) + h.prims.size() * sizeof(LeafPrim));
     }
     void release() {
         nodes.release();
         prims.release();
+        qnodes.release();
     }
 };
 

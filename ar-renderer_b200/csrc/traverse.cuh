@@ -36,6 +36,15 @@ struct __align__(16) LeafPrim {
     float4 v2;  // triangle: e2, end-of-leaf mark (int bits 1 on a leaf's last slot, else 0)
 };
 
+// 4-wide node, collapsed on the host from the binary tree: the four child boxes stored per axis
+// (child i in component i of each float4) and the four child references; 128 bytes, one L2 line.
+// Unused child slots carry an inverted box (+inf / -inf), which the slab test always rejects.
+struct __align__(16) QNode {
+    float4 lox, loy, loz, hix, hiy, hiz;
+    int4 child;  // >= 0: interior QNode; < 0: leaf whose first slot is ~child
+    int4 pad;
+};
+
 constexpr int kStackSize = 64;
 // 1 + 2 * 1.2e-7f * 3 evaluated in float, the far-distance widening of bvh.cpp:143-151.
 constexpr float kWiden = 0x1.00000cp+0f;
@@ -265,6 +274,97 @@ __device__ __forceinline__ bool traverse_step(const WNode *__restrict__ nodes, c
         }
         if (nHit && nT < s.tMax) {
             s.ref = nRef;
+            return false;
+        }
+    } else {
+        const LeafPrim *p = prims + ~s.ref;
+        for (bool last = false; !last; ++p) {
+            float4 v0 = __ldg(&p->v0), v1 = __ldg(&p->v1), v2 = __ldg(&p->v2);
+            last = __float_as_int(v2.w) != 0;
+            float t, u = 0.f, v = 0.f;
+            bool h;
+            if (kSpheres && __float_as_int(v1.w) == 1)
+                h = hit_sphere(r, v0, v1, s.tMax, &t);
+            else
+                h = hit_triangle(r, v0, v1, v2, s.tMax, &t, &u, &v);
+            if (h) {
+                s.found = true;
+                if (kAny) return true;
+                s.tMax = t;
+                s.hit.t = t;
+                s.hit.u = u;
+                s.hit.v = v;
+                s.hit.prim = __float_as_int(v0.w);
+            }
+        }
+    }
+    while (s.sp > 0) {
+        --s.sp;
+        if (stackT[s.sp] < s.tMax) {
+            s.ref = stackRef[s.sp];
+            return false;
+        }
+    }
+    return true;
+}
+
+// The step traversal over the 4-wide tree: the children a node's slab tests accept (entry before
+// tMax) are visited nearest first, the others pushed with their entry distance, farthest first.
+// Box and triangle arithmetic are those of the binary traversal, so a hit's primitive and
+// distance are the reference's; only the order among hits at exactly equal distance can differ
+// (the binary traversal reproduces the reference's visit order for those).
+__device__ __forceinline__ void cswap(float &ta, int &ra, float &tb, int &rb) {
+    if (tb < ta) {
+        float t = ta;
+        ta = tb;
+        tb = t;
+        int q = ra;
+        ra = rb;
+        rb = q;
+    }
+}
+
+template <bool kAny, bool kSpheres>
+__device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
+                                               const TraceRay &r, TravState &s, int *stackRef, float *stackT,
+                                               bool *overflow) {
+    if (s.ref >= 0) {
+        const QNode *n = nodes + s.ref;
+        const float4 lx = __ldg(&n->lox), ly = __ldg(&n->loy), lz = __ldg(&n->loz);
+        const float4 hx = __ldg(&n->hix), hy = __ldg(&n->hiy), hz = __ldg(&n->hiz);
+        const int4 ch = __ldg(&n->child);
+        float t0, t1, t2, t3;
+        const float inf = __int_as_float(0x7f800000);
+        t0 = box_entry(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, &t0) && t0 < s.tMax ? t0 : inf;
+        t1 = box_entry(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, &t1) && t1 < s.tMax ? t1 : inf;
+        t2 = box_entry(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, &t2) && t2 < s.tMax ? t2 : inf;
+        t3 = box_entry(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, &t3) && t3 < s.tMax ? t3 : inf;
+        int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
+        // Sorting network for 4 (5 compare-exchanges); misses sort last at +inf.
+        cswap(t0, r0, t1, r1);
+        cswap(t2, r2, t3, r3);
+        cswap(t0, r0, t2, r2);
+        cswap(t1, r1, t3, r3);
+        cswap(t1, r1, t2, r2);
+        if (t0 < inf) {
+            const int extra = (t1 < inf) + (t2 < inf) + (t3 < inf);
+            if (s.sp + extra > kStackSize) {
+                *overflow = true;
+                return true;
+            }
+            if (t3 < inf) {
+                stackRef[s.sp] = r3;
+                stackT[s.sp++] = t3;
+            }
+            if (t2 < inf) {
+                stackRef[s.sp] = r2;
+                stackT[s.sp++] = t2;
+            }
+            if (t1 < inf) {
+                stackRef[s.sp] = r1;
+                stackT[s.sp++] = t1;
+            }
+            s.ref = r0;
             return false;
         }
     } else {

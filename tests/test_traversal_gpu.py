@@ -156,3 +156,28 @@ def test_device_resident_path_matches_host_path(gpu):
     acc.trace_host(rays, prim, t, any_hit=False)
     np.testing.assert_array_equal(prim, hp)
     acc.close()
+
+
+def test_wide_tree_matches_reference(gpu, oracle):
+    """The accel path traverses the 4-wide collapse of the tree (nearest child first); hits carry
+    the reference's primitive and distance bits, except possibly at exactly equal distances (the
+    visit order differs from the reference's), closest and any hit, on the full-size soup."""
+    verts = workloads.triangle_soup(1 << 20, seed=1)
+    rays = workloads.soup_rays(1 << 21, seed=2)
+    nodes, order, rp, rt, _, _ = _ref_closest(oracle, verts, rays)
+    acc = trace.Accel(nodes, order, verts)
+    prim = np.empty(len(rays), np.int32)
+    t = np.empty(len(rays), np.float32)
+    acc.trace_host(rays, prim, t, any_hit=False)
+    assert acc.status() == 0
+    np.testing.assert_array_equal(prim >= 0, rp >= 0)
+    assert (prim != rp).sum() <= 2
+    np.testing.assert_array_equal(_bits(t[rp >= 0]), _bits(rt[rp >= 0]))
+    arays = workloads.soup_rays(1 << 20, seed=5, any_hit=True)
+    b = oracle.SoupBVH(verts)
+    ref_occ, _ = b.trace(workloads.rays_as_f8(arays), any_hit=True)
+    b.close()
+    occ = np.empty(len(arays), np.int32)
+    acc.trace_host(arays, occ, None, any_hit=True)
+    np.testing.assert_array_equal(occ, ref_occ)
+    acc.close()
