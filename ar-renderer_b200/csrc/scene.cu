@@ -218,6 +218,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         cache.valid = true;
         cache.deviceBytes = cache.accel.bytes + int64_t(sd->primCount) * int64_t(sizeof(prgpu::Primitive));
         d.nodes = cache.accel.nodes.as<WNode>();
+        d.qnodes = cache.accel.qnodes.as<QNode>();
         d.leaves = cache.accel.prims.as<LeafPrim>();
         d.root = cache.accel.root;
         d.prims = cache.prims.as<prgpu::Primitive>();

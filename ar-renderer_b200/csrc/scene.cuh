@@ -39,6 +39,7 @@ enum ShadeClass : int {
 
 struct DevScene {
     const WNode *nodes;
+    const QNode *qnodes;   // the 4-wide collapse of the same tree
     const LeafPrim *leaves;
     RootInfo root;
     const prgpu::Primitive *prims;

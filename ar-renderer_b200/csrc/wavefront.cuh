@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
     st.tMax = kInf;
     st.found = false;
     int j = 0;
-    const WNode *nodes = s0.nodes;
+    const QNode *nodes = s0.qnodes;
     const LeafPrim *leaves = s0.leaves;
     bool active = false, exhausted = n == 0, overflow = false;
     while (!__all_sync(full, exhausted)) {
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
                 } else {
                     j = queue[q];
                     const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(P.meta[j].w));
-                    nodes = s.nodes;
+                    nodes = s.qnodes;
                     leaves = s.leaves;
                     float4 o = P.o[j], d = P.d[j];
                     r = make_trace_ray(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z));
@@ -534,7 +534,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
                 }
             }
         }
-        if (active && traverse_step<false, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+        if (active && traverse4_step<false, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
             active = false;
             P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
         }
@@ -941,7 +941,7 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
     st.tMax = 1.f - kShadowEps;
     st.found = false;
     int q = 0, rid = 0;
-    const WNode *nodes = s0.nodes;
+    const QNode *nodes = s0.qnodes;
     const LeafPrim *leaves = s0.leaves;
     bool active = false, exhausted = n == 0, overflow = false;
     while (!__all_sync(full, exhausted)) {
@@ -958,7 +958,7 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                     float4 o4 = S.o[q], d4 = S.d[q];
                     if (kBatch) rid = path_render(P.meta[__float_as_int(d4.w)].w);
                     const DevScene &s = SceneOf<kBatch>::get(s0, scenes, rid);
-                    nodes = s.nodes;
+                    nodes = s.qnodes;
                     leaves = s.leaves;
                     r = make_trace_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
                     st.tMax = 1.f - kShadowEps;
@@ -974,7 +974,7 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                 }
             }
         }
-        if (active && traverse_step<true, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+        if (active && traverse4_step<true, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
             active = false;
             if (!st.found) shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
         }
