@@ -49,8 +49,9 @@ TRIS_PER_RAY = 2.21
 # Algorithmic bytes per closest-hit ray: every visited node (32 B in the reference layout) and
 # every tested triangle (36 B) read once, the 32-byte ray read and an 8-byte hit written.
 BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
-# DRAM bytes per closest-hit launch from ncu (profiles/trace_closest_soup1m.md), or None.
-NCU_TRAFFIC_PER_LAUNCH = None
+# DRAM bytes per closest-hit launch from ncu (profiles/trace_closest_soup1m.md): read + write of a
+# 2^22-ray capture of the same kernel, scaled by the rays of a full 2^24-ray launch.
+NCU_TRAFFIC_PER_LAUNCH = (798.610688e6 + 87.031040e6) * 4
 
 
 def _peaks():
