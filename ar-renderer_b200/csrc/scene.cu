@@ -51,6 +51,12 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
     h = fnv(h, sd->filter.cdf, sizeof(sd->filter.cdf));
     if (ext && ext->lightBVH && ext->lightBVHNodeCount > 0)
         h = fnv(h, ext->lightBVH, size_t(ext->lightBVHNodeCount) * sizeof(prgpu::LightBVHNode));
+    if (ext && ext->envMap) {
+        h = fnv_v(h, *ext->envMap);
+        h = sample_hash(h, ext->envMap->texels, size_t(std::max(0, ext->envMap->width)) * size_t(std::max(0, ext->envMap->height)),
+                        4 * sizeof(float), 65536);
+    }
+    if (ext && ext->sun) h = fnv_v(h, *ext->sun);
     if (ext && ext->gridMedia && ext->gridMediumCount > 0)
         for (int32_t k = 0; k < ext->gridMediumCount; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
@@ -91,6 +97,21 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
             return fail("empty grid medium bounds");
     }
     if (!spec_ok(sd->envSpectrum, ns)) return fail("envSpectrum out of range");
+    if (ext && ext->envMap) {
+        const prgpu::EnvMapDesc &e = *ext->envMap;
+        if (e.width <= 0 || e.height <= 0 || int64_t(e.width) * e.height > (int64_t(1) << 26) || !e.texels)
+            return fail("bad environment map dimensions or data");
+        if (!spec_ok(e.illuminant, ns)) return fail("environment map illuminant out of range");
+        if (!(e.pmf >= 0.f && e.pmf <= 1.f) || !std::isfinite(e.scale)) return fail("bad environment map pmf or scale");
+    }
+    if (ext && ext->sun) {
+        const prgpu::SunDesc &u = *ext->sun;
+        if (u.spectrum < 0 || u.spectrum >= ns) return fail("sun spectrum index out of range");
+        if (!(u.cosThetaMax > -1.f && u.cosThetaMax < 1.f) || !(u.pmf >= 0.f && u.pmf <= 1.f))
+            return fail("bad sun cone or pmf");
+        float l2 = u.direction.x * u.direction.x + u.direction.y * u.direction.y + u.direction.z * u.direction.z;
+        if (!(l2 > 0.f) || !std::isfinite(l2)) return fail("bad sun direction");
+    }
     if (sd->cameraMedium < -1 || sd->cameraMedium >= nm) return fail("cameraMedium out of range");
     for (int32_t i = 0; i < sd->materialCount; ++i) {
         const prgpu::Material &m = sd->materials[i];
@@ -137,6 +158,92 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
 template <typename T> void put(DevBuf &b, const T *src, size_t n, cudaStream_t s) {
     b.ensure(std::max<size_t>(1, n) * sizeof(T));
     if (n) PRB_CUDA(cudaMemcpyAsync(b.ptr, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+// Texel radiance at wavelength l (nm): scale * S(c0 l^2 + c1 l + c2) (rgb2spec.h:13-26).
+float texel_value(const float *t, float l) {
+    float x = std::fma(l, std::fma(l, t[0], t[1]), t[2]);
+    float s = std::isinf(x) ? (x > 0.f ? 1.f : 0.f) : 0.5f + x / (2.f * std::sqrt(1.f + x * x));
+    return t[3] * s;
+}
+
+// The image environment's texels and its sampling distribution (EnvironmentLight's constructor,
+// light.cpp:217-236, with a spectral luminance in place of the RGB one; Distribution2D,
+// sampling.cpp:44-67). Rows are Distribution1D CDFs normalised to 1 (unless all zero).
+void upload_env(const prgpu::SceneExt *ext, const prgpu::SceneDesc *sd, SceneCache &cache, DevScene &d,
+                cudaStream_t s) {
+    d.envMap = DevEnvMap{};
+    d.sun = DevSun{};
+    d.sun.spectrum = -1;
+    if (ext && ext->sun) {
+        const prgpu::SunDesc &u = *ext->sun;
+        float l = std::sqrt(u.direction.x * u.direction.x + u.direction.y * u.direction.y + u.direction.z * u.direction.z);
+        V3 z = mk(u.direction.x / l, u.direction.y / l, u.direction.z / l);
+        // Orthonormal frame around z (Duff et al. 2017).
+        float sg = std::copysign(1.f, z.z), a = -1.f / (sg + z.z), b = z.x * z.y * a;
+        d.sun.x = mk(1.f + sg * z.x * z.x * a, sg * b, -sg * z.x);
+        d.sun.y = mk(b, sg + z.y * z.y * a, -z.y);
+        d.sun.z = z;
+        d.sun.cosMax = u.cosThetaMax;
+        d.sun.spectrum = u.spectrum;
+        d.sun.scale = u.scale;
+        d.sun.pmf = u.pmf;
+    }
+    if (!(ext && ext->envMap)) return;
+    const prgpu::EnvMapDesc &e = *ext->envMap;
+    const int w = e.width, h = e.height;
+    const size_t n = size_t(w) * h;
+    put(cache.envTexels, reinterpret_cast<const float4 *>(e.texels), n, s);
+    // Luminance of each texel: its spectrum times the illuminant against CIE y over the table.
+    std::vector<float> func(n), rowCdf(static_cast<size_t>(h) * (w + 1)), rowInt(static_cast<size_t>(h)),
+        marg(static_cast<size_t>(h) + 1);
+    const float *ybar = sd->cie ? sd->cie + prgpu::kSpectrumSamples : nullptr;
+    for (int v = 0; v < h; ++v) {
+        const float sinTheta = std::sin(3.14159265358979f * (float(v) + 0.5f) / float(h));
+        for (int u = 0; u < w; ++u) {
+            const float *t = e.texels + 4 * (size_t(v) * w + u);
+            double y = 0.0;
+            for (int i = 0; i < prgpu::kSpectrumSamples; ++i) {
+                float l = prgpu::kSpectrumMin + prgpu::kSpectrumStep * float(i);
+                float il = e.illuminant >= 0 ? sd->spectra[e.illuminant].v[i] : 1.f;
+                y += double(texel_value(t, l)) * il * (ybar ? ybar[i] : 1.f);
+            }
+            func[size_t(v) * w + u] = float(std::max(0.0, y)) * sinTheta + 1e-6f;
+        }
+        float *cdf = rowCdf.data() + size_t(v) * (w + 1);
+        cdf[0] = 0.f;
+        for (int u = 0; u < w; ++u) cdf[u + 1] = cdf[u] + func[size_t(v) * w + u] / float(w);
+        rowInt[size_t(v)] = cdf[w];
+        for (int u = 1; u <= w; ++u) cdf[u] = cdf[w] > 0.f ? cdf[u] / cdf[w] : float(u) / float(w);
+    }
+    marg[0] = 0.f;
+    for (int v = 0; v < h; ++v) marg[size_t(v) + 1] = marg[size_t(v)] + rowInt[size_t(v)] / float(h);
+    const float margInt = marg[size_t(h)];
+    for (int v = 1; v <= h; ++v) marg[size_t(v)] = margInt > 0.f ? marg[size_t(v)] / margInt : float(v) / float(h);
+    std::vector<float> dist;
+    dist.reserve(func.size() + rowCdf.size() + rowInt.size() + marg.size());
+    dist.insert(dist.end(), func.begin(), func.end());
+    dist.insert(dist.end(), rowCdf.begin(), rowCdf.end());
+    dist.insert(dist.end(), rowInt.begin(), rowInt.end());
+    dist.insert(dist.end(), marg.begin(), marg.end());
+    put(cache.envDist, dist.data(), dist.size(), s);
+    PRB_CUDA(cudaStreamSynchronize(s));
+    const float *base = cache.envDist.as<float>();
+    DevEnvMap &m = d.envMap;
+    m.w = w;
+    m.h = h;
+    m.texels = cache.envTexels.as<float4>();
+    m.func = base;
+    m.rowCdf = base + func.size();
+    m.rowInt = m.rowCdf + rowCdf.size();
+    m.margCdf = m.rowInt + rowInt.size();
+    m.margInt = margInt;
+    m.illuminant = e.illuminant;
+    m.scale = e.scale;
+    m.pmf = e.pmf;
+    const float rad = e.rotationDeg * 3.14159265358979f / 180.f;
+    m.rc = std::cos(rad);
+    m.rs = std::sin(rad);
 }
 
 } // namespace
@@ -209,6 +316,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         put(cache.grids, grids.data(), grids.size(), s);
         d.grids = cache.grids.as<DevGrid>();
         d.gridCount = ng;
+        upload_env(ext, sd, cache, d, s);
         put(cache.lightLeaf, leafOf.data(), leafOf.size(), s);
         PRB_CUDA(cudaStreamSynchronize(s));
         cache.hasSpheres = false;

@@ -37,6 +37,28 @@ enum ShadeClass : int {
     kClasses = 6
 };
 
+// Image environment on the device: texels (sigmoid-polynomial spectra), and the 2D sampling
+// distribution of luminance x sin(theta) as per-row CDFs and a marginal CDF.
+struct DevEnvMap {
+    int w, h;                  // w = 0: none
+    const float4 *texels;      // c0, c1, c2, scale
+    const float *func;         // w * h
+    const float *rowCdf;       // h x (w + 1)
+    const float *rowInt;       // h
+    const float *margCdf;      // h + 1
+    float margInt;
+    int illuminant;
+    float scale, pmf;
+    float rc, rs;              // cos / sin of the rotation about +y (light to world)
+};
+
+struct DevSun {
+    V3 x, y, z;                // frame around the sun direction z
+    float cosMax;
+    int spectrum;              // -1: none
+    float scale, pmf;
+};
+
 struct DevScene {
     const WNode *nodes;
     const QNode *qnodes;   // the 4-wide collapse of the same tree
@@ -69,6 +91,8 @@ struct DevScene {
     int mediumCount;
     const DevGrid *grids;
     int gridCount;
+    DevEnvMap envMap;
+    DevSun sun;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).
     int maxDepth;            // <= 0: unlimited
     float clampY;            // 0: off
@@ -79,7 +103,8 @@ struct SceneCache {
     uint64_t key = 0;
     bool valid = false;
     DeviceAccel accel;
-    DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData;
+    DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
+        envDist;
     DevScene ds{};
     bool hasSpheres = false;
     int64_t deviceBytes = 0;
@@ -96,6 +121,8 @@ struct SceneCache {
         lightLeaf.release();
         grids.release();
         gridData.release();
+        envTexels.release();
+        envDist.release();
         valid = false;
     }
 };

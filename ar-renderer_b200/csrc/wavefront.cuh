@@ -264,6 +264,101 @@ __device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
     return lbvh_pmf(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, li, p, n);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Image environment and sun (src/lights/light.cpp:217-297, src/lights/sky.cpp:84-109)
+
+// Equirectangular mapping with +y up (light.h:287-297) and the map's rotation about +y.
+__device__ __forceinline__ V3 env_to_world(const DevEnvMap &m, V3 v) {
+    return mk(m.rc * v.x + m.rs * v.z, v.y, -m.rs * v.x + m.rc * v.z);
+}
+__device__ __forceinline__ V3 env_to_light(const DevEnvMap &m, V3 v) {
+    return mk(m.rc * v.x - m.rs * v.z, v.y, m.rs * v.x + m.rc * v.z);
+}
+__device__ __forceinline__ void dir_to_equirect(V3 d, float *u, float *v) {
+    float theta = acosf(clampf(d.y, -1.f, 1.f));
+    float phi = atan2f(d.z, d.x);
+    if (phi < 0.f) phi += 2.f * kPi;
+    *u = phi * kInv2Pi;
+    *v = theta * kInvPi;
+}
+
+__device__ __forceinline__ float texel_at(const float4 &t, float l) {
+    float x = fmaf(l, fmaf(l, t.x, t.y), t.z);
+    float sg = isinf(x) ? (x > 0.f ? 1.f : 0.f) : 0.5f + x / (2.f * sqrtf(1.f + x * x));
+    return t.w * sg;
+}
+
+// Radiance of the map towards world direction d: bilinear texel spectra with horizontal wrap
+// (EnvironmentLight::Lookup, light.cpp:238-261), times the illuminant and the scale.
+__device__ SS env_lookup(const DevScene &s, V3 d, const Lambda &lam) {
+    const DevEnvMap &m = s.envMap;
+    float u, v;
+    dir_to_equirect(normalize(env_to_light(m, d)), &u, &v);
+    float x = u * m.w - 0.5f, y = v * m.h - 0.5f;
+    int x0 = int(floorf(x)), y0 = int(floorf(y));
+    float dx = x - x0, dy = y - y0;
+    SS r = splat(0.f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int xi = x0 + (k & 1), yi = y0 + (k >> 1);
+        xi = ((xi % m.w) + m.w) % m.w;
+        yi = min(max(yi, 0), m.h - 1);
+        float wgt = ((k & 1) ? dx : 1.f - dx) * ((k >> 1) ? dy : 1.f - dy);
+        float4 t = __ldg(m.texels + size_t(yi) * m.w + xi);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) r.v[i] += wgt * texel_at(t, lam.l[i]);
+    }
+    if (m.illuminant >= 0) r = r * tab4(s.spectra, m.illuminant, lam);
+    return r * m.scale;
+}
+
+// Distribution1D::SampleContinuous over a CDF of n + 1 entries (sampling.cpp).
+__device__ __forceinline__ float dist1d_sample(const float *cdf, int n, float u, int *off) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) <= u) lo = mid;
+        else hi = mid;
+    }
+    float c0 = __ldg(cdf + lo), c1 = __ldg(cdf + lo + 1);
+    float du = u - c0;
+    if (c1 - c0 > 0.f) du /= c1 - c0;
+    *off = lo;
+    return (float(lo) + du) / float(n);
+}
+
+// Direction and solid-angle pdf from the map's 2D distribution (EnvironmentLight::SampleLi).
+__device__ bool env_sample(const DevScene &s, float u0, float u1, V3 *wi, float *pdf) {
+    const DevEnvMap &m = s.envMap;
+    if (!(m.margInt > 0.f)) return false;
+    int iv, iu;
+    float v = dist1d_sample(m.margCdf, m.h, u1, &iv);
+    float u = dist1d_sample(m.rowCdf + size_t(iv) * (m.w + 1), m.w, u0, &iu);
+    float rowInt = __ldg(m.rowInt + iv);
+    if (!(rowInt > 0.f)) return false;
+    float mapPdf = (__ldg(m.func + size_t(iv) * m.w + iu) / rowInt) * (rowInt / m.margInt);
+    float theta = v * kPi, phi = u * 2.f * kPi;
+    float st = sinf(theta);
+    if (!(st > 0.f) || !(mapPdf > 0.f)) return false;
+    *wi = env_to_world(m, mk(st * cosf(phi), cosf(theta), st * sinf(phi)));
+    *pdf = mapPdf / (2.f * kPi * kPi * st);
+    return true;
+}
+
+// Solid-angle pdf of sampling world direction d (EnvironmentLight::PDF_Li).
+__device__ float env_pdf(const DevScene &s, V3 d) {
+    const DevEnvMap &m = s.envMap;
+    if (!(m.margInt > 0.f)) return 0.f;
+    float u, v;
+    dir_to_equirect(normalize(env_to_light(m, d)), &u, &v);
+    float st = sinf(v * kPi);
+    if (!(st > 0.f)) return 0.f;
+    int iu = min(max(int(u * m.w), 0), m.w - 1), iv = min(max(int(v * m.h), 0), m.h - 1);
+    return __ldg(m.func + size_t(iv) * m.w + iu) / m.margInt / (2.f * kPi * kPi * st);
+}
+
+__device__ __forceinline__ float sun_pdf(const DevSun &u) { return 1.f / (2.f * kPi * (1.f - u.cosMax)); }
+
 struct LightSample {
     V3 wi, target;
     SS Le;
@@ -277,24 +372,54 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
     LightSample ls;
     ls.ok = false;
     ls.delta = false;
-    if (ul < s.envPmf && s.envSpectrum >= 0) {
-        float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
-        sincosf(2.f * kPi * u1, &sp, &cp);
-        ls.wi = mk(r * cp, r * sp, z);
-        ls.target = p + ls.wi * (2.f * s.worldRadius);
-        ls.Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
-        ls.pdf = s.envPmf * kInv4Pi;
-        ls.ok = true;
-        return ls;
+    // Infinite lights first: constant environment, image environment, sun, each with its pmf.
+    float acc = 0.f;
+    if (s.envSpectrum >= 0) {
+        if (ul < s.envPmf) {
+            float z = 1.f - 2.f * u0, r = safe_sqrt(1.f - z * z), sp, cp;
+            sincosf(2.f * kPi * u1, &sp, &cp);
+            ls.wi = mk(r * cp, r * sp, z);
+            ls.target = p + ls.wi * (2.f * s.worldRadius);
+            ls.Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
+            ls.pdf = s.envPmf * kInv4Pi;
+            ls.ok = true;
+            return ls;
+        }
+        acc = s.envPmf;
+    }
+    if (s.envMap.w > 0) {
+        if (ul < acc + s.envMap.pmf) {
+            float pdf;
+            if (!env_sample(s, u0, u1, &ls.wi, &pdf)) return ls;
+            ls.target = p + ls.wi * (2.f * s.worldRadius);
+            ls.Le = env_lookup(s, ls.wi, lam);
+            ls.pdf = s.envMap.pmf * pdf;
+            ls.ok = nonzero(ls.Le) && ls.pdf > 0.f;
+            return ls;
+        }
+        acc += s.envMap.pmf;
+    }
+    if (s.sun.spectrum >= 0) {
+        if (ul < acc + s.sun.pmf) {
+            // SampleUniformCone (sampling.h): cos theta = (1 - u0) + u0 cos theta_max.
+            float ct = (1.f - u0) + u0 * s.sun.cosMax, st = safe_sqrt(1.f - ct * ct), sp, cp;
+            sincosf(2.f * kPi * u1, &sp, &cp);
+            ls.wi = s.sun.x * (st * cp) + s.sun.y * (st * sp) + s.sun.z * ct;
+            ls.target = p + ls.wi * (2.f * s.worldRadius);
+            ls.Le = tab4(s.spectra, s.sun.spectrum, lam) * s.sun.scale;
+            ls.pdf = s.sun.pmf * sun_pdf(s.sun);
+            ls.ok = true;
+            return ls;
+        }
+        acc += s.sun.pmf;
     }
     int li = -1;
     float pmf = 0.f;
     if (s.lbvhCount > 0) {
-        float u = fminf((ul - s.envPmf) / s.lbvhProb, kOneMinusEps);
+        float u = fminf((ul - acc) / s.lbvhProb, kOneMinusEps);
         li = lbvh_sample(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, p, n, u, &pmf);
     } else {
         if (s.lightCount == 0) return ls;
-        float acc = s.envSpectrum >= 0 ? s.envPmf : 0.f;
         li = s.lightCount - 1;
         for (int i = 0; i < s.lightCount; ++i) {
             acc += s.lights[i].pmf;
@@ -754,11 +879,24 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
             }
         }
         if (!handled && !found) {
-            // Escaped: environment emission with MIS against the previous BSDF / phase sample.
+            // Escaped: emission of every infinite light with MIS against the previous BSDF /
+            // phase sample.
             if (s.envSpectrum >= 0) {
                 SS Le = tab4(s.spectra, s.envSpectrum, lam) * s.envScale;
                 float w = 1.f;
                 if (depth > 0 && !specular) w = power_heuristic(prevPdf, s.envPmf * kInv4Pi);
+                add(beta * Le * w);
+            }
+            if (s.envMap.w > 0) {
+                SS Le = env_lookup(s, d, lam);
+                float w = 1.f;
+                if (depth > 0 && !specular) w = power_heuristic(prevPdf, s.envMap.pmf * env_pdf(s, d));
+                add(beta * Le * w);
+            }
+            if (s.sun.spectrum >= 0 && dot(normalize(d), s.sun.z) >= s.sun.cosMax) {
+                SS Le = tab4(s.spectra, s.sun.spectrum, lam) * s.sun.scale;
+                float w = 1.f;
+                if (depth > 0 && !specular) w = power_heuristic(prevPdf, s.sun.pmf * sun_pdf(s.sun));
                 add(beta * Le * w);
             }
             alive = false;

@@ -111,10 +111,21 @@ class GridMediumDesc(C.Structure):
                 ("density", C.c_void_p)]
 
 
+class EnvMapDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("texels", C.c_void_p), ("illuminant", C.c_int32),
+                ("scale", C.c_float), ("rotationDeg", C.c_float), ("pmf", C.c_float)]
+
+
+class SunDesc(C.Structure):
+    _fields_ = [("direction", C.c_float * 3), ("cosThetaMax", C.c_float), ("spectrum", C.c_int32),
+                ("scale", C.c_float), ("pmf", C.c_float)]
+
+
 class SceneExt(C.Structure):
     _fields_ = [("structSize", C.c_uint32), ("lightBVHNodeCount", C.c_int32), ("lightBVH", C.c_void_p),
                 ("lightBVHProb", C.c_float), ("wavefrontPaths", C.c_int32), ("blockSize", C.c_int32),
-                ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p)]
+                ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p),
+                ("envMap", C.c_void_p), ("sun", C.c_void_p)]
 
 
 class BatchItem(C.Structure):
@@ -142,7 +153,8 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 48
+assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 64
+assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72
 assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512
 

@@ -170,6 +170,43 @@ def indirect_scene(seed: int = 0, width: int = 64, height: int = 64, spp: int = 
     return s
 
 
+def outdoor_scene_json(width: int = 32, height: int = 32, spp: int = 64, max_depth: int = 8, elevation: float = 30.0,
+                       azimuth: float = 40.0, turbidity: float = 3.0, sky_resolution: int = 64,
+                       env_file: str | None = None, env_rotation: float = 0.0, sun_scale: float = 1.0,
+                       sky_scale: float = 1.0) -> dict:
+    """An outdoor test scene in the reference's JSON form: a 20 x 20 ground (albedo 0.3) with a
+    Lambertian, a gold and a BK7 sphere, lit by the reference's Preetham sun and sky (sun_sky) or,
+    with env_file, by an image environment map."""
+    mats = {"ground": {"type": "diffuse", "reflectance": [0.3, 0.3, 0.3]},
+            "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+            "gold": {"type": "conductor", "metal": "Au", "roughness": 0.3},
+            "bk7": {"type": "dielectric", "ior": "BK7"}}
+    geometry = {"ground": {"type": "mesh", "positions": [-10, 0, -10, -10, 0, 10, 10, 0, 10, 10, 0, -10],
+                           "indices": [0, 1, 2, 0, 2, 3]},
+                "s0": {"type": "sphere", "center": [-1.2, 0.5, 0], "radius": 0.5},
+                "s1": {"type": "sphere", "center": [0, 0.5, 0], "radius": 0.5},
+                "s2": {"type": "sphere", "center": [1.2, 0.5, 0], "radius": 0.5}}
+    objects = [{"name": "ground", "geometry": "ground", "material": "ground"},
+               {"name": "s0", "geometry": "s0", "material": "red"},
+               {"name": "s1", "geometry": "s1", "material": "gold"},
+               {"name": "s2", "geometry": "s2", "material": "bk7"}]
+    if env_file is None:
+        lights = {"sky": {"type": "sun_sky", "elevation": elevation, "azimuth": azimuth, "turbidity": turbidity,
+                          "resolution": sky_resolution, "sun_scale": sun_scale, "sky_scale": sky_scale}}
+    else:
+        lights = {"env": {"type": "environment", "file": env_file, "intensity": 1.0, "rotation": env_rotation}}
+    return {"materials": mats, "media": {}, "geometry": geometry, "objects": objects, "lights": lights,
+            "cameras": {"cam": {"type": "pinhole", "position": [0, 1.4, 4.0], "look_at": [0, 0.4, 0], "fov_y": 40}},
+            "render": {"camera": "cam", "seed": 0, "film": {"width": width, "height": height, "filter": "box"},
+                       "integrator": {"type": "path", "spp": spp, "max_depth": max_depth}}}
+
+
+def sun_direction(elevation: float, azimuth: float) -> np.ndarray:
+    """The reference loader's sun direction (scene_loader.cpp:977-984)."""
+    el, az = math.radians(elevation), math.radians(azimuth)
+    return np.array([math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az)], np.float32)
+
+
 def uneven_batch(count: int = 48, seed: int = 4242) -> list:
     """The uneven batch: `count` renders of the box family, scene seeds 0..count-1, each with a
     resolution drawn uniformly from {128, 256, 512, 1024}^2, spp from {16, 64, 256} and max depth

@@ -218,6 +218,31 @@ struct GridMediumDesc {
     const float *density;       // nx * ny * nz floats, x fastest: index (z * ny + y) * nx + x
 };
 
+// Image environment light (pr::EnvironmentLight with a map, src/lights/light.cpp:217-297), as a
+// latitude-longitude map with +y up (uv of a direction by DirToEquirect, light.h:292-297).
+// Texels hold the sigmoid-polynomial spectra the reference's RGB uplift produces
+// (RGBUnboundedSample, src/core/rgb2spec.cpp:328-336): radiance(lambda) = scale *
+// S(c0 lambda^2 + c1 lambda + c2) with S(x) = 1/2 + x / (2 sqrt(1 + x^2)) and lambda in nm,
+// times the illuminant spectrum (D65 for RGB illuminants, rgb2spec.cpp:338-343). Lookups are
+// bilinear with horizontal wrap; sampling follows a 2D distribution of luminance x sin(theta).
+struct EnvMapDesc {
+    int32_t width, height;
+    const float *texels;      // width * height * 4 floats: c0, c1, c2, scale (row 0 = theta 0)
+    int32_t illuminant;       // spectrum index multiplied into every texel, -1 = none
+    float scale;
+    float rotationDeg;        // rotation of the map about +y (Transform::Rotate, light.cpp:219-220)
+    float pmf;                // selection probability of this light in next-event estimation
+};
+
+// Sun disk (pr::SunLight, src/lights/sky.cpp:84-109): uniform radiance inside a cone.
+struct SunDesc {
+    Float3 direction;         // towards the sun (normalised on upload)
+    float cosThetaMax;        // cosine of the angular radius
+    int32_t spectrum;         // radiance spectrum index
+    float scale;
+    float pmf;                // selection probability of this light in next-event estimation
+};
+
 // Optional extras for prgpu_render_ex (zero-initialise, then set structSize = sizeof(SceneExt)).
 struct SceneExt {
     uint32_t structSize;
@@ -231,6 +256,8 @@ struct SceneExt {
                                     // (one Adam step per wavefront chunk), bit 2 fresh weights first
     int32_t gridMediumCount;
     const GridMediumDesc *gridMedia;
+    const EnvMapDesc *envMap;       // null = none
+    const SunDesc *sun;             // null = none
 };
 
 // One render of a batch (prgpu_render_batch): its scene, optional extension, parameters and film.

@@ -69,6 +69,10 @@ def ref_lib() -> C.CDLL:
         lib.prref_render.restype = C.c_double
         lib.prref_light_bvh_sample.argtypes = [_P, C.c_int64, _P, _P, _P]
         lib.prref_scene_light_count.argtypes = [_P]
+        lib.prref_scene_infinite.argtypes = [_P, C.c_int, _P, _P]
+        lib.prref_rgb_uplift.argtypes = [C.c_int64, _P, _P]
+        lib.prref_preetham_sky.argtypes = [_P, C.c_float, C.c_float, C.c_int, C.c_int, _P]
+        lib.prref_sun_radiance.argtypes = [_P, C.c_float, C.c_float, C.c_int64, _P, _P]
         lib.prref_scene_grid_count.argtypes = [_P]
         lib.prref_scene_grid_info.argtypes = [_P, C.c_int, C.c_char_p, C.c_int, _P]
         # The RGB->spectrum table is built once (a few seconds) and cached beside the library.
@@ -172,6 +176,14 @@ class RefScene:
     def light_count(self) -> int:
         return self.lib.prref_scene_light_count(self.h)
 
+    def infinite_lights(self):
+        """(type, pmf) of the exported scene's image-environment (2) and sun (3) lights."""
+        self.export()
+        t = np.zeros(8, np.int32)
+        p = np.zeros(8, np.float32)
+        n = self.lib.prref_scene_infinite(self.h, 8, _p(t), _p(p))
+        return [(int(t[i]), float(p[i])) for i in range(min(n, 8))]
+
     def grid_media(self):
         """Heterogeneous media of the export, in index order (index = mediumCount + k): a list of
         (name, bounds (2, 3) float32 in medium space as the loader fitted them)."""
@@ -211,3 +223,27 @@ def set_threads(n: int) -> None:
 
 def thread_count() -> int:
     return ref_lib().prref_thread_count()
+
+
+def rgb_uplift(rgb: np.ndarray) -> np.ndarray:
+    """(n, 4) sigmoid-polynomial coefficients (c0, c1, c2, scale) of unbounded RGB values, as the
+    reference's RGB-to-spectrum table gives them."""
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    out = np.zeros((rgb.shape[0], 4), np.float32)
+    ref_lib().prref_rgb_uplift(rgb.shape[0], _p(rgb), _p(out))
+    return out
+
+
+def preetham_sky(sun_dir, turbidity: float, ground_albedo: float, width: int, height: int) -> np.ndarray:
+    d = np.ascontiguousarray(sun_dir, np.float32)
+    out = np.zeros((height, width, 3), np.float32)
+    ref_lib().prref_preetham_sky(_p(d), turbidity, ground_albedo, width, height, _p(out))
+    return out
+
+
+def sun_radiance(sun_dir, turbidity: float, radius_deg: float, lam: np.ndarray) -> np.ndarray:
+    d = np.ascontiguousarray(sun_dir, np.float32)
+    lam = np.ascontiguousarray(lam, np.float32)
+    out = np.zeros(lam.shape[0], np.float32)
+    ref_lib().prref_sun_radiance(_p(d), turbidity, radius_deg, lam.shape[0], _p(lam), _p(out))
+    return out

@@ -340,6 +340,9 @@ struct SceneHandle {
     // Heterogeneous media, in first-use order: exported as indices mediumCount + k (the layout of
     // the GPU module's grid-media extension); their parameters come from the scene file.
     std::vector<const pr::Medium *> grids;
+    // Infinite lights besides the constant environment: type 2 image environment, 3 sun; their
+    // light-sampler pmfs (renormalised with the exported lights').
+    std::vector<std::pair<int, float>> infinite;
     int interfaceMat = -1;
 
     int Spec(const Spectrum &s) {
@@ -573,6 +576,12 @@ API const prgpu::SceneDesc *prref_scene_export(void *hp, char *err, int errLen) 
             envScale = env->Scale();
             envPmf = pmf;
             pmfSum += pmf;
+        } else if (dynamic_cast<const EnvironmentLight *>(l)) {
+            h->infinite.push_back({2, pmf});
+            pmfSum += pmf;
+        } else if (dynamic_cast<const SunLight *>(l)) {
+            h->infinite.push_back({3, pmf});
+            pmfSum += pmf;
         } else {
             h->Warn("light type not exported");
         }
@@ -580,6 +589,7 @@ API const prgpu::SceneDesc *prref_scene_export(void *hp, char *err, int errLen) 
     if (pmfSum > 0) {
         for (auto &l : h->lights) l.pmf /= pmfSum;
         envPmf /= pmfSum;
+        for (auto &i : h->infinite) i.second /= pmfSum;
     }
     const BVH &bvh = scene.GetBVH();
     h->nodes.clear();
@@ -736,6 +746,73 @@ API int prref_scene_light_count(void *hp) { return int(static_cast<SceneHandle *
 
 // Heterogeneous media of the last export (index mediumCount + k): their names in the scene file and
 // the density-field bounds in medium space after the loader fitted them (scene_loader.cpp:1302-1308).
+// Infinite lights of the last export other than the constant environment (the GPU module's
+// SceneExt::envMap / sun): count, then per light its type (2 image environment, 3 sun) and pmf.
+API int prref_scene_infinite(void *hp, int max, int *types, float *pmfs) {
+    auto *h = static_cast<SceneHandle *>(hp);
+    int n = int(h->infinite.size());
+    for (int i = 0; i < std::min(n, max); ++i) {
+        types[i] = h->infinite[size_t(i)].first;
+        pmfs[i] = h->infinite[size_t(i)].second;
+    }
+    return n;
+}
+
+// The reference's RGB uplift of unbounded RGB values (RGBUnboundedSample, rgb2spec.cpp:328-336) as
+// sigmoid-polynomial coefficients: out 4 floats per colour (c0, c1, c2, scale), reconstructed from
+// the polynomial's values at 400, 550 and 700 nm (its coefficients are not exposed).
+API void prref_rgb_uplift(int64_t n, const float *rgb, float *out) {
+    const RGBToSpectrumTable &table = RGBToSpectrumTable::Get();
+    for (int64_t i = 0; i < n; ++i) {
+        RGB c(rgb[3 * i], rgb[3 * i + 1], rgb[3 * i + 2]);
+        float m = std::max(0.f, c.Max());
+        float *o = out + 4 * i;
+        if (m == 0.f) {
+            o[0] = o[1] = o[2] = 0.f;
+            o[3] = 0.f;
+            continue;
+        }
+        float scale = 2 * m;
+        RGBSigmoidPolynomial rsp = table(c * (1 / scale));
+        const double L[3] = {400.0, 550.0, 700.0};
+        double x[3];
+        for (int k = 0; k < 3; ++k) {
+            double y = 2.0 * double(rsp(float(L[k]))) - 1.0;
+            y = std::max(-0.999999, std::min(0.999999, y));
+            x[k] = y / std::sqrt(1.0 - y * y);
+        }
+        // Quadratic through (L_k, x_k): c0 l^2 + c1 l + c2.
+        double d01 = (x[1] - x[0]) / (L[1] - L[0]), d12 = (x[2] - x[1]) / (L[2] - L[1]);
+        double c0 = (d12 - d01) / (L[2] - L[0]);
+        double c1 = d01 - c0 * (L[0] + L[1]);
+        double c2 = x[0] - c0 * L[0] * L[0] - c1 * L[0];
+        o[0] = float(c0);
+        o[1] = float(c1);
+        o[2] = float(c2);
+        o[3] = scale;
+    }
+}
+
+// MakePreethamSky (sky.cpp:146-205): linear RGB, width x height x 3.
+API void prref_preetham_sky(const float *sunDir, float turbidity, float groundAlbedo, int width, int height, float *rgb) {
+    auto img = MakePreethamSky(Normalize(Vec3f(sunDir[0], sunDir[1], sunDir[2])), turbidity, groundAlbedo, width, height);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x) {
+            RGB c = img->Get(x, y);
+            float *o = rgb + 3 * (size_t(y) * width + x);
+            o[0] = c.r;
+            o[1] = c.g;
+            o[2] = c.b;
+        }
+}
+
+// MakeSunRadiance (sky.cpp:207-233) at n wavelengths.
+API void prref_sun_radiance(const float *sunDir, float turbidity, float radiusDeg, int64_t n, const float *lambda,
+                            float *out) {
+    auto s = MakeSunRadiance(Normalize(Vec3f(sunDir[0], sunDir[1], sunDir[2])), turbidity, radiusDeg);
+    for (int64_t i = 0; i < n; ++i) out[i] = (*s)(lambda[i]);
+}
+
 API int prref_scene_grid_count(void *hp) { return int(static_cast<SceneHandle *>(hp)->grids.size()); }
 
 API int prref_scene_grid_info(void *hp, int k, char *name, int nameLen, float *bounds6) {

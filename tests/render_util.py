@@ -58,6 +58,67 @@ def grid_scene_inputs(rs, s):
     return sd, ext
 
 
+def outdoor_scene_file(name: str, **kw) -> str:
+    import json
+
+    from prgpu import scenes as sc
+
+    path = os.path.join(_DIR, name + ".prscene.json")
+    os.makedirs(_DIR, exist_ok=True)
+    with open(path, "w") as f:
+        json.dump(sc.outdoor_scene_json(**kw), f)
+    return path
+
+
+def sun_sky_inputs(rs, elevation, azimuth, turbidity, sky_resolution, intensity=0.03):
+    """The GPU-side inputs of a sun_sky scene loaded by the reference: the exported SceneDesc with
+    D65 and the sun's radiance appended to its spectra, and a SceneExt carrying the Preetham sky
+    (uplifted to sigmoid-polynomial texels by the reference's table) and the sun, with the pmfs the
+    reference's light sampler gives them (scene_loader.cpp:977-996)."""
+    import ctypes as C
+    import math
+
+    import ref as oracle_ref
+    from prgpu import abi, render, scenes, spectra
+
+    base = abi.SceneDesc.from_address(rs.export())
+    sd = abi.SceneDesc()
+    C.memmove(C.addressof(sd), C.addressof(base), C.sizeof(sd))
+    old = np.ctypeslib.as_array((C.c_float * (95 * base.spectrumCount)).from_address(base.spectra)).reshape(-1, 95)
+    lam = spectra.LAMBDA.astype(np.float32)
+    d65 = np.zeros(95, np.float32)
+    assert oracle_ref.ref_lib().prref_spectrum(2, 1.0, 1.0, 1.0, None, 95, oracle_ref._p(lam), oracle_ref._p(d65)) == 0
+    sun_dir = scenes.sun_direction(elevation, azimuth)
+    radius = 0.2665
+    sun_spec = oracle_ref.sun_radiance(sun_dir, turbidity, radius, lam)
+    table = np.ascontiguousarray(np.concatenate([old, d65[None], sun_spec[None]]), np.float32)
+    sd.spectra = table.ctypes.data
+    sd.spectrumCount = table.shape[0]
+    pmfs = dict(rs.infinite_lights())
+    sky = oracle_ref.preetham_sky(sun_dir, turbidity, 0.3, sky_resolution, sky_resolution // 2)
+    texels = np.ascontiguousarray(oracle_ref.rgb_uplift(sky.reshape(-1, 3)), np.float32)
+    env = abi.EnvMapDesc()
+    env.width, env.height = sky_resolution, sky_resolution // 2
+    env.texels = texels.ctypes.data
+    env.illuminant = base.spectrumCount
+    env.scale = intensity
+    env.rotationDeg = 0.0
+    env.pmf = pmfs.get(2, 0.0)
+    sun = abi.SunDesc()
+    for i in range(3):
+        sun.direction[i] = float(sun_dir[i])
+    sun.cosThetaMax = math.cos(math.radians(radius))
+    sun.spectrum = base.spectrumCount + 1
+    sun.scale = intensity
+    sun.pmf = pmfs.get(3, 0.0)
+    ext = render.make_ext()
+    ext.envMap = C.addressof(env)
+    ext.sun = C.addressof(sun)
+    ext._keep += [env, sun, texels]
+    sd._keep = table
+    return sd, ext
+
+
 def luminance_y(img: np.ndarray) -> np.ndarray:
     return img[..., 1]
 
