@@ -83,6 +83,19 @@ class HostScene:
         self.prims.append(r)
         self._prim_count += len(tri)
 
+    def spheres(self, centers, radii, materials, medium_inside=-1, medium_outside=-1):
+        """Analytic spheres (the reference's Sphere shape, shape.cpp:42-85)."""
+        c = np.asarray(centers, np.float32).reshape(-1, 3)
+        r = np.zeros(len(c), abi.PRIMITIVE)
+        r["type"] = abi.PRIM_SPHERE
+        r["material"] = np.asarray(materials, np.int32)
+        r["light"] = -1
+        r["mediumInside"], r["mediumOutside"] = medium_inside, medium_outside
+        r["p0"] = c
+        r["r"] = np.asarray(radii, np.float32)
+        self.prims.append(r)
+        self._prim_count += len(c)
+
     # -- finalisation ---------------------------------------------------------------------
     def finish(self, cam_pos, cam_target, fov_y, width, height, max_leaf=2):
         self.prim_array = np.concatenate(self.prims) if self.prims else np.zeros(0, abi.PRIMITIVE)
@@ -97,10 +110,22 @@ class HostScene:
         for l, pw in zip(self.lights, power):
             l["pmf"] = pw / power.sum() if power.sum() > 0 else 0.0
         self.light_array = np.array(self.lights, dtype=abi.LIGHT) if self.lights else np.zeros(1, abi.LIGHT)
-        tris = np.stack([self.prim_array["p0"], self.prim_array["p1"], self.prim_array["p2"]], axis=1)
-        self.nodes, self.order = trace.build_bvh_triangles(tris, max_leaf=max_leaf)
-        pts = np.concatenate([tris.reshape(-1, 3), np.asarray([cam_pos], np.float32)])
-        lo, hi = pts.min(0), pts.max(0)
+        pa = self.prim_array
+        sph = pa["type"] == abi.PRIM_SPHERE
+        if not sph.any():
+            tris = np.stack([pa["p0"], pa["p1"], pa["p2"]], axis=1)
+            self.nodes, self.order = trace.build_bvh_triangles(tris, max_leaf=max_leaf)
+            lo = np.minimum(tris.reshape(-1, 3).min(0), np.asarray(cam_pos, np.float32))
+            hi = np.maximum(tris.reshape(-1, 3).max(0), np.asarray(cam_pos, np.float32))
+        else:
+            bmin = np.minimum(np.minimum(pa["p0"], pa["p1"]), pa["p2"])
+            bmax = np.maximum(np.maximum(pa["p0"], pa["p1"]), pa["p2"])
+            rr = pa["r"][sph, None]
+            bmin[sph] = pa["p0"][sph] - rr
+            bmax[sph] = pa["p0"][sph] + rr
+            self.nodes, self.order = trace.build_bvh_bounds(bmin, bmax, max_leaf=max_leaf)
+            lo = np.minimum(bmin.min(0), np.asarray(cam_pos, np.float32))
+            hi = np.maximum(bmax.max(0), np.asarray(cam_pos, np.float32))
         self.world_center = 0.5 * (lo + hi)
         self.world_radius = max(float(np.linalg.norm(hi - self.world_center)), 1e-3)
         # Camera: right-handed look-at, camera space +x right, +y up, +z forward.
@@ -214,3 +239,201 @@ def build_box_scene(s: scenes.BoxScene) -> HostScene:
         h.mesh(p, f, mats["bk7"], normals=n, medium_inside=med, medium_outside=fog)
     return h.finish(cam_pos=(0.0, -0.1, 0.98), cam_target=(0.0, -0.45, -0.3), fov_y=s.fov_y, width=s.width,
                     height=s.height)
+
+
+def box_mesh(lo, hi):
+    """(8 x 3 float32 corners, 12 x 3 indices) of an axis-aligned box, triangles counter-clockwise
+    seen from outside (outward geometric normals)."""
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    v = np.array([[(hi if (k >> a) & 1 else lo)[a] for a in range(3)] for k in range(8)], np.float32)
+    f = [[0, 2, 3, 0, 3, 1], [4, 5, 7, 4, 7, 6], [0, 1, 5, 0, 5, 4], [2, 6, 7, 2, 7, 3], [0, 4, 6, 0, 6, 2],
+         [1, 3, 7, 1, 7, 5]]
+    return v, np.asarray(f, np.int64).reshape(-1, 3)
+
+
+def fbm_heightfield(res: int, octaves: int = 8, seed: int = 0) -> np.ndarray:
+    """(res, res) float32 fractional Brownian motion of value noise (bilinear lattice noise, gain
+    0.5, lacunarity 2), seeded."""
+    rng = np.random.default_rng(seed)
+    h = np.zeros((res, res), np.float32)
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = 4 * 2 ** o
+        lat = rng.random((cells + 1, cells + 1)).astype(np.float32)
+        t = np.linspace(0, cells, res, endpoint=False, dtype=np.float32)
+        i = t.astype(np.int32)
+        f = t - i
+        f = f * f * (3 - 2 * f)
+        a = lat[i][:, i] * (1 - f)[None, :] + lat[i][:, i + 1] * f[None, :]
+        b = lat[i + 1][:, i] * (1 - f)[None, :] + lat[i + 1][:, i + 1] * f[None, :]
+        h += amp * (a * (1 - f)[:, None] + b * f[:, None])
+        total += amp
+        amp *= 0.5
+    return h / total
+
+
+def fbm_cloud(res: int, octaves: int = 5, seed: int = 1, max_density: float = 4.0) -> np.ndarray:
+    """(res, res, res) float32 cloud density: fBm value noise thresholded and faded by an
+    ellipsoidal falloff towards the grid's edges, scaled to max_density."""
+    rng = np.random.default_rng(seed)
+    c = (np.arange(res, dtype=np.float32) + 0.5) / res
+    d = np.zeros((res, res, res), np.float32)
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        cells = 3 * 2 ** o
+        lat = rng.random((cells + 1,) * 3).astype(np.float32)
+        t = c * cells
+        i = np.minimum(t.astype(np.int32), cells - 1)
+        f = t - i
+        f = f * f * (3 - 2 * f)
+        acc = np.zeros((res, res, res), np.float32)
+        for dz in (0, 1):
+            wz = (f if dz else 1 - f)[:, None, None]
+            for dy in (0, 1):
+                wy = (f if dy else 1 - f)[None, :, None]
+                for dx in (0, 1):
+                    wx = (f if dx else 1 - f)[None, None, :]
+                    acc += lat[np.ix_(i + dz, i + dy, i + dx)] * wz * wy * wx
+        d += amp * acc
+        total += amp
+        amp *= 0.5
+    d /= total
+    z, y, x = np.meshgrid(c * 2 - 1, c * 2 - 1, c * 2 - 1, indexing="ij")
+    fall = np.clip(1 - (x * x + (y * 1.6) ** 2 + z * z), 0, 1)
+    dens = np.clip((d * fall - 0.25) * 4.0, 0, 1) * max_density
+    return dens.astype(np.float32)
+
+
+METALS = ("Au", "Ag", "Cu", "Al")
+CLOUD_TO_WORLD = np.array([[25, 0, 0, 0], [0, 6, 0, 22], [0, 0, 25, -5], [0, 0, 0, 1]], np.float64)
+CLOUD_BOX = (np.array([-25.0, 16.0, -30.0]), np.array([25.0, 28.0, 20.0]))
+SUN_ELEVATION, SUN_AZIMUTH = 20.0, math.degrees(0.6)
+CAMERA = dict(cam_pos=(0.0, 14.0, 45.0), cam_target=(0.0, 6.0, 0.0), fov_y=45.0)
+
+
+def large_scene_layout(terrain_res: int = 4096, cloud_res: int = 256, spheres: int = 200, seed: int = 0) -> dict:
+    """The seeded content of the large outdoor scene, shared by its host-built form
+    (build_large_scene) and its reference JSON form: terrain vertices / triangles over
+    [-50, 50]^2 (fBm height x 8), the cloud density ((nz, ny, nx) over [-1, 1]^3 in medium space,
+    placed by CLOUD_TO_WORLD inside CLOUD_BOX) and the spheres (centre, radius, metal, GGX alpha)."""
+    rng = np.random.default_rng(seed)
+    hf = fbm_heightfield(terrain_res, 8, seed) * 8.0
+    g = np.linspace(-50, 50, terrain_res, dtype=np.float32)
+    X, Z = np.meshgrid(g, g)
+    verts = np.stack([X, hf, Z], -1).reshape(-1, 3)
+    ii = np.arange(terrain_res - 1)
+    q = (ii[:, None] * terrain_res + ii[None, :]).ravel()
+    tris = np.stack([q, q + terrain_res, q + terrain_res + 1, q, q + terrain_res + 1, q + 1], 1).reshape(-1, 3)
+    sph = []
+    for k in range(spheres):
+        x, z = rng.uniform(-30, 30, 2)
+        rr = float(rng.uniform(0.3, 1.2))
+        iz = int(np.clip((z + 50) / 100 * (terrain_res - 1), 0, terrain_res - 1))
+        ix = int(np.clip((x + 50) / 100 * (terrain_res - 1), 0, terrain_res - 1))
+        sph.append(((float(x), float(hf[iz, ix]) + rr, float(z)), rr, METALS[k % 4], float(rng.uniform(0.05, 0.5))))
+    return {"verts": verts, "tris": tris, "spheres": sph, "density": fbm_cloud(cloud_res, 5, seed + 1, 4.0)}
+
+
+def build_large_scene(width: int = 3840, height: int = 2160, terrain_res: int = 4096, cloud_res: int = 256,
+                      spheres: int = 200, seed: int = 0):
+    """The large outdoor scene: a terrain_res^2 fBm heightfield (8 octaves, 2 (res - 1)^2 triangles,
+    Lambert 0.3) over [-50, 50]^2, a cloud_res^3 fBm cloud density grid above it (max density 4,
+    albedo 0.95, Henyey-Greenstein g = 0.8, spectral / ratio tracking inside an interface box),
+    `spheres` analytic GGX conductor spheres (Au / Ag / Cu / Al, alpha uniform in [0.05, 0.5]) on
+    the terrain, a sun 20 degrees above the horizon and a sky. Lighting stand-ins: the sun is a
+    5,800 K blackbody cone of the reference's angular radius and the sky an importance-sampled
+    equirect map with a zenith-to-horizon gradient of an 8,000 K blackbody (the reference builds a
+    Preetham sky on the host, which this builder does not restate).
+    Returns (HostScene, SceneExt)."""
+    from . import media, render
+
+    lay = large_scene_layout(terrain_res, cloud_res, spheres, seed)
+    h = HostScene()
+    ground = h.material(type=abi.MAT_DIFFUSE, albedo=h.spectrum(spectra.constant(0.3)))
+    h.mesh(lay["verts"], lay["tris"], ground)
+    metals = {}
+    for name in METALS:
+        n_, k_ = spectra.metal_nk(name)
+        metals[name] = (h.spectrum(n_), h.spectrum(k_))
+    ms = [h.material(type=abi.MAT_CONDUCTOR, eta=metals[m][0], k=metals[m][1], alphaX=a, alphaY=a)
+          for _, _, m, a in lay["spheres"]]
+    if ms:
+        h.spheres([c for c, _, _, _ in lay["spheres"]], [r for _, r, _, _ in lay["spheres"]], ms)
+    absorb = h.spectrum(spectra.constant(0.05))
+    scatter = h.spectrum(spectra.constant(0.95))
+    sky_ill = h.spectrum(spectra.blackbody(8000.0) / spectra.blackbody(8000.0).max())
+    sun_spec = h.spectrum(spectra.blackbody(5800.0) / spectra.blackbody(5800.0).max())
+    grid = media.grid_desc(absorb, scatter, lay["density"], [[-1, -1, -1], [1, 1, 1]], scale=1.0, g=0.8,
+                           world_to_medium=media.affine_inverse(CLOUD_TO_WORLD))
+    # The cloud's interface box, outward-facing: rays that cross it enter and leave grid medium 0
+    # (grids are numbered after the SceneDesc's homogeneous media, of which there are none).
+    bverts, bidx = box_mesh(*CLOUD_BOX)
+    h.mesh(bverts, bidx, h.material(type=abi.MAT_INTERFACE), medium_inside=len(h.media), medium_outside=-1)
+    h.finish(width=width, height=height, max_leaf=4, **CAMERA)
+    # Sky: a 256 x 128 equirect map of flat sigmoid-polynomial texels (c0 = c1 = c2 = 0, so the
+    # spectrum is scale / 2 x the illuminant) with a zenith-to-horizon gradient and a dark ground.
+    sw, sh = 256, 128
+    cos_t = np.cos((np.arange(sh, dtype=np.float32) + 0.5) / sh * np.pi)
+    lum = np.where(cos_t > 0, 0.35 + 0.65 * (1 - cos_t) ** 2, 0.05)
+    texels = np.zeros((sh, sw, 4), np.float32)
+    texels[:, :, 3] = 2.0 * lum[:, None]
+    env = abi.EnvMapDesc()
+    env.width, env.height = sw, sh
+    env.texels = texels.ctypes.data
+    env.illuminant, env.scale, env.rotationDeg, env.pmf = sky_ill, 1.0, 0.0, 0.5
+    sd = abi.SunDesc()
+    for i, v in enumerate(scenes.sun_direction(SUN_ELEVATION, SUN_AZIMUTH)):
+        sd.direction[i] = float(v)
+    sd.cosThetaMax = math.cos(math.radians(0.2665))
+    sd.spectrum, sd.scale, sd.pmf = sun_spec, 2.0e4, 0.5
+    ext = render.make_ext(grid_media=[grid])
+    ext.envMap = C.addressof(env)
+    ext.sun = C.addressof(sd)
+    ext._keep += [env, texels, sd, grid, lay["density"]]
+    return h, ext
+
+
+def write_large_scene_json(path: str, width: int, height: int, spp: int = 16, max_depth: int = 64,
+                           terrain_res: int = 48, cloud_res: int = 24, spheres: int = 12, seed: int = 0,
+                           turbidity: float = 3.0, sky_resolution: int = 64) -> str:
+    """The large outdoor scene in the reference's JSON form (the same seeded layout as
+    build_large_scene; the cloud written as a .vol beside the JSON), lit by the reference's own
+    Preetham sun and sky (turbidity, sun elevation 20 degrees). Returns the path."""
+    import json
+    import os
+
+    from . import media
+
+    lay = large_scene_layout(terrain_res, cloud_res, spheres, seed)
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    vol = media.write_vol(os.path.abspath(path) + ".vol", lay["density"], [[-1, -1, -1], [1, 1, 1]])
+    f32 = lambda a: [float(x) for x in np.asarray(a, np.float32).ravel()]
+    mats = {"ground": {"type": "diffuse", "reflectance": [0.3, 0.3, 0.3]}, "boundary": {"type": "interface"}}
+    geometry = {"terrain": {"type": "mesh", "positions": f32(lay["verts"]),
+                            "indices": [int(x) for x in lay["tris"].ravel()]}}
+    objects = [{"name": "terrain", "geometry": "terrain", "material": "ground"}]
+    for k, (c, r, metal, alpha) in enumerate(lay["spheres"]):
+        mats[f"metal{k}"] = {"type": "conductor", "metal": metal, "roughness": math.sqrt(alpha)}
+        geometry[f"ball{k}"] = {"type": "sphere", "center": f32(c), "radius": float(np.float32(r))}
+        objects.append({"name": f"ball{k}", "geometry": f"ball{k}", "material": f"metal{k}"})
+    bv, bi = box_mesh(*CLOUD_BOX)
+    geometry["cloudbox"] = {"type": "mesh", "positions": f32(bv), "indices": [int(x) for x in bi.ravel()],
+                            "closed": True}
+    objects.append({"name": "cloudbox", "geometry": "cloudbox", "material": "boundary", "interior": "cloud",
+                    "exterior": None})
+    doc = {
+        "materials": mats,
+        "media": {"cloud": {"type": "grid", "file": vol, "sigma_a": [0.05, 0.05, 0.05], "sigma_s": [0.95, 0.95, 0.95],
+                            "g": 0.8, "scale": 1.0, "bounds": [[-1, -1, -1], [1, 1, 1]],
+                            "transform": {"matrix": f32(CLOUD_TO_WORLD)}}},
+        "geometry": geometry, "objects": objects,
+        "lights": {"sky": {"type": "sun_sky", "elevation": SUN_ELEVATION, "azimuth": SUN_AZIMUTH,
+                           "turbidity": turbidity, "resolution": sky_resolution}},
+        "cameras": {"cam": {"type": "pinhole", "position": list(CAMERA["cam_pos"]),
+                            "look_at": list(CAMERA["cam_target"]), "fov_y": CAMERA["fov_y"]}},
+        "render": {"camera": "cam", "seed": seed, "film": {"width": width, "height": height, "filter": "box"},
+                   "integrator": {"type": "path", "spp": spp, "max_depth": max_depth}},
+    }
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    return path

@@ -289,6 +289,61 @@ def run_reference_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def large_scene_bench(args, device: int):
+    """The large outdoor scene (prgpu.hostscene.build_large_scene): a 4096^2 fBm heightfield
+    (33.5M triangles), a 256^3 fBm cloud grid medium, 200 analytic GGX conductor spheres, a sun
+    cone and an importance-sampled sky map, 3840 x 2160, depth 64, rendered through
+    prgpu_render_ex. One step = --ls-spp samples per pixel; value = path samples/s of device time,
+    plain BSDF sampling; guided = the same with the guide network sampling diffuse vertices and
+    training online. No CPU baseline: the reference renders this scene at well under 1 spp per
+    minute of this bench's budget."""
+    from prgpu import hostscene, render
+
+    t0 = time.perf_counter()
+    hs, ext = hostscene.build_large_scene(args.ls_width, args.ls_height, terrain_res=args.ls_terrain,
+                                          cloud_res=args.ls_cloud)
+    build_s = time.perf_counter() - t0
+    desc = hs.desc()
+    w, h, spp, depth = args.ls_width, args.ls_height, args.ls_spp, 64
+    film = np.zeros((h, w, 3))
+    t0 = time.perf_counter()
+    render.render_ex(desc, w, h, 1, seed=1, max_depth=depth, ext=ext, out=film)
+    first_s = time.perf_counter() - t0
+    out = {"workload": f"large outdoor scene: {args.ls_terrain}^2 fBm terrain ({2 * (args.ls_terrain - 1) ** 2:,} triangles), "
+                       f"{args.ls_cloud}^3 fBm cloud grid, 200 GGX conductor spheres, sun + sky map, {w}x{h}, "
+                       f"{spp} spp per step, depth 64",
+           "metric": "path samples/s", "unit": "path samples/s", "host_scene_build_s": build_s,
+           "first_render_s_with_upload": first_s, "steps": args.ls_steps}
+    for name, flags in (("plain", 0), ("guided", render.GUIDE_SAMPLE | render.GUIDE_TRAIN)):
+        e = abi_copy_ext(ext, flags | (render.GUIDE_RESET if flags else 0))
+        render.render_ex(desc, w, h, 1, seed=2, max_depth=depth, ext=e, out=film)
+        e.flags = flags
+        dev, st = [], None
+        for k in range(args.ls_steps):
+            _, st = render.render_ex(desc, w, h, spp, first_sample=(k + 1) * spp, seed=1, max_depth=depth, ext=e,
+                                     out=film, stats=True)
+            dev.append(st.deviceMs)
+        r = {"value": w * h * spp / (statistics.mean(dev) * 1e-3), "ms_per_step": statistics.mean(dev),
+             "kernel_ms": {"closest": st.traceMs, "shade": st.shadeMs, "shadow": st.shadowMs, "film": st.filmMs},
+             "rays_per_step": {"closest": int(st.closestRays), "shadow": int(st.shadowRays)},
+             "bounces_per_sample": st.bounces / max(1, st.pathSamples)}
+        if name == "plain":
+            out.update(r)
+        else:
+            out["guided"] = r
+    return out
+
+
+def abi_copy_ext(ext, flags: int):
+    """A copy of a SceneExt with other guide flags (the arrays stay owned by the original)."""
+    from prgpu import abi
+
+    e = abi.SceneExt.from_buffer_copy(ext)
+    e.flags = flags
+    e._keep = [ext]
+    return e
+
+
 def main():
     global N_RAYS
     ap = argparse.ArgumentParser()
@@ -312,6 +367,16 @@ def main():
                          "conditional graphs)")
     ap.add_argument("--batch-spp-div", type=int, default=1,
                     help="divide every render's spp (profiling captures only; the JSON says so)")
+    ap.add_argument("--large-scene", action="store_true",
+                    help="also run the large outdoor scene (33.5M-triangle terrain, cloud grid, 4K film; opt-in: "
+                         "about a minute of host scene build)")
+    ap.add_argument("--large-scene-only", action="store_true", help="run only the large outdoor scene")
+    ap.add_argument("--ls-spp", type=int, default=4)
+    ap.add_argument("--ls-steps", type=int, default=2)
+    ap.add_argument("--ls-width", type=int, default=3840)
+    ap.add_argument("--ls-height", type=int, default=2160)
+    ap.add_argument("--ls-terrain", type=int, default=4096)
+    ap.add_argument("--ls-cloud", type=int, default=256)
     args = ap.parse_args()
     N_RAYS = args.rays
     args.warmup = max(args.warmup, 3)
@@ -326,6 +391,9 @@ def main():
         return
     if args.batch_only:
         print(json.dumps(batch_bench(args, local, cpu=not args.no_cpu_baseline)))
+        return
+    if args.large_scene_only:
+        print(json.dumps(large_scene_bench(args, local)))
         return
 
     import torch
@@ -430,6 +498,9 @@ def main():
     bt = None
     if world == 1 and not args.no_batch:
         bt = batch_bench(args, local, cpu=not args.no_cpu_baseline)
+    ls = None
+    if world == 1 and args.large_scene:
+        ls = large_scene_bench(args, local)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -456,6 +527,8 @@ def main():
         "path_tracer": pt,
         "uneven_batch": bt,
     }
+    if ls is not None:
+        line["large_scene"] = ls
     print(json.dumps(line), flush=True)
 
 

@@ -119,6 +119,46 @@ def sun_sky_inputs(rs, elevation, azimuth, turbidity, sky_resolution, intensity=
     return sd, ext
 
 
+def large_scene_inputs(rs, path, turbidity=3.0, sky_resolution=64):
+    """The GPU-side inputs of the large outdoor scene loaded by the reference: the sun and sky of
+    sun_sky_inputs plus the cloud's sigma_a / sigma_s tables appended to the spectra and the cloud
+    grid (read back from the .vol the scene names) as grid medium 0."""
+    import ctypes as C
+
+    import ref as oracle_ref
+    from prgpu import abi, hostscene, media, spectra
+
+    sd, ext = sun_sky_inputs(rs, hostscene.SUN_ELEVATION, hostscene.SUN_AZIMUTH, turbidity, sky_resolution)
+    old = np.ctypeslib.as_array((C.c_float * (95 * sd.spectrumCount)).from_address(sd.spectra)).reshape(-1, 95)
+    lam = spectra.LAMBDA.astype(np.float32)
+    rows = []
+    for v in (0.05, 0.95):
+        out = np.zeros(95, dtype=np.float32)
+        assert oracle_ref.ref_lib().prref_spectrum(1, v, v, v, None, 95, oracle_ref._p(lam), oracle_ref._p(out)) == 0
+        rows.append(out)
+    table = np.ascontiguousarray(np.concatenate([old, np.stack(rows)]), np.float32)
+    na = sd.spectrumCount
+    sd.spectra = table.ctypes.data
+    sd.spectrumCount = table.shape[0]
+    sd._keep = (sd._keep, table)
+    grids = rs.grid_media()
+    assert [g[0] for g in grids] == ["cloud"], grids
+    import json
+
+    with open(path) as f:
+        doc = json.load(f)
+    density, _ = media.read_vol(doc["media"]["cloud"]["file"])
+    desc = media.grid_desc(na, na + 1, density, grids[0][1], scale=1.0, g=0.8,
+                           world_to_medium=media.affine_inverse(hostscene.CLOUD_TO_WORLD))
+    from prgpu.media import grid_array
+
+    arr = grid_array([desc])
+    ext.gridMediumCount = 1
+    ext.gridMedia = C.cast(arr, C.c_void_p)
+    ext._keep += [desc, arr, density]
+    return sd, ext
+
+
 def luminance_y(img: np.ndarray) -> np.ndarray:
     return img[..., 1]
 

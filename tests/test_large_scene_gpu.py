@@ -1,0 +1,48 @@
+"""The large outdoor scene family on the GPU against the oracle: an fBm heightfield terrain, an
+fBm cloud in a grid medium (spectral tracking and ratio-tracked shadows through an interface box),
+analytic GGX conductor spheres of four metals and the reference's Preetham sun and sky, at a
+size the reference PathIntegrator renders in seconds, from one scene file."""
+
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import render_util as ru
+from prgpu import hostscene, render
+
+pytestmark = pytest.mark.gpu
+
+
+def test_large_scene_family_agrees_with_reference(gpu, oracle):
+    """48 x 27, depth 64: a 48^2 terrain (4,418 triangles), a 24^3 cloud and 12 spheres. Per-pixel
+    z of the mean over 16 renders of 64 spp each side, |z| < 4 on >= 99.5% of values; mean
+    luminance within 4 standard errors of the per-render means."""
+    w, h = 48, 27
+    path = hostscene.write_large_scene_json(os.path.join(tempfile.gettempdir(), "prb_scenes", "large_small.prscene.json"),
+                                            w, h, terrain_res=48, cloud_res=24, spheres=12)
+    rs = oracle.RefScene(path)
+    sd, ext = ru.large_scene_inputs(rs, path)
+    g = np.stack([render.render_ex(sd, w, h, 64, seed=1000 + k, max_depth=64, ext=ext) / 64 for k in range(16)])
+    c = np.stack([rs.render(64, 2000 + k, 64)[0].astype(np.float64) / 64 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"large scene: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+
+
+def test_host_built_large_scene_renders(gpu):
+    """The host-built form (prgpu.hostscene.build_large_scene: analytic spheres in the BVH, the
+    cloud through SceneExt, the sky map and the sun) at 64 x 36 with a 128^2 terrain: finite,
+    non-negative, non-black and deterministic for a seed."""
+    hs, ext = hostscene.build_large_scene(64, 36, terrain_res=128, cloud_res=32, spheres=40)
+    desc = hs.desc()
+    a = render.render_ex(desc, 64, 36, 16, seed=3, max_depth=64, ext=ext)
+    b = render.render_ex(desc, 64, 36, 16, seed=3, max_depth=64, ext=ext)
+    assert np.isfinite(a).all() and (a >= 0).all()
+    assert np.array_equal(a, b)
+    assert a[..., 1].mean() > 0
