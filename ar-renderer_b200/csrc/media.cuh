@@ -2,8 +2,10 @@
 // medium of pr::GridMedium -- trilinear cell-centred density (src/media/medium.cpp:117-128),
 // clipping of the segment to the grid bounds in medium space (medium.cpp:182-203), ratio tracking
 // with Russian roulette for shadow transmittance (medium.cpp:205-230) and spectral tracking for
-// free-flight sampling (medium.cpp:232-285), both against the global majorant
-// maxDensity * max(sigma_t).
+// free-flight sampling (medium.cpp:232-285). The reference tracks against the global majorant
+// maxDensity * max(sigma_t); these walk a table of per-macro-cell majorants instead (the same
+// estimators with a piecewise-constant rate, so the same expectations, with far fewer null
+// collisions in sparse media).
 #pragma once
 
 #include "scene.cuh"
@@ -85,6 +87,61 @@ __device__ __forceinline__ void grid_sigma(const DevScene &s, const DevGrid &g, 
     *ss = tab4(s.spectra, g.sigmaS, lam) * g.scale;
 }
 
+// The free-flight process of a grid medium along its clipped medium-space ray mo + md t,
+// t in [t0, t1): a walk over the macro cells the ray crosses (3D DDA), sampling exponential steps
+// at each cell's own rate mu = majorant x sMax and restarting at every cell boundary (the process
+// is memoryless), so empty cells cost one step of the walk and no density lookups. Calls
+// f(t, mu) at each tentative collision; f returns false to stop. Bounded: at most 100,000
+// collisions and mx + my + mz + 3 cells.
+template <class F>
+__device__ __forceinline__ void majorant_walk(const DevGrid &g, V3 mo, V3 md, float t0, float t1, float sMax, Pcg &rng,
+                                              F &&f) {
+    const int M[3] = {g.mx, g.my, g.mz};
+    const float o[3] = {mo.x, mo.y, mo.z}, dd[3] = {md.x, md.y, md.z};
+    int c[3], step[3];
+    float tNext[3], dt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float ext = g.bmax[a] - g.bmin[a];
+        float sc = ext > 0.f ? float(M[a]) / ext : 0.f;
+        float u0 = (o[a] + dd[a] * t0 - g.bmin[a]) * sc, du = dd[a] * sc;
+        c[a] = min(max(int(floorf(u0)), 0), M[a] - 1);
+        if (du > 0.f) {
+            tNext[a] = t0 + (float(c[a] + 1) - u0) / du;
+            dt[a] = 1.f / du;
+            step[a] = 1;
+        } else if (du < 0.f) {
+            tNext[a] = t0 + (float(c[a]) - u0) / du;
+            dt[a] = -1.f / du;
+            step[a] = -1;
+        } else {
+            tNext[a] = INFINITY;
+            dt[a] = 0.f;
+            step[a] = 0;
+        }
+    }
+    float t = t0;
+    int collisions = 0;
+    for (int cells = 0; cells < M[0] + M[1] + M[2] + 3; ++cells) {
+        int a = tNext[0] < tNext[1] ? (tNext[0] < tNext[2] ? 0 : 2) : (tNext[1] < tNext[2] ? 1 : 2);
+        float segEnd = fminf(tNext[a], t1);
+        float mu = __ldg(g.majorant + (size_t(c[2]) * M[1] + c[1]) * M[0] + c[0]) * sMax;
+        if (mu > 0.f) {
+            float inv = 1.f / mu;
+            for (;;) {
+                t -= logf(1.f - rng.uniform()) * inv;
+                if (t >= segEnd) break;
+                if (!f(t, mu) || ++collisions >= 100000) return;
+            }
+        }
+        if (!(tNext[a] < t1)) return;
+        t = segEnd;
+        c[a] += step[a];
+        if (c[a] < 0 || c[a] >= M[a]) return;
+        tNext[a] += dt[a];
+    }
+}
+
 // Ratio-tracking transmittance over [0, dist) along the unit direction d, Russian roulette once
 // the largest channel drops below 0.1 (unbiased). rng: a stream for this segment.
 __device__ SS grid_tr(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float dist, Pcg &rng) {
@@ -94,24 +151,27 @@ __device__ SS grid_tr(const DevScene &s, const DevGrid &g, const Lambda &lam, V3
     SS sa, ss;
     grid_sigma(s, g, lam, &sa, &ss);
     SS st = sa + ss;
-    float mu = g.maxDensity * max_c(st);
-    if (mu <= 0.f) return splat(1.f);
-    float invMu = 1.f / mu;
+    float sMax = max_c(st);
+    if (!(sMax > 0.f)) return splat(1.f);
     SS T = splat(1.f);
-    float t = t0;
-    for (int iter = 0; iter < 100000; ++iter) {
-        t -= logf(1.f - rng.uniform()) * invMu;
-        if (t >= t1) break;
-        float den = grid_density(g, mo + md * t);
+    majorant_walk(g, mo, md, t0, t1, sMax, rng, [&](float t, float mu) {
+        float den = grid_density(g, mo + md * t) / mu;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) T.v[i] *= fmaxf(0.f, 1.f - st.v[i] * (den * invMu));
+        for (int i = 0; i < 4; ++i) T.v[i] *= fmaxf(0.f, 1.f - st.v[i] * den);
         float m = max_c(T);
-        if (m <= 0.f) return splat(0.f);
+        if (m <= 0.f) {
+            T = splat(0.f);
+            return false;
+        }
         if (m < 0.1f) {
-            if (rng.uniform() < 0.5f) return splat(0.f);
+            if (rng.uniform() < 0.5f) {
+                T = splat(0.f);
+                return false;
+            }
             T = T * 2.f;
         }
-    }
+        return true;
+    });
     return T;
 }
 
@@ -135,10 +195,8 @@ __device__ int grid_sample(const DevScene &s, const DevGrid &g, const Lambda &la
     if (!grid_clip(g, o, d, tMax, &mo, &md, &t0, &t1)) return 0;
     SS sa, ss;
     grid_sigma(s, g, lam, &sa, &ss);
-    SS st = sa + ss;
-    float mu = g.maxDensity * max_c(st);
-    if (mu <= 0.f) return 0;
-    float invMu = 1.f / mu;
+    float sMax = max_c(sa + ss);
+    if (!(sMax > 0.f)) return 0;
     auto avg = [&](const SS &v) {
         float sum = 0.f;
         int n = 0;
@@ -150,32 +208,32 @@ __device__ int grid_sample(const DevScene &s, const DevGrid &g, const Lambda &la
             }
         return n ? sum / n : 0.f;
     };
-    float t = t0;
-    for (int iter = 0; iter < 100000; ++iter) {
-        t -= logf(1.f - rng.uniform()) * invMu;
-        if (t >= t1) break;
+    int event = 0;
+    majorant_walk(g, mo, md, t0, t1, sMax, rng, [&](float t, float mu) {
         float den = grid_density(g, mo + md * t);
         SS sA = sa * den, sS = ss * den;
         SS sN = splat(mu) + sA * -1.f + sS * -1.f;
         float pa = avg(sA), ps = avg(sS), pn = avg(sN);
         float norm = pa + ps + pn;
-        if (norm <= 0.f) continue;
+        if (norm <= 0.f) return true;
         float xi = rng.uniform() * norm;
         if (xi < ps) {
             *tOut = t;
             *weight = *weight * sS * (1.f / (mu * ps / norm));
-            return 1;
+            event = 1;
+            return false;
         }
         if (xi < ps + pa) {
             *tOut = t;
             *weight = splat(0.f);
-            return 2;
+            event = 2;
+            return false;
         }
         *weight = *weight * sN * (1.f / (mu * pn / norm));
-        if (!nonzero(*weight)) return 0;
-    }
-    *tOut = tMax;
-    return 0;
+        return nonzero(*weight);
+    });
+    if (event == 0) *tOut = tMax;
+    return event;
 }
 
 // A PCG stream for a shadow segment, from its geometry (ratio tracking needs randomness the path

@@ -85,7 +85,7 @@ struct RenderState {
     int *hostActive = nullptr;          // pinned: the active-queue length, polled between bounce blocks
     cudaEvent_t ev[4 * kBouncesPerPoll + 2] = {};
     bool events = false;
-    int residentExtend[2] = {0, 0}, residentShadow[4] = {0, 0, 0, 0};
+    int residentExtend[2] = {0, 0}, residentShadow[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 std::unique_ptr<RenderState> gRender[64];
@@ -127,6 +127,9 @@ void ensure_capacity(RenderState &rs, int cap) {
     rs.S.w = reinterpret_cast<float *>(take(cap * sizeof(float)));
     rs.queues.ensure(size_t(2) * cap * sizeof(int));
     rs.classQueues.ensure(size_t(kClasses) * cap * sizeof(int));
+    // The interface walk's queue reuses the class queues: they are dead between shading and the
+    // next closest-hit pass, and a bounce queues at most one shadow entry per path.
+    rs.S.walk = rs.classQueues.as<int>();
     rs.counters.ensure(kCntSlots * sizeof(int));
     rs.stats.ensure(kStatSlots * sizeof(unsigned long long));
     rs.capacity = cap;
@@ -139,8 +142,9 @@ int grid_for(const DeviceState &ds, int64_t work, int perSm = 8) {
 
 using ShadowAnyFn = void (*)(DevScene, const DevScene *, Paths, Shadows, int *);
 
-// variant bit 0: spheres present, bit 1: media present.
+// variant bit 0: spheres present, bit 1: media present, bit 2: medium interfaces present.
 ShadowAnyFn shadow_any_kernel(int variant) {
+    if (variant & 4) return (variant & 1) ? k_shadow_any<true, true, false, true> : k_shadow_any<false, true, false, true>;
     switch (variant & 3) {
     case 0: return k_shadow_any<false, false>;
     case 1: return k_shadow_any<true, false>;
@@ -177,7 +181,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
         PRB_CUDA(cudaMallocHost(&rs.hostActive, sizeof(int)));
         rs.residentExtend[0] = resident_blocks_of(k_extend<false>);
         rs.residentExtend[1] = resident_blocks_of(k_extend<true>);
-        for (int v = 0; v < 4; ++v) rs.residentShadow[v] = resident_blocks_of(shadow_any_kernel(v));
+        for (int v = 0; v < 8; ++v) rs.residentShadow[v] = resident_blocks_of(shadow_any_kernel(v));
         rs.events = true;
     }
     int *cnt = rs.counters.as<int>();
@@ -188,7 +192,8 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     uint64_t launches = 0;
     const int sph = rs.scene.hasSpheres ? 1 : 0;
     const int sms = ds.prop.multiProcessorCount;
-    const int shadowVariant = sph | (scene.mediumCount + scene.gridCount > 0 ? 2 : 0);
+    const int shadowVariant =
+        sph | (scene.mediumCount + scene.gridCount > 0 ? 2 : 0) | (scene.hasInterfaces ? 6 : 0);
     const ShadowAnyFn shadowAny = shadow_any_kernel(shadowVariant);
     const int gExtend = sms * rs.residentExtend[sph], gShadow = sms * rs.residentShadow[shadowVariant];
     const int gShade = sms * 8;
@@ -249,11 +254,11 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     if (guideMode) k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
                     else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
+                    shadowAny<<<gShadow, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                     if (scene.hasInterfaces) {
                         if (sph) k_shadow_walk<true><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                         else k_shadow_walk<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
-                    } else {
-                        shadowAny<<<gShadow, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
+                        ++launches;
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 3], st));
                     k_advance<<<1, 1, 0, st>>>(cnt, dstats);
@@ -641,7 +646,7 @@ uint64_t batch_shape_key(int device, int count, const prgpu::BatchItem *items) {
 struct BatchLaunch {
     void (*extend)(DevScene, const DevScene *, Paths, int *, const int *);
     void (*shadowAny)(DevScene, const DevScene *, Paths, Shadows, int *);
-    void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, const int *);
+    void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, int *);
     bool walls;
     int gExtend, gShadow, gShade, gWide, shadeBlock, capacity;
 };
@@ -651,12 +656,13 @@ BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
     BatchLaunch L{};
     L.walls = key.variant & 4;
     L.extend = sph ? k_extend<true, true> : k_extend<false, true>;
-    L.shadowAny = sph ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
-                      : (media ? k_shadow_any<false, true, true> : k_shadow_any<false, false, true>);
+    L.shadowAny = L.walls ? (sph ? k_shadow_any<true, true, true, true> : k_shadow_any<false, true, true, true>)
+                  : sph   ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
+                          : (media ? k_shadow_any<false, true, true> : k_shadow_any<false, false, true>);
     L.shadowWalk = sph ? k_shadow_walk<true, true> : k_shadow_walk<false, true>;
     const int sms = ds.prop.multiProcessorCount;
     L.gExtend = sms * resident_blocks_of(L.extend);
-    L.gShadow = L.walls ? sms * 8 : sms * resident_blocks_of(L.shadowAny);
+    L.gShadow = sms * resident_blocks_of(L.shadowAny);
     int perSm = 0;
     PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade<true>, key.shadeBlock, 0));
     L.gShade = sms * std::max(1, perSm);
@@ -689,8 +695,11 @@ int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &
         k_classify<true><<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, cnt, qin, cq, rs.capacity);
         ShadeArgs sa{none, scenes, rs.P, rs.S, cq, rs.capacity, qout, cnt, 0, L.capacity / 2};
         k_shade<true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
-        if (L.walls) L.shadowWalk<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
-        else L.shadowAny<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        L.shadowAny<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+        if (L.walls) {
+            L.shadowWalk<<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
+            ++launches;
+        }
         k_advance<<<1, 1, 0, st>>>(cnt, dstats);
         launches += 5;
         std::swap(qin, qout);

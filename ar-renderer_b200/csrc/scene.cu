@@ -167,6 +167,51 @@ float texel_value(const float *t, float l) {
     return t[3] * s;
 }
 
+// Macro cells per axis of a grid's majorant table: one per 8 voxels, at most 32.
+static int macro_cells(int n) { return std::max(1, std::min(32, (n + 7) / 8)); }
+
+// Per macro cell, the largest voxel among those the trilinear lookup can touch for a point inside
+// the cell (voxel centres within one voxel of it), widened by one more voxel on every side so that
+// rounding in the lookup's or the walk's coordinates can never leave a point under its bound.
+static std::vector<float> macro_majorants(const float *d, int nx, int ny, int nz, int *mx, int *my, int *mz) {
+    const int n[3] = {nx, ny, nz};
+    int m[3];
+    std::vector<int> lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        m[a] = macro_cells(n[a]);
+        for (int c = 0; c < m[a]; ++c) {
+            double x0 = double(c) * n[a] / m[a] - 0.5, x1 = double(c + 1) * n[a] / m[a] - 0.5;
+            lo[a].push_back(std::max(0, int(std::floor(x0)) - 1));
+            hi[a].push_back(std::min(n[a] - 1, int(std::floor(x1)) + 2));
+        }
+    }
+    *mx = m[0], *my = m[1], *mz = m[2];
+    // Separable running maxima: along x, then y, then z.
+    std::vector<float> ax(size_t(m[0]) * ny * nz), ay(size_t(m[0]) * m[1] * nz), az(size_t(m[0]) * m[1] * m[2]);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int c = 0; c < m[0]; ++c) {
+                float v = 0.f;
+                for (int x = lo[0][size_t(c)]; x <= hi[0][size_t(c)]; ++x) v = std::max(v, d[(size_t(z) * ny + y) * nx + x]);
+                ax[(size_t(z) * ny + y) * m[0] + c] = v;
+            }
+    for (int z = 0; z < nz; ++z)
+        for (int c = 0; c < m[1]; ++c)
+            for (int x = 0; x < m[0]; ++x) {
+                float v = 0.f;
+                for (int y = lo[1][size_t(c)]; y <= hi[1][size_t(c)]; ++y) v = std::max(v, ax[(size_t(z) * ny + y) * m[0] + x]);
+                ay[(size_t(z) * m[1] + c) * m[0] + x] = v;
+            }
+    for (int c = 0; c < m[2]; ++c)
+        for (int y = 0; y < m[1]; ++y)
+            for (int x = 0; x < m[0]; ++x) {
+                float v = 0.f;
+                for (int z = lo[2][size_t(c)]; z <= hi[2][size_t(c)]; ++z) v = std::max(v, ay[(size_t(z) * m[1] + y) * m[0] + x]);
+                az[(size_t(c) * m[1] + y) * m[0] + x] = v;
+            }
+    return az;
+}
+
 // The image environment's texels and its sampling distribution (EnvironmentLight's constructor,
 // light.cpp:217-236, with a spectral luminance in place of the RGB one; Distribution2D,
 // sampling.cpp:44-67). Rows are Distribution1D CDFs normalised to 1 (unless all zero).
@@ -267,8 +312,17 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
                                      : t == prgpu::MatConductor  ? kClassConductor
                                      : t == prgpu::MatDielectric ? kClassDielectric
                                                                  : kClassOther);
+            if (t == prgpu::MatInterface) cls[size_t(i)] |= kTransparentBit;
         }
         put(cache.primClass, cls.data(), cls.size(), s);
+        std::vector<LeafPrim> walls;
+        for (const LeafPrim &lp : h.prims) {
+            int32_t id;
+            std::memcpy(&id, &lp.v0.w, sizeof(id));
+            if (id >= 0 && id < sd->primCount && (cls[size_t(id)] & kTransparentBit)) walls.push_back(lp);
+        }
+        cache.wallCount = walls.size() <= size_t(kMaxWallList) ? int(walls.size()) : -1;
+        if (cache.wallCount > 0) put(cache.walls, walls.data(), walls.size(), s);
         put(cache.mats, sd->materials, size_t(sd->materialCount), s);
         put(cache.lights, sd->lights, size_t(sd->lightCount), s);
         put(cache.spectra, sd->spectra, size_t(sd->spectrumCount), s);
@@ -283,8 +337,10 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         int32_t ng = (ext && ext->gridMediumCount > 0) ? ext->gridMediumCount : 0;
         std::vector<DevGrid> grids(size_t(std::max(1, ng)));
         size_t total = 0;
-        for (int32_t k = 0; k < ng; ++k)
-            total += size_t(ext->gridMedia[k].nx) * ext->gridMedia[k].ny * ext->gridMedia[k].nz;
+        for (int32_t k = 0; k < ng; ++k) {
+            const prgpu::GridMediumDesc &g = ext->gridMedia[k];
+            total += size_t(g.nx) * g.ny * g.nz + size_t(macro_cells(g.nx)) * macro_cells(g.ny) * macro_cells(g.nz);
+        }
         cache.gridData.ensure(std::max<size_t>(1, total) * sizeof(float));
         size_t off = 0;
         for (int32_t k = 0; k < ng; ++k) {
@@ -308,10 +364,14 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
             std::vector<float> clean(g.density, g.density + n);
             for (float &v : clean)
                 if (!std::isfinite(v) || v < 0.f) v = 0.f;
+            std::vector<float> maj = macro_majorants(clean.data(), g.nx, g.ny, g.nz, &dg.mx, &dg.my, &dg.mz);
+            dg.majorant = dg.density + n;
             PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.density), clean.data(), n * sizeof(float),
                                      cudaMemcpyHostToDevice, s));
+            PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.majorant), maj.data(), maj.size() * sizeof(float),
+                                     cudaMemcpyHostToDevice, s));
             PRB_CUDA(cudaStreamSynchronize(s));
-            off += n;
+            off += n + maj.size();
         }
         put(cache.grids, grids.data(), grids.size(), s);
         d.grids = cache.grids.as<DevGrid>();
@@ -331,6 +391,8 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         d.root = cache.accel.root;
         d.prims = cache.prims.as<prgpu::Primitive>();
         d.primClass = cache.primClass.as<uint8_t>();
+        d.walls = cache.wallCount > 0 ? cache.walls.as<LeafPrim>() : nullptr;
+        d.wallCount = cache.wallCount;
         d.mats = cache.mats.as<prgpu::Material>();
         d.lights = cache.lights.as<prgpu::Light>();
         d.spectra = cache.spectra.as<float>();

@@ -15,6 +15,8 @@
 namespace prb {
 
 // A heterogeneous medium on the device (GridMediumDesc with its density grid resident in HBM).
+constexpr int kMaxWallList = 64;
+
 struct DevGrid {
     float w2m[12];
     float bmin[3], bmax[3];
@@ -23,6 +25,10 @@ struct DevGrid {
     float scale, g;
     int sigmaA, sigmaS;
     const float *density;
+    // Macro-cell majorants: mx * my * mz cells tiling the bounds, x fastest, each >= the
+    // trilinear density anywhere in the cell (a one-voxel margin on every side).
+    int mx, my, mz;
+    const float *majorant;
 };
 
 // Shading classes: the closest-hit kernel files every finished path under one of these, and the
@@ -65,7 +71,8 @@ struct DevScene {
     const LeafPrim *leaves;
     RootInfo root;
     const prgpu::Primitive *prims;
-    const uint8_t *primClass;    // shading class of each primitive's material (ShadeClass)
+    const uint8_t *primClass;    // shading class of each primitive's material (ShadeClass), | kTransparentBit
+                                 // for medium interfaces
     const prgpu::Material *mats;
     const prgpu::Light *lights;
     int lightCount;
@@ -79,6 +86,10 @@ struct DevScene {
     prgpu::Camera cam;
     float norm;           // 1 / (4 * integral of CIE y): XYZ normalisation of one sample
     int hasInterfaces;
+    // The medium-interface primitives as leaf slots, for the shadow walk's closest-hit queries
+    // (brute force over at most kMaxWallList); wallCount < 0: too many, the walk uses the tree.
+    const LeafPrim *walls;
+    int wallCount;
     uint32_t filterType;
     float filterRadius, filterSigma, filterNorm;
     const float *filterCdf;  // kFilterBins + 1
@@ -104,9 +115,10 @@ struct SceneCache {
     bool valid = false;
     DeviceAccel accel;
     DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
-        envDist;
+        envDist, walls;
     DevScene ds{};
     bool hasSpheres = false;
+    int wallCount = 0;
     int64_t deviceBytes = 0;
     void release() {
         accel.release();
@@ -123,6 +135,7 @@ struct SceneCache {
         gridData.release();
         envTexels.release();
         envDist.release();
+        walls.release();
         valid = false;
     }
 };

@@ -245,8 +245,12 @@ struct TravState {
     int ref, sp;
     float tMax;
     bool found;
+    bool crossed;  // kSkipTransparent: a transparent primitive was intersected before tMax
     Hit hit;
 };
+
+// Bit of a primitive's class byte marking it transparent to shadow rays (a medium interface).
+constexpr uint8_t kTransparentBit = 0x80;
 
 template <bool kAny, bool kSpheres>
 __device__ __forceinline__ bool traverse_step(const WNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
@@ -324,10 +328,12 @@ __device__ __forceinline__ void cswap(float &ta, int &ra, float &tb, int &rb) {
     }
 }
 
-template <bool kAny, bool kSpheres>
+// kSkipTransparent: primitives whose class byte (cls) has kTransparentBit do not count as hits;
+// intersecting one sets s.crossed.
+template <bool kAny, bool kSpheres, bool kSkipTransparent = false>
 __device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
                                                const TraceRay &r, TravState &s, int *stackRef, float *stackT,
-                                               bool *overflow) {
+                                               bool *overflow, const uint8_t *__restrict__ cls = nullptr) {
     if (s.ref >= 0) {
         const QNode *n = nodes + s.ref;
         const float4 lx = __ldg(&n->lox), ly = __ldg(&n->loy), lz = __ldg(&n->loz);
@@ -379,6 +385,10 @@ __device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, 
             else
                 h = hit_triangle(r, v0, v1, v2, s.tMax, &t, &u, &v);
             if (h) {
+                if (kSkipTransparent && (__ldg(cls + __float_as_int(v0.w)) & kTransparentBit)) {
+                    s.crossed = true;
+                    continue;
+                }
                 s.found = true;
                 if (kAny) return true;
                 s.tMax = t;

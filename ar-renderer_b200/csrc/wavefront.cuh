@@ -55,11 +55,13 @@ struct Shadows {
     float4 *d;   // target - origin, w: path index (int bits)
     float4 *c;   // contribution before transmittance
     float *w;    // spectral MIS scale applied to L
+    int *walk;   // entries whose segment crosses a medium interface (scenes with interfaces)
 };
 
 // Device counters of one wavefront: queue lengths, the persistent kernels' work counters, status.
 enum {
     kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
+    kCntWalk = 6,  // shadow entries queued for the interface walk
     // Batched form: live paths per half of the path slots after the last bounce, and the
     // survivors being counted during the current one.
     kCntLive0 = 8, kCntLive1 = 9, kCntNextLive0 = 10, kCntNextLive1 = 11,
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(256) k_classify(DevScene s0, const DevScene *s
             const int4 mt = P.meta[j];
             const int prim = __float_as_int(P.hit[j].w);
             const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(mt.w));
-            c = mt.z >= 0 ? kClassMedium : (prim < 0 ? kClassMiss : int(__ldg(s.primClass + prim)));
+            c = mt.z >= 0 ? kClassMedium : (prim < 0 ? kClassMiss : int(__ldg(s.primClass + prim) & ~kTransparentBit));
             rank = atomicAdd(&hist[c], 1);
         }
         __syncthreads();
@@ -1060,11 +1062,13 @@ __device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P,
     P.Lhero[j] = make_float4(Lh.x + c.v[0], Lh.y + c.v[1], Lh.z + c.v[2], Lh.w + c.v[3]);
 }
 
-// Visibility of queued NEE samples in scenes without medium interfaces: any-hit queries up to
-// 1 - ShadowEpsilon of the segment, by persistent warps with lane refill. kMedia: the scene has
-// media, so accepted segments carry a transmittance (kept out of the medium-free variant, whose
-// traversal loop would otherwise pay registers for the ratio-tracking code).
-template <bool kSpheres, bool kMedia, bool kBatch = false>
+// Visibility of queued NEE samples: any-hit queries up to 1 - ShadowEpsilon of the segment, by
+// persistent warps with lane refill. kMedia: the scene has media, so accepted segments carry a
+// transmittance (kept out of the medium-free variant, whose traversal loop would otherwise pay
+// registers for the ratio-tracking code). kWalls: the scene has medium interfaces; they are
+// transparent to this query, an occluded segment is done, an unoccluded one that crossed no
+// interface stays in its starting medium, and the rest go to the walk queue (k_shadow_walk).
+template <bool kSpheres, bool kMedia, bool kBatch = false, bool kWalls = false>
 __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene *scenes, Paths P, Shadows S,
                                                     int *counters) {
     const unsigned full = 0xffffffffu;
@@ -1078,10 +1082,12 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
     st.sp = 0;
     st.tMax = 1.f - kShadowEps;
     st.found = false;
+    st.crossed = false;
     int q = 0, rid = 0;
     const QNode *nodes = s0.qnodes;
     const LeafPrim *leaves = s0.leaves;
-    bool active = false, exhausted = n == 0, overflow = false;
+    const uint8_t *cls = s0.primClass;
+    bool active = false, exhausted = n == 0, overflow = false, toWalk = false;
     while (!__all_sync(full, exhausted)) {
         unsigned need = __ballot_sync(full, !active && !exhausted);
         if (need) {
@@ -1098,10 +1104,12 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                     const DevScene &s = SceneOf<kBatch>::get(s0, scenes, rid);
                     nodes = s.qnodes;
                     leaves = s.leaves;
+                    cls = s.primClass;
                     r = make_trace_ray(mk(o4.x, o4.y, o4.z), mk(d4.x, d4.y, d4.z));
                     st.tMax = 1.f - kShadowEps;
                     st.sp = 0;
                     st.found = false;
+                    st.crossed = false;
                     float te;
                     active = !s.root.empty &&
                              box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
@@ -1112,9 +1120,23 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                 }
             }
         }
-        if (active && traverse4_step<true, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+        if (active && traverse4_step<true, kSpheres, kWalls>(nodes, leaves, r, st, stackRef, stackT, &overflow, cls)) {
             active = false;
-            if (!st.found) shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
+            if (!st.found) {
+                if (kWalls && st.crossed) toWalk = true;
+                else shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
+            }
+        }
+        if (kWalls) {
+            const unsigned m = __ballot_sync(full, toWalk);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(counters + kCntWalk, __popc(m));
+                base = __shfl_sync(full, base, leader);
+                if (toWalk) S.walk[base + __popc(m & ((1u << lane) - 1u))] = q;
+                toWalk = false;
+            }
         }
     }
     if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
@@ -1135,17 +1157,70 @@ __global__ void k_advance(int *counters, unsigned long long *stats) {
     counters[kCntShadow] = 0;
     counters[kCntExtendWork] = 0;
     counters[kCntShadowWork] = 0;
+    counters[kCntWalk] = 0;
 #pragma unroll
     for (int c = 0; c < kClasses; ++c) counters[kCntClass0 + c] = 0;
 }
 
-// Visibility of queued NEE samples in scenes with medium interfaces: a walk through the boundary
-// surfaces with homogeneous transmittance (src/scene/scene.cpp:41-59).
+// Closest hit of a ray on the 4-wide tree within [0, tMax) (one thread, whole traversal).
+template <bool kSpheres>
+__device__ __forceinline__ bool closest4(const DevScene &s, const TraceRay &r, float tMax, Hit *h, bool *overflow) {
+    float te;
+    if (s.root.empty ||
+        !box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4], s.root.box[5], &te) ||
+        !(te < tMax))
+        return false;
+    int stackRef[kStackSize];
+    float stackT[kStackSize];
+    TravState st;
+    st.ref = s.root.ref;
+    st.sp = 0;
+    st.tMax = tMax;
+    st.found = false;
+    st.crossed = false;
+    while (!traverse4_step<false, kSpheres>(s.qnodes, s.leaves, r, st, stackRef, stackT, overflow)) {
+    }
+    if (st.found) *h = st.hit;
+    return st.found;
+}
+
+// Closest medium interface along a ray within [0, tMax): brute force over the scene's short
+// interface list (the leaf slots' own hit arithmetic), else the whole tree.
+template <bool kSpheres>
+__device__ __forceinline__ bool closest_wall(const DevScene &s, const TraceRay &r, float tMax, Hit *h, bool *overflow) {
+    if (s.wallCount < 0) return closest4<kSpheres>(s, r, tMax, h, overflow);
+    bool found = false;
+    for (int i = 0; i < s.wallCount; ++i) {
+        const LeafPrim *p = s.walls + i;
+        float4 v0 = __ldg(&p->v0), v1 = __ldg(&p->v1), v2 = __ldg(&p->v2);
+        float t, u = 0.f, v = 0.f;
+        bool hh;
+        if (kSpheres && __float_as_int(v1.w) == 1)
+            hh = hit_sphere(r, v0, v1, tMax, &t);
+        else
+            hh = hit_triangle(r, v0, v1, v2, tMax, &t, &u, &v);
+        if (hh) {
+            tMax = t;
+            h->t = t;
+            h->u = u;
+            h->v = v;
+            h->prim = __float_as_int(v0.w);
+            found = true;
+        }
+    }
+    return found;
+}
+
+// The queued NEE samples whose segment crosses a medium interface: a walk through the boundary
+// surfaces with each medium's transmittance (src/scene/scene.cpp:41-59). k_shadow_any has
+// already found these segments free of opaque surfaces, so each step needs only the nearest
+// interface.
 template <bool kSpheres, bool kBatch = false>
 __global__ void __launch_bounds__(256) k_shadow_walk(DevScene s0, const DevScene *scenes, Paths P, Shadows S,
-                                                     const int *counters) {
-    int n = counters[kCntShadow];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+                                                     int *counters) {
+    int n = counters[kCntWalk];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int q = S.walk[i];
         float4 o4 = S.o[q], d4 = S.d[q];
         int medium = __float_as_int(o4.w), j = __float_as_int(d4.w);
         const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(P.meta[j].w));
@@ -1153,38 +1228,27 @@ __global__ void __launch_bounds__(256) k_shadow_walk(DevScene s0, const DevScene
         V3 target = o + dd;
         SS T = splat(1.f);
         bool overflow = false;
-        Lambda lam;
-        bool needLam = medium >= 0 || s.hasInterfaces;
-        if (needLam) lam = load_lam(P, j);
-        if (!s.hasInterfaces) {
-            TraceRay r = make_trace_ray(o, dd);
+        Lambda lam = load_lam(P, j);
+        bool blocked = true;
+        for (int it = 0; it < 256; ++it) {
+            V3 d = target - o;
+            TraceRay r = make_trace_ray(o, d);
             Hit h;
-            bool occ = !s.root.empty &&
-                       traverse<true, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
-            if (occ) continue;
-            if (medium >= 0) T = segment_tr(s, medium, lam, o, dd, 1.f);
-        } else {
-            bool blocked = true;
-            for (int it = 0; it < 256; ++it) {
-                V3 d = target - o;
-                TraceRay r = make_trace_ray(o, d);
-                Hit h;
-                h.prim = -1;
-                bool hit = !s.root.empty &&
-                           traverse<false, kSpheres>(s.nodes, s.leaves, s.root.box, s.root.ref, r, 1.f - kShadowEps, &h, &overflow);
-                if (hit && s.mats[s.prims[h.prim].material].type != prgpu::MatInterface) break;
-                if (medium >= 0) T = T * segment_tr(s, medium, lam, o, d, hit ? h.t : 1.f);
-                if (!hit || !nonzero(T)) {
-                    blocked = false;
-                    break;
-                }
-                const prgpu::Primitive &pr = s.prims[h.prim];
-                Surf sf = shade_point(s, pr, h.t, h.u, h.v, o, d);
-                medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
-                o = offset_origin(sf.p, sf.n, d);
+            h.prim = -1;
+            bool hit = closest_wall<kSpheres>(s, r, 1.f - kShadowEps, &h, &overflow);
+            if (hit && !(__ldg(s.primClass + h.prim) & kTransparentBit)) break;
+            if (medium >= 0) T = T * segment_tr(s, medium, lam, o, d, hit ? h.t : 1.f);
+            if (!hit || !nonzero(T)) {
+                blocked = false;
+                break;
             }
-            if (blocked) continue;
+            const prgpu::Primitive &pr = s.prims[h.prim];
+            Surf sf = shade_point(s, pr, h.t, h.u, h.v, o, d);
+            medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
+            o = offset_origin(sf.p, sf.n, d);
         }
+        if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
+        if (blocked) continue;
         SS c = from_f4(S.c[q]) * T;
         float w = S.w[q];
         float4 L = P.L[j], Lh = P.Lhero[j];

@@ -326,7 +326,7 @@ def large_scene_bench(args, device: int):
         r = {"value": w * h * spp / (statistics.mean(dev) * 1e-3), "ms_per_step": statistics.mean(dev),
              "kernel_ms": {"closest": st.traceMs, "shade": st.shadeMs, "shadow": st.shadowMs, "film": st.filmMs},
              "rays_per_step": {"closest": int(st.closestRays), "shadow": int(st.shadowRays)},
-             "bounces_per_sample": st.bounces / max(1, st.pathSamples)}
+             "closest_rays_per_sample": st.closestRays / (w * h * spp)}
         if name == "plain":
             out.update(r)
         else:
