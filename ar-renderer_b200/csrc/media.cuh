@@ -88,11 +88,12 @@ __device__ __forceinline__ void grid_sigma(const DevScene &s, const DevGrid &g, 
 }
 
 // The free-flight process of a grid medium along its clipped medium-space ray mo + md t,
-// t in [t0, t1): a walk over the macro cells the ray crosses (3D DDA), sampling exponential steps
-// at each cell's own rate mu = majorant x sMax and restarting at every cell boundary (the process
-// is memoryless), so empty cells cost one step of the walk and no density lookups. Calls
-// f(t, mu) at each tentative collision; f returns false to stop. Bounded: at most 100,000
-// collisions and mx + my + mz + 3 cells.
+// t in [t0, t1): a walk over the macro cells the ray crosses (3D DDA) with the piecewise-constant
+// rate mu = cell majorant x sMax. Each tentative collision draws a unit-rate exponential optical
+// depth and spends it across the cells (mu x length per cell) until it runs out, so a crossing
+// costs no random numbers and an empty cell no density lookups. Calls f(t, mu) at each tentative
+// collision; f returns false to stop. Bounded: at most 100,000 collisions and mx + my + mz + 3
+// cells.
 template <class F>
 __device__ __forceinline__ void majorant_walk(const DevGrid &g, V3 mo, V3 md, float t0, float t1, float sMax, Pcg &rng,
                                               F &&f) {
@@ -121,17 +122,22 @@ __device__ __forceinline__ void majorant_walk(const DevGrid &g, V3 mo, V3 md, fl
         }
     }
     float t = t0;
+    float tau = -logf(1.f - rng.uniform());  // optical depth left to the next tentative collision
     int collisions = 0;
     for (int cells = 0; cells < M[0] + M[1] + M[2] + 3; ++cells) {
         int a = tNext[0] < tNext[1] ? (tNext[0] < tNext[2] ? 0 : 2) : (tNext[1] < tNext[2] ? 1 : 2);
         float segEnd = fminf(tNext[a], t1);
         float mu = __ldg(g.majorant + (size_t(c[2]) * M[1] + c[1]) * M[0] + c[0]) * sMax;
         if (mu > 0.f) {
-            float inv = 1.f / mu;
             for (;;) {
-                t -= logf(1.f - rng.uniform()) * inv;
-                if (t >= segEnd) break;
+                float tc = t + tau / mu;
+                if (!(tc < segEnd)) {
+                    tau = fmaxf(0.f, tau - mu * fmaxf(0.f, segEnd - t));
+                    break;
+                }
+                t = tc;
                 if (!f(t, mu) || ++collisions >= 100000) return;
+                tau = -logf(1.f - rng.uniform());
             }
         }
         if (!(tNext[a] < t1)) return;
