@@ -2,8 +2,10 @@
 // per-device state behind every other entry point. Layout checks pin the v4 structs to the byte
 // offsets of src/gpu/gpu_api.h so that a reference host can pass its own structs unchanged.
 
+#include <cstring>
 #include <cstddef>
 #include <memory>
+#include <vector>
 
 #include "device.cuh"
 #include "../../include/prgpu_api.h"
@@ -80,6 +82,16 @@ using namespace prb;
 PRGPU_API int prgpu_api_version() { return prgpu::kApiVersion; }
 
 PRGPU_API int prgpu_ext_version() { return prgpu::kExtVersion; }
+
+namespace prb {
+std::vector<float> sheen_albedo_table();
+}
+
+PRGPU_API void prgpu_sheen_albedo_table(float *out) {
+    if (!out) return;
+    std::vector<float> t = prb::sheen_albedo_table();
+    std::memcpy(out, t.data(), t.size() * sizeof(float));
+}
 
 PRGPU_API uint64_t prgpu_launch_count() { return gLaunchCount.load(); }
 

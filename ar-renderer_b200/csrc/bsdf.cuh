@@ -11,6 +11,8 @@ namespace prb {
 
 enum : uint32_t { kFlagReflection = 1, kFlagTransmission = 2, kFlagDiffuse = 4, kFlagGlossy = 8, kFlagSpecular = 16 };
 enum : int { kLobeDiffuse = 0, kLobeConductor = 1, kLobeDielectric = 2, kLobeThin = 3, kLobeNone = 4 };
+// Which scattering kinds a sample or pdf may use (pbrt-v4's BxDFReflTransFlags).
+enum : int { kSampleR = 1, kSampleT = 2, kSampleAll = 3 };
 
 // Trowbridge-Reitz microfacet distribution with the visible-normal sampling of Heitz (2018).
 struct Ggx {
@@ -228,7 +230,7 @@ __device__ __forceinline__ float dielectric_f(const Lobe &l, V3 wo, V3 wi, bool 
     return radiance ? ft / sqr(etap) : ft;
 }
 
-__device__ __forceinline__ float dielectric_pdf(const Lobe &l, V3 wo, V3 wi) {
+__device__ __forceinline__ float dielectric_pdf(const Lobe &l, V3 wo, V3 wi, int mode = kSampleAll) {
     if (l.etaD == 1.f || l.mf.smooth()) return 0.f;
     float co = wo.z, ci = wi.z;
     bool refl = ci * co > 0.f;
@@ -239,6 +241,8 @@ __device__ __forceinline__ float dielectric_pdf(const Lobe &l, V3 wo, V3 wi) {
     wm = face_forward(normalize(wm), mk(0.f, 0.f, 1.f));
     if (dot(wm, wi) * ci < 0.f || dot(wm, wo) * co < 0.f) return 0.f;
     float R = fr_dielectric(dot(wo, wm), l.etaD), T = 1.f - R;
+    if (!(mode & kSampleR)) R = 0.f;
+    if (!(mode & kSampleT)) T = 0.f;
     if (R == 0.f && T == 0.f) return 0.f;
     if (refl) return l.mf.pdf(wo, wm) / (4.f * fabsf(dot(wo, wm))) * R / (R + T);
     float denom = sqr(dot(wi, wm) + dot(wo, wm) / etap);
@@ -254,25 +258,28 @@ __device__ __forceinline__ SS lobe_f(const Lobe &l, V3 wo, V3 wi, bool radiance 
     }
 }
 
-__device__ __forceinline__ float lobe_pdf(const Lobe &l, V3 wo, V3 wi) {
+// mode: the scattering kinds the matching sample may use (kSampleAll in the path tracer; the
+// layered walks restrict interfaces to reflection or transmission).
+__device__ __forceinline__ float lobe_pdf(const Lobe &l, V3 wo, V3 wi, int mode = kSampleAll) {
     switch (l.kind) {
-    case kLobeDiffuse: return same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
+    case kLobeDiffuse: return (mode & kSampleR) && same_hemi(wo, wi) ? fabsf(wi.z) * kInvPi : 0.f;
     case kLobeConductor: {
-        if (!same_hemi(wo, wi) || l.mf.smooth()) return 0.f;
+        if (!(mode & kSampleR) || !same_hemi(wo, wi) || l.mf.smooth()) return 0.f;
         V3 wm = wo + wi;
         if (len2(wm) == 0.f) return 0.f;
         wm = face_forward(normalize(wm), mk(0.f, 0.f, 1.f));
         return l.mf.pdf(wo, wm) / (4.f * fabsf(dot(wo, wm)));
     }
-    case kLobeDielectric: return dielectric_pdf(l, wo, wi);
+    case kLobeDielectric: return dielectric_pdf(l, wo, wi, mode);
     default: return 0.f;
     }
 }
 
 // Importance sampling; false when no direction is produced.
 __device__ __forceinline__ bool lobe_sample(const Lobe &l, V3 wo, float uc, float u0, float u1, BSample *s,
-                                            bool radiance = true) {
+                                            bool radiance = true, int mode = kSampleAll) {
     s->eta = 1.f;
+    if ((l.kind == kLobeDiffuse || l.kind == kLobeConductor) && !(mode & kSampleR)) return false;
     switch (l.kind) {
     case kLobeDiffuse: {
         V3 wi = cosine_hemisphere(u0, u1);
@@ -316,6 +323,8 @@ __device__ __forceinline__ bool lobe_sample(const Lobe &l, V3 wo, float uc, floa
             R += sqr(T) * R / (1.f - sqr(R));
             T = 1.f - R;
         }
+        if (!(mode & kSampleR)) R = 0.f;
+        if (!(mode & kSampleT)) T = 0.f;
         if (R == 0.f && T == 0.f) return false;
         if (uc < R / (R + T)) {
             V3 wi = mk(-wo.x, -wo.y, wo.z);
@@ -335,6 +344,8 @@ __device__ __forceinline__ bool lobe_sample(const Lobe &l, V3 wo, float uc, floa
     case kLobeDielectric: {
         if (l.etaD == 1.f || l.mf.smooth()) {
             float R = fr_dielectric(wo.z, l.etaD), T = 1.f - R;
+            if (!(mode & kSampleR)) R = 0.f;
+            if (!(mode & kSampleT)) T = 0.f;
             if (R == 0.f && T == 0.f) return false;
             if (uc < R / (R + T)) {
                 V3 wi = mk(-wo.x, -wo.y, wo.z);
@@ -357,6 +368,8 @@ __device__ __forceinline__ bool lobe_sample(const Lobe &l, V3 wo, float uc, floa
         }
         V3 wm = l.mf.sample_wm(wo, u0, u1);
         float R = fr_dielectric(dot(wo, wm), l.etaD), T = 1.f - R;
+        if (!(mode & kSampleR)) R = 0.f;
+        if (!(mode & kSampleT)) T = 0.f;
         if (R == 0.f && T == 0.f) return false;
         if (uc < R / (R + T)) {
             V3 wi = -wo + wm * (2.f * dot(wo, wm));

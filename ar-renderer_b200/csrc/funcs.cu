@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "bsdf.cuh"
+#include "layered.cuh"
 #include "device.cuh"
 #include "lights.cuh"
 
@@ -34,6 +35,32 @@ __global__ void k_eval_bxdf(int kind, Lobe lobe, bool radiance, int64_t n, const
             y[13] = s.wi.z;
             y[14] = float(s.flags);
             y[15] = s.eta;
+        }
+    }
+}
+
+// The coated / sheen BSDF on local-frame inputs (same in / out layout as k_eval_bxdf; out[15] is
+// 1 when the sampled pdf is only proportional).
+__global__ void k_eval_full(FullBsdf b, int64_t n, const float *__restrict__ in, float *__restrict__ out) {
+    for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+        const float *x = in + 9 * j;
+        float *y = out + 16 * j;
+        V3 wo = mk(x[0], x[1], x[2]), wi = mk(x[3], x[4], x[5]);
+        SS f = full_f(b, wo, wi);
+        for (int i = 0; i < 4; ++i) y[i] = f.v[i];
+        y[4] = full_pdf(b, wo, wi);
+        for (int i = 5; i < 16; ++i) y[i] = 0.f;
+        BSample s;
+        bool proportional = false;
+        if (full_sample(b, wo, x[6], x[7], x[8], &s, &proportional)) {
+            y[5] = 1.f;
+            for (int i = 0; i < 4; ++i) y[6 + i] = s.f.v[i];
+            y[10] = s.pdf;
+            y[11] = s.wi.x;
+            y[12] = s.wi.y;
+            y[13] = s.wi.z;
+            y[14] = float(s.flags);
+            y[15] = proportional ? 1.f : 0.f;
         }
     }
 }
@@ -171,6 +198,76 @@ PRGPU_API int prgpu_eval_bxdf(int deviceIndex, int kind, const float *params, in
     return run_eval(deviceIndex, n, 9, 16, in, out, err, errLen, [&](int g, cudaStream_t s, const float *i, float *o) {
         k_eval_bxdf<<<g, 256, 0, s>>>(kind, l, radiance, n, i, o);
     });
+}
+
+PRGPU_API int prgpu_eval_full_bsdf(int deviceIndex, const float *params, const float *sheenTable, int64_t n,
+                                   const float *in, float *out, char *err, int errLen) {
+    if (!params || params[1] < 0.f || params[1] > 2.f || (params[0] != 0.f && params[1] > 1.f) ||
+        params[25] < 0.f || params[25] > 4096.f || params[26] < 0.f || params[26] > 4096.f ||
+        (params[27] > 0.f && !sheenTable)) {
+        set_err(err, errLen, "bad coated / sheen BSDF parameters");
+        return 1;
+    }
+    auto ss = [&](int o) {
+        SS v;
+        for (int i = 0; i < 4; ++i) v.v[i] = params[o + i];
+        return v;
+    };
+    auto ggx = [](float ax, float ay) {
+        Ggx g{ax, ay};
+        if (!(std::max(ax, ay) < 1e-3f)) {
+            g.ax = std::max(ax, 1e-4f);
+            g.ay = std::max(ay, 1e-4f);
+        }
+        return g;
+    };
+    const int kind = int(params[1]);
+    Lobe base;
+    base.kind = kind == 0 ? kLobeDiffuse : kind == 1 ? kLobeConductor : kLobeDielectric;
+    base.R = ss(2);
+    base.eta = ss(6);
+    base.k = ss(10);
+    base.etaD = params[14];
+    base.mf = ggx(params[15], params[16]);
+    FullBsdf b;
+    b.black = false;
+    b.layered = params[0] != 0.f;
+    b.sheen = params[27] > 0.f;
+    b.base = base;
+    if (b.layered) {
+        b.lay.top.kind = kLobeDielectric;
+        b.lay.top.etaD = params[17];
+        b.lay.top.mf = ggx(params[18], params[18]);
+        b.lay.bottom = base;
+        b.lay.thickness = std::max(params[19], 1.17549435e-38f);
+        b.lay.g = params[20];
+        b.lay.albedo = ss(21);
+        b.lay.hasAlbedo = false;
+        for (int i = 0; i < 4; ++i) b.lay.hasAlbedo = b.lay.hasAlbedo || b.lay.albedo.v[i] != 0.f;
+        b.lay.maxDepth = int(params[25]);
+        b.lay.nSamples = std::max(1, int(params[26]));
+    }
+    float *table = nullptr;
+    if (b.sheen) {
+        for (int i = 0; i < 4; ++i) b.sh.color.v[i] = std::max(0.f, params[29 + i]);
+        b.sh.alpha = std::min(1.f, std::max(0.05f, params[28]));
+        b.sh.weight = std::min(1.f, std::max(0.f, params[27]));
+        float cmax = std::max(std::max(b.sh.color.v[0], b.sh.color.v[1]), std::max(b.sh.color.v[2], b.sh.color.v[3]));
+        b.sh.colorMax = std::min(1.f, std::max(0.f, cmax));
+        if (cudaMalloc(&table, sizeof(float) * kSheenAlphaBins * kSheenMuBins) != cudaSuccess ||
+            cudaMemcpy(table, sheenTable, sizeof(float) * kSheenAlphaBins * kSheenMuBins, cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+            if (table) cudaFree(table);
+            set_err(err, errLen, "sheen table upload failed");
+            return 1;
+        }
+        b.sh.table = table;
+    }
+    int rc = run_eval(deviceIndex, n, 9, 16, in, out, err, errLen, [&](int g, cudaStream_t s, const float *i, float *o) {
+        k_eval_full<<<g, 256, 0, s>>>(b, n, i, o);
+    });
+    if (table) cudaFree(table);
+    return rc;
 }
 
 PRGPU_API int prgpu_eval_phase(int deviceIndex, int64_t n, const float *in, float *out, char *err, int errLen) {

@@ -116,8 +116,15 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
     for (int32_t i = 0; i < sd->materialCount; ++i) {
         const prgpu::Material &m = sd->materials[i];
         if (m.type > prgpu::MatCoatedConductor) return fail("unknown material type");
-        if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor || m.sheenWeight > 0)
-            return fail("coated and sheen materials are not supported by this module yet");
+        if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor) {
+            if (!spec_ok(m.coatEta, ns) || (m.coatAlbedo >= 0 && !spec_ok(m.coatAlbedo, ns)))
+                return fail("coat spectrum index out of range");
+            if (m.coatMaxDepth < 0 || m.coatMaxDepth > 4096 || m.coatSamples < 0 || m.coatSamples > 4096)
+                return fail("coat walk depth / sample count out of range [0, 4096]");
+            if (!(m.thickness >= 0.f) || !std::isfinite(m.thickness)) return fail("bad coat thickness");
+        }
+        if (m.sheenWeight > 0 && m.sheenColor >= 0 && !spec_ok(m.sheenColor, ns))
+            return fail("sheen spectrum index out of range");
         if (!spec_ok(m.albedo, ns) || !spec_ok(m.albedoB, ns) || !spec_ok(m.eta, ns) || !spec_ok(m.k, ns))
             return fail("material spectrum index out of range");
     }
@@ -166,6 +173,53 @@ float texel_value(const float *t, float l) {
     float s = std::isinf(x) ? (x > 0.f ? 1.f : 0.f) : 0.5f + x / (2.f * std::sqrt(1.f + x * x));
     return t[3] * s;
 }
+
+} // namespace
+
+// The sheen lobe's directional albedo on [16 roughness] x [32 cos theta] nodes, for a host that
+// passes no table: the reference's SheenBxDF::Albedo integration (bxdf.cpp:538-560) restated --
+// 32 x 32 stratified cosine-weighted directions (concentric disk), f cos / pdf averaged in double.
+std::vector<float> sheen_albedo_table() {
+    const int nMu = prgpu::kSheenMu, nAlpha = prgpu::kSheenAlpha, nS = 32;
+    std::vector<float> t(size_t(nMu) * nAlpha);
+    const float pi = 3.14159265358979f;
+    for (int ia = 0; ia < nAlpha; ++ia) {
+        const float a = (1.f - float(ia) / (nAlpha - 1)) * 0.05f + float(ia) / (nAlpha - 1) * 1.f;
+        for (int im = 0; im < nMu; ++im) {
+            const float mu = std::max(1e-3f, float(im) / (nMu - 1));
+            const float wo[3] = {std::sqrt(std::max(0.f, 1 - mu * mu)), 0.f, mu};
+            double sum = 0;
+            for (int i = 0; i < nS; ++i)
+                for (int j = 0; j < nS; ++j) {
+                    float ox = 2.f * ((i + 0.5f) / nS) - 1.f, oy = 2.f * ((j + 0.5f) / nS) - 1.f, x = 0.f, y = 0.f;
+                    if (ox != 0.f || oy != 0.f) {
+                        float r, th;
+                        if (std::fabs(ox) > std::fabs(oy)) {
+                            r = ox;
+                            th = pi / 4 * (oy / ox);
+                        } else {
+                            r = oy;
+                            th = pi / 2 - pi / 4 * (ox / oy);
+                        }
+                        x = r * std::cos(th);
+                        y = r * std::sin(th);
+                    }
+                    const float wi[3] = {x, y, std::sqrt(std::max(0.f, 1 - x * x - y * y))};
+                    const float co = std::fabs(wo[2]), ci = std::fabs(wi[2]);
+                    if (co == 0.f || ci == 0.f) continue;
+                    float h[3] = {wo[0] + wi[0], wo[1] + wi[1], wo[2] + wi[2]};
+                    const float hl = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+                    const float hz = h[2] / hl, inv = 1.f / a, sin2 = std::max(0.f, 1 - hz * hz);
+                    const float D = (2 + inv) * std::pow(sin2, 0.5f * inv) / (2 * pi);
+                    sum += D / (4 * (ci + co - ci * co)) * pi;
+                }
+            t[size_t(ia) * nMu + im] = float(sum / (nS * nS));
+        }
+    }
+    return t;
+}
+
+namespace {
 
 // Macro cells per axis of a grid's majorant table: one per 8 voxels, at most 32.
 static int macro_cells(int n) { return std::max(1, std::min(32, (n + 7) / 8)); }
@@ -312,6 +366,8 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
                                      : t == prgpu::MatConductor  ? kClassConductor
                                      : t == prgpu::MatDielectric ? kClassDielectric
                                                                  : kClassOther);
+            const prgpu::Material &mi = sd->materials[sd->prims[i].material];
+            if (mi.sheenWeight > 0 && mi.sheenColor >= 0) cls[size_t(i)] = uint8_t(kClassOther);
             if (t == prgpu::MatInterface) cls[size_t(i)] |= kTransparentBit;
         }
         put(cache.primClass, cls.data(), cls.size(), s);
@@ -323,6 +379,15 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         }
         cache.wallCount = walls.size() <= size_t(kMaxWallList) ? int(walls.size()) : -1;
         if (cache.wallCount > 0) put(cache.walls, walls.data(), walls.size(), s);
+        cache.hasSheen = false;
+        for (int32_t i = 0; i < sd->materialCount; ++i)
+            if (sd->materials[i].sheenWeight > 0 && sd->materials[i].sheenColor >= 0) cache.hasSheen = true;
+        if (cache.hasSheen) {
+            std::vector<float> table = sd->sheenAlbedo
+                                           ? std::vector<float>(sd->sheenAlbedo, sd->sheenAlbedo + prgpu::kSheenAlpha * prgpu::kSheenMu)
+                                           : sheen_albedo_table();
+            put(cache.sheen, table.data(), table.size(), s);
+        }
         put(cache.mats, sd->materials, size_t(sd->materialCount), s);
         put(cache.lights, sd->lights, size_t(sd->lightCount), s);
         put(cache.spectra, sd->spectra, size_t(sd->spectrumCount), s);
@@ -391,6 +456,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         d.root = cache.accel.root;
         d.prims = cache.prims.as<prgpu::Primitive>();
         d.primClass = cache.primClass.as<uint8_t>();
+        d.sheenTable = cache.hasSheen ? cache.sheen.as<float>() : nullptr;
         d.walls = cache.wallCount > 0 ? cache.walls.as<LeafPrim>() : nullptr;
         d.wallCount = cache.wallCount;
         d.mats = cache.mats.as<prgpu::Material>();

@@ -90,6 +90,7 @@ struct DevScene {
     // (brute force over at most kMaxWallList); wallCount < 0: too many, the walk uses the tree.
     const LeafPrim *walls;
     int wallCount;
+    const float *sheenTable;  // sheen directional albedo [16 alpha][32 mu], null without sheen
     uint32_t filterType;
     float filterRadius, filterSigma, filterNorm;
     const float *filterCdf;  // kFilterBins + 1
@@ -115,10 +116,11 @@ struct SceneCache {
     bool valid = false;
     DeviceAccel accel;
     DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
-        envDist, walls;
+        envDist, walls, sheen;
     DevScene ds{};
     bool hasSpheres = false;
     int wallCount = 0;
+    bool hasSheen = false;
     int64_t deviceBytes = 0;
     void release() {
         accel.release();
@@ -136,9 +138,13 @@ struct SceneCache {
         envTexels.release();
         envDist.release();
         walls.release();
+        sheen.release();
         valid = false;
     }
 };
+
+// The sheen directional-albedo table a host passes in SceneDesc::sheenAlbedo, computed on the host.
+std::vector<float> sheen_albedo_table();
 
 // Validates sd (and ext) and makes the cache hold it on the device. Throws CudaError on device
 // failure; returns false with a message on invalid input.

@@ -26,6 +26,7 @@
 
 #include "bsdf.cuh"
 #include "guide.cuh"
+#include "layered.cuh"
 #include "lights.cuh"
 #include "media.cuh"
 #include "scene.cuh"
@@ -238,6 +239,76 @@ __device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, 
     default: break;
     }
     return l;
+}
+
+// True for the materials shaded through FullBsdf: coats and anything with a sheen lobe.
+__device__ __forceinline__ bool full_material(const prgpu::Material &m) {
+    return m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor ||
+           (m.sheenWeight > 0.f && m.sheenColor >= 0);
+}
+
+// Builds the coated / sheen BSDF of material m (the reference's CoatedDiffuseMaterial,
+// CoatedConductorMaterial and Material::GetBSDF sheen wrapper, material.cpp:5-14, 117-166); may
+// terminate the secondary wavelengths (dispersive coat).
+__device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam,
+                                       FullBsdf *b) {
+    b->layered = b->sheen = b->black = false;
+    if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor) {
+        float coatEta = tab(s.spectra, m.coatEta, lam.l[0]);
+        if (m.coatDispersive) lam.terminate_secondary();
+        if (coatEta == 0.f) coatEta = 1.f;
+        Layered &L = b->lay;
+        b->layered = true;
+        L.top.kind = kLobeDielectric;
+        L.top.etaD = coatEta;
+        L.top.mf = make_ggx(m.coatAlpha, m.coatAlpha);
+        L.thickness = fmaxf(m.thickness, 1.17549435e-38f);
+        L.g = m.coatG;
+        L.albedo = splat(0.f);
+        if (m.coatAlbedo >= 0) {
+            L.albedo = tab4(s.spectra, m.coatAlbedo, lam);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) L.albedo.v[i] = fmaxf(0.f, L.albedo.v[i]);
+        }
+        L.hasAlbedo = nonzero(L.albedo);
+        L.maxDepth = m.coatMaxDepth;
+        L.nSamples = max(1, m.coatSamples);
+        if (m.type == prgpu::MatCoatedDiffuse) {
+            L.bottom.kind = kLobeDiffuse;
+            L.bottom.R = diffuse_albedo(s, m, u, v, lam);
+        } else {
+            // The conductor sits under the coat: its n, k are relative to the coat's IOR.
+            L.bottom.kind = kLobeConductor;
+            L.bottom.etaD = 1.f;
+            L.bottom.mf = make_ggx(m.alphaX, m.alphaY);
+            if (m.eta >= 0) {
+                L.bottom.eta = tab4(s.spectra, m.eta, lam) * (1.f / coatEta);
+                L.bottom.k = tab4(s.spectra, m.k, lam) * (1.f / coatEta);
+            } else {
+                SS r = tab4(s.spectra, m.albedo, lam);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    float ri = clampf(r.v[i], 0.f, 0.9999f);
+                    L.bottom.eta.v[i] = 1.f;
+                    L.bottom.k.v[i] = 2.f * sqrtf(ri) / safe_sqrt(1.f - ri);
+                }
+            }
+        }
+    } else {
+        b->base = make_lobe(s, m, u, v, lam);
+        b->black = b->base.kind == kLobeNone;
+    }
+    if (!b->black && m.sheenWeight > 0.f && m.sheenColor >= 0 && s.sheenTable) {
+        Sheen &sh = b->sh;
+        b->sheen = true;
+        sh.color = tab4(s.spectra, m.sheenColor, lam);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) sh.color.v[i] = fmaxf(0.f, sh.color.v[i]);
+        sh.alpha = clampf(m.sheenRoughness, 0.05f, 1.f);
+        sh.weight = clampf(m.sheenWeight, 0.f, 1.f);
+        sh.colorMax = clampf(max_c(sh.color), 0.f, 1.f);
+        sh.table = s.sheenTable;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -755,7 +826,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         // The shadow ray starts in the medium on the light's side of the vertex (medIn / medOut
         // for surfaces, the current medium for medium vertices where ng = 0).
         auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut,
-                       const GuideMix *gmix) {
+                       const GuideMix *gmix, const FullBsdf *full = nullptr) {
             float ul = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
             LightSample ls = sample_light(s, p, ng, lam, ul, u0, u1);
             if (!ls.ok) return;
@@ -772,6 +843,11 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     if (gmix)
                         spdf = gmix->c * guide_pdf_folded(*gmix, ls.wi, ns, dot(wo, ns) > 0.f ? 1.f : -1.f) +
                                (1.f - gmix->c) * spdf;
+            } else if (full) {
+                V3 wol = fr->to_local(wo), wil = fr->to_local(ls.wi);
+                if (wol.z == 0.f) return;
+                f = full_f(*full, wol, wil) * fabsf(dot(ls.wi, ns));
+                spdf = full_pdf(*full, wol, wil);
             } else {
                 float ph = hg_phase(dot(wo, ls.wi), g);
                 f = splat(ph);
@@ -930,53 +1006,71 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 alive = false;
             } else {
                 ++depth;
-                Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
                 Frame fr = frame_from_xz(sf.dpdu, sf.ns);
                 V3 wo = -d;
                 V3 wol = fr.to_local(wo);
                 BSample bs;
                 bool ok;
+                float misPdf;  // the BSDF density for MIS against later light hits
+                // Coats and sheen shade through FullBsdf (stochastic layered walks, out of line); a
+                // proportional sampling pdf takes the estimated density for MIS (path.cpp:219).
+                const bool isFull = full_material(m);
+                FullBsdf fb;
+                Lobe lobe;
+                if (isFull)
+                    make_full(s, m, sf.u, sf.v, lam, &fb);
+                else
+                    lobe = make_lobe(s, m, sf.u, sf.v, lam);
+                GuideMix gm;
+                bool guided = false, inRange = false;
+                int recIndex = 0;
                 if constexpr (kGuide) {
-                    GuideMix gm;
                     // The guide is trained on, and applied at, the first kGuideVertices diffuse
                     // vertices of each path.
-                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse;
-                    const bool inRange = diffuseVertex && gcount < kGuideVertices;
-                    const bool guided = (a.guideMode & 1) && inRange;
-                    const int recIndex = gcount;
+                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse && !isFull;
+                    inRange = diffuseVertex && gcount < kGuideVertices;
+                    guided = (a.guideMode & 1) && inRange;
+                    recIndex = gcount;
                     if (inRange) ++gcount;
                     if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut);
-                    if (lobe.non_specular())
-                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
-                            guided ? &gm : nullptr);
-                    float pbGuide = 0.f;
-                    if (guided) {
-                        // One-sample MIS of the guide and the BSDF: wi ~ c q + (1 - c) p_bsdf.
-                        float us = rng.uniform(), uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                        V3 wiw;
-                        ok = wol.z != 0.f;
-                        const float side = dot(wo, sf.ns) > 0.f ? 1.f : -1.f;
-                        if (us < gm.c) {
-                            wiw = guide_sample(gm, uc, u0, u1);
-                            if (dot(wiw, sf.ns) * side < 0.f) wiw = guide_mirror(wiw, sf.ns);
-                        } else {
-                            BSample b2;
-                            ok = ok && lobe_sample(lobe, wol, uc, u0, u1, &b2);
-                            wiw = fr.from_local(b2.wi);
-                        }
-                        V3 wil = fr.to_local(wiw);
-                        pbGuide = lobe_pdf(lobe, wol, wil);
-                        bs.f = lobe_f(lobe, wol, wil);
-                        bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
-                        bs.wi = wil;
-                        bs.flags = kFlagReflection | kFlagDiffuse;
-                        bs.eta = 1.f;
+                }
+                if (isFull ? full_non_specular(fb) : lobe.non_specular())
+                    nee(sf.p, sf.n, isFull ? nullptr : &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
+                        guided ? &gm : nullptr, isFull ? &fb : nullptr);
+                float pbGuide = 0.f;
+                bool proportional = false;
+                if (isFull) {
+                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &proportional);
+                } else if (guided) {
+                    // One-sample MIS of the guide and the BSDF: wi ~ c q + (1 - c) p_bsdf.
+                    float us = rng.uniform(), uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    V3 wiw;
+                    ok = wol.z != 0.f;
+                    const float side = dot(wo, sf.ns) > 0.f ? 1.f : -1.f;
+                    if (us < gm.c) {
+                        wiw = guide_sample(gm, uc, u0, u1);
+                        if (dot(wiw, sf.ns) * side < 0.f) wiw = guide_mirror(wiw, sf.ns);
                     } else {
-                        float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                        ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                        BSample b2;
+                        ok = ok && lobe_sample(lobe, wol, uc, u0, u1, &b2);
+                        wiw = fr.from_local(b2.wi);
                     }
-                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
-                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                    V3 wil = fr.to_local(wiw);
+                    pbGuide = lobe_pdf(lobe, wol, wil);
+                    bs.f = lobe_f(lobe, wol, wil);
+                    bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
+                    bs.wi = wil;
+                    bs.flags = kFlagReflection | kFlagDiffuse;
+                    bs.eta = 1.f;
+                } else {
+                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                }
+                ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                     isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
+                if constexpr (kGuide) {
                     float4 *rec = a.guideRec + 4 * (size_t(j) * kGuideVertices + recIndex);
                     if (ok && (a.guideMode & 2) && inRange) {
                         // First diffuse vertex of the path: record (x, n, wo, wi, p_bsdf, mean beta).
@@ -992,20 +1086,13 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                         rec[2] = make_float4(wo.x, wo.y, wo.z, 0.f);
                         rec[3] = make_float4(wiw.x, wiw.y, wiw.z, __int_as_float(1));
                     }
-                } else {
-                    if (lobe.non_specular())
-                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr);
-                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                    ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
-                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
-                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
                 }
                 if (!ok) {
                     alive = false;
                 } else {
                     V3 wi = fr.from_local(bs.wi);
                     beta = beta * bs.f * (fabsf(dot(wi, sf.ns)) / bs.pdf);
-                    prevPdf = bs.pdf;
+                    prevPdf = misPdf;
                     specular = (bs.flags & kFlagSpecular) != 0u;
                     if (bs.flags & kFlagTransmission) etaScale *= sqr(bs.eta);
                     prevP = sf.p;

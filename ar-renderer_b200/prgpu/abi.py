@@ -209,6 +209,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_accel_bytes", [_P], C.c_int64)
         _bind(lib, "prgpu_accel_destroy", [_P], None)
         _bind(lib, "prgpu_eval_bxdf", [C.c_int, C.c_int, _P, C.c_int64, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_eval_full_bsdf", [C.c_int, _P, _P, C.c_int64, _P, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_sheen_albedo_table", [_P], None)
         _bind(lib, "prgpu_eval_phase", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_homogeneous", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_light_bvh", [C.c_int, _P, C.c_int32, C.c_int32, C.c_float, C.c_int64, _P, _P, _P,

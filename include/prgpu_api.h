@@ -317,6 +317,12 @@ struct RenderStats {
 // Returns prgpu::kApiVersion (4). Replaces prgpu_api_version, gpu_api.h:173.
 PRGPU_API int prgpu_api_version();
 
+// Fills out[kSheenAlpha * kSheenMu] with the sheen lobe's directional albedo at the table nodes
+// ([roughness 0.05..1][cos theta 0..1]), computed on the host as the reference's
+// SheenBxDF::Albedo does (src/materials/bxdf.cpp:538-560): the table a host may pass in
+// SceneDesc::sheenAlbedo. A scene with sheen and a null table gets this one. No device work.
+PRGPU_API void prgpu_sheen_albedo_table(float *out);
+
 // Writes up to max CUDA devices; returns the number written. Replaces prgpu_list_devices,
 // gpu_api.h:166-167 (backend reads "cuda").
 PRGPU_API int prgpu_list_devices(prgpu::DeviceInfo *out, int max);
@@ -433,6 +439,15 @@ PRGPU_API uint64_t prgpu_launch_count();
 //   out 16 floats per item: f[4], pdf, sampled (0/1), sample f[4], pdf, wi[3], flags, eta.
 PRGPU_API int prgpu_eval_bxdf(int deviceIndex, int kind, const float *params, int64_t n, const float *in, float *out,
                               char *err, int errLen);
+// Coated and sheen BSDFs on identical local-frame inputs (pr::LayeredBxDF over a diffuse or
+// conductor base, src/materials/bxdf.cpp:260-518, and pr::SheenBxDF over it or over a single lobe,
+// bxdf.cpp:520-631). params (36 floats): layered, base kind (0 diffuse, 1 conductor, 2 dielectric),
+// R[4], eta[4], k[4], etaD, alphaX, alphaY, coat eta, coat alpha, thickness, g, albedo[4],
+// maxDepth, nSamples, sheen weight, sheen roughness, sheen colour[4], 2 unused; sheenTable: the
+// [16 roughness][32 cos theta] sheen albedo table (needed when the sheen weight is > 0). in / out
+// as prgpu_eval_bxdf, with out[15] = 1 when the sampled pdf is only proportional.
+PRGPU_API int prgpu_eval_full_bsdf(int deviceIndex, const float *params, const float *sheenTable, int64_t n,
+                                   const float *in, float *out, char *err, int errLen);
 // Henyey-Greenstein (src/materials/bxdf.cpp:64-80): in 7 floats (cosTheta, g, wo[3], u0, u1);
 // out 5 floats (phase value, sampled wi[3], its pdf).
 PRGPU_API int prgpu_eval_phase(int deviceIndex, int64_t n, const float *in, float *out, char *err, int errLen);

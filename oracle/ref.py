@@ -45,6 +45,8 @@ def ref_lib() -> C.CDLL:
         lib.prref_soup_trace.argtypes = [_P, _P, C.c_int64, C.c_int, _P, _P, _P, _P]
         lib.prref_soup_trace.restype = C.c_double
         lib.prref_bxdf.argtypes = [C.c_int, _P, C.c_int64, _P, _P]
+        lib.prref_full_bsdf.argtypes = [_P, C.c_int64, _P, _P]
+        lib.prref_sheen_table.argtypes = [_P]
         lib.prref_fr_dielectric.argtypes = [C.c_float, C.c_float]
         lib.prref_fr_dielectric.restype = C.c_float
         lib.prref_fr_complex.argtypes = [C.c_float, C.c_float, C.c_float]

@@ -193,6 +193,63 @@ API void prref_bxdf(int kind, const float *params, int64_t n, const float *in, f
     }
 }
 
+// Coated / sheen BxDFs on identical local-frame inputs: pr::LayeredBxDF (dielectric coat over a
+// diffuse or conductor base, two-sided) and pr::SheenBxDF over it or over a single lobe.
+// params (36 floats): layered, base kind (0 diffuse, 1 conductor, 2 dielectric), R[4], eta[4],
+//   k[4], etaD, alphaX, alphaY, coat eta, coat alpha, thickness, g, albedo[4], maxDepth,
+//   nSamples, sheen weight, sheen roughness, sheen colour[4], 2 unused
+// in (9 floats): wo[3], wi[3], uc, u0, u1
+// out (16 floats): f[4], pdf, sample: ok, f[4], pdf, wi[3], flags, pdf-is-proportional
+API void prref_full_bsdf(const float *params, int64_t n, const float *in, float *out) {
+    auto ss = [&](int o) {
+        SampledSpectrum v;
+        for (int i = 0; i < 4; ++i) v[i] = params[o + i];
+        return v;
+    };
+    const bool layered = params[0] != 0;
+    const int kind = int(params[1]);
+    TrowbridgeReitzDistribution baseMf(params[15], params[16]);
+    DiffuseBxDF diffuse(ss(2));
+    ConductorBxDF conductor(baseMf, ss(6), ss(10));
+    DielectricBxDF dielectric(params[14], baseMf);
+    const BxDF *base = kind == 0 ? static_cast<const BxDF *>(&diffuse)
+                       : kind == 1 ? static_cast<const BxDF *>(&conductor)
+                                   : static_cast<const BxDF *>(&dielectric);
+    DielectricBxDF coat(params[17], TrowbridgeReitzDistribution(params[18], params[18]));
+    LayeredBxDF lay(&coat, base, params[19], ss(21), params[20], true, int(params[25]), int(params[26]));
+    const BxDF *b = layered ? static_cast<const BxDF *>(&lay) : base;
+    SheenBxDF sheen(b, ss(29), params[28], params[27]);
+    if (params[27] > 0) b = &sheen;
+    for (int64_t j = 0; j < n; ++j) {
+        const float *x = in + 9 * j;
+        float *y = out + 16 * j;
+        Vec3f wo(x[0], x[1], x[2]), wi(x[3], x[4], x[5]);
+        SampledSpectrum f = b->f(wo, wi, TransportMode::Radiance);
+        for (int i = 0; i < 4; ++i) y[i] = f[i];
+        y[4] = b->PDF(wo, wi, TransportMode::Radiance, BxDFReflTransFlags::All);
+        auto bs = b->Sample_f(wo, x[6], Vec2f(x[7], x[8]), TransportMode::Radiance, BxDFReflTransFlags::All);
+        std::memset(y + 5, 0, 11 * sizeof(float));
+        if (bs) {
+            y[5] = 1;
+            for (int i = 0; i < 4; ++i) y[6 + i] = bs->f[i];
+            y[10] = bs->pdf;
+            y[11] = bs->wi.x;
+            y[12] = bs->wi.y;
+            y[13] = bs->wi.z;
+            y[14] = float(uint32_t(bs->flags));
+            y[15] = bs->pdfIsProportional ? 1.f : 0.f;
+        }
+    }
+}
+
+// The sheen lobe's directional albedo at the table nodes ([16 roughness][32 cos theta]).
+API void prref_sheen_table(float *out) {
+    for (int ia = 0; ia < prgpu::kSheenAlpha; ++ia)
+        for (int im = 0; im < prgpu::kSheenMu; ++im)
+            out[ia * prgpu::kSheenMu + im] =
+                SheenBxDF::Albedo(float(im) / (prgpu::kSheenMu - 1), 0.05f + 0.95f * float(ia) / (prgpu::kSheenAlpha - 1));
+}
+
 // Scalar Fresnel terms (known-answer tests): FrDielectric and FrComplex (per wavelength).
 API float prref_fr_dielectric(float cosI, float eta) { return FrDielectric(cosI, eta); }
 API float prref_fr_complex(float cosI, float eta, float k) {
@@ -398,6 +455,22 @@ struct SceneHandle {
             m->albedo = SpecTex(p.reflectance, &m->albedoB, &m->checkerScale);
         }
     }
+    // Coat parameters of CoatedDiffuse / CoatedConductor materials (material.h:129-136).
+    void Coat(const CoatParams &c, prgpu::Material *m) {
+        m->coatEta = Spec(c.eta);
+        m->coatDispersive = c.eta->IsConstant() ? 0 : 1;
+        m->coatAlpha = TrowbridgeReitzDistribution::RoughnessToAlpha(FloatTex(c.roughness, 0.f));
+        m->thickness = FloatTex(c.thickness, 0.01f);
+        m->coatAlbedo = -1;
+        if (c.albedo) {
+            int d;
+            float sc;
+            m->coatAlbedo = SpecTex(c.albedo, &d, &sc);
+        }
+        m->coatG = c.g;
+        m->coatMaxDepth = c.maxDepth;
+        m->coatSamples = c.nSamples;
+    }
     int MediumIndex(const pr::Medium *md) {
         if (!md) return -1;
         auto it = medCache.find(md);
@@ -451,10 +524,25 @@ struct SceneHandle {
             float ur = FloatTex(g->URoughness(), 0.f), vr = g->VRoughness() ? FloatTex(g->VRoughness(), ur) : ur;
             m.alphaX = TrowbridgeReitzDistribution::RoughnessToAlpha(ur);
             m.alphaY = TrowbridgeReitzDistribution::RoughnessToAlpha(vr);
+        } else if (auto *cd = dynamic_cast<const CoatedDiffuseMaterial *>(mat)) {
+            m.albedo = SpecTex(cd->Reflectance(), &m.albedoB, &m.checkerScale);
+            Coat(cd->Coat(), &m);
+            m.type = prgpu::MatCoatedDiffuse;
+        } else if (auto *cc = dynamic_cast<const CoatedConductorMaterial *>(mat)) {
+            Conductor(cc->Conductor(), &m);
+            Coat(cc->Coat(), &m);
+            m.type = prgpu::MatCoatedConductor;
         } else {
             Warn("unsupported material exported as grey diffuse");
             m.type = prgpu::MatDiffuse;
             m.albedo = Spec(ConstantSpectrum(0.5f));
+        }
+        if (mat && mat->HasSheen() && mat->Sheen().color) {
+            int d;
+            float sc;
+            m.sheenColor = SpecTex(mat->Sheen().color, &d, &sc);
+            m.sheenRoughness = FloatTex(mat->Sheen().roughness, 0.3f);
+            m.sheenWeight = mat->Sheen().weight;
         }
         materials.push_back(m);
         int id = int(materials.size() - 1);
