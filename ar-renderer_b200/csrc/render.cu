@@ -250,9 +250,13 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
                     ShadeArgs sa{scene,       nullptr, rs.P, rs.S, cq, rs.capacity, qout, cnt, rp.maxDepth, 0,
-                                 rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode};
+                                 rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin};
                     if (guideMode) k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
                     else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
+                    if (scene.hasFull) {
+                        k_shade<false, false, true><<<gShade, 256, 0, st>>>(sa);
+                        ++launches;
+                    }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
                     shadowAny<<<gShadow, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                     if (scene.hasInterfaces) {
@@ -647,7 +651,7 @@ struct BatchLaunch {
     void (*extend)(DevScene, const DevScene *, Paths, int *, const int *);
     void (*shadowAny)(DevScene, const DevScene *, Paths, Shadows, int *);
     void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, int *);
-    bool walls;
+    bool walls, full;
     int gExtend, gShadow, gShade, gWide, shadeBlock, capacity;
 };
 
@@ -655,6 +659,7 @@ BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
     const bool sph = key.variant & 1, media = key.variant & 2;
     BatchLaunch L{};
     L.walls = key.variant & 4;
+    L.full = key.variant & 8;
     L.extend = sph ? k_extend<true, true> : k_extend<false, true>;
     L.shadowAny = L.walls ? (sph ? k_shadow_any<true, true, true, true> : k_shadow_any<false, true, true, true>)
                   : sph   ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
@@ -693,8 +698,12 @@ int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &
     for (int b = 0; b < 2; ++b) {
         L.extend<<<L.gExtend, 256, 0, st>>>(none, scenes, rs.P, cnt, qin);
         k_classify<true><<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, cnt, qin, cq, rs.capacity);
-        ShadeArgs sa{none, scenes, rs.P, rs.S, cq, rs.capacity, qout, cnt, 0, L.capacity / 2};
+        ShadeArgs sa{none, scenes, rs.P, rs.S, cq, rs.capacity, qout, cnt, 0, L.capacity / 2, nullptr, nullptr, 0, qin};
         k_shade<true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+        if (L.full) {
+            k_shade<true, false, true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+            ++launches;
+        }
         L.shadowAny<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
         if (L.walls) {
             L.shadowWalk<<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
@@ -757,7 +766,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     std::vector<size_t> filmOff(static_cast<size_t>(count));
     size_t filmTotal = 0;
     int sph = 0;
-    bool media = false, walls = false;
+    bool media = false, walls = false, full = false;
     for (int i = 0; i < count; ++i) {
         if (!bs.caches[size_t(i)]) bs.caches[size_t(i)] = std::make_unique<SceneCache>();
         std::string e;
@@ -775,6 +784,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
         if (bs.caches[size_t(i)]->hasSpheres) sph = 1;
         if (d.mediumCount + d.gridCount > 0) media = true;
         if (d.hasInterfaces) walls = true;
+        if (d.hasFull) full = true;
     }
     std::vector<BatchChunk> chunks;
     std::vector<BatchWave> waves;
@@ -807,7 +817,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     BatchGraphKey key;
     key.capacity = capacity;
     key.shadeBlock = shadeBlock;
-    key.variant = sph | (media ? 2 : 0) | (walls ? 4 : 0);
+    key.variant = sph | (media ? 2 : 0) | (walls ? 4 : 0) | (full ? 8 : 0);
     key.ptrs[0] = bs.paths.pathBuf.ptr;
     key.ptrs[1] = bs.paths.shadowBuf.ptr;
     key.ptrs[2] = bs.scenes.ptr;

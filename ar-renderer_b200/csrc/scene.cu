@@ -478,8 +478,14 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
     d.cam = sd->camera;
     d.norm = sd->cieYIntegral > 0 ? 1.f / (4.f * sd->cieYIntegral) : 0.f;
     d.hasInterfaces = 0;
-    for (int32_t i = 0; i < sd->materialCount; ++i)
-        if (sd->materials[i].type == prgpu::MatInterface) d.hasInterfaces = 1;
+    d.hasFull = 0;
+    for (int32_t i = 0; i < sd->materialCount; ++i) {
+        const prgpu::Material &m = sd->materials[i];
+        if (m.type == prgpu::MatInterface) d.hasInterfaces = 1;
+        if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor ||
+            (m.sheenWeight > 0 && m.sheenColor >= 0))
+            d.hasFull = 1;
+    }
     d.filterType = sd->filter.type;
     d.filterRadius = sd->filter.radius;
     d.filterSigma = sd->filter.sigma;

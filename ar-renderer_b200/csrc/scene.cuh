@@ -86,6 +86,7 @@ struct DevScene {
     prgpu::Camera cam;
     float norm;           // 1 / (4 * integral of CIE y): XYZ normalisation of one sample
     int hasInterfaces;
+    int hasFull;  // some material is coated or has sheen (the kFull shading pass runs)
     // The medium-interface primitives as leaf slots, for the shadow walk's closest-hit queries
     // (brute force over at most kMaxWallList); wallCount < 0: too many, the walk uses the tree.
     const LeafPrim *walls;

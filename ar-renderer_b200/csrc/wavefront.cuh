@@ -63,6 +63,7 @@ struct Shadows {
 enum {
     kCntActive = 0, kCntNext = 1, kCntShadow = 2, kCntStatus = 3, kCntExtendWork = 4, kCntShadowWork = 5,
     kCntWalk = 6,  // shadow entries queued for the interface walk
+    kCntFull = 7,  // paths deferred to the coated / sheen shading pass
     // Batched form: live paths per half of the path slots after the last bounce, and the
     // survivors being counted during the current one.
     kCntLive0 = 8, kCntLive1 = 9, kCntNextLive0 = 10, kCntNextLive1 = 11,
@@ -757,10 +758,16 @@ struct ShadeArgs {
     const float *guideOut;
     float4 *guideRec;
     int guideMode;
+    // Paths that reached a coated / sheen surface, deferred by the main pass to the kFull pass
+    // (the ping-pong queue being consumed, free while shading runs).
+    int *fullQ;
 };
 
-// One bounce of PathIntegrator::Li for every active path (path.cpp:155-236).
-template <bool kBatch = false, bool kGuide = false>
+// One bounce of PathIntegrator::Li for every active path (path.cpp:155-236). The main pass
+// (kFull = false) defers paths that reach a coated or sheen surface, after their free flight and
+// emission, to the fullQ queue; the kFull pass shades those surfaces. Keeping the layered code out
+// of the main pass keeps its register allocation that of the plain materials.
+template <bool kBatch = false, bool kGuide = false, bool kFull = false>
 __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
     // The classes laid end to end: entry q belongs to the class whose prefix range holds it.
@@ -768,16 +775,18 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     start[0] = 0;
 #pragma unroll
     for (int c = 0; c < kClasses; ++c) start[c + 1] = start[c] + a.counters[kCntClass0 + c];
-    const int n = start[kClasses];
+    const int n = kFull ? a.counters[kCntFull] : start[kClasses];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int c = 0, first = 0;
+        int c = kClassOther, first = 0;
+        if constexpr (!kFull) {
 #pragma unroll
-        for (int k = 1; k < kClasses; ++k)
-            if (q >= start[k]) {
-                c = k;
-                first = start[k];
-            }
-        int j = a.classQ[size_t(c) * a.classCap + (q - first)];
+            for (int k = 1; k < kClasses; ++k)
+                if (q >= start[k]) {
+                    c = k;
+                    first = start[k];
+                }
+        }
+        int j = kFull ? a.fullQ[q] : a.classQ[size_t(c) * a.classCap + (q - first)];
         int4 meta = P.meta[j];
         const DevScene &s = SceneOf<kBatch>::get(a.s, a.scenes, path_render(meta.w));
         const int maxDepth = kBatch ? s.maxDepth : a.maxDepth;
@@ -795,10 +804,10 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         int crossings = (flags >> 8) & 0xffff;
         float4 pp4 = P.prevP[j], pn4 = P.prevN[j];
         V3 prevP = mk(pp4.x, pp4.y, pp4.z), prevN = mk(pn4.x, pn4.y, pn4.z);
-        int iters = __float_as_int(pn4.w) + 1;
+        int iters = __float_as_int(pn4.w) + (kFull ? 0 : 1);
         int prim = __float_as_int(hit.w);
-        bool alive = true;
-        if constexpr (kGuide) if (a.guideMode & 2) {
+        bool alive = true, deferred = false;
+        if constexpr (kGuide && !kFull) if (a.guideMode & 2) {
             // A record taken at this path's previous vertex: its radiance snapshot is the sum so far
             // (that vertex's NEE included, nothing from here on), so the final sum minus it is the
             // light that came along the sampled direction.
@@ -885,7 +894,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         // Participating medium along the segment: hero-driven free flight in homogeneous media
         // (medium.cpp:71-103, with the rPath pdf ratios of path-level spectral MIS), spectral
         // tracking in grid media (medium.cpp:232-285, wavelength-neutral: rPath unchanged).
-        if (!handled && medium >= 0) {
+        if (!kFull && !handled && medium >= 0) {
             float tMax = found ? hit.x : kInf;
             int event = 0;  // 0: the segment is crossed, 1: real scattering at t, 2: the path ends
             float t = tMax, g = 0.f;
@@ -956,7 +965,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 }
             }
         }
-        if (!handled && !found) {
+        if (!kFull && !handled && !found) {
             // Escaped: emission of every infinite light with MIS against the previous BSDF /
             // phase sample.
             if (s.envSpectrum >= 0) {
@@ -983,7 +992,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         if (!handled) {
             const prgpu::Primitive &pr = s.prims[prim];
             Surf sf = shade_point(s, pr, hit.x, hit.y, hit.z, o, d);
-            if (pr.light >= 0) {
+            if (!kFull && pr.light >= 0) {
                 const prgpu::Light &l = s.lights[pr.light];
                 SS Le = emitted(s, l, sf.n, -d, lam);
                 if (nonzero(Le)) {
@@ -1004,6 +1013,8 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 }
             } else if (m.type == prgpu::MatBlack || (maxDepth > 0 && depth >= maxDepth)) {
                 alive = false;
+            } else if (!kFull && full_material(m)) {
+                deferred = true;
             } else {
                 ++depth;
                 Frame fr = frame_from_xz(sf.dpdu, sf.ns);
@@ -1012,65 +1023,62 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 BSample bs;
                 bool ok;
                 float misPdf;  // the BSDF density for MIS against later light hits
-                // Coats and sheen shade through FullBsdf (stochastic layered walks, out of line); a
-                // proportional sampling pdf takes the estimated density for MIS (path.cpp:219).
-                const bool isFull = full_material(m);
-                FullBsdf fb;
-                Lobe lobe;
-                if (isFull)
+                if constexpr (kFull) {
+                    // Coats and sheen (FullBsdf: stochastic layered walks, out of line); a
+                    // proportional sampling pdf takes the estimated density for MIS (path.cpp:219).
+                    FullBsdf fb;
                     make_full(s, m, sf.u, sf.v, lam, &fb);
-                else
-                    lobe = make_lobe(s, m, sf.u, sf.v, lam);
-                GuideMix gm;
-                bool guided = false, inRange = false;
-                int recIndex = 0;
+                    if (full_non_specular(fb))
+                        nee(sf.p, sf.n, nullptr, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr, &fb);
+                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    bool proportional = false;
+                    ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &proportional);
+                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                    misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
+                } else {
+                Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
                 if constexpr (kGuide) {
+                    GuideMix gm;
                     // The guide is trained on, and applied at, the first kGuideVertices diffuse
                     // vertices of each path.
-                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse && !isFull;
-                    inRange = diffuseVertex && gcount < kGuideVertices;
-                    guided = (a.guideMode & 1) && inRange;
-                    recIndex = gcount;
+                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse;
+                    const bool inRange = diffuseVertex && gcount < kGuideVertices;
+                    const bool guided = (a.guideMode & 1) && inRange;
+                    const int recIndex = gcount;
                     if (inRange) ++gcount;
                     if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut);
-                }
-                if (isFull ? full_non_specular(fb) : lobe.non_specular())
-                    nee(sf.p, sf.n, isFull ? nullptr : &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
-                        guided ? &gm : nullptr, isFull ? &fb : nullptr);
-                float pbGuide = 0.f;
-                bool proportional = false;
-                if (isFull) {
-                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                    ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &proportional);
-                } else if (guided) {
-                    // One-sample MIS of the guide and the BSDF: wi ~ c q + (1 - c) p_bsdf.
-                    float us = rng.uniform(), uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                    V3 wiw;
-                    ok = wol.z != 0.f;
-                    const float side = dot(wo, sf.ns) > 0.f ? 1.f : -1.f;
-                    if (us < gm.c) {
-                        wiw = guide_sample(gm, uc, u0, u1);
-                        if (dot(wiw, sf.ns) * side < 0.f) wiw = guide_mirror(wiw, sf.ns);
+                    if (lobe.non_specular())
+                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
+                            guided ? &gm : nullptr);
+                    float pbGuide = 0.f;
+                    if (guided) {
+                        // One-sample MIS of the guide and the BSDF: wi ~ c q + (1 - c) p_bsdf.
+                        float us = rng.uniform(), uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                        V3 wiw;
+                        ok = wol.z != 0.f;
+                        const float side = dot(wo, sf.ns) > 0.f ? 1.f : -1.f;
+                        if (us < gm.c) {
+                            wiw = guide_sample(gm, uc, u0, u1);
+                            if (dot(wiw, sf.ns) * side < 0.f) wiw = guide_mirror(wiw, sf.ns);
+                        } else {
+                            BSample b2;
+                            ok = ok && lobe_sample(lobe, wol, uc, u0, u1, &b2);
+                            wiw = fr.from_local(b2.wi);
+                        }
+                        V3 wil = fr.to_local(wiw);
+                        pbGuide = lobe_pdf(lobe, wol, wil);
+                        bs.f = lobe_f(lobe, wol, wil);
+                        bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
+                        bs.wi = wil;
+                        bs.flags = kFlagReflection | kFlagDiffuse;
+                        bs.eta = 1.f;
                     } else {
-                        BSample b2;
-                        ok = ok && lobe_sample(lobe, wol, uc, u0, u1, &b2);
-                        wiw = fr.from_local(b2.wi);
+                        float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                        ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
                     }
-                    V3 wil = fr.to_local(wiw);
-                    pbGuide = lobe_pdf(lobe, wol, wil);
-                    bs.f = lobe_f(lobe, wol, wil);
-                    bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
-                    bs.wi = wil;
-                    bs.flags = kFlagReflection | kFlagDiffuse;
-                    bs.eta = 1.f;
-                } else {
-                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-                    ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
-                }
-                ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
-                     isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
-                misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
-                if constexpr (kGuide) {
+                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
                     float4 *rec = a.guideRec + 4 * (size_t(j) * kGuideVertices + recIndex);
                     if (ok && (a.guideMode & 2) && inRange) {
                         // First diffuse vertex of the path: record (x, n, wo, wi, p_bsdf, mean beta).
@@ -1086,6 +1094,15 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                         rec[2] = make_float4(wo.x, wo.y, wo.z, 0.f);
                         rec[3] = make_float4(wiw.x, wiw.y, wiw.z, __int_as_float(1));
                     }
+                } else {
+                    if (lobe.non_specular())
+                        nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr);
+                    float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
+                    ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
+                    ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
+                         isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
+                }
+                misPdf = bs.pdf;
                 }
                 if (!ok) {
                     alive = false;
@@ -1121,6 +1138,10 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                                       (flags & (0xff << kRenderShift)));
             P.prevP[j] = make_float4(prevP.x, prevP.y, prevP.z, pp4.w);
             P.prevN[j] = make_float4(prevN.x, prevN.y, prevN.z, __int_as_float(iters));
+            if (!kFull && deferred) {
+                a.fullQ[warp_append(a.counters + kCntFull)] = j;
+                continue;
+            }
             a.queueOut[warp_append(a.counters + kCntNext)] = j;
             if (kBatch) {
                 // Survivors per slot half (warp-aggregated): the batch loop films a wave once its
@@ -1245,6 +1266,7 @@ __global__ void k_advance(int *counters, unsigned long long *stats) {
     counters[kCntExtendWork] = 0;
     counters[kCntShadowWork] = 0;
     counters[kCntWalk] = 0;
+    counters[kCntFull] = 0;
 #pragma unroll
     for (int c = 0; c < kClasses; ++c) counters[kCntClass0 + c] = 0;
 }
