@@ -137,6 +137,11 @@ class BatchConfig(C.Structure):
                 ("flags", C.c_int32)]
 
 
+class CheckpointHeader(C.Structure):
+    _fields_ = [("integrator", C.c_uint32), ("maxDepth", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
+                ("chains", C.c_int32), ("fingerprint", C.c_uint64), ("seed", C.c_uint64)]
+
+
 class BatchStats(C.Structure):
     _fields_ = [("pathSamples", C.c_uint64), ("closestRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("waves", C.c_uint64), ("loopIterations", C.c_uint64), ("deviceMs", C.c_double),
@@ -231,6 +236,11 @@ def host_lib() -> C.CDLL:
         lib.prhost_build_bvh_triangles.restype = C.c_int64
         lib.prhost_build_light_bvh.argtypes = [_P, C.c_int32, _P]
         lib.prhost_build_light_bvh.restype = C.c_int32
+        lib.prhost_checkpoint_write.argtypes = [C.c_char_p, _P, _P, C.c_uint64, _P, C.c_uint64, C.c_char_p, C.c_int]
+        lib.prhost_checkpoint_write.restype = C.c_int
+        lib.prhost_checkpoint_read.argtypes = [C.c_char_p, _P, _P, C.c_uint64, _P, C.c_uint64, C.POINTER(C.c_uint64),
+                                               C.c_char_p, C.c_int]
+        lib.prhost_checkpoint_read.restype = C.c_int
         _host = lib
     return _host
 

@@ -36,3 +36,35 @@ PRHOST_API int64_t prhost_build_bvh_triangles(const prgpu::Float3 *verts, int64_
 // the node count or -1.
 PRHOST_API int32_t prhost_build_light_bvh(const float *lightBounds13, int32_t lightCount,
                                           prgpu::LightBVHNode *nodesOut);
+
+namespace prhost {
+
+// Header of a progressive-render checkpoint (the fields src/integrators/integrator.cpp:18-28
+// writes after the "PRCKPT02" magic). A resume is refused unless every field matches.
+struct CheckpointHeader {
+    uint32_t integrator;   // pr::IntegratorType (0 path, 1 BDPT, 2 MMLT, 3 PSSMLT) | 0x100 for a GPU render
+    int32_t maxDepth;      // the integrator's max depth (0 = unlimited)
+    int32_t width, height; // film size
+    int32_t chains;        // pr::IntegratorSettings::chains (written for every integrator)
+    uint64_t fingerprint;  // scene fingerprint (pr::Scene::Fingerprint, scene.cpp:61-70)
+    uint64_t seed;         // render seed
+};
+
+} // namespace prhost
+
+// Writes a checkpoint in the reference's PRCKPT02 layout (integrator.cpp:30-60, film.cpp:61-73):
+// magic, header, filmCount (= width * height * 3) FP64 XYZ accumulators, then bodySize bytes of
+// integrator state (the GPU path tracer stores its samples per pixel as one int32). Written to
+// "<path>.tmp" and renamed over path. Returns 0, or 1 with err set. Replaces pr::WriteCheckpoint.
+PRHOST_API int prhost_checkpoint_write(const char *path, const prhost::CheckpointHeader *header, const double *film,
+                                       uint64_t filmCount, const void *body, uint64_t bodySize, char *err,
+                                       int errLen);
+
+// Reads a checkpoint written for exactly *expected (integrator.cpp:62-90, film.cpp:75-84): the
+// film into film[filmCount], the body into body[bodyCapacity] (its size in *bodySize). Returns 0;
+// 1 cannot open or bad arguments; 2 not a checkpoint; 3 made for another scene / integrator /
+// device / resolution / seed / depth; 4 truncated or corrupt -- with the reference's messages in
+// err. Replaces pr::ReadCheckpoint.
+PRHOST_API int prhost_checkpoint_read(const char *path, const prhost::CheckpointHeader *expected, double *film,
+                                      uint64_t filmCount, void *body, uint64_t bodyCapacity, uint64_t *bodySize,
+                                      char *err, int errLen);

@@ -47,6 +47,10 @@ def ref_lib() -> C.CDLL:
         lib.prref_bxdf.argtypes = [C.c_int, _P, C.c_int64, _P, _P]
         lib.prref_full_bsdf.argtypes = [_P, C.c_int64, _P, _P]
         lib.prref_sheen_table.argtypes = [_P]
+        lib.prref_checkpoint_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                               _P, C.c_int32, C.c_char_p, C.c_int]
+        lib.prref_checkpoint_read.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
+                                              _P, C.POINTER(C.c_int32), C.c_char_p, C.c_int]
         lib.prref_fr_dielectric.argtypes = [C.c_float, C.c_float]
         lib.prref_fr_dielectric.restype = C.c_float
         lib.prref_fr_complex.argtypes = [C.c_float, C.c_float, C.c_float]

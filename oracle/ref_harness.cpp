@@ -20,6 +20,7 @@
 #include "core/film.h"
 #include "core/parallel.h"
 #include "core/rgb2spec.h"
+#include "core/serialize.h"
 #include "core/spectrum.h"
 #include "geometry/bvh.h"
 #include "geometry/shape.h"
@@ -240,6 +241,72 @@ API void prref_full_bsdf(const float *params, int64_t n, const float *in, float 
             y[15] = bs->pdfIsProportional ? 1.f : 0.f;
         }
     }
+}
+
+// Checkpoints through the reference's own WriteCheckpoint / ReadCheckpoint (integrator.cpp:30-90)
+// for a path-tracer render (body: the samples per pixel as int32). The film's accumulators are set
+// exactly through Film::ReadAccumulators from a scratch file (AddPixelXYZ takes floats).
+static void checkpoint_setup(RenderControl *c, IntegratorSettings *s, uint64_t fingerprint, uint64_t seed, int device,
+                             int maxDepth) {
+    c->fingerprint = fingerprint;
+    c->seed = seed;
+    s->type = IntegratorType::Path;
+    s->device = device;
+    s->maxDepth = maxDepth;
+}
+
+API int prref_checkpoint_write(const char *path, int width, int height, int device, int maxDepth, uint64_t fingerprint,
+                               uint64_t seed, const double *film, int32_t passes, char *err, int errLen) {
+    FilmSettings fs;
+    fs.width = width;
+    fs.height = height;
+    Film f(fs);
+    std::string scratch = std::string(path) + ".acc";
+    FILE *t = std::fopen(scratch.c_str(), "wb");
+    uint64_t n = uint64_t(width) * height * 3;
+    bool ok = t && std::fwrite(&n, sizeof(n), 1, t) == 1 && std::fwrite(film, sizeof(double), n, t) == n;
+    if (t) std::fclose(t);
+    t = ok ? std::fopen(scratch.c_str(), "rb") : nullptr;
+    ok = t && f.ReadAccumulators(t);
+    if (t) std::fclose(t);
+    std::remove(scratch.c_str());
+    RenderControl c;
+    IntegratorSettings s;
+    c.checkpointPath = path;
+    checkpoint_setup(&c, &s, fingerprint, seed, device, maxDepth);
+    std::string e;
+    ok = ok && WriteCheckpoint(c, s, f, [&](BinaryWriter &w) { w.Put(int32_t(passes)); }, &e);
+    if (!ok) std::snprintf(err, size_t(errLen), "%s", e.c_str());
+    return ok ? 0 : 1;
+}
+
+API int prref_checkpoint_read(const char *path, int width, int height, int device, int maxDepth, uint64_t fingerprint,
+                              uint64_t seed, double *film, int32_t *passes, char *err, int errLen) {
+    FilmSettings fs;
+    fs.width = width;
+    fs.height = height;
+    Film f(fs);
+    RenderControl c;
+    IntegratorSettings s;
+    c.resumePath = path;
+    checkpoint_setup(&c, &s, fingerprint, seed, device, maxDepth);
+    std::string e;
+    if (!ReadCheckpoint(c, s, f, [&](BinaryReader &r) { return r.Get(passes); }, &e)) {
+        std::snprintf(err, size_t(errLen), "%s", e.c_str());
+        return 1;
+    }
+    // The accumulators leave through a scratch file (PixelXYZ rounds them to float).
+    std::string scratch = std::string(path) + ".acc";
+    FILE *t = std::fopen(scratch.c_str(), "wb");
+    bool ok = t && f.WriteAccumulators(t);
+    if (t) std::fclose(t);
+    t = ok ? std::fopen(scratch.c_str(), "rb") : nullptr;
+    uint64_t n = 0;
+    ok = t && std::fread(&n, sizeof(n), 1, t) == 1 && n == uint64_t(width) * height * 3 &&
+         std::fread(film, sizeof(double), n, t) == n;
+    if (t) std::fclose(t);
+    std::remove(scratch.c_str());
+    return ok ? 0 : 1;
 }
 
 // The sheen lobe's directional albedo at the table nodes ([16 roughness][32 cos theta]).
