@@ -63,8 +63,10 @@ static_assert(sizeof(prgpu::Light) == 48 && offsetof(prgpu::Light, position) == 
               offsetof(prgpu::Light, pmf) == 40);
 static_assert(sizeof(prgpu::Camera) == 80 && offsetof(prgpu::Camera, width) == 64);
 static_assert(sizeof(prgpu::GridMediumDesc) == 112 && offsetof(prgpu::GridMediumDesc, density) == 104);
-static_assert(sizeof(prgpu::SceneExt) == 64 && offsetof(prgpu::SceneExt, gridMedia) == 40 &&
-              offsetof(prgpu::SceneExt, sun) == 56);
+static_assert(sizeof(prgpu::SceneExt) == 80 && offsetof(prgpu::SceneExt, gridMedia) == 40 &&
+              offsetof(prgpu::SceneExt, sun) == 56 && offsetof(prgpu::SceneExt, deltaLights) == 72);
+static_assert(sizeof(prgpu::DeltaLightDesc) == 104 && offsetof(prgpu::DeltaLightDesc, frame) == 48 &&
+              offsetof(prgpu::DeltaLightDesc, profile) == 96);
 static_assert(sizeof(prgpu::EnvMapDesc) == 32 && sizeof(prgpu::SunDesc) == 28);
 static_assert(prgpu::kGuideParams == prb::kGuideParams);
 static_assert(sizeof(prgpu::BatchItem) == 48 && offsetof(prgpu::BatchItem, outXYZ) == 40 &&

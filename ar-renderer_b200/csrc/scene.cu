@@ -57,6 +57,13 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
                         4 * sizeof(float), 65536);
     }
     if (ext && ext->sun) h = fnv_v(h, *ext->sun);
+    if (ext && ext->deltaLights && ext->deltaLightCount > 0)
+        for (int32_t k = 0; k < ext->deltaLightCount; ++k) {
+            const prgpu::DeltaLightDesc &l = ext->deltaLights[k];
+            h = fnv_v(h, l);
+            if (l.type == prgpu::DeltaGoniometric && l.profile && l.nV > 0 && l.nH > 0)
+                h = fnv(h, l.profile, (size_t(l.nV) + size_t(l.nH) + size_t(l.nV) * size_t(l.nH)) * sizeof(float));
+        }
     if (ext && ext->gridMedia && ext->gridMediumCount > 0)
         for (int32_t k = 0; k < ext->gridMediumCount; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
@@ -111,6 +118,19 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
             return fail("bad sun cone or pmf");
         float l2 = u.direction.x * u.direction.x + u.direction.y * u.direction.y + u.direction.z * u.direction.z;
         if (!(l2 > 0.f) || !std::isfinite(l2)) return fail("bad sun direction");
+    }
+    if (ext && (ext->deltaLightCount < 0 || ext->deltaLightCount > 4096 || (ext->deltaLightCount > 0 && !ext->deltaLights)))
+        return fail("bad delta light count or table");
+    for (int32_t k = 0; ext && k < ext->deltaLightCount; ++k) {
+        const prgpu::DeltaLightDesc &l = ext->deltaLights[k];
+        if (l.type > prgpu::DeltaGoniometric) return fail("unknown delta light type");
+        if (l.spectrum < 0 || l.spectrum >= ns) return fail("delta light spectrum index out of range");
+        if (!(l.pmf >= 0.f && l.pmf <= 1.f) || !std::isfinite(l.scale)) return fail("bad delta light pmf or scale");
+        float l2 = l.direction.x * l.direction.x + l.direction.y * l.direction.y + l.direction.z * l.direction.z;
+        if (l.type != prgpu::DeltaGoniometric && !(l2 > 0.f && std::isfinite(l2))) return fail("bad delta light direction");
+        if (l.type == prgpu::DeltaGoniometric &&
+            (l.nV <= 0 || l.nH <= 0 || int64_t(l.nV) * l.nH > (int64_t(1) << 22) || !l.profile))
+            return fail("bad goniometric profile");
     }
     if (sd->cameraMedium < -1 || sd->cameraMedium >= nm) return fail("cameraMedium out of range");
     for (int32_t i = 0; i < sd->materialCount; ++i) {
@@ -266,6 +286,51 @@ static std::vector<float> macro_majorants(const float *d, int nx, int ny, int nz
     return az;
 }
 
+// Spot, distant and goniometric lights: the descriptor table and the profiles, concatenated.
+void upload_deltas(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d, cudaStream_t s) {
+    d.deltas = nullptr;
+    d.deltaCount = 0;
+    const int32_t n = ext && ext->deltaLights ? ext->deltaLightCount : 0;
+    if (n <= 0) return;
+    std::vector<DevDelta> t(static_cast<size_t>(n));
+    std::vector<float> prof;
+    std::vector<size_t> off(static_cast<size_t>(n), 0);
+    for (int32_t k = 0; k < n; ++k) {
+        const prgpu::DeltaLightDesc &l = ext->deltaLights[k];
+        DevDelta &g = t[size_t(k)];
+        g.type = int(l.type);
+        g.spectrum = l.spectrum;
+        g.scale = l.scale;
+        g.pmf = l.pmf;
+        g.pos = mk(l.position.x, l.position.y, l.position.z);
+        V3 dir = mk(l.direction.x, l.direction.y, l.direction.z);
+        float len = std::sqrt(dir.x * dir.x + dir.y * dir.y + dir.z * dir.z);
+        g.dir = len > 0.f ? mk(dir.x / len, dir.y / len, dir.z / len) : mk(0.f, 0.f, 1.f);
+        g.cosStart = l.cosFalloffStart;
+        g.cosEnd = l.cosFalloffEnd;
+        g.fx = mk(l.frame[0], l.frame[1], l.frame[2]);
+        g.fy = mk(l.frame[3], l.frame[4], l.frame[5]);
+        g.fz = mk(l.frame[6], l.frame[7], l.frame[8]);
+        g.nV = l.nV;
+        g.nH = l.nH;
+        g.profile = nullptr;
+        if (l.type == prgpu::DeltaGoniometric) {
+            off[size_t(k)] = prof.size();
+            const size_t m = size_t(l.nV) + size_t(l.nH) + size_t(l.nV) * size_t(l.nH);
+            prof.insert(prof.end(), l.profile, l.profile + m);
+        }
+    }
+    if (!prof.empty()) {
+        put(cache.deltaProfiles, prof.data(), prof.size(), s);
+        for (int32_t k = 0; k < n; ++k)
+            if (t[size_t(k)].type == prgpu::DeltaGoniometric) t[size_t(k)].profile = cache.deltaProfiles.as<float>() + off[size_t(k)];
+    }
+    put(cache.deltas, t.data(), t.size(), s);
+    PRB_CUDA(cudaStreamSynchronize(s));
+    d.deltas = cache.deltas.as<DevDelta>();
+    d.deltaCount = n;
+}
+
 // The image environment's texels and its sampling distribution (EnvironmentLight's constructor,
 // light.cpp:217-236, with a spectral luminance in place of the RGB one; Distribution2D,
 // sampling.cpp:44-67). Rows are Distribution1D CDFs normalised to 1 (unless all zero).
@@ -288,6 +353,7 @@ void upload_env(const prgpu::SceneExt *ext, const prgpu::SceneDesc *sd, SceneCac
         d.sun.scale = u.scale;
         d.sun.pmf = u.pmf;
     }
+    upload_deltas(ext, cache, d, s);
     if (!(ext && ext->envMap)) return;
     const prgpu::EnvMapDesc &e = *ext->envMap;
     const int w = e.width, h = e.height;

@@ -65,6 +65,17 @@ struct DevSun {
     float scale, pmf;
 };
 
+// A spot, distant or goniometric light (prgpu::DeltaLightDesc on the device).
+struct DevDelta {
+    int type, spectrum;
+    float scale, pmf;
+    V3 pos, dir;             // dir: spot axis; distant: towards the light
+    float cosStart, cosEnd;  // spot falloff
+    V3 fx, fy, fz;           // goniometric profile frame
+    int nV, nH;
+    const float *profile;    // vAngles[nV], hAngles[nH], candela[nH][nV]
+};
+
 struct DevScene {
     const WNode *nodes;
     const QNode *qnodes;   // the 4-wide collapse of the same tree
@@ -106,6 +117,8 @@ struct DevScene {
     int gridCount;
     DevEnvMap envMap;
     DevSun sun;
+    const DevDelta *deltas;
+    int deltaCount;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).
     int maxDepth;            // <= 0: unlimited
     float clampY;            // 0: off
@@ -117,7 +130,7 @@ struct SceneCache {
     bool valid = false;
     DeviceAccel accel;
     DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
-        envDist, walls, sheen;
+        envDist, walls, sheen, deltas, deltaProfiles;
     DevScene ds{};
     bool hasSpheres = false;
     int wallCount = 0;
@@ -140,6 +153,8 @@ struct SceneCache {
         envDist.release();
         walls.release();
         sheen.release();
+        deltas.release();
+        deltaProfiles.release();
         valid = false;
     }
 };

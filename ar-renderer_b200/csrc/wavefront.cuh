@@ -442,6 +442,60 @@ struct LightSample {
 };
 
 // Chooses a light and a point on it as seen from p (normal n, zero in media).
+// SmoothStep(x, a, b) of the reference's math (a == b: a step at a).
+__device__ __forceinline__ float smooth_step(float x, float a, float b) {
+    if (a == b) return x < a ? 0.f : 1.f;
+    float t = clampf((x - a) / (b - a), 0.f, 1.f);
+    return t * t * (3.f - 2.f * t);
+}
+
+// Largest i in [0, n - 2] with v[i] <= x (FindInterval over a sorted table).
+__device__ __forceinline__ int find_interval(const float *v, int n, float x) {
+    int lo = 0, hi = n - 1;
+    if (!(__ldg(v) <= x)) return 0;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(v + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return min(lo, n - 2);
+}
+
+// Relative intensity of a type C IES profile towards the profile-frame direction w
+// (IESProfile::Evaluate / EvaluateAngles, ies.cpp:79-109): theta from the nadir axis, phi folded
+// by the symmetry the last horizontal angle implies, then linear in theta and in phi.
+__device__ float ies_eval(const DevDelta &l, V3 w) {
+    const float *va = l.profile, *ha = l.profile + l.nV, *cd = l.profile + l.nV + l.nH;
+    const float deg = 57.295779513082320876f;
+    float theta = acosf(clampf(w.z, -1.f, 1.f)) * deg;
+    float phi = atan2f(w.y, w.x) * deg;
+    const int nV = l.nV, nH = l.nH;
+    if (theta < __ldg(va) || theta > __ldg(va + nV - 1)) return 0.f;
+    float hLast = __ldg(ha + nH - 1);
+    phi = fmodf(phi, 360.f);
+    if (phi < 0.f) phi += 360.f;
+    if (nH == 1 || hLast == 0.f) {
+        phi = 0.f;
+    } else if (hLast <= 90.f) {
+        phi = fmodf(phi, 180.f);
+        if (phi > 90.f) phi = 180.f - phi;
+    } else if (hLast <= 180.f) {
+        if (phi > 180.f) phi = 360.f - phi;
+    }
+    auto lookupV = [&](int hi) {
+        if (nV == 1) return __ldg(cd + size_t(hi) * nV);
+        int vi = find_interval(va, nV, theta);
+        float t = (theta - __ldg(va + vi)) / fmaxf(1e-6f, __ldg(va + vi + 1) - __ldg(va + vi));
+        t = clampf(t, 0.f, 1.f);
+        float a0 = __ldg(cd + size_t(hi) * nV + vi), a1 = __ldg(cd + size_t(hi) * nV + vi + 1);
+        return (1.f - t) * a0 + t * a1;
+    };
+    if (nH == 1) return lookupV(0);
+    int hi = find_interval(ha, nH, phi);
+    float t = clampf((phi - __ldg(ha + hi)) / fmaxf(1e-6f, __ldg(ha + hi + 1) - __ldg(ha + hi)), 0.f, 1.f);
+    return (1.f - t) * lookupV(hi) + t * lookupV(hi + 1);
+}
+
 __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
     LightSample ls;
     ls.ok = false;
@@ -486,6 +540,38 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
             return ls;
         }
         acc += s.sun.pmf;
+    }
+    // Spot, distant and goniometric lights (delta distributions: pdf = the selection pmf).
+    for (int k = 0; k < s.deltaCount; ++k) {
+        const DevDelta &l = s.deltas[k];
+        if (!(ul < acc + l.pmf)) {
+            acc += l.pmf;
+            continue;
+        }
+        ls.delta = true;
+        ls.pdf = l.pmf;
+        if (l.type == prgpu::DeltaDistant) {  // DistantLight::SampleLi, sky.cpp:52-61
+            ls.wi = l.dir;
+            ls.target = p + l.dir * (2.f * s.worldRadius);
+            ls.Le = tab4(s.spectra, l.spectrum, lam) * l.scale;
+        } else {
+            V3 dd = l.pos - p;
+            float d2 = len2(dd);
+            if (!(d2 > 0.f)) return ls;
+            ls.wi = dd * rsqrtf(d2);
+            float f;
+            if (l.type == prgpu::DeltaSpot) {  // SpotLight::SampleLi, light.cpp:168-192
+                f = smooth_step(dot(-ls.wi, l.dir), l.cosEnd, l.cosStart);
+            } else {  // GoniometricLight::SampleLi, sky.cpp:12-26
+                V3 w = -ls.wi;
+                f = ies_eval(l, mk(dot(w, l.fx), dot(w, l.fy), dot(w, l.fz)));
+            }
+            if (!(f > 0.f)) return ls;
+            ls.target = l.pos;
+            ls.Le = tab4(s.spectra, l.spectrum, lam) * (l.scale * f / d2);
+        }
+        ls.ok = ls.pdf > 0.f;
+        return ls;
     }
     int li = -1;
     float pmf = 0.f;

@@ -121,11 +121,22 @@ class SunDesc(C.Structure):
                 ("scale", C.c_float), ("pmf", C.c_float)]
 
 
+DELTA_SPOT, DELTA_DISTANT, DELTA_GONIOMETRIC = range(3)
+
+
+class DeltaLightDesc(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("spectrum", C.c_int32), ("scale", C.c_float), ("pmf", C.c_float),
+                ("position", C.c_float * 3), ("direction", C.c_float * 3), ("cosFalloffStart", C.c_float),
+                ("cosFalloffEnd", C.c_float), ("frame", C.c_float * 9), ("nV", C.c_int32), ("nH", C.c_int32),
+                ("pad", C.c_int32), ("profile", C.c_void_p)]
+
+
 class SceneExt(C.Structure):
     _fields_ = [("structSize", C.c_uint32), ("lightBVHNodeCount", C.c_int32), ("lightBVH", C.c_void_p),
                 ("lightBVHProb", C.c_float), ("wavefrontPaths", C.c_int32), ("blockSize", C.c_int32),
                 ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p),
-                ("envMap", C.c_void_p), ("sun", C.c_void_p)]
+                ("envMap", C.c_void_p), ("sun", C.c_void_p), ("deltaLightCount", C.c_int32), ("pad", C.c_int32),
+                ("deltaLights", C.c_void_p)]
 
 
 class BatchItem(C.Structure):
@@ -158,7 +169,7 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 64
+assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 80 and C.sizeof(DeltaLightDesc) == 104
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72
 assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512

@@ -53,11 +53,12 @@ GUIDE_SAMPLE, GUIDE_TRAIN, GUIDE_RESET = 1, 2, 4
 
 
 def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
-             block_size: int = 0, grid_media=None, guide: int = 0) -> abi.SceneExt:
+             block_size: int = 0, grid_media=None, guide: int = 0, delta_lights=None) -> abi.SceneExt:
     """SceneExt for prgpu_render_ex. grid_media: GridMediumDesc records (media.grid_desc), indexed
     after the SceneDesc's homogeneous media. guide: GUIDE_SAMPLE (sample diffuse vertices with the
     guide network), GUIDE_TRAIN (train it online, one Adam step per wavefront chunk), GUIDE_RESET
-    (fresh weights first). The record keeps the arrays it points at alive."""
+    (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric). The
+    record keeps the arrays it points at alive."""
     e = abi.SceneExt()
     e.structSize = C.sizeof(abi.SceneExt)
     if light_bvh is not None and len(light_bvh):
@@ -74,6 +75,11 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
         e.gridMediumCount = len(arr)
         e.gridMedia = C.cast(arr, C.c_void_p)
         e._keep.append(arr)
+    if delta_lights:
+        arr = (abi.DeltaLightDesc * len(delta_lights))(*delta_lights)
+        e.deltaLightCount = len(arr)
+        e.deltaLights = C.cast(arr, C.c_void_p)
+        e._keep += [arr, delta_lights]
     return e
 
 

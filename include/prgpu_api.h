@@ -244,6 +244,27 @@ struct SunDesc {
 };
 
 // Optional extras for prgpu_render_ex (zero-initialise, then set structSize = sizeof(SceneExt)).
+// A delta light the v4 light table cannot describe (src/lights/light.h:143-240): a spot light
+// (SpotLight, light.cpp:161-192), a distant light (DistantLight, sky.cpp:52-63) or a goniometric
+// point light with a type C IES profile (GoniometricLight / IESProfile, sky.cpp:12-26,
+// ies.cpp:79-109). Selected with probability pmf alongside the SceneDesc lights and the infinite
+// lights (all pmfs together sum to 1).
+enum DeltaLightType : uint32_t { DeltaSpot = 0, DeltaDistant = 1, DeltaGoniometric = 2 };
+struct DeltaLightDesc {
+    uint32_t type;
+    int32_t spectrum;        // intensity (spot, goniometric) or irradiance (distant) spectrum index
+    float scale;
+    float pmf;
+    Float3 position;         // spot, goniometric
+    Float3 direction;        // spot: cone axis (where it shines); distant: towards the light
+    float cosFalloffStart;   // spot: cos of the falloff start and of the cone's half width
+    float cosFalloffEnd;
+    float frame[9];          // goniometric: profile frame rows x, y, z (z = the profile's nadir)
+    int32_t nV, nH;          // goniometric: vertical and horizontal angle counts
+    int32_t pad;
+    const float *profile;    // goniometric: vAngles[nV], hAngles[nH] (degrees), candela[nH][nV] / peak
+};
+
 struct SceneExt {
     uint32_t structSize;
     int32_t lightBVHNodeCount;      // 0 = power-based light selection (the v4 behaviour)
@@ -258,6 +279,9 @@ struct SceneExt {
     const GridMediumDesc *gridMedia;
     const EnvMapDesc *envMap;       // null = none
     const SunDesc *sun;             // null = none
+    int32_t deltaLightCount;
+    int32_t pad;
+    const DeltaLightDesc *deltaLights;
 };
 
 // One render of a batch (prgpu_render_batch): its scene, optional extension, parameters and film.

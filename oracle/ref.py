@@ -183,12 +183,13 @@ class RefScene:
         return self.lib.prref_scene_light_count(self.h)
 
     def infinite_lights(self):
-        """(type, pmf) of the exported scene's image-environment (2) and sun (3) lights."""
+        """(type, pmf) of the exported lights outside the v4 table, in scene order: image environment
+        (2), sun (3), spot (4), distant (5), goniometric (6)."""
         self.export()
-        t = np.zeros(8, np.int32)
-        p = np.zeros(8, np.float32)
-        n = self.lib.prref_scene_infinite(self.h, 8, _p(t), _p(p))
-        return [(int(t[i]), float(p[i])) for i in range(min(n, 8))]
+        t = np.zeros(64, np.int32)
+        p = np.zeros(64, np.float32)
+        n = self.lib.prref_scene_infinite(self.h, 64, _p(t), _p(p))
+        return [(int(t[i]), float(p[i])) for i in range(min(n, 64))]
 
     def grid_media(self):
         """Heterogeneous media of the export, in index order (index = mediumCount + k): a list of

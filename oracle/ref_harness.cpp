@@ -464,8 +464,8 @@ struct SceneHandle {
     // Heterogeneous media, in first-use order: exported as indices mediumCount + k (the layout of
     // the GPU module's grid-media extension); their parameters come from the scene file.
     std::vector<const pr::Medium *> grids;
-    // Infinite lights besides the constant environment: type 2 image environment, 3 sun; their
-    // light-sampler pmfs (renormalised with the exported lights').
+    // Lights outside the v4 table, in scene order: type 2 image environment, 3 sun, 4 spot,
+    // 5 distant, 6 goniometric; their light-sampler pmfs (renormalised with the exported lights').
     std::vector<std::pair<int, float>> infinite;
     int interfaceMat = -1;
 
@@ -736,6 +736,15 @@ API const prgpu::SceneDesc *prref_scene_export(void *hp, char *err, int errLen) 
             pmfSum += pmf;
         } else if (dynamic_cast<const SunLight *>(l)) {
             h->infinite.push_back({3, pmf});
+            pmfSum += pmf;
+        } else if (dynamic_cast<const SpotLight *>(l)) {
+            h->infinite.push_back({4, pmf});
+            pmfSum += pmf;
+        } else if (dynamic_cast<const DistantLight *>(l)) {
+            h->infinite.push_back({5, pmf});
+            pmfSum += pmf;
+        } else if (dynamic_cast<const GoniometricLight *>(l)) {
+            h->infinite.push_back({6, pmf});
             pmfSum += pmf;
         } else {
             h->Warn("light type not exported");
