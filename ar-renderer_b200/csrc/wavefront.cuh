@@ -863,7 +863,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     for (int c = 0; c < kClasses; ++c) start[c + 1] = start[c] + a.counters[kCntClass0 + c];
     const int n = kFull ? a.counters[kCntFull] : start[kClasses];
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int c = kClassOther, first = 0;
+        int c = kFull ? int(kClassOther) : 0, first = 0;
         if constexpr (!kFull) {
 #pragma unroll
             for (int k = 1; k < kClasses; ++k)
