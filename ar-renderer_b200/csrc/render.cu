@@ -78,6 +78,7 @@ struct RenderState {
     SceneCache scene;
     DevBuf pathBuf, shadowBuf, queues, classQueues, counters, stats, film;
     DevBuf guideFeat, guideOut, guideRec, guideTrain;  // guided form (allocated on first use)
+    DevBuf sceneTable;  // the render's DevScene in device memory, for the shading kernels
     int guideCap = 0;
     int capacity = 0;
     Paths P{};
@@ -176,6 +177,10 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     int npixChunk = int(std::min<int64_t>(npix, pathTarget));
     int S = std::max(1, std::min(spp, pathTarget / npixChunk));
     ensure_capacity(rs, npixChunk * S);
+    // The shading kernels read the scene from device memory, as the batched form does: their
+    // out-of-line helpers then take it by pointer instead of copying the kernel parameter.
+    rs.sceneTable.ensure(sizeof(DevScene));
+    PRB_CUDA(cudaMemcpyAsync(rs.sceneTable.ptr, &scene, sizeof(DevScene), cudaMemcpyHostToDevice, st));
     if (!rs.events) {
         for (auto &e : rs.ev) PRB_CUDA(cudaEventCreate(&e));
         PRB_CUDA(cudaMallocHost(&rs.hostActive, sizeof(int)));
@@ -249,12 +254,19 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                         launches += 1 + kGuideInferLaunches;
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
-                    ShadeArgs sa{scene,       nullptr, rs.P, rs.S, cq, rs.capacity, qout, cnt, rp.maxDepth, 0,
-                                 rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin};
-                    if (guideMode) k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
-                    else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
+                    ShadeArgs sa{scene, rs.sceneTable.as<DevScene>(), rs.P, rs.S, cq, rs.capacity, qout, cnt,
+                                 rp.maxDepth, 0, rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin};
+                    const bool dl = scene.deltaCount > 0;
+                    if (guideMode) {
+                        if (dl) k_shade<false, true, false, true><<<gShade, 256, 0, st>>>(sa);
+                        else k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
+                    } else {
+                        if (dl) k_shade<false, false, false, true><<<gShade, 256, 0, st>>>(sa);
+                        else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
+                    }
                     if (scene.hasFull) {
-                        k_shade<false, false, true><<<gShade, 256, 0, st>>>(sa);
+                        if (dl) k_shade<false, false, true, true><<<gShade, 256, 0, st>>>(sa);
+                        else k_shade<false, false, true><<<gShade, 256, 0, st>>>(sa);
                         ++launches;
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
@@ -651,6 +663,8 @@ struct BatchLaunch {
     void (*extend)(DevScene, const DevScene *, Paths, int *, const int *);
     void (*shadowAny)(DevScene, const DevScene *, Paths, Shadows, int *);
     void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, int *);
+    void (*shade)(ShadeArgs);
+    void (*shadeFull)(ShadeArgs);
     bool walls, full;
     int gExtend, gShadow, gShade, gWide, shadeBlock, capacity;
 };
@@ -660,6 +674,9 @@ BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
     BatchLaunch L{};
     L.walls = key.variant & 4;
     L.full = key.variant & 8;
+    const bool dl = key.variant & 16;
+    L.shade = dl ? k_shade<true, false, false, true> : k_shade<true>;
+    L.shadeFull = dl ? k_shade<true, false, true, true> : k_shade<true, false, true>;
     L.extend = sph ? k_extend<true, true> : k_extend<false, true>;
     L.shadowAny = L.walls ? (sph ? k_shadow_any<true, true, true, true> : k_shadow_any<false, true, true, true>)
                   : sph   ? (media ? k_shadow_any<true, true, true> : k_shadow_any<true, false, true>)
@@ -669,7 +686,7 @@ BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
     L.gExtend = sms * resident_blocks_of(L.extend);
     L.gShadow = sms * resident_blocks_of(L.shadowAny);
     int perSm = 0;
-    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_shade<true>, key.shadeBlock, 0));
+    PRB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, L.shade, key.shadeBlock, 0));
     L.gShade = sms * std::max(1, perSm);
     L.gWide = sms * 8;
     L.shadeBlock = key.shadeBlock;
@@ -699,9 +716,9 @@ int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &
         L.extend<<<L.gExtend, 256, 0, st>>>(none, scenes, rs.P, cnt, qin);
         k_classify<true><<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, cnt, qin, cq, rs.capacity);
         ShadeArgs sa{none, scenes, rs.P, rs.S, cq, rs.capacity, qout, cnt, 0, L.capacity / 2, nullptr, nullptr, 0, qin};
-        k_shade<true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+        L.shade<<<L.gShade, L.shadeBlock, 0, st>>>(sa);
         if (L.full) {
-            k_shade<true, false, true><<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+            L.shadeFull<<<L.gShade, L.shadeBlock, 0, st>>>(sa);
             ++launches;
         }
         L.shadowAny<<<L.gShadow, 256, 0, st>>>(none, scenes, rs.P, rs.S, cnt);
@@ -766,7 +783,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     std::vector<size_t> filmOff(static_cast<size_t>(count));
     size_t filmTotal = 0;
     int sph = 0;
-    bool media = false, walls = false, full = false;
+    bool media = false, walls = false, full = false, deltas = false;
     for (int i = 0; i < count; ++i) {
         if (!bs.caches[size_t(i)]) bs.caches[size_t(i)] = std::make_unique<SceneCache>();
         std::string e;
@@ -785,6 +802,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
         if (d.mediumCount + d.gridCount > 0) media = true;
         if (d.hasInterfaces) walls = true;
         if (d.hasFull) full = true;
+        if (d.deltaCount > 0) deltas = true;
     }
     std::vector<BatchChunk> chunks;
     std::vector<BatchWave> waves;
@@ -817,7 +835,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
     BatchGraphKey key;
     key.capacity = capacity;
     key.shadeBlock = shadeBlock;
-    key.variant = sph | (media ? 2 : 0) | (walls ? 4 : 0) | (full ? 8 : 0);
+    key.variant = sph | (media ? 2 : 0) | (walls ? 4 : 0) | (full ? 8 : 0) | (deltas ? 16 : 0);
     key.ptrs[0] = bs.paths.pathBuf.ptr;
     key.ptrs[1] = bs.paths.shadowBuf.ptr;
     key.ptrs[2] = bs.scenes.ptr;

@@ -496,6 +496,37 @@ __device__ float ies_eval(const DevDelta &l, V3 w) {
     return (1.f - t) * lookupV(hi) + t * lookupV(hi + 1);
 }
 
+// A spot, distant or goniometric light's sample towards p (delta distributions: pdf = the
+// selection pmf).
+__device__ __forceinline__ LightSample sample_delta_light(const DevScene &s, const DevDelta &l, V3 p, const Lambda &lam) {
+    LightSample ls;
+    ls.ok = false;
+    ls.delta = true;
+    ls.pdf = l.pmf;
+    if (l.type == prgpu::DeltaDistant) {  // DistantLight::SampleLi, sky.cpp:52-61
+        ls.wi = l.dir;
+        ls.target = p + l.dir * (2.f * s.worldRadius);
+        ls.Le = tab4(s.spectra, l.spectrum, lam) * l.scale;
+    } else {
+        V3 dd = l.pos - p;
+        float d2 = len2(dd);
+        if (!(d2 > 0.f)) return ls;
+        ls.wi = dd * rsqrtf(d2);
+        float f;
+        if (l.type == prgpu::DeltaSpot) {  // SpotLight::SampleLi, light.cpp:168-192
+            f = smooth_step(dot(-ls.wi, l.dir), l.cosEnd, l.cosStart);
+        } else {  // GoniometricLight::SampleLi, sky.cpp:12-26
+            V3 w = -ls.wi;
+            f = ies_eval(l, mk(dot(w, l.fx), dot(w, l.fy), dot(w, l.fz)));
+        }
+        if (!(f > 0.f)) return ls;
+        ls.target = l.pos;
+        ls.Le = tab4(s.spectra, l.spectrum, lam) * (l.scale * f / d2);
+    }
+    ls.ok = ls.pdf > 0.f;
+    return ls;
+}
+
 __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
     LightSample ls;
     ls.ok = false;
@@ -540,38 +571,6 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
             return ls;
         }
         acc += s.sun.pmf;
-    }
-    // Spot, distant and goniometric lights (delta distributions: pdf = the selection pmf).
-    for (int k = 0; k < s.deltaCount; ++k) {
-        const DevDelta &l = s.deltas[k];
-        if (!(ul < acc + l.pmf)) {
-            acc += l.pmf;
-            continue;
-        }
-        ls.delta = true;
-        ls.pdf = l.pmf;
-        if (l.type == prgpu::DeltaDistant) {  // DistantLight::SampleLi, sky.cpp:52-61
-            ls.wi = l.dir;
-            ls.target = p + l.dir * (2.f * s.worldRadius);
-            ls.Le = tab4(s.spectra, l.spectrum, lam) * l.scale;
-        } else {
-            V3 dd = l.pos - p;
-            float d2 = len2(dd);
-            if (!(d2 > 0.f)) return ls;
-            ls.wi = dd * rsqrtf(d2);
-            float f;
-            if (l.type == prgpu::DeltaSpot) {  // SpotLight::SampleLi, light.cpp:168-192
-                f = smooth_step(dot(-ls.wi, l.dir), l.cosEnd, l.cosStart);
-            } else {  // GoniometricLight::SampleLi, sky.cpp:12-26
-                V3 w = -ls.wi;
-                f = ies_eval(l, mk(dot(w, l.fx), dot(w, l.fy), dot(w, l.fz)));
-            }
-            if (!(f > 0.f)) return ls;
-            ls.target = l.pos;
-            ls.Le = tab4(s.spectra, l.spectrum, lam) * (l.scale * f / d2);
-        }
-        ls.ok = ls.pdf > 0.f;
-        return ls;
     }
     int li = -1;
     float pmf = 0.f;
@@ -829,7 +828,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
 
 struct ShadeArgs {
     DevScene s;
-    const DevScene *scenes;  // batched form: the renders' scenes, indexed by path_render
+    const DevScene *scenes;  // the renders' scenes in device memory (batched form: by path_render)
     Paths P;
     Shadows S;
     const int *classQ;       // the closest-hit kernel's per-class queues (kClasses x classCap)
@@ -852,8 +851,9 @@ struct ShadeArgs {
 // One bounce of PathIntegrator::Li for every active path (path.cpp:155-236). The main pass
 // (kFull = false) defers paths that reach a coated or sheen surface, after their free flight and
 // emission, to the fullQ queue; the kFull pass shades those surfaces. Keeping the layered code out
-// of the main pass keeps its register allocation that of the plain materials.
-template <bool kBatch = false, bool kGuide = false, bool kFull = false>
+// of the main pass keeps its register allocation that of the plain materials. kDelta: the scene has
+// spot / distant / goniometric lights.
+template <bool kBatch = false, bool kGuide = false, bool kFull = false, bool kDelta = false>
 __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
     // The classes laid end to end: entry q belongs to the class whose prefix range holds it.
@@ -874,7 +874,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         }
         int j = kFull ? a.fullQ[q] : a.classQ[size_t(c) * a.classCap + (q - first)];
         int4 meta = P.meta[j];
-        const DevScene &s = SceneOf<kBatch>::get(a.s, a.scenes, path_render(meta.w));
+        const DevScene &s = a.scenes[kBatch ? path_render(meta.w) : 0];
         const int maxDepth = kBatch ? s.maxDepth : a.maxDepth;
         float4 o4 = P.o[j], d4 = P.d[j], hit = P.hit[j];
         V3 o = mk(o4.x, o4.y, o4.z), d = mk(d4.x, d4.y, d4.z);
@@ -923,7 +923,24 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         auto nee = [&](V3 p, V3 ng, const Lobe *lobe, const Frame *fr, V3 ns, V3 wo, float g, int medIn, int medOut,
                        const GuideMix *gmix, const FullBsdf *full = nullptr) {
             float ul = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
-            LightSample ls = sample_light(s, p, ng, lam, ul, u0, u1);
+            LightSample ls;
+            bool picked = false;
+            if constexpr (kDelta) {
+                // The spot / distant / goniometric lights take the first band of ul; the light
+                // sampler gets the rest, its own bands (infinite lights, then bounded lights)
+                // summing to what is left.
+                float acc = 0.f;
+                for (int k = 0; k < s.deltaCount && !picked; ++k) {
+                    const DevDelta &l = s.deltas[k];
+                    if (ul < acc + l.pmf) {
+                        ls = sample_delta_light(s, l, p, lam);
+                        picked = true;
+                    }
+                    acc += l.pmf;
+                }
+                ul -= acc;
+            }
+            if (!picked) ls = sample_light(s, p, ng, lam, ul, u0, u1);
             if (!ls.ok) return;
             int med = dot(ls.wi, ng) > 0.f ? medOut : medIn;
             SS f;
