@@ -12,6 +12,7 @@
 
 #include "guide_host.h"
 #include "wavefront.cuh"
+#include "aov.cuh"
 
 namespace prb {
 // ---------------------------------------------------------------------------------------------
@@ -1083,6 +1084,75 @@ PRGPU_API int prgpu_render_ex(int deviceIndex, const prgpu::SceneDesc *scene, co
         return 1;
     }
     return render_common(deviceIndex, scene, ext, params, nullptr, outXYZ, stats, err, errLen);
+}
+
+PRGPU_API int prgpu_render_aov(int deviceIndex, const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext,
+                               const prgpu::AovParams *p, float *outRGB, char *err, int errLen) {
+    std::lock_guard<std::mutex> lock(gApiMutex);
+    try {
+        if (!sd || sd->apiVersion != prgpu::kApiVersion) {
+            set_err(err, errLen, "API version mismatch");
+            return 1;
+        }
+        if (!p || !outRGB || p->type < 0 || p->type > 3 || p->spp <= 0 || p->spp > (1 << 20)) {
+            set_err(err, errLen, "bad AOV parameters");
+            return 1;
+        }
+        if (p->type == 0 && (p->d65Spectrum < 0 || p->d65Spectrum >= sd->spectrumCount)) {
+            set_err(err, errLen, "D65 spectrum index out of range");
+            return 1;
+        }
+        if (ext && ext->structSize != sizeof(prgpu::SceneExt)) {
+            set_err(err, errLen, "SceneExt size mismatch");
+            return 1;
+        }
+        if (deviceIndex < 0 || deviceIndex >= 64) {
+            set_err(err, errLen, "no such GPU device");
+            return 1;
+        }
+        DeviceState &ds = device_state(deviceIndex);
+        RenderState &rs = render_state(deviceIndex);
+        std::string e;
+        if (!upload_scene(ds, sd, ext, rs.scene, &e)) {
+            set_err(err, errLen, e);
+            return 1;
+        }
+        cudaStream_t st = ds.stream;
+        const DevScene &scene = rs.scene.ds;
+        const size_t n = size_t(sd->camera.width) * size_t(sd->camera.height) * 3;
+        rs.sceneTable.ensure(sizeof(DevScene));
+        PRB_CUDA(cudaMemcpyAsync(rs.sceneTable.ptr, &scene, sizeof(DevScene), cudaMemcpyHostToDevice, st));
+        DevBuf out;
+        out.ensure(n * sizeof(float));
+        rs.counters.ensure(kCntSlots * sizeof(int));
+        int *cnt = rs.counters.as<int>();
+        PRB_CUDA(cudaMemsetAsync(cnt, 0, kCntSlots * sizeof(int), st));
+        AovArgs a{};
+        a.type = p->type;
+        a.spp = p->spp;
+        a.seed = p->seed;
+        a.throughSpecular = p->throughSpecular;
+        a.d65 = p->d65Spectrum;
+        std::memcpy(a.adapt, p->whiteAdaptation, sizeof(a.adapt));
+        std::memcpy(a.toRGB, p->xyzToRGB, sizeof(a.toRGB));
+        k_aov<<<ds.prop.multiProcessorCount * 8, 128, 0, st>>>(rs.sceneTable.as<DevScene>(), a, out.as<float>(),
+                                                               cnt + kCntStatus);
+        count_launch(1);
+        PRB_CUDA(cudaGetLastError());
+        int status = 0;
+        PRB_CUDA(cudaMemcpyAsync(outRGB, out.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+        PRB_CUDA(cudaMemcpyAsync(&status, cnt + kCntStatus, sizeof(int), cudaMemcpyDeviceToHost, st));
+        PRB_CUDA(cudaStreamSynchronize(st));
+        out.release();
+        if (status & kStatusStack) {
+            set_err(err, errLen, "traversal stack overflow (BVH deeper than the traversal stack)");
+            return 1;
+        }
+        return 0;
+    } catch (const CudaError &ce) {
+        set_err(err, errLen, ce.msg);
+        return 1;
+    }
 }
 
 PRGPU_API int prgpu_render_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,

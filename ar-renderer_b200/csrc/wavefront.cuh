@@ -684,6 +684,26 @@ template <> struct SceneOf<true> {
 
 // Camera sample `sample` of pixel `pix` (PerspectiveCamera::GenerateRay, camera.cpp:36-48, with
 // SampleVisible wavelengths and filter importance sampling) into path slot j, queued if valid.
+// Camera ray through film position (fx, fy) with lens sample (l0, l1) (PerspectiveCamera::
+// GenerateRay, camera.cpp:36-48): world origin and unit direction.
+__device__ __forceinline__ void camera_ray(const DevScene &s, float fx, float fy, float l0, float l1, V3 *o, V3 *d) {
+    const prgpu::Camera &c = s.cam;
+    V3 dir = normalize(mk((2.f * fx / c.width - 1.f) * c.tanHalfFov * c.aspect, (1.f - 2.f * fy / c.height) * c.tanHalfFov, 1.f));
+    V3 org = mk(0.f, 0.f, 0.f);
+    if (c.lensRadius > 0.f) {
+        float lx, ly;
+        concentric_disk(l0, l1, &lx, &ly);
+        V3 pf = dir * (c.focalDistance / dir.z);
+        org = mk(lx * c.lensRadius, ly * c.lensRadius, 0.f);
+        dir = normalize(pf - org);
+    }
+    const float *M = c.cameraToWorld;
+    *o = mk(M[0] * org.x + M[1] * org.y + M[2] * org.z + M[3], M[4] * org.x + M[5] * org.y + M[6] * org.z + M[7],
+            M[8] * org.x + M[9] * org.y + M[10] * org.z + M[11]);
+    *d = normalize(mk(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
+                      M[8] * dir.x + M[9] * dir.y + M[10] * dir.z));
+}
+
 __device__ __forceinline__ void raygen_path(const DevScene &s, const Paths &P, int j, int pix, uint64_t sample,
                                             uint64_t seed, int rid, int *counters, int *queue) {
     {
@@ -694,22 +714,8 @@ __device__ __forceinline__ void raygen_path(const DevScene &s, const Paths &P, i
         float dx = filter_sample_1d(s, rng.uniform(), &pdfX), dy = filter_sample_1d(s, rng.uniform(), &pdfY);
         float fw = filter_eval_1d(s, dx) * filter_eval_1d(s, dy) * s.filterNorm / (pdfX * pdfY);
         float l0 = rng.uniform(), l1 = rng.uniform();
-        const prgpu::Camera &c = s.cam;
-        float fx = float(px) + 0.5f + dx, fy = float(py) + 0.5f + dy;
-        V3 dir = normalize(mk((2.f * fx / c.width - 1.f) * c.tanHalfFov * c.aspect, (1.f - 2.f * fy / c.height) * c.tanHalfFov, 1.f));
-        V3 org = mk(0.f, 0.f, 0.f);
-        if (c.lensRadius > 0.f) {
-            float lx, ly;
-            concentric_disk(l0, l1, &lx, &ly);
-            V3 pf = dir * (c.focalDistance / dir.z);
-            org = mk(lx * c.lensRadius, ly * c.lensRadius, 0.f);
-            dir = normalize(pf - org);
-        }
-        const float *M = c.cameraToWorld;
-        V3 o = mk(M[0] * org.x + M[1] * org.y + M[2] * org.z + M[3], M[4] * org.x + M[5] * org.y + M[6] * org.z + M[7],
-                  M[8] * org.x + M[9] * org.y + M[10] * org.z + M[11]);
-        V3 dw = normalize(mk(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
-                             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z));
+        V3 o, dw;
+        camera_ray(s, float(px) + 0.5f + dx, float(py) + 0.5f + dy, l0, l1, &o, &dw);
         bool valid = fw != 0.f && isfinite(fw);
         P.o[j] = make_float4(o.x, o.y, o.z, 1.f);
         P.d[j] = make_float4(dw.x, dw.y, dw.z, 1.f);

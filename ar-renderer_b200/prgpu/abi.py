@@ -148,6 +148,11 @@ class BatchConfig(C.Structure):
                 ("flags", C.c_int32)]
 
 
+class AovParams(C.Structure):
+    _fields_ = [("type", C.c_int32), ("spp", C.c_int32), ("seed", C.c_uint64), ("throughSpecular", C.c_int32),
+                ("d65Spectrum", C.c_int32), ("whiteAdaptation", C.c_float * 9), ("xyzToRGB", C.c_float * 9)]
+
+
 class CheckpointHeader(C.Structure):
     _fields_ = [("integrator", C.c_uint32), ("maxDepth", C.c_int32), ("width", C.c_int32), ("height", C.c_int32),
                 ("chains", C.c_int32), ("fingerprint", C.c_uint64), ("seed", C.c_uint64)]
@@ -170,6 +175,7 @@ class RenderStats(C.Structure):
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
 assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 80 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72
 assert SceneDesc.camera.offset == 140 and SceneDesc.filter.offset == 220 and SceneDesc.cieYIntegral.offset == 512
@@ -227,6 +233,7 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_eval_bxdf", [C.c_int, C.c_int, _P, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_full_bsdf", [C.c_int, _P, _P, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_sheen_albedo_table", [_P], None)
+        _bind(lib, "prgpu_render_aov", [C.c_int, _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_phase", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_homogeneous", [C.c_int, C.c_int64, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_eval_light_bvh", [C.c_int, _P, C.c_int32, C.c_int32, C.c_float, C.c_int64, _P, _P, _P,

@@ -131,3 +131,26 @@ def autotune_batch(items, device: int = 0) -> abi.BatchConfig:
                                             C.cast(C.pointer(out), C.c_void_p), err, len(err))
     abi.check(rc, err, "prgpu_autotune_batch")
     return out
+
+
+AOV_ALBEDO, AOV_NORMAL, AOV_DEPTH, AOV_POSITION = range(4)
+
+
+def render_aov(scene, width: int, height: int, kind: int, spp: int, seed: int = 0, through_specular: bool = False,
+               d65_spectrum: int = -1, white_adaptation=None, xyz_to_rgb=None, ext: abi.SceneExt | None = None,
+               device: int = 0) -> np.ndarray:
+    """prgpu_render_aov: (height, width, 3) float32 guide buffer. Albedo needs the SceneDesc index
+    of a D65 spectrum and the host's colour matrices (white adaptation, XYZ -> linear sRGB)."""
+    p = abi.AovParams()
+    p.type, p.spp, p.seed, p.throughSpecular, p.d65Spectrum = kind, spp, seed, 1 if through_specular else 0, d65_spectrum
+    for dst, src in ((p.whiteAdaptation, white_adaptation), (p.xyzToRGB, xyz_to_rgb)):
+        vals = np.eye(3).ravel() if src is None else np.asarray(src, np.float64).ravel()
+        for i in range(9):
+            dst[i] = float(vals[i])
+    out = np.zeros((height, width, 3), np.float32)
+    err = abi.err_buf()
+    extp = C.cast(C.pointer(ext), C.c_void_p) if ext is not None else None
+    rc = abi.gpu_lib().prgpu_render_aov(device, _desc_ptr(scene), extp, C.cast(C.pointer(p), C.c_void_p), abi.ptr(out),
+                                        err, len(err))
+    abi.check(rc, err, "prgpu_render_aov")
+    return out

@@ -284,6 +284,17 @@ struct SceneExt {
     const DeltaLightDesc *deltaLights;
 };
 
+// Parameters of prgpu_render_aov (pr::RenderAOV, src/integrators/aov.h:10-21).
+struct AovParams {
+    int32_t type;             // 0 albedo, 1 normal, 2 depth, 3 position (pr::AOVType)
+    int32_t spp;              // jittered samples per pixel
+    uint64_t seed;
+    int32_t throughSpecular;  // follow perfectly specular chains (denoiser guides)
+    int32_t d65Spectrum;      // SceneDesc::spectra index of the D65 illuminant (albedo)
+    float whiteAdaptation[9]; // albedo: XYZ white adaptation, then ...
+    float xyzToRGB[9];        // ... XYZ -> linear sRGB, both row-major (color.cpp:92-99)
+};
+
 // One render of a batch (prgpu_render_batch): its scene, optional extension, parameters and film.
 struct BatchItem {
     const SceneDesc *scene;
@@ -417,6 +428,15 @@ PRGPU_API void prgpu_accel_destroy(prgpu_accel accel);
 // wave after wave with no host round trip. Each film gets exactly the bits prgpu_render_ex would
 // add for that item alone. config may be null (all settings autotuned). No counterpart in the
 // reference, whose host renders one scene per call (src/integrators/gpu_path.cpp:458-509).
+// Auxiliary buffer of a scene at its film resolution (pr::RenderAOV, src/integrators/aov.cpp:147-196):
+// albedo (linear sRGB directional albedo of the first visible surface, coverage-weighted), world
+// shading normal (normalised sum), depth (nearest along the camera ray, 1e10 where nothing is hit)
+// or position (mean over hits); throughSpecular follows mirrors and glass to the first
+// non-specular surface (or into a scattering medium: its single-scattering albedo). outRGB:
+// width * height * 3 floats, overwritten. Returns 0, or 1 with err set.
+PRGPU_API int prgpu_render_aov(int deviceIndex, const prgpu::SceneDesc *scene, const prgpu::SceneExt *ext,
+                               const prgpu::AovParams *params, float *outRGB, char *err, int errLen);
+
 PRGPU_API int prgpu_render_batch(int deviceIndex, int32_t count, const prgpu::BatchItem *items,
                                  const prgpu::BatchConfig *config, prgpu::BatchStats *stats, char *err, int errLen);
 

@@ -47,6 +47,8 @@ def ref_lib() -> C.CDLL:
         lib.prref_bxdf.argtypes = [C.c_int, _P, C.c_int64, _P, _P]
         lib.prref_full_bsdf.argtypes = [_P, C.c_int64, _P, _P]
         lib.prref_sheen_table.argtypes = [_P]
+        lib.prref_render_aov.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, _P]
+        lib.prref_aov_matrices.argtypes = [_P, _P]
         lib.prref_checkpoint_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
                                                _P, C.c_int32, C.c_char_p, C.c_int]
         lib.prref_checkpoint_read.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_uint64,
@@ -181,6 +183,12 @@ class RefScene:
 
     def light_count(self) -> int:
         return self.lib.prref_scene_light_count(self.h)
+
+    def render_aov(self, kind: int, spp: int, seed: int, through_specular: bool) -> np.ndarray:
+        """pr::RenderAOV: (height, width, 3) float32 (kind 0 albedo, 1 normal, 2 depth, 3 position)."""
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        self.lib.prref_render_aov(self.h, kind, spp, seed, 1 if through_specular else 0, _p(out))
+        return out
 
     def infinite_lights(self):
         """(type, pmf) of the exported lights outside the v4 table, in scene order: image environment

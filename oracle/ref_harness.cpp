@@ -17,6 +17,7 @@
 // hand its GPU module.
 
 #include "cameras/camera.h"
+#include "core/color.h"
 #include "core/film.h"
 #include "core/parallel.h"
 #include "core/rgb2spec.h"
@@ -25,6 +26,7 @@
 #include "geometry/bvh.h"
 #include "geometry/shape.h"
 #include "gpu/gpu_api.h"
+#include "integrators/aov.h"
 #include "integrators/integrator.h"
 #include "integrators/path.h"
 #include "lights/light.h"
@@ -991,4 +993,29 @@ API int prref_scene_grid_info(void *hp, int k, char *name, int nameLen, float *b
         bounds6[3 + a] = b.pMax[a];
     }
     return 0;
+}
+
+// pr::RenderAOV on the loaded scene (type: 0 albedo, 1 normal, 2 depth, 3 position) into
+// out[width * height * 3]; and the two colour matrices its albedo uses (white adaptation of the
+// spectral D65 white, then XYZ -> linear sRGB; color.cpp:92-99), row-major.
+API void prref_render_aov(void *hp, int type, int spp, uint64_t seed, int throughSpecular, float *out) {
+    auto *h = static_cast<SceneHandle *>(hp);
+    Image img = RenderAOV(*h->scene, AOVType(type), spp, seed, throughSpecular != 0);
+    for (int y = 0; y < img.Height(); ++y)
+        for (int x = 0; x < img.Width(); ++x) {
+            RGB c = img.Get(x, y);
+            float *o = out + 3 * (size_t(y) * img.Width() + x);
+            o[0] = c.r;
+            o[1] = c.g;
+            o[2] = c.b;
+        }
+}
+
+API void prref_aov_matrices(float *adapt9, float *toRGB9) {
+    const Mat3 &a = SpectralWhiteAdaptation(), &m = XYZToRGBMatrix(ColorSpaceId::sRGB);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            adapt9[3 * i + j] = a.m[i][j];
+            toRGB9[3 * i + j] = m.m[i][j];
+        }
 }
