@@ -52,6 +52,7 @@ constexpr float kWiden = 0x1.00000cp+0f;
 struct TraceRay {
     V3 o, d, inv;
     int neg[3];
+    bool infInv;  // a direction component is +-0: some slab tests can produce NaN
 };
 
 __device__ __forceinline__ TraceRay make_trace_ray(V3 o, V3 d) {
@@ -62,6 +63,7 @@ __device__ __forceinline__ TraceRay make_trace_ray(V3 o, V3 d) {
     r.neg[0] = r.inv.x < 0.f;
     r.neg[1] = r.inv.y < 0.f;
     r.neg[2] = r.inv.z < 0.f;
+    r.infInv = isinf(r.inv.x) || isinf(r.inv.y) || isinf(r.inv.z);
     return r;
 }
 
@@ -90,6 +92,25 @@ __device__ __forceinline__ bool box_entry(const TraceRay &r, float lox, float lo
     if (tzMax < tMaxX) tMaxX = tzMax;
     *tEntry = tMin;
     return tMaxX > 0.f;
+}
+
+// The same slab test without branches, for rays whose reciprocal direction is finite: the same
+// products, and max of the entries / min of the (widened) exits. For such rays every entry is at
+// most its own slab's exit unless that exit is negative, so "max entry <= min exit" is the
+// reference's pairwise tests and the results (accept, entry distance) are identical; rays with an
+// infinite reciprocal use box_entry (its NaN handling differs from fminf / fmaxf).
+__device__ __forceinline__ bool box_entry_nb(const TraceRay &r, float lox, float loy, float loz, float hix, float hiy,
+                                             float hiz, float *tEntry) {
+    float nx = r.neg[0] ? hix : lox, fx = r.neg[0] ? lox : hix;
+    float ny = r.neg[1] ? hiy : loy, fy = r.neg[1] ? loy : hiy;
+    float nz = r.neg[2] ? hiz : loz, fz = r.neg[2] ? loz : hiz;
+    float t0 = fmaxf(fmaxf(__fmul_rn(__fsub_rn(nx, r.o.x), r.inv.x), __fmul_rn(__fsub_rn(ny, r.o.y), r.inv.y)),
+                     __fmul_rn(__fsub_rn(nz, r.o.z), r.inv.z));
+    float t1 = fminf(fminf(__fmul_rn(__fmul_rn(__fsub_rn(fx, r.o.x), r.inv.x), kWiden),
+                           __fmul_rn(__fmul_rn(__fsub_rn(fy, r.o.y), r.inv.y), kWiden)),
+                     __fmul_rn(__fmul_rn(__fsub_rn(fz, r.o.z), r.inv.z), kWiden));
+    *tEntry = t0;
+    return t0 <= t1 && t1 > 0.f;
 }
 
 // Möller-Trumbore in the reference's exact operation order (shape.cpp:202-222).
@@ -341,10 +362,17 @@ __device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, 
         const int4 ch = __ldg(&n->child);
         float t0, t1, t2, t3;
         const float inf = __int_as_float(0x7f800000);
-        t0 = box_entry(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, &t0) && t0 < s.tMax ? t0 : inf;
-        t1 = box_entry(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, &t1) && t1 < s.tMax ? t1 : inf;
-        t2 = box_entry(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, &t2) && t2 < s.tMax ? t2 : inf;
-        t3 = box_entry(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, &t3) && t3 < s.tMax ? t3 : inf;
+        if (!r.infInv) {
+            t0 = box_entry_nb(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, &t0) && t0 < s.tMax ? t0 : inf;
+            t1 = box_entry_nb(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, &t1) && t1 < s.tMax ? t1 : inf;
+            t2 = box_entry_nb(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, &t2) && t2 < s.tMax ? t2 : inf;
+            t3 = box_entry_nb(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, &t3) && t3 < s.tMax ? t3 : inf;
+        } else {
+            t0 = box_entry(r, lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, &t0) && t0 < s.tMax ? t0 : inf;
+            t1 = box_entry(r, lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, &t1) && t1 < s.tMax ? t1 : inf;
+            t2 = box_entry(r, lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, &t2) && t2 < s.tMax ? t2 : inf;
+            t3 = box_entry(r, lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, &t3) && t3 < s.tMax ? t3 : inf;
+        }
         int r0 = ch.x, r1 = ch.y, r2 = ch.z, r3 = ch.w;
         // Sorting network for 4 (5 compare-exchanges); misses sort last at +inf.
         cswap(t0, r0, t1, r1);
