@@ -57,6 +57,16 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
                         4 * sizeof(float), 65536);
     }
     if (ext && ext->sun) h = fnv_v(h, *ext->sun);
+    if (ext && ext->textures && ext->textureCount > 0) {
+        for (int32_t k = 0; k < ext->textureCount; ++k) {
+            const prgpu::ImageTextureDesc &t = ext->textures[k];
+            h = fnv_v(h, t);
+            h = sample_hash(h, t.rgb, size_t(std::max(0, t.width)) * size_t(std::max(0, t.height)), 3 * sizeof(float), 65536);
+        }
+        if (ext->materialTextures && ext->materialTextureCount > 0)
+            h = fnv(h, ext->materialTextures, size_t(ext->materialTextureCount) * sizeof(prgpu::MaterialTextures));
+        h = fnv_v(h, ext->rgbToSpectrum);
+    }
     if (ext && ext->deltaLights && ext->deltaLightCount > 0)
         for (int32_t k = 0; k < ext->deltaLightCount; ++k) {
             const prgpu::DeltaLightDesc &l = ext->deltaLights[k];
@@ -118,6 +128,20 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
             return fail("bad sun cone or pmf");
         float l2 = u.direction.x * u.direction.x + u.direction.y * u.direction.y + u.direction.z * u.direction.z;
         if (!(l2 > 0.f) || !std::isfinite(l2)) return fail("bad sun direction");
+    }
+    if (ext && (ext->textureCount < 0 || ext->textureCount > 65536 || (ext->textureCount > 0 && !ext->textures) ||
+                (ext->materialTextureCount != 0 && ext->materialTextureCount != sd->materialCount) ||
+                (ext->materialTextureCount > 0 && !ext->materialTextures)))
+        return fail("bad texture tables");
+    for (int32_t k = 0; ext && k < ext->textureCount; ++k) {
+        const prgpu::ImageTextureDesc &t = ext->textures[k];
+        if (t.width <= 0 || t.height <= 0 || int64_t(t.width) * t.height > (int64_t(1) << 28) || !t.rgb || t.wrap > 2)
+            return fail("bad image texture");
+    }
+    for (int32_t i = 0; ext && i < ext->materialTextureCount; ++i) {
+        const int32_t r = ext->materialTextures[i].reflectance;
+        if (r < -1 || r >= ext->textureCount) return fail("material texture index out of range");
+        if (r >= 0 && !ext->rgbToSpectrum) return fail("textured materials need the RGB -> spectrum table");
     }
     if (ext && (ext->deltaLightCount < 0 || ext->deltaLightCount > 4096 || (ext->deltaLightCount > 0 && !ext->deltaLights)))
         return fail("bad delta light count or table");
@@ -286,6 +310,51 @@ static std::vector<float> macro_majorants(const float *d, int nx, int ny, int nz
     return az;
 }
 
+// Image textures: the descriptors, their texels concatenated, the per-material indices and the
+// RGB -> spectrum table.
+void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d, cudaStream_t s) {
+    d.textures = nullptr;
+    d.matTex = nullptr;
+    d.rgbZ = d.rgbCoeffs = nullptr;
+    d.texCount = 0;
+    const int32_t n = ext && ext->textures ? ext->textureCount : 0;
+    const int32_t nm = ext && ext->materialTextures ? ext->materialTextureCount : 0;
+    bool used = false;
+    for (int32_t i = 0; i < nm; ++i) used = used || ext->materialTextures[i].reflectance >= 0;
+    if (n <= 0 || !used) return;
+    size_t total = 0;
+    for (int32_t k = 0; k < n; ++k) total += size_t(ext->textures[k].width) * ext->textures[k].height * 3;
+    cache.texData.ensure(total * sizeof(float));
+    std::vector<DevTex> t(static_cast<size_t>(n));
+    size_t off = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        const prgpu::ImageTextureDesc &x = ext->textures[k];
+        const size_t m = size_t(x.width) * x.height * 3;
+        PRB_CUDA(cudaMemcpyAsync(cache.texData.as<float>() + off, x.rgb, m * sizeof(float), cudaMemcpyHostToDevice, s));
+        DevTex &g = t[size_t(k)];
+        g.w = x.width;
+        g.h = x.height;
+        g.rgb = cache.texData.as<float>() + off;
+        g.wrap = int(x.wrap);
+        g.flipV = x.flipV ? 1 : 0;
+        g.su = x.scaleU, g.sv = x.scaleV, g.ou = x.offsetU, g.ov = x.offsetV;
+        g.scale[0] = x.rgbScale[0], g.scale[1] = x.rgbScale[1], g.scale[2] = x.rgbScale[2];
+        off += m;
+    }
+    std::vector<int> mt(static_cast<size_t>(nm));
+    for (int32_t i = 0; i < nm; ++i) mt[size_t(i)] = ext->materialTextures[i].reflectance;
+    put(cache.textures, t.data(), t.size(), s);
+    put(cache.matTex, mt.data(), mt.size(), s);
+    const size_t tableFloats = 64 + size_t(3) * 64 * 64 * 64 * 3;
+    put(cache.rgbTable, ext->rgbToSpectrum, tableFloats, s);
+    PRB_CUDA(cudaStreamSynchronize(s));
+    d.textures = cache.textures.as<DevTex>();
+    d.matTex = cache.matTex.as<int>();
+    d.rgbZ = cache.rgbTable.as<float>();
+    d.rgbCoeffs = d.rgbZ + 64;
+    d.texCount = n;
+}
+
 // Spot, distant and goniometric lights: the descriptor table and the profiles, concatenated.
 void upload_deltas(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d, cudaStream_t s) {
     d.deltas = nullptr;
@@ -354,6 +423,7 @@ void upload_env(const prgpu::SceneExt *ext, const prgpu::SceneDesc *sd, SceneCac
         d.sun.pmf = u.pmf;
     }
     upload_deltas(ext, cache, d, s);
+    upload_textures(ext, cache, d, s);
     if (!(ext && ext->envMap)) return;
     const prgpu::EnvMapDesc &e = *ext->envMap;
     const int w = e.width, h = e.height;

@@ -76,6 +76,15 @@ struct DevDelta {
     const float *profile;    // vAngles[nV], hAngles[nH], candela[nH][nV]
 };
 
+// An image texture on the device (prgpu::ImageTextureDesc).
+struct DevTex {
+    int w, h;
+    const float *rgb;
+    int wrap, flipV;
+    float su, sv, ou, ov;
+    float scale[3];
+};
+
 struct DevScene {
     const WNode *nodes;
     const QNode *qnodes;   // the 4-wide collapse of the same tree
@@ -119,6 +128,11 @@ struct DevScene {
     DevSun sun;
     const DevDelta *deltas;
     int deltaCount;
+    // Image textures: per material the reflectance texture (-1 none), and the RGB uplift table.
+    const DevTex *textures;
+    const int *matTex;
+    const float *rgbZ, *rgbCoeffs;
+    int texCount;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).
     int maxDepth;            // <= 0: unlimited
     float clampY;            // 0: off
@@ -130,7 +144,7 @@ struct SceneCache {
     bool valid = false;
     DeviceAccel accel;
     DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
-        envDist, walls, sheen, deltas, deltaProfiles;
+        envDist, walls, sheen, deltas, deltaProfiles, textures, texData, matTex, rgbTable;
     DevScene ds{};
     bool hasSpheres = false;
     int wallCount = 0;
@@ -155,6 +169,10 @@ struct SceneCache {
         sheen.release();
         deltas.release();
         deltaProfiles.release();
+        textures.release();
+        texData.release();
+        matTex.release();
+        rgbTable.release();
         valid = false;
     }
 };

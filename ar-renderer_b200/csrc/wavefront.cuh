@@ -242,6 +242,91 @@ __device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, 
     return l;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Image textures (pr::ImageData::Lookup / ImageSpectrumTexture::Evaluate, texture.cpp:8-53) and the
+// albedo uplift through the RGB -> spectrum table (RGBToSpectrumTable, rgb2spec.cpp:278-305).
+
+__device__ __forceinline__ int tex_wrap(int v, int n, int mode) {
+    if (mode == prgpu::WrapClamp) return min(max(v, 0), n - 1);
+    if (mode == prgpu::WrapMirror) {
+        int period = 2 * n;
+        v %= period;
+        if (v < 0) v += period;
+        return v < n ? v : period - 1 - v;
+    }
+    v %= n;
+    return v < 0 ? v + n : v;
+}
+
+__device__ void tex_rgb(const DevTex &t, float u, float v, float rgb[3]) {
+    u = u * t.su + t.ou;
+    v = v * t.sv + t.ov;
+    if (t.flipV) v = 1.f - v;
+    float x = u * t.w - 0.5f, y = v * t.h - 0.5f;
+    int x0 = int(floorf(x)), y0 = int(floorf(y));
+    float dx = x - x0, dy = y - y0;
+    int xa = tex_wrap(x0, t.w, t.wrap), xb = tex_wrap(x0 + 1, t.w, t.wrap);
+    int ya = tex_wrap(y0, t.h, t.wrap), yb = tex_wrap(y0 + 1, t.h, t.wrap);
+    const float *a = t.rgb + 3 * (size_t(ya) * t.w + xa), *b = t.rgb + 3 * (size_t(ya) * t.w + xb);
+    const float *c = t.rgb + 3 * (size_t(yb) * t.w + xa), *d = t.rgb + 3 * (size_t(yb) * t.w + xb);
+    for (int i = 0; i < 3; ++i)
+        rgb[i] = ((1.f - dx) * (1.f - dy) * __ldg(a + i) + dx * (1.f - dy) * __ldg(b + i) + (1.f - dx) * dy * __ldg(c + i) +
+                  dx * dy * __ldg(d + i)) * t.scale[i];
+}
+
+// Sigmoid-polynomial reflectance of an sRGB triple at the 4 wavelengths (RGBAlbedoSpectrum).
+__device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lambda &lam) {
+    float rgb[3] = {clampf(r, 0.f, 1.f), clampf(g, 0.f, 1.f), clampf(b, 0.f, 1.f)};
+    float c[3];
+    if (rgb[0] == rgb[1] && rgb[1] == rgb[2]) {
+        const float v = rgb[0], inf = __int_as_float(0x7f800000);
+        c[0] = c[1] = 0.f;
+        c[2] = v <= 0.f ? -inf : (v >= 1.f ? inf : (v - .5f) / sqrtf(v * (1.f - v)));
+    } else {
+        const int res = 64;
+        int maxc = (rgb[0] > rgb[1]) ? ((rgb[0] > rgb[2]) ? 0 : 2) : ((rgb[1] > rgb[2]) ? 1 : 2);
+        float z = rgb[maxc];
+        float x = rgb[(maxc + 1) % 3] * (res - 1) / z, y = rgb[(maxc + 2) % 3] * (res - 1) / z;
+        int xi = min(int(x), res - 2), yi = min(int(y), res - 2);
+        int lo = 0, hi = res - 1;  // largest zi in [0, res - 2] with zNodes[zi] < z
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (__ldg(s.rgbZ + mid) < z) lo = mid;
+            else hi = mid;
+        }
+        int zi = min(lo, res - 2);
+        float z0 = __ldg(s.rgbZ + zi), z1 = __ldg(s.rgbZ + zi + 1);
+        float dx = x - xi, dy = y - yi, dz = (z - z0) / (z1 - z0);
+        auto co = [&](int zz, int yy, int xx, int i) {
+            return __ldg(s.rgbCoeffs + 3 * (((size_t(maxc) * res + zz) * res + yy) * res + xx) + i);
+        };
+        auto lerp = [](float t, float a, float b2) { return (1.f - t) * a + t * b2; };
+        for (int i = 0; i < 3; ++i)
+            c[i] = lerp(dz, lerp(dy, lerp(dx, co(zi, yi, xi, i), co(zi, yi, xi + 1, i)),
+                                 lerp(dx, co(zi, yi + 1, xi, i), co(zi, yi + 1, xi + 1, i))),
+                        lerp(dy, lerp(dx, co(zi + 1, yi, xi, i), co(zi + 1, yi, xi + 1, i)),
+                             lerp(dx, co(zi + 1, yi + 1, xi, i), co(zi + 1, yi + 1, xi + 1, i))));
+    }
+    SS out;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float xv = fmaf(lam.l[i], fmaf(lam.l[i], c[0], c[1]), c[2]);
+        out.v[i] = isinf(xv) ? (xv > 0.f ? 1.f : 0.f) : 0.5f + xv / (2.f * sqrtf(1.f + xv * xv));
+    }
+    return out;
+}
+
+// The reflectance of material index mi from its image texture, when it has one.
+__device__ __forceinline__ bool textured_albedo(const DevScene &s, int mi, float u, float v, const Lambda &lam, SS *R) {
+    if (s.texCount <= 0 || !s.matTex) return false;
+    const int t = __ldg(s.matTex + mi);
+    if (t < 0) return false;
+    float rgb[3];
+    tex_rgb(s.textures[t], u, v, rgb);
+    *R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
+    return true;
+}
+
 // True for the materials shaded through FullBsdf: coats and anything with a sheen lobe.
 __device__ __forceinline__ bool full_material(const prgpu::Material &m) {
     return m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor ||
@@ -858,7 +943,7 @@ struct ShadeArgs {
 // (kFull = false) defers paths that reach a coated or sheen surface, after their free flight and
 // emission, to the fullQ queue; the kFull pass shades those surfaces. Keeping the layered code out
 // of the main pass keeps its register allocation that of the plain materials. kDelta: the scene has
-// spot / distant / goniometric lights.
+// spot / distant / goniometric lights or image textures (their code is instantiated only then).
 template <bool kBatch = false, bool kGuide = false, bool kFull = false, bool kDelta = false>
 __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
@@ -1137,6 +1222,11 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     // proportional sampling pdf takes the estimated density for MIS (path.cpp:219).
                     FullBsdf fb;
                     make_full(s, m, sf.u, sf.v, lam, &fb);
+                    if constexpr (kDelta) {
+                        Lobe &base = fb.layered ? fb.lay.bottom : fb.base;
+                        if (!fb.black && base.kind == kLobeDiffuse)
+                            textured_albedo(s, int(&m - s.mats), sf.u, sf.v, lam, &base.R);
+                    }
                     if (full_non_specular(fb))
                         nee(sf.p, sf.n, nullptr, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr, &fb);
                     float uc = rng.uniform(), u0 = rng.uniform(), u1 = rng.uniform();
@@ -1147,6 +1237,8 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
                 } else {
                 Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
+                if constexpr (kDelta)
+                    if (lobe.kind == kLobeDiffuse) textured_albedo(s, int(&m - s.mats), sf.u, sf.v, lam, &lobe.R);
                 if constexpr (kGuide) {
                     GuideMix gm;
                     // The guide is trained on, and applied at, the first kGuideVertices diffuse

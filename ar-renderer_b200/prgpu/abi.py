@@ -131,12 +131,26 @@ class DeltaLightDesc(C.Structure):
                 ("pad", C.c_int32), ("profile", C.c_void_p)]
 
 
+WRAP_REPEAT, WRAP_CLAMP, WRAP_MIRROR = range(3)
+
+
+class ImageTextureDesc(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("rgb", C.c_void_p), ("wrap", C.c_uint32),
+                ("flipV", C.c_uint32), ("scaleU", C.c_float), ("scaleV", C.c_float), ("offsetU", C.c_float),
+                ("offsetV", C.c_float), ("rgbScale", C.c_float * 3), ("pad", C.c_uint32)]
+
+
+class MaterialTextures(C.Structure):
+    _fields_ = [("reflectance", C.c_int32), ("pad", C.c_int32)]
+
+
 class SceneExt(C.Structure):
     _fields_ = [("structSize", C.c_uint32), ("lightBVHNodeCount", C.c_int32), ("lightBVH", C.c_void_p),
                 ("lightBVHProb", C.c_float), ("wavefrontPaths", C.c_int32), ("blockSize", C.c_int32),
                 ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p),
                 ("envMap", C.c_void_p), ("sun", C.c_void_p), ("deltaLightCount", C.c_int32), ("pad", C.c_int32),
-                ("deltaLights", C.c_void_p)]
+                ("deltaLights", C.c_void_p), ("textureCount", C.c_int32), ("materialTextureCount", C.c_int32),
+                ("textures", C.c_void_p), ("materialTextures", C.c_void_p), ("rgbToSpectrum", C.c_void_p)]
 
 
 class BatchItem(C.Structure):
@@ -174,7 +188,8 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 80 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 112 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 8
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72

@@ -53,12 +53,16 @@ GUIDE_SAMPLE, GUIDE_TRAIN, GUIDE_RESET = 1, 2, 4
 
 
 def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
-             block_size: int = 0, grid_media=None, guide: int = 0, delta_lights=None) -> abi.SceneExt:
+             block_size: int = 0, grid_media=None, guide: int = 0, delta_lights=None, textures=None,
+             material_textures=None, rgb_to_spectrum: np.ndarray | None = None) -> abi.SceneExt:
     """SceneExt for prgpu_render_ex. grid_media: GridMediumDesc records (media.grid_desc), indexed
     after the SceneDesc's homogeneous media. guide: GUIDE_SAMPLE (sample diffuse vertices with the
     guide network), GUIDE_TRAIN (train it online, one Adam step per wavefront chunk), GUIDE_RESET
-    (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric). The
-    record keeps the arrays it points at alive."""
+    (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric).
+    textures / material_textures / rgb_to_spectrum: image textures (image_texture), the
+    reflectance texture index of each SceneDesc material (-1 none) and the RGB -> spectrum table
+    (zNodes[64] then coefficients[3][64][64][64][3]). The record keeps the arrays it points at
+    alive."""
     e = abi.SceneExt()
     e.structSize = C.sizeof(abi.SceneExt)
     if light_bvh is not None and len(light_bvh):
@@ -80,7 +84,41 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
         e.deltaLightCount = len(arr)
         e.deltaLights = C.cast(arr, C.c_void_p)
         e._keep += [arr, delta_lights]
+    if textures:
+        arr = (abi.ImageTextureDesc * len(textures))(*textures)
+        e.textureCount = len(arr)
+        e.textures = C.cast(arr, C.c_void_p)
+        e._keep += [arr, textures]
+    if material_textures is not None:
+        mt = (abi.MaterialTextures * len(material_textures))()
+        for i, t in enumerate(material_textures):
+            mt[i].reflectance = t
+        e.materialTextureCount = len(mt)
+        e.materialTextures = C.cast(mt, C.c_void_p)
+        e._keep.append(mt)
+    if rgb_to_spectrum is not None:
+        table = np.ascontiguousarray(rgb_to_spectrum, np.float32)
+        assert table.size == 64 + 3 * 64 ** 3 * 3
+        e.rgbToSpectrum = table.ctypes.data
+        e._keep.append(table)
     return e
+
+
+def image_texture(rgb: np.ndarray, wrap: int = abi.WRAP_REPEAT, flip_v: bool = True, uv_scale=(1.0, 1.0),
+                  uv_offset=(0.0, 0.0), multiplier=(1.0, 1.0, 1.0)) -> abi.ImageTextureDesc:
+    """An ImageTextureDesc over rgb ((height, width, 3) float32 linear, row 0 first; kept alive by
+    the record)."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    t = abi.ImageTextureDesc()
+    t.height, t.width = img.shape[0], img.shape[1]
+    t.rgb = img.ctypes.data
+    t.wrap, t.flipV = wrap, 1 if flip_v else 0
+    t.scaleU, t.scaleV = float(uv_scale[0]), float(uv_scale[1])
+    t.offsetU, t.offsetV = float(uv_offset[0]), float(uv_offset[1])
+    for i in range(3):
+        t.rgbScale[i] = float(multiplier[i])
+    t._keep = img
+    return t
 
 
 def render_batch(items, config: abi.BatchConfig | None = None, stats: bool = False, device: int = 0):

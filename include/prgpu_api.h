@@ -265,6 +265,27 @@ struct DeltaLightDesc {
     const float *profile;    // goniometric: vAngles[nV], hAngles[nH] (degrees), candela[nH][nV] / peak
 };
 
+// An RGB image texture (pr::ImageData + pr::ImageSpectrumTexture, src/materials/texture.h:60-105,
+// texture.cpp:8-53): bilinear lookup with a wrap mode, the UV mapping, an RGB scale, and the
+// albedo uplift of the looked-up colour through the RGB -> spectrum table.
+enum TextureWrap : uint32_t { WrapRepeat = 0, WrapClamp = 1, WrapMirror = 2 };
+struct ImageTextureDesc {
+    int32_t width, height;
+    const float *rgb;        // width * height * 3 linear RGB, row 0 first (pr::Image)
+    uint32_t wrap;           // TextureWrap
+    uint32_t flipV;          // look up at v' = 1 - v
+    float scaleU, scaleV, offsetU, offsetV;  // pr::UVMapping
+    float rgbScale[3];
+    uint32_t pad;
+};
+
+// Per SceneDesc material: the image texture of its reflectance (diffuse and coated diffuse
+// materials), -1 for none.
+struct MaterialTextures {
+    int32_t reflectance;
+    int32_t pad;
+};
+
 struct SceneExt {
     uint32_t structSize;
     int32_t lightBVHNodeCount;      // 0 = power-based light selection (the v4 behaviour)
@@ -282,6 +303,13 @@ struct SceneExt {
     int32_t deltaLightCount;
     int32_t pad;
     const DeltaLightDesc *deltaLights;
+    int32_t textureCount;
+    int32_t materialTextureCount;   // 0, or SceneDesc::materialCount
+    const ImageTextureDesc *textures;
+    const MaterialTextures *materialTextures;
+    // RGB -> sigmoid-polynomial table (pr::RGBToSpectrumTable, rgb2spec.h:28-46): zNodes[64] then
+    // coefficients[3][64][64][64][3]; required when a material has a texture.
+    const float *rgbToSpectrum;
 };
 
 // Parameters of prgpu_render_aov (pr::RenderAOV, src/integrators/aov.h:10-21).

@@ -1,0 +1,119 @@
+"""Image reflectance textures on the GPU against the reference PathIntegrator (pr::ImageData lookup
+and ImageSpectrumTexture with the albedo uplift through pr::RGBToSpectrumTable:
+src/materials/texture.cpp:8-53, src/core/rgb2spec.cpp:278-305): an outdoor scene whose ground is a
+diffuse quad textured by a colour image (repeat wrap, UV scale and offset, an RGB multiplier) and
+one sphere with a coated diffuse textured material, from one scene file. The reference loads the
+image; the module gets the same texels, the material -> texture table and the reference's own
+uplift table (the file its RGBToSpectrumTable caches beside the oracle library)."""
+
+import json
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import render_util as ru
+from prgpu import abi, render
+
+pytestmark = pytest.mark.gpu
+
+
+def _uplift_table():
+    import ref as oracle_ref
+
+    oracle_ref.ref_lib()  # builds the table (cached) on first load
+    path = os.path.join(oracle_ref.REF_DIR, "prender_rgb2spec_srgb_v1.bin")
+    raw = np.fromfile(path, np.uint8)
+    res = int(raw[8:12].view(np.int32)[0])
+    assert res == 64
+    return raw[12:].view(np.float32).copy()
+
+
+def _texture():
+    h, w = 24, 32
+    v, u = np.meshgrid((np.arange(h) + 0.5) / h, (np.arange(w) + 0.5) / w, indexing="ij")
+    img = np.zeros((h, w, 3), np.float32)
+    check = ((np.floor(u * 4) + np.floor(v * 3)) % 2).astype(np.float32)
+    img[..., 0] = 0.15 + 0.75 * check * u
+    img[..., 1] = 0.2 + 0.6 * (1 - check) * v
+    img[..., 2] = 0.1 + 0.5 * (u * v)
+    return img
+
+
+def _write_pfm(path, img):
+    h, w, _ = img.shape
+    with open(path, "wb") as f:
+        f.write(f"PF\n{w} {h}\n-1.0\n".encode())
+        f.write(np.ascontiguousarray(img[::-1], dtype="<f4").tobytes())
+
+
+def test_image_textures_agree_with_reference(gpu, oracle):
+    """48 x 32, depth 6: per-pixel z of the mean over 16 renders of 256 spp each side, |z| < 4 on
+    >= 99.5 % of values; mean luminance within 4 standard errors."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    img = _texture()
+    pfm = os.path.join(d, "ground_tex.pfm")
+    _write_pfm(pfm, img)
+    doc = ru_outdoor_doc(w, h, pfm)
+    path = os.path.join(d, "textures.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    desc = rs.export()
+    sd = abi.SceneDesc.from_address(desc)
+    names = list(doc["materials"])
+    # The exported material order follows first use by the objects (ground, then the spheres).
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    assert sd.materialCount == len(used), (sd.materialCount, used)
+    tex_of = {"ground": 0, "tex_coat": 1}
+    mat_tex = [tex_of.get(n, -1) for n in used]
+    textures = [render.image_texture(img, uv_scale=(3.0, 2.0), uv_offset=(0.25, 0.1), multiplier=(1.0, 0.9, 1.1)),
+                render.image_texture(img, wrap=abi.WRAP_MIRROR, uv_scale=(2.0, 2.0))]
+    ext = render.make_ext(textures=textures, material_textures=mat_tex, rgb_to_spectrum=_uplift_table())
+    g = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"textures: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    # The textures matter: without them the module renders the exporter's average colours.
+    flat = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.9
+
+
+def ru_outdoor_doc(w, h, pfm):
+    """Ground quad (UVs 0..1) with the image texture, a plain sphere, a coated diffuse sphere with a
+    mirrored-wrap texture, lit by a constant sky and a distant-free point light."""
+    return {
+        "textures": {"groundtex": {"type": "image", "file": pfm, "colorspace": "linear", "wrap": "repeat",
+                                   "flip_v": True, "uv_scale": [3.0, 2.0], "uv_offset": [0.25, 0.1],
+                                   "multiplier": [1.0, 0.9, 1.1]},
+                     "coattex": {"type": "image", "file": pfm, "colorspace": "linear", "wrap": "mirror",
+                                 "flip_v": True, "uv_scale": [2.0, 2.0]}},
+        "materials": {"ground": {"type": "diffuse", "reflectance": {"texture": "groundtex"}},
+                      "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+                      "tex_coat": {"type": "coated_diffuse", "reflectance": {"texture": "coattex"},
+                                   "coat_roughness": 0.1}},
+        "media": {},
+        "geometry": {"ground": {"type": "mesh", "positions": [-3, 0, -3, -3, 0, 3, 3, 0, 3, 3, 0, -3],
+                                "uvs": [0, 0, 0, 1, 1, 1, 1, 0], "indices": [0, 1, 2, 0, 2, 3]},
+                     "s0": {"type": "sphere", "center": [-0.8, 0.5, 0], "radius": 0.5},
+                     "s1": {"type": "sphere", "center": [0.8, 0.5, 0.2], "radius": 0.5}},
+        "objects": [{"name": "ground", "geometry": "ground", "material": "ground"},
+                    {"name": "s0", "geometry": "s0", "material": "red"},
+                    {"name": "s1", "geometry": "s1", "material": "tex_coat"}],
+        "lights": {"sky": {"type": "environment", "color": [0.6, 0.7, 0.9], "intensity": 1.0},
+                   "lamp": {"type": "point", "position": [0.5, 2.5, 1.5], "intensity": 3.0, "temperature": 4500}},
+        "cameras": {"cam": {"type": "pinhole", "position": [0, 1.8, 3.5], "look_at": [0, 0.2, 0], "fov_y": 50}},
+        "render": {"camera": "cam", "seed": 0, "film": {"width": w, "height": h, "filter": "box"},
+                   "integrator": {"type": "path", "spp": 16, "max_depth": 6}},
+    }
