@@ -139,9 +139,11 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
             return fail("bad image texture");
     }
     for (int32_t i = 0; ext && i < ext->materialTextureCount; ++i) {
-        const int32_t r = ext->materialTextures[i].reflectance;
-        if (r < -1 || r >= ext->textureCount) return fail("material texture index out of range");
+        const int32_t r = ext->materialTextures[i].reflectance, nmap = ext->materialTextures[i].normalMap;
+        if (r < -1 || r >= ext->textureCount || nmap < -1 || nmap >= ext->textureCount)
+            return fail("material texture index out of range");
         if (r >= 0 && !ext->rgbToSpectrum) return fail("textured materials need the RGB -> spectrum table");
+        if (!std::isfinite(ext->materialTextures[i].normalStrength)) return fail("bad normal map strength");
     }
     if (ext && (ext->deltaLightCount < 0 || ext->deltaLightCount > 4096 || (ext->deltaLightCount > 0 && !ext->deltaLights)))
         return fail("bad delta light count or table");
@@ -320,7 +322,8 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
     const int32_t n = ext && ext->textures ? ext->textureCount : 0;
     const int32_t nm = ext && ext->materialTextures ? ext->materialTextureCount : 0;
     bool used = false;
-    for (int32_t i = 0; i < nm; ++i) used = used || ext->materialTextures[i].reflectance >= 0;
+    for (int32_t i = 0; i < nm; ++i)
+        used = used || ext->materialTextures[i].reflectance >= 0 || ext->materialTextures[i].normalMap >= 0;
     if (n <= 0 || !used) return;
     size_t total = 0;
     for (int32_t k = 0; k < n; ++k) total += size_t(ext->textures[k].width) * ext->textures[k].height * 3;
@@ -341,17 +344,24 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         g.scale[0] = x.rgbScale[0], g.scale[1] = x.rgbScale[1], g.scale[2] = x.rgbScale[2];
         off += m;
     }
-    std::vector<int> mt(static_cast<size_t>(nm));
-    for (int32_t i = 0; i < nm; ++i) mt[size_t(i)] = ext->materialTextures[i].reflectance;
+    std::vector<int4> mt(static_cast<size_t>(nm));
+    for (int32_t i = 0; i < nm; ++i) {
+        const prgpu::MaterialTextures &x = ext->materialTextures[i];
+        int sbits;
+        std::memcpy(&sbits, &x.normalStrength, sizeof(sbits));
+        mt[size_t(i)] = make_int4(x.reflectance, x.normalMap, sbits, x.normalFlipGreen ? 1 : 0);
+    }
     put(cache.textures, t.data(), t.size(), s);
     put(cache.matTex, mt.data(), mt.size(), s);
-    const size_t tableFloats = 64 + size_t(3) * 64 * 64 * 64 * 3;
-    put(cache.rgbTable, ext->rgbToSpectrum, tableFloats, s);
+    if (ext->rgbToSpectrum) {
+        const size_t tableFloats = 64 + size_t(3) * 64 * 64 * 64 * 3;
+        put(cache.rgbTable, ext->rgbToSpectrum, tableFloats, s);
+    }
     PRB_CUDA(cudaStreamSynchronize(s));
     d.textures = cache.textures.as<DevTex>();
-    d.matTex = cache.matTex.as<int>();
-    d.rgbZ = cache.rgbTable.as<float>();
-    d.rgbCoeffs = d.rgbZ + 64;
+    d.matTex = cache.matTex.as<int4>();
+    d.rgbZ = ext->rgbToSpectrum ? cache.rgbTable.as<float>() : nullptr;
+    d.rgbCoeffs = d.rgbZ ? d.rgbZ + 64 : nullptr;
     d.texCount = n;
 }
 

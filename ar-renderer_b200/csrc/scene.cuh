@@ -130,7 +130,7 @@ struct DevScene {
     int deltaCount;
     // Image textures: per material the reflectance texture (-1 none), and the RGB uplift table.
     const DevTex *textures;
-    const int *matTex;
+    const int4 *matTex;  // per material: reflectance texture, normal map, strength (float bits), flip green
     const float *rgbZ, *rgbCoeffs;
     int texCount;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).

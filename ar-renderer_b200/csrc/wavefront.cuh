@@ -319,12 +319,50 @@ __device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lam
 // The reflectance of material index mi from its image texture, when it has one.
 __device__ __forceinline__ bool textured_albedo(const DevScene &s, int mi, float u, float v, const Lambda &lam, SS *R) {
     if (s.texCount <= 0 || !s.matTex) return false;
-    const int t = __ldg(s.matTex + mi);
+    const int t = s.matTex[mi].x;
     if (t < 0) return false;
     float rgb[3];
     tex_rgb(s.textures[t], u, v, rgb);
     *R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
     return true;
+}
+
+// Tangent-space normal map of material index mi (Material::PerturbShading, material.cpp:41-60):
+// the map's colour as a direction in the frame of the shading dpdu and normal (the bitangent along
+// dp/dv), scaled in the tangent plane, kept in the geometric hemisphere; dpdu follows it.
+__device__ void normal_map(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
+    if (s.texCount <= 0 || !s.matTex) return;
+    const int4 mt = s.matTex[mi];
+    if (mt.y < 0) return;
+    float c[3];
+    tex_rgb(s.textures[mt.y], sf->u, sf->v, c);
+    const float strength = __int_as_float(mt.z);
+    V3 t = mk(2.f * c[0] - 1.f, 2.f * c[1] - 1.f, 2.f * c[2] - 1.f);
+    t.x *= strength;
+    t.y *= mt.w ? -strength : strength;
+    // dp/dv of the parameterization (Sphere / Triangle::Intersect, shape.cpp:75-82, 238-251).
+    V3 dpdv;
+    if (pr.type == prgpu::PrimSphere) {
+        V3 rel = sf->p - f3(pr.p0);
+        float cosT = clampf(rel.y / pr.r, -1.f, 1.f), sinT = safe_sqrt(1.f - cosT * cosT);
+        dpdv = sinT > 1e-6f ? mk(cosT * rel.x / sinT, -pr.r * sinT, cosT * rel.z / sinT) * kPi : mk(0.f, 0.f, 0.f);
+        if (len2(dpdv) < 1e-12f) dpdv = frame_from_z(sf->n).y;
+    } else {
+        V3 p0 = f3(pr.p0), p1 = f3(pr.p1), p2 = f3(pr.p2);
+        float du02 = pr.u0 - pr.u2, du12 = pr.u1 - pr.u2, dv02 = pr.v0 - pr.v2, dv12 = pr.v1 - pr.v2;
+        float det = du02 * dv12 - dv02 * du12;
+        dpdv = fabsf(det) < 1e-9f ? frame_from_z(sf->n).y : ((p1 - p2) * du02 - (p0 - p2) * du12) * (1.f / det);
+        if (!isfinite(dpdv.x)) dpdv = frame_from_z(sf->n).y;
+    }
+    Frame f = frame_from_xz(sf->dpdu, sf->ns);
+    if (dot(f.y, dpdv) < 0.f) f.y = -f.y;
+    V3 n = f.x * t.x + f.y * t.y + f.z * fmaxf(t.z, 1e-3f);
+    float l = len(n);
+    if (!(l > 0.f) || !isfinite(l)) return;
+    V3 ns = n * (1.f / l);
+    if (dot(ns, sf->n) < 0.f) ns = -ns;
+    sf->ns = ns;
+    sf->dpdu = sf->dpdu - ns * dot(sf->dpdu, ns);
 }
 
 // True for the materials shaded through FullBsdf: coats and anything with a sheen lobe.
@@ -1211,6 +1249,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 deferred = true;
             } else {
                 ++depth;
+                if constexpr (kDelta) normal_map(s, int(&m - s.mats), pr, &sf);
                 Frame fr = frame_from_xz(sf.dpdu, sf.ns);
                 V3 wo = -d;
                 V3 wol = fr.to_local(wo);

@@ -59,8 +59,9 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
     after the SceneDesc's homogeneous media. guide: GUIDE_SAMPLE (sample diffuse vertices with the
     guide network), GUIDE_TRAIN (train it online, one Adam step per wavefront chunk), GUIDE_RESET
     (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric).
-    textures / material_textures / rgb_to_spectrum: image textures (image_texture), the
-    reflectance texture index of each SceneDesc material (-1 none) and the RGB -> spectrum table
+    textures / material_textures / rgb_to_spectrum: image textures (image_texture), per SceneDesc
+    material its reflectance texture index (-1 none) or a tuple (reflectance, normal map,
+    strength, flip green), and the RGB -> spectrum table
     (zNodes[64] then coefficients[3][64][64][64][3]). The record keeps the arrays it points at
     alive."""
     e = abi.SceneExt()
@@ -92,7 +93,10 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
     if material_textures is not None:
         mt = (abi.MaterialTextures * len(material_textures))()
         for i, t in enumerate(material_textures):
-            mt[i].reflectance = t
+            # an int (reflectance texture) or (reflectance, normal map, strength, flip green)
+            r, nm, st, fg = (t, -1, 1.0, False) if isinstance(t, (int, np.integer)) else tuple(t)
+            mt[i].reflectance, mt[i].normalMap = int(r), int(nm)
+            mt[i].normalStrength, mt[i].normalFlipGreen = float(st), 1 if fg else 0
         e.materialTextureCount = len(mt)
         e.materialTextures = C.cast(mt, C.c_void_p)
         e._keep.append(mt)

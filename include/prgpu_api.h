@@ -280,10 +280,13 @@ struct ImageTextureDesc {
 };
 
 // Per SceneDesc material: the image texture of its reflectance (diffuse and coated diffuse
-// materials), -1 for none.
+// materials) and of its tangent-space normal map (any material; pr::NormalMapParams,
+// material.h:30-36, applied as Material::PerturbShading, material.cpp:41-60), -1 for none.
 struct MaterialTextures {
     int32_t reflectance;
-    int32_t pad;
+    int32_t normalMap;
+    float normalStrength;      // scales the map's tangent-plane components
+    uint32_t normalFlipGreen;  // the map's green channel points along -v
 };
 
 struct SceneExt {

@@ -117,3 +117,57 @@ def ru_outdoor_doc(w, h, pfm):
         "render": {"camera": "cam", "seed": 0, "film": {"width": w, "height": h, "filter": "box"},
                    "integrator": {"type": "path", "spp": 16, "max_depth": 6}},
     }
+
+
+def _normal_image():
+    h, w = 32, 32
+    v, u = np.meshgrid((np.arange(h) + 0.5) / h, (np.arange(w) + 0.5) / w, indexing="ij")
+    n = np.stack([0.6 * np.sin(2 * np.pi * 3 * u), 0.5 * np.cos(2 * np.pi * 2 * v), np.ones_like(u)], -1)
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    return ((n + 1) * 0.5).astype(np.float32)
+
+
+def test_normal_maps_agree_with_reference(gpu, oracle):
+    """A normal-mapped diffuse ground (strength 0.8) and a normal-mapped rough gold sphere (green
+    flipped, mirror wrap), lit by a point light and a constant sky: the same z statistics as above."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    nimg = _normal_image()
+    pfm = os.path.join(d, "normal_map.pfm")
+    _write_pfm(pfm, nimg)
+    doc = ru_outdoor_doc(w, h, pfm)
+    doc["textures"] = {"nmap": {"type": "image", "file": pfm, "colorspace": "linear", "wrap": "repeat",
+                                "flip_v": True, "uv_scale": [2.0, 2.0]},
+                       "nmap2": {"type": "image", "file": pfm, "colorspace": "linear", "wrap": "mirror",
+                                 "flip_v": True, "uv_scale": [3.0, 1.5]}}
+    doc["materials"] = {"ground": {"type": "diffuse", "reflectance": [0.6, 0.55, 0.5],
+                                   "normal_map": {"texture": "nmap", "strength": 0.8}},
+                        "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+                        "tex_coat": {"type": "conductor", "metal": "Au", "roughness": 0.35,
+                                     "normal_map": {"texture": "nmap2", "flip_green": True}}}
+    path = os.path.join(d, "normal_maps.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    desc = rs.export()
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    maps = {"ground": (-1, 0, 0.8, False), "tex_coat": (-1, 1, 1.0, True)}
+    mat_tex = [maps.get(n, (-1, -1, 1.0, False)) for n in used]
+    textures = [render.image_texture(nimg, uv_scale=(2.0, 2.0)),
+                render.image_texture(nimg, wrap=abi.WRAP_MIRROR, uv_scale=(3.0, 1.5))]
+    ext = render.make_ext(textures=textures, material_textures=mat_tex)
+    g = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"normal maps: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
