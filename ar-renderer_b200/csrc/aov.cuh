@@ -52,7 +52,7 @@ __device__ ChainEnd follow_chain(const DevScene &s, V3 o, V3 d, Hit h, bool thro
         const prgpu::Primitive &pr = s.prims[h.prim];
         const prgpu::Material &m = s.mats[pr.material];
         Surf sf = shade_point(s, pr, h.t, h.u, h.v, o, d);
-        normal_map(s, int(&m - s.mats), pr, &sf);
+        perturb_shading(s, int(&m - s.mats), pr, &sf);
         e.sf = sf;
         e.wo = -d;
         e.prim = h.prim;

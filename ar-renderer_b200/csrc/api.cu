@@ -66,7 +66,7 @@ static_assert(sizeof(prgpu::GridMediumDesc) == 112 && offsetof(prgpu::GridMedium
 static_assert(sizeof(prgpu::SceneExt) == 112 && offsetof(prgpu::SceneExt, gridMedia) == 40 &&
               offsetof(prgpu::SceneExt, sun) == 56 && offsetof(prgpu::SceneExt, deltaLights) == 72 &&
               offsetof(prgpu::SceneExt, rgbToSpectrum) == 104);
-static_assert(sizeof(prgpu::ImageTextureDesc) == 56 && sizeof(prgpu::MaterialTextures) == 16);
+static_assert(sizeof(prgpu::ImageTextureDesc) == 56 && sizeof(prgpu::MaterialTextures) == 32);
 static_assert(sizeof(prgpu::DeltaLightDesc) == 104 && offsetof(prgpu::DeltaLightDesc, frame) == 48 &&
               offsetof(prgpu::DeltaLightDesc, profile) == 96);
 static_assert(sizeof(prgpu::EnvMapDesc) == 32 && sizeof(prgpu::SunDesc) == 28);

@@ -140,8 +140,11 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
     }
     for (int32_t i = 0; ext && i < ext->materialTextureCount; ++i) {
         const int32_t r = ext->materialTextures[i].reflectance, nmap = ext->materialTextures[i].normalMap;
-        if (r < -1 || r >= ext->textureCount || nmap < -1 || nmap >= ext->textureCount)
+        const int32_t bmap = ext->materialTextures[i].bumpMap, bch = ext->materialTextures[i].bumpChannel;
+        if (r < -1 || r >= ext->textureCount || nmap < -1 || nmap >= ext->textureCount || bmap < -1 ||
+            bmap >= ext->textureCount || bch < -1 || bch > 2)
             return fail("material texture index out of range");
+        if (!std::isfinite(ext->materialTextures[i].bumpScale)) return fail("bad bump map scale");
         if (r >= 0 && !ext->rgbToSpectrum) return fail("textured materials need the RGB -> spectrum table");
         if (!std::isfinite(ext->materialTextures[i].normalStrength)) return fail("bad normal map strength");
     }
@@ -323,7 +326,8 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
     const int32_t nm = ext && ext->materialTextures ? ext->materialTextureCount : 0;
     bool used = false;
     for (int32_t i = 0; i < nm; ++i)
-        used = used || ext->materialTextures[i].reflectance >= 0 || ext->materialTextures[i].normalMap >= 0;
+        used = used || ext->materialTextures[i].reflectance >= 0 || ext->materialTextures[i].normalMap >= 0 ||
+               ext->materialTextures[i].bumpMap >= 0;
     if (n <= 0 || !used) return;
     size_t total = 0;
     for (int32_t k = 0; k < n; ++k) total += size_t(ext->textures[k].width) * ext->textures[k].height * 3;
@@ -344,12 +348,14 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         g.scale[0] = x.rgbScale[0], g.scale[1] = x.rgbScale[1], g.scale[2] = x.rgbScale[2];
         off += m;
     }
-    std::vector<int4> mt(static_cast<size_t>(nm));
+    std::vector<int4> mt(static_cast<size_t>(2 * nm));
     for (int32_t i = 0; i < nm; ++i) {
         const prgpu::MaterialTextures &x = ext->materialTextures[i];
-        int sbits;
+        int sbits, bbits;
         std::memcpy(&sbits, &x.normalStrength, sizeof(sbits));
-        mt[size_t(i)] = make_int4(x.reflectance, x.normalMap, sbits, x.normalFlipGreen ? 1 : 0);
+        std::memcpy(&bbits, &x.bumpScale, sizeof(bbits));
+        mt[size_t(2 * i)] = make_int4(x.reflectance, x.normalMap, sbits, x.normalFlipGreen ? 1 : 0);
+        mt[size_t(2 * i + 1)] = make_int4(x.bumpMap, x.bumpChannel, bbits, 0);
     }
     put(cache.textures, t.data(), t.size(), s);
     put(cache.matTex, mt.data(), mt.size(), s);

@@ -130,7 +130,9 @@ struct DevScene {
     int deltaCount;
     // Image textures: per material the reflectance texture (-1 none), and the RGB uplift table.
     const DevTex *textures;
-    const int4 *matTex;  // per material: reflectance texture, normal map, strength (float bits), flip green
+    // per material two entries: (reflectance texture, normal map, strength bits, flip green) and
+    // (bump map, channel, scale bits, 0)
+    const int4 *matTex;
     const float *rgbZ, *rgbCoeffs;
     int texCount;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).

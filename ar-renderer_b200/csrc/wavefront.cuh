@@ -319,7 +319,7 @@ __device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lam
 // The reflectance of material index mi from its image texture, when it has one.
 __device__ __forceinline__ bool textured_albedo(const DevScene &s, int mi, float u, float v, const Lambda &lam, SS *R) {
     if (s.texCount <= 0 || !s.matTex) return false;
-    const int t = s.matTex[mi].x;
+    const int t = s.matTex[2 * mi].x;
     if (t < 0) return false;
     float rgb[3];
     tex_rgb(s.textures[t], u, v, rgb);
@@ -327,42 +327,96 @@ __device__ __forceinline__ bool textured_albedo(const DevScene &s, int mi, float
     return true;
 }
 
-// Tangent-space normal map of material index mi (Material::PerturbShading, material.cpp:41-60):
-// the map's colour as a direction in the frame of the shading dpdu and normal (the bitangent along
-// dp/dv), scaled in the tangent plane, kept in the geometric hemisphere; dpdu follows it.
-__device__ void normal_map(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
-    if (s.texCount <= 0 || !s.matTex) return;
-    const int4 mt = s.matTex[mi];
-    if (mt.y < 0) return;
-    float c[3];
-    tex_rgb(s.textures[mt.y], sf->u, sf->v, c);
-    const float strength = __int_as_float(mt.z);
-    V3 t = mk(2.f * c[0] - 1.f, 2.f * c[1] - 1.f, 2.f * c[2] - 1.f);
-    t.x *= strength;
-    t.y *= mt.w ? -strength : strength;
-    // dp/dv of the parameterization (Sphere / Triangle::Intersect, shape.cpp:75-82, 238-251).
-    V3 dpdv;
+// dp/du and dp/dv of the parameterization at a hit (Sphere / Triangle::Intersect, shape.cpp:75-82,
+// 237-251): the sphere's scaled by 2 pi and pi, a coordinate system where they degenerate.
+__device__ void surface_dpduv(const prgpu::Primitive &pr, const Surf &sf, V3 *dpdu, V3 *dpdv) {
     if (pr.type == prgpu::PrimSphere) {
-        V3 rel = sf->p - f3(pr.p0);
+        V3 rel = sf.p - f3(pr.p0);
         float cosT = clampf(rel.y / pr.r, -1.f, 1.f), sinT = safe_sqrt(1.f - cosT * cosT);
-        dpdv = sinT > 1e-6f ? mk(cosT * rel.x / sinT, -pr.r * sinT, cosT * rel.z / sinT) * kPi : mk(0.f, 0.f, 0.f);
-        if (len2(dpdv) < 1e-12f) dpdv = frame_from_z(sf->n).y;
-    } else {
-        V3 p0 = f3(pr.p0), p1 = f3(pr.p1), p2 = f3(pr.p2);
-        float du02 = pr.u0 - pr.u2, du12 = pr.u1 - pr.u2, dv02 = pr.v0 - pr.v2, dv12 = pr.v1 - pr.v2;
-        float det = du02 * dv12 - dv02 * du12;
-        dpdv = fabsf(det) < 1e-9f ? frame_from_z(sf->n).y : ((p1 - p2) * du02 - (p0 - p2) * du12) * (1.f / det);
-        if (!isfinite(dpdv.x)) dpdv = frame_from_z(sf->n).y;
+        *dpdu = mk(-rel.z, 0.f, rel.x) * (2.f * kPi);
+        *dpdv = sinT > 1e-6f ? mk(cosT * rel.x / sinT, -pr.r * sinT, cosT * rel.z / sinT) * kPi : mk(0.f, 0.f, 0.f);
+        V3 n = pr.flip ? -sf.n : sf.n;
+        if (len2(*dpdu) < 1e-12f || len2(*dpdv) < 1e-12f) {
+            Frame f = frame_from_z(n);
+            *dpdu = f.x;
+            *dpdv = f.y;
+        }
+        return;
     }
-    Frame f = frame_from_xz(sf->dpdu, sf->ns);
-    if (dot(f.y, dpdv) < 0.f) f.y = -f.y;
-    V3 n = f.x * t.x + f.y * t.y + f.z * fmaxf(t.z, 1e-3f);
-    float l = len(n);
-    if (!(l > 0.f) || !isfinite(l)) return;
-    V3 ns = n * (1.f / l);
+    V3 p0 = f3(pr.p0), p1 = f3(pr.p1), p2 = f3(pr.p2);
+    V3 n = normalize(cross(p1 - p0, p2 - p0));
+    float du02 = pr.u0 - pr.u2, du12 = pr.u1 - pr.u2, dv02 = pr.v0 - pr.v2, dv12 = pr.v1 - pr.v2;
+    float det = du02 * dv12 - dv02 * du12;
+    bool degenerate = fabsf(det) < 1e-9f;
+    if (!degenerate) {
+        float inv = 1.f / det;
+        *dpdu = ((p0 - p2) * dv12 - (p1 - p2) * dv02) * inv;
+        *dpdv = ((p1 - p2) * du02 - (p0 - p2) * du12) * inv;
+        degenerate = len2(cross(*dpdu, n)) == 0.f || !isfinite(dpdu->x) || !isfinite(dpdv->x);
+    }
+    if (degenerate) {
+        Frame f = frame_from_z(n);
+        *dpdu = f.x;
+        *dpdv = f.y;
+    }
+}
+
+__device__ __forceinline__ float height_at(const DevTex &t, int channel, float u, float v) {
+    float c[3];
+    tex_rgb(t, u, v, c);
+    return channel < 0 ? (c[0] + c[1] + c[2]) / 3.f : c[channel];
+}
+
+// Bump and normal maps of material index mi (Material::PerturbShading, material.cpp:16-60): the
+// bump map's finite-difference height gradient tilts dp/du and dp/dv along the shading normal;
+// the normal map's colour is a direction in the frame of the shading dp/du and normal (the
+// bitangent along dp/dv), scaled in the tangent plane; the result stays in the geometric
+// hemisphere and the shading dp/du follows it.
+__device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
+    if (s.texCount <= 0 || !s.matTex) return;
+    const int4 mt = s.matTex[2 * mi], bt = s.matTex[2 * mi + 1];
+    if (mt.y < 0 && bt.x < 0) return;
+    V3 dpdu, dpdv;
+    surface_dpduv(pr, *sf, &dpdu, &dpdv);
+    V3 ns = sf->ns, dpdus = dpdu;
+    bool changed = false;
+    if (bt.x >= 0) {
+        const DevTex &t = s.textures[bt.x];
+        const float du = 1.f / 2048.f, dv = 1.f / 2048.f, scale = __int_as_float(bt.z);
+        float h0 = height_at(t, bt.y, sf->u, sf->v);
+        float dhdu = (height_at(t, bt.y, sf->u + du, sf->v) - h0) / du * scale;
+        float dhdv = (height_at(t, bt.y, sf->u, sf->v + dv) - h0) / dv * scale;
+        V3 bu = dpdu + ns * dhdu, bv = dpdv + ns * dhdv;
+        V3 n = cross(bu, bv);
+        float l = len(n);
+        if (l > 0.f && isfinite(l)) {
+            n = n * (1.f / l);
+            if (dot(n, ns) < 0.f) n = -n;
+            ns = n;
+            dpdus = bu;
+            changed = true;
+        }
+    }
+    if (mt.y >= 0) {
+        float c[3];
+        tex_rgb(s.textures[mt.y], sf->u, sf->v, c);
+        const float strength = __int_as_float(mt.z);
+        V3 t = mk(2.f * c[0] - 1.f, 2.f * c[1] - 1.f, 2.f * c[2] - 1.f);
+        t.x *= strength;
+        t.y *= mt.w ? -strength : strength;
+        Frame f = frame_from_xz(dpdus, ns);
+        if (dot(f.y, dpdv) < 0.f) f.y = -f.y;
+        V3 n = f.x * t.x + f.y * t.y + f.z * fmaxf(t.z, 1e-3f);
+        float l = len(n);
+        if (l > 0.f && isfinite(l)) {
+            ns = n * (1.f / l);
+            changed = true;
+        }
+    }
+    if (!changed) return;
     if (dot(ns, sf->n) < 0.f) ns = -ns;
     sf->ns = ns;
-    sf->dpdu = sf->dpdu - ns * dot(sf->dpdu, ns);
+    sf->dpdu = dpdus - ns * dot(dpdus, ns);
 }
 
 // True for the materials shaded through FullBsdf: coats and anything with a sheen lobe.
@@ -1249,7 +1303,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 deferred = true;
             } else {
                 ++depth;
-                if constexpr (kDelta) normal_map(s, int(&m - s.mats), pr, &sf);
+                if constexpr (kDelta) perturb_shading(s, int(&m - s.mats), pr, &sf);
                 Frame fr = frame_from_xz(sf.dpdu, sf.ns);
                 V3 wo = -d;
                 V3 wol = fr.to_local(wo);

@@ -142,7 +142,8 @@ class ImageTextureDesc(C.Structure):
 
 class MaterialTextures(C.Structure):
     _fields_ = [("reflectance", C.c_int32), ("normalMap", C.c_int32), ("normalStrength", C.c_float),
-                ("normalFlipGreen", C.c_uint32)]
+                ("normalFlipGreen", C.c_uint32), ("bumpMap", C.c_int32), ("bumpChannel", C.c_int32),
+                ("bumpScale", C.c_float), ("pad", C.c_uint32)]
 
 
 class SceneExt(C.Structure):
@@ -190,7 +191,7 @@ class RenderStats(C.Structure):
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
 assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 112 and C.sizeof(DeltaLightDesc) == 104
-assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 16
+assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 32
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72

@@ -61,7 +61,7 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
     (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric).
     textures / material_textures / rgb_to_spectrum: image textures (image_texture), per SceneDesc
     material its reflectance texture index (-1 none) or a tuple (reflectance, normal map,
-    strength, flip green), and the RGB -> spectrum table
+    strength, flip green[, bump map, bump channel, bump scale]), and the RGB -> spectrum table
     (zNodes[64] then coefficients[3][64][64][64][3]). The record keeps the arrays it points at
     alive."""
     e = abi.SceneExt()
@@ -93,10 +93,13 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
     if material_textures is not None:
         mt = (abi.MaterialTextures * len(material_textures))()
         for i, t in enumerate(material_textures):
-            # an int (reflectance texture) or (reflectance, normal map, strength, flip green)
-            r, nm, st, fg = (t, -1, 1.0, False) if isinstance(t, (int, np.integer)) else tuple(t)
-            mt[i].reflectance, mt[i].normalMap = int(r), int(nm)
-            mt[i].normalStrength, mt[i].normalFlipGreen = float(st), 1 if fg else 0
+            # an int (reflectance texture) or (reflectance, normal map, strength, flip green
+            # [, bump map, bump channel, bump scale])
+            v = (t, -1, 1.0, False) if isinstance(t, (int, np.integer)) else tuple(t)
+            v = v + (-1, -1, 0.01)[len(v) - 4:] if len(v) < 7 else v
+            mt[i].reflectance, mt[i].normalMap = int(v[0]), int(v[1])
+            mt[i].normalStrength, mt[i].normalFlipGreen = float(v[2]), 1 if v[3] else 0
+            mt[i].bumpMap, mt[i].bumpChannel, mt[i].bumpScale = int(v[4]), int(v[5]), float(v[6])
         e.materialTextureCount = len(mt)
         e.materialTextures = C.cast(mt, C.c_void_p)
         e._keep.append(mt)

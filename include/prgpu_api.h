@@ -280,13 +280,19 @@ struct ImageTextureDesc {
 };
 
 // Per SceneDesc material: the image texture of its reflectance (diffuse and coated diffuse
-// materials) and of its tangent-space normal map (any material; pr::NormalMapParams,
-// material.h:30-36, applied as Material::PerturbShading, material.cpp:41-60), -1 for none.
+// materials), of its tangent-space normal map and of its bump (height) map (any material;
+// pr::NormalMapParams / BumpMapParams, material.h:30-41, applied as Material::PerturbShading,
+// material.cpp:16-60), -1 for none. A height map's texture carries the float texture's
+// multiplier in all three rgbScale components.
 struct MaterialTextures {
     int32_t reflectance;
     int32_t normalMap;
     float normalStrength;      // scales the map's tangent-plane components
     uint32_t normalFlipGreen;  // the map's green channel points along -v
+    int32_t bumpMap;
+    int32_t bumpChannel;       // -1 the mean of r, g, b; 0, 1, 2 one channel
+    float bumpScale;
+    uint32_t pad;
 };
 
 struct SceneExt {

@@ -171,3 +171,65 @@ def test_normal_maps_agree_with_reference(gpu, oracle):
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
+
+
+def _height_image():
+    h, w = 32, 32
+    v, u = np.meshgrid((np.arange(h) + 0.5) / h, (np.arange(w) + 0.5) / w, indexing="ij")
+    img = np.zeros((h, w, 3), np.float32)
+    img[..., 0] = 0.5 + 0.5 * np.sin(2 * np.pi * 3 * u) * np.cos(2 * np.pi * 2 * v)
+    img[..., 1] = 0.5 + 0.4 * np.cos(2 * np.pi * 4 * v)
+    img[..., 2] = u * v
+    return img
+
+
+def test_bump_maps_agree_with_reference(gpu, oracle):
+    """A bump-mapped diffuse ground (mean of the channels, scale 0.2, multiplier 1.5) and a rough gold
+    sphere with a bump map (red channel) under a normal map (both perturbations in the reference's
+    order), lit by a point light and a constant sky: the same z statistics as above."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    himg, nimg = _height_image(), _normal_image()
+    hpfm, npfm = os.path.join(d, "height_map.pfm"), os.path.join(d, "normal_map2.pfm")
+    _write_pfm(hpfm, himg)
+    _write_pfm(npfm, nimg)
+    doc = ru_outdoor_doc(w, h, hpfm)
+    doc["textures"] = {"height": {"type": "image", "file": hpfm, "wrap": "repeat", "flip_v": True,
+                                  "uv_scale": [2.0, 2.0], "multiplier": 1.5},
+                       "height2": {"type": "image", "file": hpfm, "wrap": "mirror", "flip_v": True,
+                                   "uv_scale": [3.0, 1.5]},
+                       "nmap": {"type": "image", "file": npfm, "colorspace": "linear", "wrap": "repeat",
+                                "flip_v": True, "uv_scale": [1.0, 1.0]}}
+    doc["materials"] = {"ground": {"type": "diffuse", "reflectance": [0.6, 0.55, 0.5],
+                                   "bump_map": {"texture": "height", "scale": 0.2}},
+                        "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+                        "tex_coat": {"type": "conductor", "metal": "Au", "roughness": 0.3,
+                                     "bump_map": {"texture": "height2", "channel": "r", "scale": 0.05},
+                                     "normal_map": {"texture": "nmap", "strength": 0.5}}}
+    path = os.path.join(d, "bump_maps.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    desc = rs.export()
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    maps = {"ground": (-1, -1, 1.0, False, 0, -1, 0.2), "tex_coat": (-1, 2, 0.5, False, 1, 0, 0.05)}
+    mat_tex = [maps.get(n, -1) for n in used]
+    textures = [render.image_texture(himg, uv_scale=(2.0, 2.0), multiplier=(1.5, 1.5, 1.5)),
+                render.image_texture(himg, wrap=abi.WRAP_MIRROR, uv_scale=(3.0, 1.5)),
+                render.image_texture(nimg)]
+    ext = render.make_ext(textures=textures, material_textures=mat_tex)
+    g = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"bump maps: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
