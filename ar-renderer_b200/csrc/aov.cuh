@@ -68,6 +68,7 @@ __device__ ChainEnd follow_chain(const DevScene &s, V3 o, V3 d, Hit h, bool thro
         if (full_material(m)) {
             FullBsdf fb;
             make_full(s, m, sf.u, sf.v, lam, &fb);
+            if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, fb.layered ? &fb.lay.bottom : &fb.base);
             if (fb.black || full_non_specular(fb)) {
                 e.valid = true;
                 return e;
@@ -76,7 +77,7 @@ __device__ ChainEnd follow_chain(const DevScene &s, V3 o, V3 d, Hit h, bool thro
             ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &prop);
         } else {
             Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
-            if (lobe.kind == kLobeDiffuse) textured_albedo(s, int(&m - s.mats), sf.u, sf.v, lam, &lobe.R);
+            textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &lobe);
             if (lobe.flags() == 0u || lobe.non_specular()) {
                 e.valid = true;
                 return e;
@@ -182,14 +183,12 @@ __global__ void __launch_bounds__(128) k_aov(const DevScene *sp, AovArgs a, floa
                                 FullBsdf fb;
                                 make_full(s, m, e.sf.u, e.sf.v, lam, &fb);
                                 Lobe &base = fb.layered ? fb.lay.bottom : fb.base;
-                                if (!fb.black && base.kind == kLobeDiffuse)
-                                    textured_albedo(s, int(&m - s.mats), e.sf.u, e.sf.v, lam, &base.R);
+                                if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{e.sf.p, e.sf.u, e.sf.v}, lam, &base);
                                 bool prop;
                                 ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &prop);
                             } else {
                                 Lobe lobe = make_lobe(s, m, e.sf.u, e.sf.v, lam);
-                                if (lobe.kind == kLobeDiffuse)
-                                    textured_albedo(s, int(&m - s.mats), e.sf.u, e.sf.v, lam, &lobe.R);
+                                textured_lobe(s, int(&m - s.mats), TexCtx{e.sf.p, e.sf.u, e.sf.v}, lam, &lobe);
                                 ok = wol.z != 0.f && lobe.flags() != 0u && lobe_sample(lobe, wol, uc, u0, u1, &bs);
                             }
                             ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f;

@@ -257,7 +257,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
                     ShadeArgs sa{scene, rs.sceneTable.as<DevScene>(), rs.P, rs.S, cq, rs.capacity, qout, cnt,
                                  rp.maxDepth, 0, rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin};
-                    const bool dl = scene.deltaCount > 0 || scene.texCount > 0;
+                    const bool dl = scene.deltaCount > 0 || scene.matTex != nullptr;
                     if (guideMode) {
                         if (dl) k_shade<false, true, false, true><<<gShade, 256, 0, st>>>(sa);
                         else k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
@@ -803,7 +803,7 @@ bool run_batch(DeviceState &ds, BatchState &bs, int count, const prgpu::BatchIte
         if (d.mediumCount + d.gridCount > 0) media = true;
         if (d.hasInterfaces) walls = true;
         if (d.hasFull) full = true;
-        if (d.deltaCount > 0 || d.texCount > 0) deltas = true;
+        if (d.deltaCount > 0 || d.matTex != nullptr) deltas = true;
     }
     std::vector<BatchChunk> chunks;
     std::vector<BatchWave> waves;

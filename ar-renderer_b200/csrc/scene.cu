@@ -57,8 +57,10 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
                         4 * sizeof(float), 65536);
     }
     if (ext && ext->sun) h = fnv_v(h, *ext->sun);
-    if (ext && ext->textures && ext->textureCount > 0) {
-        for (int32_t k = 0; k < ext->textureCount; ++k) {
+    if (ext && ext->textureNodes && ext->textureNodeCount > 0)
+        h = fnv(h, ext->textureNodes, size_t(ext->textureNodeCount) * sizeof(prgpu::TextureNode));
+    if (ext && ((ext->textures && ext->textureCount > 0) || (ext->textureNodes && ext->textureNodeCount > 0))) {
+        for (int32_t k = 0; ext->textures && k < ext->textureCount; ++k) {
             const prgpu::ImageTextureDesc &t = ext->textures[k];
             h = fnv_v(h, t);
             h = sample_hash(h, t.rgb, size_t(std::max(0, t.width)) * size_t(std::max(0, t.height)), 3 * sizeof(float), 65536);
@@ -84,6 +86,43 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
 }
 
 bool spec_ok(int32_t id, int32_t n) { return id >= -1 && id < n; }
+
+// A texture tree rooted at `node` (-1 none): indices in range, at most 8 nodes deep (so no
+// cycles), noise only as a float texture or as the blend of a mix, constants of spectrum trees
+// naming a spectrum.
+bool texture_tree_ok(const prgpu::SceneExt *ext, const prgpu::SceneDesc *sd, int32_t node, bool spectrum, int depth) {
+    if (node == -1) return depth > 0 ? false : true;
+    if (node < 0 || node >= ext->textureNodeCount || depth >= 8) return false;
+    const prgpu::TextureNode &t = ext->textureNodes[node];
+    switch (t.type) {
+    case prgpu::TexConstant:
+        return spectrum ? (t.a >= 0 && t.a < sd->spectrumCount) : std::isfinite(t.value);
+    case prgpu::TexImage:
+        return t.a >= 0 && t.a < ext->textureCount && t.channel >= -1 && t.channel <= 2;
+    case prgpu::TexChecker:
+        return std::isfinite(t.scaleU) && std::isfinite(t.scaleV) && std::isfinite(t.offsetU) &&
+               std::isfinite(t.offsetV) && texture_tree_ok(ext, sd, t.a, spectrum, depth + 1) &&
+               texture_tree_ok(ext, sd, t.b, spectrum, depth + 1);
+    case prgpu::TexNoise:
+        return !spectrum && t.octaves >= 1 && t.octaves <= 32 && std::isfinite(t.frequency) &&
+               std::isfinite(t.offset[0]) && std::isfinite(t.offset[1]) && std::isfinite(t.offset[2]);
+    case prgpu::TexMix:
+        return t.t >= 0 && t.t < ext->textureNodeCount && ext->textureNodes[t.t].type == prgpu::TexNoise &&
+               texture_tree_ok(ext, sd, t.t, false, depth + 1) && texture_tree_ok(ext, sd, t.a, spectrum, depth + 1) &&
+               texture_tree_ok(ext, sd, t.b, spectrum, depth + 1);
+    default: return false;
+    }
+}
+
+// True when the (already validated) tree looks up an image.
+bool texture_tree_has_image(const prgpu::SceneExt *ext, int32_t node, int depth) {
+    if (node < 0 || depth >= 8) return false;
+    const prgpu::TextureNode &t = ext->textureNodes[node];
+    if (t.type == prgpu::TexImage) return true;
+    if (t.type == prgpu::TexChecker || t.type == prgpu::TexMix)
+        return texture_tree_has_image(ext, t.a, depth + 1) || texture_tree_has_image(ext, t.b, depth + 1);
+    return false;
+}
 
 bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::string *err) {
     auto fail = [&](const std::string &m) {
@@ -138,13 +177,24 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
         if (t.width <= 0 || t.height <= 0 || int64_t(t.width) * t.height > (int64_t(1) << 28) || !t.rgb || t.wrap > 2)
             return fail("bad image texture");
     }
+    if (ext && (ext->textureNodeCount < 0 || ext->textureNodeCount > 65536 ||
+                (ext->textureNodeCount > 0 && !ext->textureNodes)))
+        return fail("bad texture node table");
+    for (int32_t i = 0; ext && i < ext->materialTextureCount; ++i) {
+        const prgpu::MaterialTextures &x = ext->materialTextures[i];
+        if (!texture_tree_ok(ext, sd, x.reflectanceNode, true, 0) || !texture_tree_ok(ext, sd, x.bumpNode, false, 0) ||
+            !texture_tree_ok(ext, sd, x.roughnessNodeU, false, 0) || !texture_tree_ok(ext, sd, x.roughnessNodeV, false, 0))
+            return fail("bad texture tree (index out of range, deeper than 8 nodes, or a node of the wrong kind)");
+        if (x.reflectanceNode >= 0 && !ext->rgbToSpectrum && texture_tree_has_image(ext, x.reflectanceNode, 0))
+            return fail("textured materials need the RGB -> spectrum table");
+        if (!std::isfinite(x.bumpScale)) return fail("bad bump map scale");
+    }
     for (int32_t i = 0; ext && i < ext->materialTextureCount; ++i) {
         const int32_t r = ext->materialTextures[i].reflectance, nmap = ext->materialTextures[i].normalMap;
         const int32_t bmap = ext->materialTextures[i].bumpMap, bch = ext->materialTextures[i].bumpChannel;
         if (r < -1 || r >= ext->textureCount || nmap < -1 || nmap >= ext->textureCount || bmap < -1 ||
             bmap >= ext->textureCount || bch < -1 || bch > 2)
             return fail("material texture index out of range");
-        if (!std::isfinite(ext->materialTextures[i].bumpScale)) return fail("bad bump map scale");
         if (r >= 0 && !ext->rgbToSpectrum) return fail("textured materials need the RGB -> spectrum table");
         if (!std::isfinite(ext->materialTextures[i].normalStrength)) return fail("bad normal map strength");
     }
@@ -322,13 +372,17 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
     d.matTex = nullptr;
     d.rgbZ = d.rgbCoeffs = nullptr;
     d.texCount = 0;
+    d.texNodes = nullptr;
     const int32_t n = ext && ext->textures ? ext->textureCount : 0;
     const int32_t nm = ext && ext->materialTextures ? ext->materialTextureCount : 0;
+    const int32_t nn = ext && ext->textureNodes ? ext->textureNodeCount : 0;
     bool used = false;
-    for (int32_t i = 0; i < nm; ++i)
-        used = used || ext->materialTextures[i].reflectance >= 0 || ext->materialTextures[i].normalMap >= 0 ||
-               ext->materialTextures[i].bumpMap >= 0;
-    if (n <= 0 || !used) return;
+    for (int32_t i = 0; i < nm; ++i) {
+        const prgpu::MaterialTextures &x = ext->materialTextures[i];
+        used = used || (n > 0 && (x.reflectance >= 0 || x.normalMap >= 0 || x.bumpMap >= 0)) ||
+               (nn > 0 && (x.reflectanceNode >= 0 || x.bumpNode >= 0 || x.roughnessNodeU >= 0 || x.roughnessNodeV >= 0));
+    }
+    if (!used) return;
     size_t total = 0;
     for (int32_t k = 0; k < n; ++k) total += size_t(ext->textures[k].width) * ext->textures[k].height * 3;
     cache.texData.ensure(total * sizeof(float));
@@ -348,24 +402,29 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         g.scale[0] = x.rgbScale[0], g.scale[1] = x.rgbScale[1], g.scale[2] = x.rgbScale[2];
         off += m;
     }
-    std::vector<int4> mt(static_cast<size_t>(2 * nm));
+    std::vector<int4> mt(static_cast<size_t>(3 * nm));
     for (int32_t i = 0; i < nm; ++i) {
         const prgpu::MaterialTextures &x = ext->materialTextures[i];
         int sbits, bbits;
         std::memcpy(&sbits, &x.normalStrength, sizeof(sbits));
         std::memcpy(&bbits, &x.bumpScale, sizeof(bbits));
-        mt[size_t(2 * i)] = make_int4(x.reflectance, x.normalMap, sbits, x.normalFlipGreen ? 1 : 0);
-        mt[size_t(2 * i + 1)] = make_int4(x.bumpMap, x.bumpChannel, bbits, 0);
+        const bool img = n > 0, trees = nn > 0;
+        mt[size_t(3 * i)] = make_int4(img ? x.reflectance : -1, img ? x.normalMap : -1, sbits, x.normalFlipGreen ? 1 : 0);
+        mt[size_t(3 * i + 1)] = make_int4(img ? x.bumpMap : -1, x.bumpChannel, bbits, trees ? x.reflectanceNode : -1);
+        mt[size_t(3 * i + 2)] = make_int4(trees ? x.bumpNode : -1, trees ? x.roughnessNodeU : -1,
+                                          trees ? x.roughnessNodeV : -1, 0);
     }
-    put(cache.textures, t.data(), t.size(), s);
+    if (n > 0) put(cache.textures, t.data(), t.size(), s);
     put(cache.matTex, mt.data(), mt.size(), s);
+    if (nn > 0) put(cache.texNodes, ext->textureNodes, size_t(nn), s);
     if (ext->rgbToSpectrum) {
         const size_t tableFloats = 64 + size_t(3) * 64 * 64 * 64 * 3;
         put(cache.rgbTable, ext->rgbToSpectrum, tableFloats, s);
     }
     PRB_CUDA(cudaStreamSynchronize(s));
-    d.textures = cache.textures.as<DevTex>();
+    d.textures = n > 0 ? cache.textures.as<DevTex>() : nullptr;
     d.matTex = cache.matTex.as<int4>();
+    d.texNodes = nn > 0 ? cache.texNodes.as<prgpu::TextureNode>() : nullptr;
     d.rgbZ = ext->rgbToSpectrum ? cache.rgbTable.as<float>() : nullptr;
     d.rgbCoeffs = d.rgbZ ? d.rgbZ + 64 : nullptr;
     d.texCount = n;

@@ -128,11 +128,12 @@ struct DevScene {
     DevSun sun;
     const DevDelta *deltas;
     int deltaCount;
-    // Image textures: per material the reflectance texture (-1 none), and the RGB uplift table.
+    // Image textures and procedural texture trees; matTex is null unless a material uses one.
     const DevTex *textures;
-    // per material two entries: (reflectance texture, normal map, strength bits, flip green) and
-    // (bump map, channel, scale bits, 0)
+    // per material three entries: (reflectance texture, normal map, strength bits, flip green),
+    // (bump map, channel, scale bits, reflectance tree) and (bump tree, roughness trees u, v, 0)
     const int4 *matTex;
+    const prgpu::TextureNode *texNodes;
     const float *rgbZ, *rgbCoeffs;
     int texCount;
     // Per-render settings of the batched form (the single-render kernels take them as arguments).
@@ -146,7 +147,7 @@ struct SceneCache {
     bool valid = false;
     DeviceAccel accel;
     DevBuf prims, primClass, mats, lights, spectra, media, filterCdf, lbvh, lightLeaf, grids, gridData, envTexels,
-        envDist, walls, sheen, deltas, deltaProfiles, textures, texData, matTex, rgbTable;
+        envDist, walls, sheen, deltas, deltaProfiles, textures, texData, matTex, texNodes, rgbTable;
     DevScene ds{};
     bool hasSpheres = false;
     int wallCount = 0;
@@ -174,6 +175,7 @@ struct SceneCache {
         textures.release();
         texData.release();
         matTex.release();
+        texNodes.release();
         rgbTable.release();
         valid = false;
     }

@@ -316,15 +316,191 @@ __device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lam
     return out;
 }
 
-// The reflectance of material index mi from its image texture, when it has one.
-__device__ __forceinline__ bool textured_albedo(const DevScene &s, int mi, float u, float v, const Lambda &lam, SS *R) {
-    if (s.texCount <= 0 || !s.matTex) return false;
-    const int t = s.matTex[2 * mi].x;
-    if (t < 0) return false;
-    float rgb[3];
-    tex_rgb(s.textures[t], u, v, rgb);
-    *R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
-    return true;
+// ---------------------------------------------------------------------------------------------
+// Procedural textures: improved Perlin noise (K. Perlin, "Improving Noise", SIGGRAPH 2002: his
+// published permutation, the quintic fade and the 12-edge gradient hash; pr::PerlinNoise / FBm,
+// src/core/noise.cpp:36-64), NoiseFloatTexture (texture.cpp:55-60) and the TextureNode trees.
+
+static __device__ const unsigned char kPerlinPerm[256] = {
+    151, 160, 137, 91, 90, 15, 131, 13, 201, 95, 96, 53, 194, 233, 7, 225, 140, 36, 103, 30, 69, 142,
+    8, 99, 37, 240, 21, 10, 23, 190, 6, 148, 247, 120, 234, 75, 0, 26, 197, 62, 94, 252, 219, 203, 117, 35,
+    11, 32, 57, 177, 33, 88, 237, 149, 56, 87, 174, 20, 125, 136, 171, 168, 68, 175, 74, 165, 71, 134, 139,
+    48, 27, 166, 77, 146, 158, 231, 83, 111, 229, 122, 60, 211, 133, 230, 220, 105, 92, 41, 55, 46, 245, 40,
+    244, 102, 143, 54, 65, 25, 63, 161, 1, 216, 80, 73, 209, 76, 132, 187, 208, 89, 18, 169, 200, 196, 135,
+    130, 116, 188, 159, 86, 164, 100, 109, 198, 173, 186, 3, 64, 52, 217, 226, 250, 124, 123, 5, 202, 38,
+    147, 118, 126, 255, 82, 85, 212, 207, 206, 59, 227, 47, 16, 58, 17, 182, 189, 28, 42, 223, 183, 170, 213,
+    119, 248, 152, 2, 44, 154, 163, 70, 221, 153, 101, 155, 167, 43, 172, 9, 129, 22, 39, 253, 19, 98, 108,
+    110, 79, 113, 224, 232, 178, 185, 112, 104, 218, 246, 97, 228, 251, 34, 242, 193, 238, 210, 144, 12, 191,
+    179, 162, 241, 81, 51, 145, 235, 249, 14, 239, 107, 49, 192, 214, 31, 181, 199, 106, 157, 184, 84, 204,
+    176, 115, 121, 50, 45, 127, 4, 150, 254, 138, 236, 205, 93, 222, 114, 67, 29, 24, 72, 243, 141, 128, 195,
+    78, 66, 215, 61, 156, 180};
+
+__device__ __forceinline__ int perlin_perm(int i) { return kPerlinPerm[i & 255]; }
+__device__ __forceinline__ float perlin_fade(float t) { return t * t * t * (t * (t * 6.f - 15.f) + 10.f); }
+__device__ __forceinline__ float perlin_grad(int h, float x, float y, float z) {
+    h &= 15;
+    const float u = h < 8 ? x : y;
+    const float v = h < 4 ? y : (h == 12 || h == 14 ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+__device__ __forceinline__ float perlin_lerp(float t, float a, float b) { return (1.f - t) * a + t * b; }
+
+__device__ float perlin_noise(V3 p) {
+    const float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
+    const int X = int(fx) & 255, Y = int(fy) & 255, Z = int(fz) & 255;
+    const float x = p.x - fx, y = p.y - fy, z = p.z - fz;
+    const float u = perlin_fade(x), v = perlin_fade(y), w = perlin_fade(z);
+    const int A = perlin_perm(X) + Y, AA = perlin_perm(A) + Z, AB = perlin_perm(A + 1) + Z;
+    const int B = perlin_perm(X + 1) + Y, BA = perlin_perm(B) + Z, BB = perlin_perm(B + 1) + Z;
+    const float n0 = perlin_lerp(v, perlin_lerp(u, perlin_grad(perlin_perm(AA), x, y, z),
+                                                perlin_grad(perlin_perm(BA), x - 1.f, y, z)),
+                                 perlin_lerp(u, perlin_grad(perlin_perm(AB), x, y - 1.f, z),
+                                             perlin_grad(perlin_perm(BB), x - 1.f, y - 1.f, z)));
+    const float n1 = perlin_lerp(v, perlin_lerp(u, perlin_grad(perlin_perm(AA + 1), x, y, z - 1.f),
+                                                perlin_grad(perlin_perm(BA + 1), x - 1.f, y, z - 1.f)),
+                                 perlin_lerp(u, perlin_grad(perlin_perm(AB + 1), x, y - 1.f, z - 1.f),
+                                             perlin_grad(perlin_perm(BB + 1), x - 1.f, y - 1.f, z - 1.f)));
+    return perlin_lerp(w, n0, n1);
+}
+
+// Fractional Brownian motion: octaves of noise at doubling frequency and halving amplitude,
+// normalised by the amplitude sum; |noise| per octave for turbulence.
+__device__ float fbm_noise(V3 p, int octaves, bool turbulence) {
+    float sum = 0.f, amp = 0.5f, freq = 1.f, norm = 0.f;
+    const int n = max(1, octaves);
+    for (int i = 0; i < n; ++i) {
+        const float v = perlin_noise(p * freq);
+        sum += amp * (turbulence ? fabsf(v) : v);
+        norm += amp;
+        amp *= 0.5f;
+        freq *= 2.f;
+    }
+    return sum / norm;
+}
+
+// Where a texture is evaluated: the hit point and its (u, v).
+struct TexCtx {
+    V3 p;
+    float u, v;
+};
+
+__device__ float noise_node(const prgpu::TextureNode &n, const TexCtx &c) {
+    V3 p = (n.flags & prgpu::TexNoiseWorldSpace) ? c.p : mk(c.u, c.v, 0.f);
+    p = (p + mk(n.offset[0], n.offset[1], n.offset[2])) * n.frequency;
+    const bool turb = (n.flags & prgpu::TexNoiseTurbulence) != 0;
+    const float v = fbm_noise(p, n.octaves, turb);
+    return turb ? clampf(v * 1.6f, 0.f, 1.f) : clampf(0.5f + 0.5f * v * 1.4f, 0.f, 1.f);
+}
+
+// Walks the texture tree under `root` as a weighted sum over its leaves: a checker passes its
+// weight to the child its (s, t) cell picks, a mix splits it by its clamped noise. leaf(node, w)
+// adds a constant, image or noise leaf. Validated trees are at most 8 deep, so the stack of 10
+// never overflows; the guard bounds the walk all the same.
+constexpr int kTexStack = 10;
+template <class Leaf>
+__device__ __forceinline__ void walk_texture(const DevScene &s, int root, const TexCtx &c, Leaf &&leaf) {
+    int node[kTexStack];
+    float wt[kTexStack];
+    node[0] = root;
+    wt[0] = 1.f;
+    int sp = 1;
+    for (int guard = 0; sp > 0 && guard < 64; ++guard) {
+        --sp;
+        const int id = node[sp];
+        const float w = wt[sp];
+        const prgpu::TextureNode &n = s.texNodes[id];
+        if (n.type == prgpu::TexChecker) {
+            const float ss = c.u * n.scaleU + n.offsetU, tt = c.v * n.scaleV + n.offsetV;
+            const bool odd = ((int(floorf(ss)) + int(floorf(tt))) & 1) != 0;
+            node[sp] = odd ? n.b : n.a;
+            wt[sp] = w;
+            ++sp;
+        } else if (n.type == prgpu::TexMix) {
+            if (sp + 2 > kTexStack) continue;
+            const float t = clampf(noise_node(s.texNodes[n.t], c), 0.f, 1.f);
+            node[sp] = n.a;
+            wt[sp] = w * (1.f - t);
+            node[sp + 1] = n.b;
+            wt[sp + 1] = w * t;
+            sp += 2;
+        } else {
+            leaf(n, w);
+        }
+    }
+}
+
+// A spectrum tree as an albedo at the 4 wavelengths (constants from the spectrum table, images
+// uplifted through the RGB -> spectrum table).
+__device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, const Lambda &lam) {
+    SS acc = splat(0.f);
+    walk_texture(s, root, c, [&](const prgpu::TextureNode &n, float w) {
+        SS v;
+        if (n.type == prgpu::TexConstant) {
+            v = tab4(s.spectra, n.a, lam);
+        } else if (n.type == prgpu::TexImage) {
+            float rgb[3];
+            tex_rgb(s.textures[n.a], c.u, c.v, rgb);
+            v = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
+        } else {
+            return;
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) acc.v[i] += w * v.v[i];
+    });
+    return acc;
+}
+
+__device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
+    float acc = 0.f;
+    walk_texture(s, root, c, [&](const prgpu::TextureNode &n, float w) {
+        float v = 0.f;
+        if (n.type == prgpu::TexConstant) {
+            v = n.value;
+        } else if (n.type == prgpu::TexImage) {
+            float rgb[3];
+            tex_rgb(s.textures[n.a], c.u, c.v, rgb);
+            v = n.channel < 0 ? (rgb[0] + rgb[1] + rgb[2]) / 3.f : (n.channel == 0 ? rgb[0] : n.channel == 1 ? rgb[1] : rgb[2]);
+        } else if (n.type == prgpu::TexNoise) {
+            v = noise_node(n, c);
+        }
+        acc += w * v;
+    });
+    return acc;
+}
+
+// The textured parameters of material index mi at a hit, applied to its lobe: the reflectance of
+// a diffuse lobe (a tree, else an image; clamped to [0, 1] as DiffuseMaterial::GetBxDF,
+// material.cpp:73-77) and the roughness of conductor and rough dielectric lobes (trees; alpha =
+// clamp(r, 0, 1)^2, material.cpp:80-85, 110-116, 151-154).
+__device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l) {
+    if (!s.matTex) return;
+    if (l->kind == kLobeDiffuse) {
+        const int tree = s.matTex[3 * mi + 1].w, img = s.matTex[3 * mi].x;
+        if (tree >= 0) {
+            SS r = spectrum_texture(s, tree, c, lam);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) r.v[i] = clampf(r.v[i], 0.f, 1.f);
+            l->R = r;
+        } else if (img >= 0) {
+            float rgb[3];
+            tex_rgb(s.textures[img], c.u, c.v, rgb);
+            l->R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
+        }
+    } else if (l->kind == kLobeConductor || l->kind == kLobeDielectric) {
+        const int4 m2 = s.matTex[3 * mi + 2];
+        if (m2.y < 0 && m2.z < 0) return;
+        const prgpu::Material &m = s.mats[mi];
+        float ax = m.alphaX, ay = m.alphaY;
+        if (m2.y >= 0) {
+            const float r = clampf(float_texture(s, m2.y, c), 0.f, 1.f);
+            ax = r * r;
+        }
+        if (m2.z >= 0) {
+            const float r = clampf(float_texture(s, m2.z, c), 0.f, 1.f);
+            ay = r * r;
+        }
+        l->mf = make_ggx(ax, ay);
+    }
 }
 
 // dp/du and dp/dv of the parameterization at a hit (Sphere / Triangle::Intersect, shape.cpp:75-82,
@@ -373,19 +549,23 @@ __device__ __forceinline__ float height_at(const DevTex &t, int channel, float u
 // bitangent along dp/dv), scaled in the tangent plane; the result stays in the geometric
 // hemisphere and the shading dp/du follows it.
 __device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
-    if (s.texCount <= 0 || !s.matTex) return;
-    const int4 mt = s.matTex[2 * mi], bt = s.matTex[2 * mi + 1];
-    if (mt.y < 0 && bt.x < 0) return;
+    if (!s.matTex) return;
+    const int4 mt = s.matTex[3 * mi], bt = s.matTex[3 * mi + 1];
+    const int bumpTree = s.matTex[3 * mi + 2].x;
+    if (mt.y < 0 && bt.x < 0 && bumpTree < 0) return;
     V3 dpdu, dpdv;
     surface_dpduv(pr, *sf, &dpdu, &dpdv);
     V3 ns = sf->ns, dpdus = dpdu;
     bool changed = false;
-    if (bt.x >= 0) {
-        const DevTex &t = s.textures[bt.x];
+    if (bt.x >= 0 || bumpTree >= 0) {
+        // The height at (u, v) and the point moved along dp/du or dp/dv with it.
+        auto height = [&](float u, float v, V3 p) {
+            return bumpTree >= 0 ? float_texture(s, bumpTree, TexCtx{p, u, v}) : height_at(s.textures[bt.x], bt.y, u, v);
+        };
         const float du = 1.f / 2048.f, dv = 1.f / 2048.f, scale = __int_as_float(bt.z);
-        float h0 = height_at(t, bt.y, sf->u, sf->v);
-        float dhdu = (height_at(t, bt.y, sf->u + du, sf->v) - h0) / du * scale;
-        float dhdv = (height_at(t, bt.y, sf->u, sf->v + dv) - h0) / dv * scale;
+        float h0 = height(sf->u, sf->v, sf->p);
+        float dhdu = (height(sf->u + du, sf->v, sf->p + dpdu * du) - h0) / du * scale;
+        float dhdv = (height(sf->u, sf->v + dv, sf->p + dpdv * dv) - h0) / dv * scale;
         V3 bu = dpdu + ns * dhdu, bv = dpdv + ns * dhdv;
         V3 n = cross(bu, bv);
         float l = len(n);
@@ -1317,8 +1497,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     make_full(s, m, sf.u, sf.v, lam, &fb);
                     if constexpr (kDelta) {
                         Lobe &base = fb.layered ? fb.lay.bottom : fb.base;
-                        if (!fb.black && base.kind == kLobeDiffuse)
-                            textured_albedo(s, int(&m - s.mats), sf.u, sf.v, lam, &base.R);
+                        if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &base);
                     }
                     if (full_non_specular(fb))
                         nee(sf.p, sf.n, nullptr, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr, &fb);
@@ -1330,8 +1509,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
                 } else {
                 Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
-                if constexpr (kDelta)
-                    if (lobe.kind == kLobeDiffuse) textured_albedo(s, int(&m - s.mats), sf.u, sf.v, lam, &lobe.R);
+                if constexpr (kDelta) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &lobe);
                 if constexpr (kGuide) {
                     GuideMix gm;
                     // The guide is trained on, and applied at, the first kGuideVertices diffuse

@@ -143,7 +143,19 @@ class ImageTextureDesc(C.Structure):
 class MaterialTextures(C.Structure):
     _fields_ = [("reflectance", C.c_int32), ("normalMap", C.c_int32), ("normalStrength", C.c_float),
                 ("normalFlipGreen", C.c_uint32), ("bumpMap", C.c_int32), ("bumpChannel", C.c_int32),
-                ("bumpScale", C.c_float), ("pad", C.c_uint32)]
+                ("bumpScale", C.c_float), ("reflectanceNode", C.c_int32), ("bumpNode", C.c_int32),
+                ("roughnessNodeU", C.c_int32), ("roughnessNodeV", C.c_int32), ("pad", C.c_uint32)]
+
+
+TEX_CONSTANT, TEX_IMAGE, TEX_CHECKER, TEX_NOISE, TEX_MIX = 0, 1, 2, 3, 4
+TEX_NOISE_TURBULENCE, TEX_NOISE_WORLD = 1, 2
+
+
+class TextureNode(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("a", C.c_int32), ("b", C.c_int32), ("t", C.c_int32), ("channel", C.c_int32),
+                ("value", C.c_float), ("frequency", C.c_float), ("octaves", C.c_int32), ("flags", C.c_uint32),
+                ("offset", C.c_float * 3), ("scaleU", C.c_float), ("scaleV", C.c_float), ("offsetU", C.c_float),
+                ("offsetV", C.c_float)]
 
 
 class SceneExt(C.Structure):
@@ -152,7 +164,8 @@ class SceneExt(C.Structure):
                 ("flags", C.c_int32), ("gridMediumCount", C.c_int32), ("gridMedia", C.c_void_p),
                 ("envMap", C.c_void_p), ("sun", C.c_void_p), ("deltaLightCount", C.c_int32), ("pad", C.c_int32),
                 ("deltaLights", C.c_void_p), ("textureCount", C.c_int32), ("materialTextureCount", C.c_int32),
-                ("textures", C.c_void_p), ("materialTextures", C.c_void_p), ("rgbToSpectrum", C.c_void_p)]
+                ("textures", C.c_void_p), ("materialTextures", C.c_void_p), ("rgbToSpectrum", C.c_void_p),
+                ("textureNodes", C.c_void_p), ("textureNodeCount", C.c_int32), ("pad2", C.c_int32)]
 
 
 class BatchItem(C.Structure):
@@ -190,8 +203,8 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 112 and C.sizeof(DeltaLightDesc) == 104
-assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 32
+assert C.sizeof(GridMediumDesc) == 112 and C.sizeof(SceneExt) == 128 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 48 and C.sizeof(TextureNode) == 64
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72

@@ -54,16 +54,18 @@ GUIDE_SAMPLE, GUIDE_TRAIN, GUIDE_RESET = 1, 2, 4
 
 def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, wavefront_paths: int = 0,
              block_size: int = 0, grid_media=None, guide: int = 0, delta_lights=None, textures=None,
-             material_textures=None, rgb_to_spectrum: np.ndarray | None = None) -> abi.SceneExt:
+             material_textures=None, rgb_to_spectrum: np.ndarray | None = None,
+             texture_nodes=None) -> abi.SceneExt:
     """SceneExt for prgpu_render_ex. grid_media: GridMediumDesc records (media.grid_desc), indexed
     after the SceneDesc's homogeneous media. guide: GUIDE_SAMPLE (sample diffuse vertices with the
     guide network), GUIDE_TRAIN (train it online, one Adam step per wavefront chunk), GUIDE_RESET
     (fresh weights first). delta_lights: DeltaLightDesc records (spot, distant, goniometric).
     textures / material_textures / rgb_to_spectrum: image textures (image_texture), per SceneDesc
-    material its reflectance texture index (-1 none) or a tuple (reflectance, normal map,
-    strength, flip green[, bump map, bump channel, bump scale]), and the RGB -> spectrum table
-    (zNodes[64] then coefficients[3][64][64][64][3]). The record keeps the arrays it points at
-    alive."""
+    material its reflectance texture index (-1 none), a tuple (reflectance, normal map,
+    strength, flip green[, bump map, bump channel, bump scale]) or a dict of MaterialTextures
+    fields, and the RGB -> spectrum table (zNodes[64] then coefficients[3][64][64][64][3]).
+    texture_nodes: TextureNode records (texture_node) that the *Node fields of the dicts index.
+    The record keeps the arrays it points at alive."""
     e = abi.SceneExt()
     e.structSize = C.sizeof(abi.SceneExt)
     if light_bvh is not None and len(light_bvh):
@@ -93,6 +95,11 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
     if material_textures is not None:
         mt = (abi.MaterialTextures * len(material_textures))()
         for i, t in enumerate(material_textures):
+            if isinstance(t, dict):
+                x = dict(MATERIAL_TEXTURES_DEFAULT, **t)
+                for k, val in x.items():
+                    setattr(mt[i], k, val)
+                continue
             # an int (reflectance texture) or (reflectance, normal map, strength, flip green
             # [, bump map, bump channel, bump scale])
             v = (t, -1, 1.0, False) if isinstance(t, (int, np.integer)) else tuple(t)
@@ -100,15 +107,41 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
             mt[i].reflectance, mt[i].normalMap = int(v[0]), int(v[1])
             mt[i].normalStrength, mt[i].normalFlipGreen = float(v[2]), 1 if v[3] else 0
             mt[i].bumpMap, mt[i].bumpChannel, mt[i].bumpScale = int(v[4]), int(v[5]), float(v[6])
+            mt[i].reflectanceNode = mt[i].bumpNode = mt[i].roughnessNodeU = mt[i].roughnessNodeV = -1
         e.materialTextureCount = len(mt)
         e.materialTextures = C.cast(mt, C.c_void_p)
         e._keep.append(mt)
+    if texture_nodes:
+        arr = (abi.TextureNode * len(texture_nodes))(*texture_nodes)
+        e.textureNodeCount = len(arr)
+        e.textureNodes = C.cast(arr, C.c_void_p)
+        e._keep.append(arr)
     if rgb_to_spectrum is not None:
         table = np.ascontiguousarray(rgb_to_spectrum, np.float32)
         assert table.size == 64 + 3 * 64 ** 3 * 3
         e.rgbToSpectrum = table.ctypes.data
         e._keep.append(table)
     return e
+
+
+MATERIAL_TEXTURES_DEFAULT = {"reflectance": -1, "normalMap": -1, "normalStrength": 1.0, "normalFlipGreen": 0,
+                             "bumpMap": -1, "bumpChannel": -1, "bumpScale": 0.01, "reflectanceNode": -1,
+                             "bumpNode": -1, "roughnessNodeU": -1, "roughnessNodeV": -1}
+
+
+def texture_node(kind: int, a: int = -1, b: int = -1, t: int = -1, channel: int = -1, value: float = 0.0,
+                 frequency: float = 4.0, octaves: int = 5, turbulence: bool = False, world_space: bool = True,
+                 offset=(0.0, 0.0, 0.0), uv_scale=(1.0, 1.0), uv_offset=(0.0, 0.0)) -> abi.TextureNode:
+    """A TextureNode (abi.TEX_CONSTANT / TEX_IMAGE / TEX_CHECKER / TEX_NOISE / TEX_MIX); the
+    defaults are the reference loader's (noise: frequency 4, 5 octaves, world space)."""
+    n = abi.TextureNode()
+    n.type, n.a, n.b, n.t, n.channel, n.value = kind, a, b, t, channel, value
+    n.frequency, n.octaves = frequency, octaves
+    n.flags = (abi.TEX_NOISE_TURBULENCE if turbulence else 0) | (abi.TEX_NOISE_WORLD if world_space else 0)
+    n.offset[:] = [float(v) for v in offset]
+    n.scaleU, n.scaleV = float(uv_scale[0]), float(uv_scale[1])
+    n.offsetU, n.offsetV = float(uv_offset[0]), float(uv_offset[1])
+    return n
 
 
 def image_texture(rgb: np.ndarray, wrap: int = abi.WRAP_REPEAT, flip_v: bool = True, uv_scale=(1.0, 1.0),

@@ -279,11 +279,41 @@ struct ImageTextureDesc {
     uint32_t pad;
 };
 
+// A node of a procedural texture tree (pr::CheckerSpectrumTexture / CheckerFloatTexture,
+// NoiseFloatTexture, MixSpectrumTexture / MixFloatTexture and their constant and image leaves:
+// texture.h:35-205). A tree is used either as a spectrum texture (reflectance) or as a float
+// texture (bump height, roughness); its root is named by MaterialTextures.
+//   TexConstant  spectrum use: a = SceneDesc::spectra index; float use: value
+//   TexImage     a = SceneExt::textures index; spectrum use: the looked-up colour times rgbScale,
+//                uplifted as an albedo; float use: `channel` (-1 the mean of r, g, b) times
+//                rgbScale (the float texture's multiplier in all three components)
+//   TexChecker   a where floor(s) + floor(t) is even, else b; (s, t) = uv * scale + offset
+//   TexNoise     float use only: fBm of improved Perlin noise at (p + offset) * frequency, p the
+//                hit point (flags & TexNoiseWorldSpace) or (u, v, 0); octaves in [1, 32]
+//   TexMix       a (1 - t) + b t, t = node `t` (a TexNoise node) clamped to [0, 1]
+// Trees are at most 8 nodes deep.
+enum TextureNodeType : uint32_t { TexConstant = 0, TexImage = 1, TexChecker = 2, TexNoise = 3, TexMix = 4 };
+enum TextureNoiseFlags : uint32_t { TexNoiseTurbulence = 1, TexNoiseWorldSpace = 2 };
+struct TextureNode {
+    uint32_t type;
+    int32_t a, b, t;
+    int32_t channel;
+    float value;
+    float frequency;
+    int32_t octaves;
+    uint32_t flags;
+    float offset[3];
+    float scaleU, scaleV, offsetU, offsetV;
+};
+
 // Per SceneDesc material: the image texture of its reflectance (diffuse and coated diffuse
 // materials), of its tangent-space normal map and of its bump (height) map (any material;
 // pr::NormalMapParams / BumpMapParams, material.h:30-41, applied as Material::PerturbShading,
 // material.cpp:16-60), -1 for none. A height map's texture carries the float texture's
-// multiplier in all three rgbScale components.
+// multiplier in all three rgbScale components. The *Node fields name TextureNode trees instead
+// (-1 none); a reflectance or bump tree takes precedence over the image of the same slot, and the
+// roughness trees replace the GGX roughness (alpha = clamp(r, 0, 1)^2) of conductor, rough
+// dielectric and coated-conductor base lobes, each direction separately.
 struct MaterialTextures {
     int32_t reflectance;
     int32_t normalMap;
@@ -292,6 +322,10 @@ struct MaterialTextures {
     int32_t bumpMap;
     int32_t bumpChannel;       // -1 the mean of r, g, b; 0, 1, 2 one channel
     float bumpScale;
+    int32_t reflectanceNode;
+    int32_t bumpNode;
+    int32_t roughnessNodeU;
+    int32_t roughnessNodeV;
     uint32_t pad;
 };
 
@@ -319,6 +353,9 @@ struct SceneExt {
     // RGB -> sigmoid-polynomial table (pr::RGBToSpectrumTable, rgb2spec.h:28-46): zNodes[64] then
     // coefficients[3][64][64][64][3]; required when a material has a texture.
     const float *rgbToSpectrum;
+    const TextureNode *textureNodes;
+    int32_t textureNodeCount;
+    int32_t pad2;
 };
 
 // Parameters of prgpu_render_aov (pr::RenderAOV, src/integrators/aov.h:10-21).

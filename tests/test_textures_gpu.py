@@ -233,3 +233,93 @@ def test_bump_maps_agree_with_reference(gpu, oracle):
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
+
+
+def _with_albedo_spectra(rs, rgbs):
+    """The exported scene with the RGBAlbedoSpectrum of each colour appended to its spectra; the
+    appended rows' indices."""
+    import ctypes as C
+
+    import ref as oracle_ref
+    from prgpu import spectra
+
+    base = abi.SceneDesc.from_address(rs.export())
+    sd = abi.SceneDesc()
+    C.memmove(C.addressof(sd), C.addressof(base), C.sizeof(sd))
+    old = np.ctypeslib.as_array((C.c_float * (95 * base.spectrumCount)).from_address(base.spectra)).reshape(-1, 95)
+    lam = spectra.LAMBDA.astype(np.float32)
+    rows = []
+    for rgb in rgbs:
+        out = np.zeros(95, np.float32)
+        assert oracle_ref.ref_lib().prref_spectrum(0, *[float(v) for v in rgb], None, 95, oracle_ref._p(lam),
+                                                   oracle_ref._p(out)) == 0
+        rows.append(out)
+    table = np.ascontiguousarray(np.concatenate([old, np.stack(rows)]), np.float32)
+    sd.spectra = table.ctypes.data
+    sd.spectrumCount = table.shape[0]
+    sd._keep = table
+    return sd, list(range(base.spectrumCount, base.spectrumCount + len(rgbs)))
+
+
+def test_procedural_textures_agree_with_reference(gpu, oracle):
+    """Texture trees against the reference's checker / noise / mix textures: a ground whose
+    reflectance is a checker of a colour and a world-space noise blend of two colours, bump-mapped by
+    world-space fBm noise; a sphere whose reflectance blends an image and a colour by uv-space noise;
+    a gold sphere whose roughness is a turbulence blend of 0.1 and 0.6. The same z statistics as
+    above."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    img = _texture()
+    pfm = os.path.join(d, "proc_img.pfm")
+    _write_pfm(pfm, img)
+    doc = ru_outdoor_doc(w, h, pfm)
+    c0, c1, c2, c3 = [0.8, 0.3, 0.2], [0.1, 0.2, 0.7], [0.9, 0.9, 0.6], [0.2, 0.5, 0.3]
+    doc["textures"] = {
+        "chk": {"type": "checker", "a": c0, "b": {"texture": "blend"}, "uv_scale": [4.0, 4.0]},
+        "blend": {"type": "noise", "a": c1, "b": c2, "frequency": 3.0, "octaves": 4, "offset": [0.3, 0.1, -0.2]},
+        "bump": {"type": "noise", "frequency": 2.5},
+        "img": {"type": "image", "file": pfm, "colorspace": "linear", "wrap": "repeat", "flip_v": True,
+                "uv_scale": [2.0, 2.0]},
+        "mixed": {"type": "noise", "a": {"texture": "img"}, "b": c3, "frequency": 8.0, "octaves": 2, "space": "uv"},
+        "rough": {"type": "noise", "a": 0.1, "b": 0.6, "frequency": 5.0, "octaves": 3, "space": "uv",
+                  "turbulence": True},
+    }
+    doc["materials"] = {"ground": {"type": "diffuse", "reflectance": {"texture": "chk"},
+                                   "bump_map": {"texture": "bump", "scale": 0.2}},
+                        "red": {"type": "diffuse", "reflectance": {"texture": "mixed"}},
+                        "tex_coat": {"type": "conductor", "metal": "Au", "roughness": {"texture": "rough"}}}
+    path = os.path.join(d, "procedural.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    sd, (s0, s1, s2, s3) = _with_albedo_spectra(rs, [c0, c1, c2, c3])
+    T = render.texture_node
+    nodes = [T(abi.TEX_CONSTANT, a=s0), T(abi.TEX_CONSTANT, a=s1), T(abi.TEX_CONSTANT, a=s2),
+             T(abi.TEX_NOISE, frequency=3.0, octaves=4, offset=(0.3, 0.1, -0.2)),
+             T(abi.TEX_MIX, a=1, b=2, t=3), T(abi.TEX_CHECKER, a=0, b=4, uv_scale=(4.0, 4.0)),
+             T(abi.TEX_NOISE, frequency=2.5),
+             T(abi.TEX_IMAGE, a=0), T(abi.TEX_CONSTANT, a=s3), T(abi.TEX_NOISE, frequency=8.0, octaves=2, world_space=False),
+             T(abi.TEX_MIX, a=7, b=8, t=9),
+             T(abi.TEX_CONSTANT, value=0.1), T(abi.TEX_CONSTANT, value=0.6),
+             T(abi.TEX_NOISE, frequency=5.0, octaves=3, world_space=False, turbulence=True), T(abi.TEX_MIX, a=11, b=12, t=13)]
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    slots = {"ground": {"reflectanceNode": 5, "bumpNode": 6, "bumpScale": 0.2}, "red": {"reflectanceNode": 10},
+             "tex_coat": {"roughnessNodeU": 14, "roughnessNodeV": 14}}
+    ext = render.make_ext(textures=[render.image_texture(img, uv_scale=(2.0, 2.0))],
+                          material_textures=[slots.get(n, {}) for n in used], texture_nodes=nodes,
+                          rgb_to_spectrum=_uplift_table())
+    g = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"procedural textures: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
