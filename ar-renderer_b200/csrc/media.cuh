@@ -8,6 +8,7 @@
 // collisions in sparse media).
 #pragma once
 
+#include "noise.cuh"
 #include "scene.cuh"
 
 namespace prb {
@@ -32,11 +33,27 @@ __device__ __forceinline__ float grid_at(const DevGrid &g, int x, int y, int z) 
 
 __device__ __forceinline__ float lerpf(float t, float a, float b) { return (1.f - t) * a + t * b; }
 
-// Density at a medium-space point: 0 outside the bounds, trilinear between cell centres inside.
+// pr::NoiseField::Density (medium.cpp:168-177) at a medium-space point inside the bounds: the
+// remapped fBm, faded towards the bounds' inscribed ellipsoid, thresholded and sharpened.
+__device__ __noinline__ float noise_field_density(const DevGrid &g, V3 p) {
+    const V3 q = (p + mk(g.noiseOffset[0], g.noiseOffset[1], g.noiseOffset[2])) * g.noiseFrequency;
+    float n = 0.5f + 0.5f * fbm_noise(q, g.noiseOctaves, false) * 1.4f;
+    if (g.noiseFalloff) {
+        const float ox = (p.x - g.bmin[0]) / (g.bmax[0] - g.bmin[0]) * 2.f - 1.f;
+        const float oy = (p.y - g.bmin[1]) / (g.bmax[1] - g.bmin[1]) * 2.f - 1.f;
+        const float oz = (p.z - g.bmin[2]) / (g.bmax[2] - g.bmin[2]) * 2.f - 1.f;
+        n *= clampf(1.f - (ox * ox + oy * oy + oz * oz), 0.f, 1.f);
+    }
+    return clampf((n - g.noiseThreshold) * g.noiseSharpness, 0.f, 1.f);
+}
+
+// Density at a medium-space point: 0 outside the bounds, trilinear between cell centres inside
+// (or the noise field's).
 __device__ __forceinline__ float grid_density(const DevGrid &g, V3 p) {
     if (!(p.x >= g.bmin[0] && p.x <= g.bmax[0] && p.y >= g.bmin[1] && p.y <= g.bmax[1] && p.z >= g.bmin[2] &&
           p.z <= g.bmax[2]))
         return 0.f;
+    if (g.noise) return noise_field_density(g, p);
     float ox = p.x - g.bmin[0], oy = p.y - g.bmin[1], oz = p.z - g.bmin[2];
     if (g.bmax[0] > g.bmin[0]) ox /= g.bmax[0] - g.bmin[0];
     if (g.bmax[1] > g.bmin[1]) oy /= g.bmax[1] - g.bmin[1];

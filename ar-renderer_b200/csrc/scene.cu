@@ -80,7 +80,8 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
         for (int32_t k = 0; k < ext->gridMediumCount; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
             h = fnv_v(h, g);
-            h = sample_hash(h, g.density, size_t(g.nx) * size_t(g.ny) * size_t(g.nz), sizeof(float), 65536);
+            if (g.field == prgpu::GridVoxels)
+                h = sample_hash(h, g.density, size_t(g.nx) * size_t(g.ny) * size_t(g.nz), sizeof(float), 65536);
         }
     return h;
 }
@@ -146,8 +147,17 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
     if (ng > 0 && !ext->gridMedia) return fail("null grid media");
     for (int32_t k = 0; k < ng; ++k) {
         const prgpu::GridMediumDesc &g = ext->gridMedia[k];
-        if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || int64_t(g.nx) * g.ny * g.nz > (int64_t(1) << 31) || !g.density)
+        if (g.field > prgpu::GridNoise) return fail("unknown grid medium field");
+        if (g.field == prgpu::GridNoise) {
+            if (g.noiseOctaves < 1 || g.noiseOctaves > 32 || !std::isfinite(g.noiseFrequency) ||
+                !std::isfinite(g.noiseThreshold) || !std::isfinite(g.noiseSharpness) || !std::isfinite(g.noiseOffset[0]) ||
+                !std::isfinite(g.noiseOffset[1]) || !std::isfinite(g.noiseOffset[2]))
+                return fail("bad noise medium parameters");
+            if (!(g.boundsMin.x < g.boundsMax.x && g.boundsMin.y < g.boundsMax.y && g.boundsMin.z < g.boundsMax.z))
+                return fail("noise media need non-empty bounds");
+        } else if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || int64_t(g.nx) * g.ny * g.nz > (int64_t(1) << 31) || !g.density) {
             return fail("bad grid medium dimensions or data");
+        }
         if (!spec_ok(g.sigmaA, ns) || !spec_ok(g.sigmaS, ns)) return fail("grid medium spectrum index out of range");
         if (!(g.boundsMin.x <= g.boundsMax.x && g.boundsMin.y <= g.boundsMax.y && g.boundsMin.z <= g.boundsMax.z))
             return fail("empty grid medium bounds");
@@ -615,17 +625,42 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         size_t total = 0;
         for (int32_t k = 0; k < ng; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
-            total += size_t(g.nx) * g.ny * g.nz + size_t(macro_cells(g.nx)) * macro_cells(g.ny) * macro_cells(g.nz);
+            if (g.field == prgpu::GridNoise) total += 1;
+            else total += size_t(g.nx) * g.ny * g.nz + size_t(macro_cells(g.nx)) * macro_cells(g.ny) * macro_cells(g.nz);
         }
         cache.gridData.ensure(std::max<size_t>(1, total) * sizeof(float));
         size_t off = 0;
         for (int32_t k = 0; k < ng; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
-            size_t n = size_t(g.nx) * g.ny * g.nz;
             DevGrid &dg = grids[size_t(k)];
             std::memcpy(dg.w2m, g.worldToMedium, sizeof(dg.w2m));
             dg.bmin[0] = g.boundsMin.x, dg.bmin[1] = g.boundsMin.y, dg.bmin[2] = g.boundsMin.z;
             dg.bmax[0] = g.boundsMax.x, dg.bmax[1] = g.boundsMax.y, dg.bmax[2] = g.boundsMax.z;
+            dg.scale = g.scale;
+            dg.g = std::min(0.99f, std::max(-0.99f, g.g));
+            dg.sigmaA = g.sigmaA;
+            dg.sigmaS = g.sigmaS;
+            dg.noise = g.field == prgpu::GridNoise ? 1 : 0;
+            if (dg.noise) {
+                // One macro cell over the bounds with the field's maximum density (1).
+                dg.nx = dg.ny = dg.nz = 0;
+                dg.density = nullptr;
+                dg.maxDensity = std::max(1.f, std::isfinite(g.maxDensity) ? g.maxDensity : 1.f);
+                dg.mx = dg.my = dg.mz = 1;
+                dg.noiseOctaves = g.noiseOctaves;
+                dg.noiseFalloff = g.noiseFalloff ? 1 : 0;
+                dg.noiseFrequency = g.noiseFrequency;
+                dg.noiseThreshold = g.noiseThreshold;
+                dg.noiseSharpness = g.noiseSharpness;
+                std::memcpy(dg.noiseOffset, g.noiseOffset, sizeof(dg.noiseOffset));
+                dg.majorant = cache.gridData.as<float>() + off;
+                PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.majorant), &dg.maxDensity, sizeof(float),
+                                         cudaMemcpyHostToDevice, s));
+                PRB_CUDA(cudaStreamSynchronize(s));
+                off += 1;
+                continue;
+            }
+            size_t n = size_t(g.nx) * g.ny * g.nz;
             dg.nx = g.nx, dg.ny = g.ny, dg.nz = g.nz;
             // Negative or non-finite voxels read as 0, as pr::VoxelGridField does (medium.cpp:108-115).
             float mx = 0.f;

@@ -29,6 +29,10 @@ struct DevGrid {
     // trilinear density anywhere in the cell (a one-voxel margin on every side).
     int mx, my, mz;
     const float *majorant;
+    // pr::NoiseField in place of the voxels (noise != 0).
+    int noise, noiseOctaves, noiseFalloff;
+    float noiseFrequency, noiseThreshold, noiseSharpness;
+    float noiseOffset[3];
 };
 
 // Shading classes: the closest-hit kernel files every finished path under one of these, and the

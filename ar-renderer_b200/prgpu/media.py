@@ -82,6 +82,28 @@ def grid_desc(sigma_a: int, sigma_s: int, density: np.ndarray, bounds, scale: fl
     return r
 
 
+def noise_desc(sigma_a: int, sigma_s: int, bounds, scale: float = 1.0, g: float = 0.0,
+               world_to_medium: np.ndarray | None = None, frequency: float = 1.5, octaves: int = 5,
+               threshold: float = 0.45, sharpness: float = 4.0, falloff: bool = True,
+               offset=(0.0, 0.0, 0.0)) -> abi.GridMediumDesc:
+    """A GridMediumDesc of a procedural noise field (pr::NoiseField; the defaults are the reference
+    loader's) over the medium-space box `bounds`."""
+    r = abi.GridMediumDesc()
+    r.sigmaA, r.sigmaS, r.scale, r.g = sigma_a, sigma_s, scale, g
+    w = np.eye(4, dtype=np.float32)[:3] if world_to_medium is None else np.asarray(world_to_medium, np.float32)
+    for i, v in enumerate(w.reshape(12)):
+        r.worldToMedium[i] = float(v)
+    b = np.asarray(bounds, dtype=np.float32).reshape(2, 3)
+    for i in range(3):
+        r.boundsMin[i] = float(b[0, i])
+        r.boundsMax[i] = float(b[1, i])
+    r.field = abi.GRID_NOISE
+    r.noiseOctaves, r.noiseFrequency = octaves, frequency
+    r.noiseThreshold, r.noiseSharpness, r.noiseFalloff = threshold, sharpness, 1 if falloff else 0
+    r.noiseOffset[:] = [float(v) for v in offset]
+    return r
+
+
 def grid_array(descs) -> C.Array:
     """A contiguous GridMediumDesc array for SceneExt::gridMedia (keeps the densities alive)."""
     arr = (abi.GridMediumDesc * len(descs))(*descs)

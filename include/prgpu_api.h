@@ -208,6 +208,11 @@ struct LightBVHNode {
 // Distances are sampled by spectral tracking and shadow transmittance by ratio tracking against a
 // global majorant maxDensity * max(sigma_t) (medium.cpp:205-285). Media are referenced from
 // Primitive::mediumInside/Outside and SceneDesc::cameraMedium with indices mediumCount + k.
+// field = GridNoise replaces the voxels by pr::NoiseField (medium.h:119-133, medium.cpp:168-177):
+// density = clamp((n - threshold) * sharpness, 0, 1) with n = 0.5 + 0.7 fBm((p + offset) *
+// frequency) of improved Perlin noise, faded by 1 - |2 (p - min) / (max - min) - 1|^2 when falloff
+// is set; 0 outside the (non-empty) bounds; the majorant is 1 unless maxDensity says more.
+enum GridField : uint32_t { GridVoxels = 0, GridNoise = 1 };
 struct GridMediumDesc {
     int32_t sigmaA, sigmaS;     // spectrum indices
     float scale, g;
@@ -216,6 +221,12 @@ struct GridMediumDesc {
     int32_t nx, ny, nz;
     float maxDensity;           // >= every voxel; 0 = computed from the data
     const float *density;       // nx * ny * nz floats, x fastest: index (z * ny + y) * nx + x
+    uint32_t field;             // GridField
+    int32_t noiseOctaves;       // [1, 32]
+    float noiseFrequency, noiseThreshold, noiseSharpness;
+    uint32_t noiseFalloff;
+    float noiseOffset[3];
+    uint32_t pad;
 };
 
 // Image environment light (pr::EnvironmentLight with a map, src/lights/light.cpp:217-297), as a

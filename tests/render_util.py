@@ -24,10 +24,11 @@ def grid_scene_file(name: str, **kw):
     return scenes.write_reference_json(s, os.path.join(_DIR, name + ".prscene.json")), s
 
 
-def grid_scene_inputs(rs, s):
+def grid_scene_inputs(rs, s, noise=None):
     """The GPU-side inputs of a grid scene loaded by the reference: the exported SceneDesc with the
     smoke's sigma_a / sigma_s tables appended (RGB-unbounded spectra, evaluated by the reference
-    at the 95 table wavelengths), and a SceneExt carrying the grid as medium mediumCount + 0."""
+    at the 95 table wavelengths), and a SceneExt carrying the grid as medium mediumCount + 0.
+    noise: media.noise_desc keyword arguments, for the scene's noise-field variant."""
     import ctypes as C
 
     import ref as oracle_ref
@@ -51,8 +52,12 @@ def grid_scene_inputs(rs, s):
     grids = rs.grid_media()
     assert [g[0] for g in grids] == ["smoke"], grids
     na = base.spectrumCount
-    desc = media.grid_desc(na, na + 1, s.grid["density"], grids[0][1], scale=s.grid["scale"], g=s.grid["g"],
-                           world_to_medium=media.affine_inverse(s.grid["matrix"]))
+    if noise is not None:
+        desc = media.noise_desc(na, na + 1, grids[0][1], scale=s.grid["scale"], g=s.grid["g"],
+                                world_to_medium=media.affine_inverse(s.grid["matrix"]), **noise)
+    else:
+        desc = media.grid_desc(na, na + 1, s.grid["density"], grids[0][1], scale=s.grid["scale"], g=s.grid["g"],
+                               world_to_medium=media.affine_inverse(s.grid["matrix"]))
     ext = render.make_ext(grid_media=[desc])
     sd._keep = table
     return sd, ext

@@ -37,6 +37,42 @@ def test_grid_smoke_agrees_with_reference_path_tracer(gpu, oracle):
     assert abs(yg / yc - 1) < 0.02, f"mean Y gpu {yg} cpu {yc}"
 
 
+@pytest.mark.parametrize("falloff", [True, False])
+def test_noise_medium_agrees_with_reference_path_tracer(gpu, oracle, falloff):
+    """The smoke room with a procedural noise field in place of the voxels (pr::NoiseField,
+    medium.cpp:168-177: fBm of improved Perlin noise, thresholded and sharpened, with and without
+    the ellipsoidal falloff), loaded by the reference from a "noise" medium: the same z statistics
+    as the voxel smoke."""
+    import json
+
+    w = h = 32
+    path, s = ru.grid_scene_file("noise_smoke_src", seed=0, width=w, height=h)
+    with open(path) as f:
+        doc = json.load(f)
+    params = {"frequency": 2.0, "octaves": 4, "threshold": 0.1 if falloff else 0.35, "sharpness": 3.0,
+              "offset": [0.2, -0.1, 0.4]}
+    smoke = doc["media"]["smoke"]
+    smoke.pop("file")
+    smoke.update(type="noise", falloff="ellipsoid" if falloff else "none", **params)
+    path = path.replace("noise_smoke_src", f"noise_smoke_{int(falloff)}")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    sd, ext = ru.grid_scene_inputs(rs, s, noise=dict(params, falloff=falloff))
+    g = _gpu_seeds(sd, ext, w, h, 128, 16, 8)
+    c = _cpu_seeds(rs, 128, 16, 8)
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    yg, yc = g[..., 1].mean(), c[..., 1].mean()
+    print(f"noise medium falloff={falloff}: frac {frac:.4f}, mean Y gpu {yg:.5f} cpu {yc:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(yg / yc - 1) < 0.02, f"mean Y gpu {yg} cpu {yc}"
+    # The field matters: thresholded to nothing, the room renders clearly brighter or darker.
+    _, eext = ru.grid_scene_inputs(rs, s, noise=dict(params, falloff=falloff, threshold=2.0))
+    ye = _gpu_seeds(sd, eext, w, h, 64, 2, 8)[..., 1].mean()
+    assert abs(ye / yc - 1) > 0.05, f"empty field mean Y {ye}, smoke {yc}"
+
+
 def test_constant_grid_equals_homogeneous_medium(gpu, oracle):
     """A grid of constant density 0.7 covering the whole interface box is the homogeneous medium of
     sigma * 0.7: spectral/ratio tracking on one side, hero-wavelength free flight and Beer-Lambert
@@ -94,4 +130,4 @@ def test_grid_medium_input_validation(gpu, oracle):
     # The scene references medium index mediumCount + 0; without the extension it is out of range.
     with pytest.raises(abi.PrgpuError, match="(?i)medium"):
         render.render_ex(sd, w, h, 1)
-    assert C.sizeof(abi.GridMediumDesc) == 112
+    assert C.sizeof(abi.GridMediumDesc) == 152
