@@ -47,13 +47,34 @@ __device__ __noinline__ float noise_field_density(const DevGrid &g, V3 p) {
     return clampf((n - g.noiseThreshold) * g.noiseSharpness, 0.f, 1.f);
 }
 
+// Density of an index-space grid (a densified NanoVDB grid; NanoVDBField::Density,
+// nanovdb_field.cpp:27-39): trilinear between voxel centres at integer coordinates, the background
+// 0 beyond the array, clamped at 0.
+__device__ __noinline__ float indexed_density(const DevGrid &g, V3 p) {
+    const float x = p.x - float(g.org[0]), y = p.y - float(g.org[1]), z = p.z - float(g.org[2]);
+    const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    const int x0 = int(fx), y0 = int(fy), z0 = int(fz);
+    const float dx = x - fx, dy = y - fy, dz = z - fz;
+    auto v = [&](int i, int j, int k) {
+        i += x0;
+        j += y0;
+        k += z0;
+        if (i < 0 || j < 0 || k < 0 || i >= g.nx || j >= g.ny || k >= g.nz) return 0.f;
+        return __ldg(g.density + (size_t(k) * g.ny + j) * g.nx + i);
+    };
+    const float c00 = lerpf(dx, v(0, 0, 0), v(1, 0, 0)), c10 = lerpf(dx, v(0, 1, 0), v(1, 1, 0));
+    const float c01 = lerpf(dx, v(0, 0, 1), v(1, 0, 1)), c11 = lerpf(dx, v(0, 1, 1), v(1, 1, 1));
+    return fmaxf(0.f, lerpf(dz, lerpf(dy, c00, c10), lerpf(dy, c01, c11)));
+}
+
 // Density at a medium-space point: 0 outside the bounds, trilinear between cell centres inside
-// (or the noise field's).
+// (or the noise field's, or the index-space grid's).
 __device__ __forceinline__ float grid_density(const DevGrid &g, V3 p) {
     if (!(p.x >= g.bmin[0] && p.x <= g.bmax[0] && p.y >= g.bmin[1] && p.y <= g.bmax[1] && p.z >= g.bmin[2] &&
           p.z <= g.bmax[2]))
         return 0.f;
     if (g.noise) return noise_field_density(g, p);
+    if (g.indexed) return indexed_density(g, p);
     float ox = p.x - g.bmin[0], oy = p.y - g.bmin[1], oz = p.z - g.bmin[2];
     if (g.bmax[0] > g.bmin[0]) ox /= g.bmax[0] - g.bmin[0];
     if (g.bmax[1] > g.bmin[1]) oy /= g.bmax[1] - g.bmin[1];

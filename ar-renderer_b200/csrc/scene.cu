@@ -80,7 +80,7 @@ uint64_t scene_key(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext) {
         for (int32_t k = 0; k < ext->gridMediumCount; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
             h = fnv_v(h, g);
-            if (g.field == prgpu::GridVoxels)
+            if (g.field != prgpu::GridNoise)
                 h = sample_hash(h, g.density, size_t(g.nx) * size_t(g.ny) * size_t(g.nz), sizeof(float), 65536);
         }
     return h;
@@ -147,7 +147,10 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
     if (ng > 0 && !ext->gridMedia) return fail("null grid media");
     for (int32_t k = 0; k < ng; ++k) {
         const prgpu::GridMediumDesc &g = ext->gridMedia[k];
-        if (g.field > prgpu::GridNoise) return fail("unknown grid medium field");
+        if (g.field > prgpu::GridIndexed) return fail("unknown grid medium field");
+        if (g.field == prgpu::GridIndexed &&
+            !(g.boundsMin.x < g.boundsMax.x && g.boundsMin.y < g.boundsMax.y && g.boundsMin.z < g.boundsMax.z))
+            return fail("index-space grids need non-empty bounds");
         if (g.field == prgpu::GridNoise) {
             if (g.noiseOctaves < 1 || g.noiseOctaves > 32 || !std::isfinite(g.noiseFrequency) ||
                 !std::isfinite(g.noiseThreshold) || !std::isfinite(g.noiseSharpness) || !std::isfinite(g.noiseOffset[0]) ||
@@ -626,6 +629,7 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
         for (int32_t k = 0; k < ng; ++k) {
             const prgpu::GridMediumDesc &g = ext->gridMedia[k];
             if (g.field == prgpu::GridNoise) total += 1;
+            else if (g.field == prgpu::GridIndexed) total += size_t(g.nx) * g.ny * g.nz + 1;
             else total += size_t(g.nx) * g.ny * g.nz + size_t(macro_cells(g.nx)) * macro_cells(g.ny) * macro_cells(g.nz);
         }
         cache.gridData.ensure(std::max<size_t>(1, total) * sizeof(float));
@@ -662,6 +666,29 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
             }
             size_t n = size_t(g.nx) * g.ny * g.nz;
             dg.nx = g.nx, dg.ny = g.ny, dg.nz = g.nz;
+            if (g.field == prgpu::GridIndexed) {
+                // Raw voxels (non-finite ones read as 0; the trilinear result is clamped at 0) and
+                // one macro cell with the largest voxel.
+                dg.indexed = 1;
+                std::memcpy(dg.org, g.indexOrigin, sizeof(dg.org));
+                std::vector<float> raw(g.density, g.density + n);
+                float mx = 0.f;
+                for (float &v : raw) {
+                    if (!std::isfinite(v)) v = 0.f;
+                    mx = std::max(mx, v);
+                }
+                dg.maxDensity = std::max(mx, std::isfinite(g.maxDensity) ? g.maxDensity : 0.f);
+                dg.mx = dg.my = dg.mz = 1;
+                dg.density = cache.gridData.as<float>() + off;
+                dg.majorant = dg.density + n;
+                PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.density), raw.data(), n * sizeof(float),
+                                         cudaMemcpyHostToDevice, s));
+                PRB_CUDA(cudaMemcpyAsync(const_cast<float *>(dg.majorant), &dg.maxDensity, sizeof(float),
+                                         cudaMemcpyHostToDevice, s));
+                PRB_CUDA(cudaStreamSynchronize(s));
+                off += n + 1;
+                continue;
+            }
             // Negative or non-finite voxels read as 0, as pr::VoxelGridField does (medium.cpp:108-115).
             float mx = 0.f;
             for (size_t i = 0; i < n; ++i)

@@ -33,6 +33,9 @@ struct DevGrid {
     int noise, noiseOctaves, noiseFalloff;
     float noiseFrequency, noiseThreshold, noiseSharpness;
     float noiseOffset[3];
+    // Index-space voxels (indexed != 0): voxel (x, y, z) at integer coordinate org + (x, y, z).
+    int indexed;
+    int org[3];
 };
 
 // Shading classes: the closest-hit kernel files every finished path under one of these, and the

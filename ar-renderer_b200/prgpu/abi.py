@@ -110,10 +110,10 @@ class GridMediumDesc(C.Structure):
                 ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("maxDensity", C.c_float),
                 ("density", C.c_void_p), ("field", C.c_uint32), ("noiseOctaves", C.c_int32),
                 ("noiseFrequency", C.c_float), ("noiseThreshold", C.c_float), ("noiseSharpness", C.c_float),
-                ("noiseFalloff", C.c_uint32), ("noiseOffset", C.c_float * 3), ("pad", C.c_uint32)]
+                ("noiseFalloff", C.c_uint32), ("noiseOffset", C.c_float * 3), ("indexOrigin", C.c_int32 * 3)]
 
 
-GRID_VOXELS, GRID_NOISE = 0, 1
+GRID_VOXELS, GRID_NOISE, GRID_INDEXED = 0, 1, 2
 
 
 class EnvMapDesc(C.Structure):
@@ -208,7 +208,7 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 152 and C.sizeof(SceneExt) == 128 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(GridMediumDesc) == 160 and C.sizeof(SceneExt) == 128 and C.sizeof(DeltaLightDesc) == 104
 assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 48 and C.sizeof(TextureNode) == 64
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28

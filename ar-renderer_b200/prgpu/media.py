@@ -104,6 +104,21 @@ def noise_desc(sigma_a: int, sigma_s: int, bounds, scale: float = 1.0, g: float 
     return r
 
 
+def indexed_desc(sigma_a: int, sigma_s: int, density: np.ndarray, index_origin, index_bounds, scale: float = 1.0,
+                 g: float = 0.0, world_to_index: np.ndarray | None = None) -> abi.GridMediumDesc:
+    """A GridMediumDesc of an index-space grid (a densified NanoVDB float grid): density
+    ((nz, ny, nx) float32, kept alive by the record) holds the voxels at integer index coordinates
+    index_origin + (x, y, z); index_bounds: the clip box in index space; world_to_index: row-major
+    3x4 (world -> the grid's index space, through the medium's transform)."""
+    d = np.ascontiguousarray(density, dtype=np.float32)
+    if d.ndim != 3:
+        raise ValueError("density must be (nz, ny, nx)")
+    r = grid_desc(sigma_a, sigma_s, d, index_bounds, scale=scale, g=g, world_to_medium=world_to_index)
+    r.field = abi.GRID_INDEXED
+    r.indexOrigin[:] = [int(v) for v in index_origin]
+    return r
+
+
 def grid_array(descs) -> C.Array:
     """A contiguous GridMediumDesc array for SceneExt::gridMedia (keeps the densities alive)."""
     arr = (abi.GridMediumDesc * len(descs))(*descs)

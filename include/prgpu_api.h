@@ -212,7 +212,14 @@ struct LightBVHNode {
 // density = clamp((n - threshold) * sharpness, 0, 1) with n = 0.5 + 0.7 fBm((p + offset) *
 // frequency) of improved Perlin noise, faded by 1 - |2 (p - min) / (max - min) - 1|^2 when falloff
 // is set; 0 outside the (non-empty) bounds; the majorant is 1 unless maxDensity says more.
-enum GridField : uint32_t { GridVoxels = 0, GridNoise = 1 };
+// field = GridIndexed takes the voxels of an index-space grid: a NanoVDB float grid densified by
+// the caller (pr::NanoVDBField, media/nanovdb_field.cpp:17-46). Medium space is then the grid's
+// index space (worldToMedium = the grid's world-to-index map after the medium's own transform);
+// voxel (x, y, z) of `density` sits at the integer index coordinate indexOrigin + (x, y, z), the
+// density is trilinear between voxel centres, 0 beyond the array (the grid's background) and
+// clamped at 0; bounds (the grid's world box in index space) clip the segments; the majorant is
+// the largest voxel.
+enum GridField : uint32_t { GridVoxels = 0, GridNoise = 1, GridIndexed = 2 };
 struct GridMediumDesc {
     int32_t sigmaA, sigmaS;     // spectrum indices
     float scale, g;
@@ -226,7 +233,7 @@ struct GridMediumDesc {
     float noiseFrequency, noiseThreshold, noiseSharpness;
     uint32_t noiseFalloff;
     float noiseOffset[3];
-    uint32_t pad;
+    int32_t indexOrigin[3];     // GridIndexed
 };
 
 // Image environment light (pr::EnvironmentLight with a map, src/lights/light.cpp:217-297), as a

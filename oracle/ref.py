@@ -83,6 +83,8 @@ def ref_lib() -> C.CDLL:
         lib.prref_sun_radiance.argtypes = [_P, C.c_float, C.c_float, C.c_int64, _P, _P]
         lib.prref_scene_grid_count.argtypes = [_P]
         lib.prref_scene_grid_info.argtypes = [_P, C.c_int, C.c_char_p, C.c_int, _P]
+        lib.prref_scene_grid_density.argtypes = [_P, C.c_int, C.c_int64, _P, _P]
+        lib.prref_write_fog_sphere.argtypes = [C.c_char_p, C.c_double, C.c_double, C.c_double]
         # The RGB->spectrum table is built once (a few seconds) and cached beside the library.
         lib.prref_set_cache_dir(REF_DIR.encode())
         _ref = lib
@@ -199,6 +201,15 @@ class RefScene:
         n = self.lib.prref_scene_infinite(self.h, 64, _p(t), _p(p))
         return [(int(t[i]), float(p[i])) for i in range(min(n, 64))]
 
+    def grid_density(self, k: int, pts: np.ndarray) -> np.ndarray:
+        """Density of grid medium k's field at medium-space points (n, 3)."""
+        pts = np.ascontiguousarray(pts, dtype=np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.float32)
+        self.export()
+        if self.lib.prref_scene_grid_density(self.h, k, len(pts), _p(pts), _p(out)) != 0:
+            raise RuntimeError("no grid medium %d" % k)
+        return out
+
     def grid_media(self):
         """Heterogeneous media of the export, in index order (index = mediumCount + k): a list of
         (name, bounds (2, 3) float32 in medium space as the loader fitted them)."""
@@ -262,3 +273,11 @@ def sun_radiance(sun_dir, turbidity: float, radius_deg: float, lam: np.ndarray) 
     out = np.zeros(lam.shape[0], np.float32)
     ref_lib().prref_sun_radiance(_p(d), turbidity, radius_deg, lam.shape[0], _p(lam), _p(out))
     return out
+
+
+def write_fog_sphere(path: str, radius: float, voxel_size: float, half_width: float = 3.0) -> str:
+    """A NanoVDB fog-volume sphere (grid "density", centred at the origin, index -> world = index x
+    voxel_size) written with NanoVDB's own tools, as the reference's tests make one."""
+    if ref_lib().prref_write_fog_sphere(path.encode(), radius, voxel_size, half_width) != 0:
+        raise RuntimeError("cannot write " + path)
+    return path

@@ -1019,3 +1019,30 @@ API void prref_aov_matrices(float *adapt9, float *toRGB9) {
             toRGB9[3 * i + j] = m.m[i][j];
         }
 }
+
+// ---------------------------------------------------------------------------------------------
+// NanoVDB fixtures and field samples: a fog sphere written with NanoVDB's own tools (as the
+// reference's tests/test_media.cpp:134-143 makes one), and the density of a loaded scene's grid
+// medium k at medium-space points (pr::DensityField::Density, media/nanovdb_field.cpp:27-39 for a
+// NanoVDB field).
+#include <nanovdb/tools/CreatePrimitives.h>
+#include <fstream>
+
+API int prref_write_fog_sphere(const char *path, double radius, double voxelSize, double halfWidth) {
+    auto handle = nanovdb::tools::createFogVolumeSphere<float>(radius, nanovdb::Vec3d(0.0), voxelSize, halfWidth,
+                                                               nanovdb::Vec3d(0.0), "density");
+    std::ofstream os(path, std::ios::binary);
+    if (!os) return 1;
+    nanovdb::io::writeUncompressedGrid(os, handle.gridData());
+    return os.good() ? 0 : 1;
+}
+
+API int prref_scene_grid_density(void *hp, int k, int64_t n, const float *pts, float *out) {
+    auto *h = static_cast<SceneHandle *>(hp);
+    if (k < 0 || k >= int(h->grids.size())) return -1;
+    auto *gm = dynamic_cast<const GridMedium *>(h->grids[size_t(k)]);
+    if (!gm) return -1;
+    const DensityField &f = const_cast<GridMedium *>(gm)->Field();
+    for (int64_t i = 0; i < n; ++i) out[i] = f.Density(Vec3f(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]));
+    return 0;
+}

@@ -24,11 +24,47 @@ def grid_scene_file(name: str, **kw):
     return scenes.write_reference_json(s, os.path.join(_DIR, name + ".prscene.json")), s
 
 
-def grid_scene_inputs(rs, s, noise=None):
+def nvdb_scene_file(name: str, radius: float = 0.8, voxel_size: float = 0.04, **kw):
+    """(path, BoxScene) of the smoke room with a NanoVDB fog sphere (written by the oracle with
+    NanoVDB's tools) in place of the voxel smoke: the same medium transform, spectra and scale, no
+    "bounds" key, so the field's own world box clips."""
+    import json
+
+    import ref as oracle_ref
+
+    path, s = grid_scene_file(name + "_src", **kw)
+    with open(path) as f:
+        doc = json.load(f)
+    nvdb = oracle_ref.write_fog_sphere(os.path.join(_DIR, name + ".nvdb"), radius, voxel_size)
+    smoke = doc["media"]["smoke"]
+    smoke.pop("bounds")
+    smoke.update(file=nvdb, grid="density")
+    path = os.path.join(_DIR, name + ".prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    return path, s
+
+
+def densify_index_grid(rs, k: int, voxel_size: float):
+    """The grid medium k of a loaded scene as index-space voxels: the field sampled at the voxel
+    centres (integer index coordinates, medium point = index x voxel_size) over its world box plus
+    one voxel on every side. Returns (density (nz, ny, nx), index origin, index-space bounds)."""
+    b = rs.grid_media()[k][1].astype(np.float64)
+    lo = np.floor(b[0] / voxel_size).astype(int) - 1
+    hi = np.ceil(b[1] / voxel_size).astype(int) + 1
+    zs, ys, xs = [np.arange(lo[a], hi[a] + 1) for a in (2, 1, 0)]
+    z, y, x = np.meshgrid(zs, ys, xs, indexing="ij")
+    pts = (np.stack([x, y, z], -1).reshape(-1, 3) * voxel_size).astype(np.float32)
+    dens = rs.grid_density(k, pts).reshape(len(zs), len(ys), len(xs))
+    return dens, lo, (b / voxel_size).astype(np.float32)
+
+
+def grid_scene_inputs(rs, s, noise=None, indexed_voxel=None):
     """The GPU-side inputs of a grid scene loaded by the reference: the exported SceneDesc with the
     smoke's sigma_a / sigma_s tables appended (RGB-unbounded spectra, evaluated by the reference
     at the 95 table wavelengths), and a SceneExt carrying the grid as medium mediumCount + 0.
-    noise: media.noise_desc keyword arguments, for the scene's noise-field variant."""
+    noise: media.noise_desc keyword arguments, for the scene's noise-field variant; indexed_voxel:
+    the voxel size of the NanoVDB variant's grid, handed over densified in its index space."""
     import ctypes as C
 
     import ref as oracle_ref
@@ -52,7 +88,11 @@ def grid_scene_inputs(rs, s, noise=None):
     grids = rs.grid_media()
     assert [g[0] for g in grids] == ["smoke"], grids
     na = base.spectrumCount
-    if noise is not None:
+    if indexed_voxel is not None:
+        dens, org, ib = densify_index_grid(rs, 0, indexed_voxel)
+        w2i = media.affine_inverse(s.grid["matrix"]).astype(np.float64) / indexed_voxel
+        desc = media.indexed_desc(na, na + 1, dens, org, ib, scale=s.grid["scale"], g=s.grid["g"], world_to_index=w2i)
+    elif noise is not None:
         desc = media.noise_desc(na, na + 1, grids[0][1], scale=s.grid["scale"], g=s.grid["g"],
                                 world_to_medium=media.affine_inverse(s.grid["matrix"]), **noise)
     else:

@@ -83,3 +83,49 @@ def test_reference_loader_reads_the_written_grid(oracle, tmp_path):
     assert [g[0] for g in grids] == ["smoke"]
     assert np.array_equal(grids[0][1], s.grid["bounds"])
     assert desc.cameraMedium == desc.mediumCount + 0
+
+
+def _trilinear_index(dens, org, p):
+    """Trilinear between voxel centres at integer index coordinates org + (x, y, z), 0 beyond the
+    array, clamped at 0 (the index-space grid the device samples)."""
+    q = p - org
+    f = np.floor(q)
+    i0 = f.astype(int)
+    d = q - f
+    nz, ny, nx = dens.shape
+
+    def v(dx, dy, dz):
+        x, y, z = i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz
+        ok = (x >= 0) & (y >= 0) & (z >= 0) & (x < nx) & (y < ny) & (z < nz)
+        out = np.zeros(len(p))
+        out[ok] = dens[z[ok], y[ok], x[ok]]
+        return out
+
+    lx = lambda a, b: (1 - d[:, 0]) * a + d[:, 0] * b
+    c00, c10 = lx(v(0, 0, 0), v(1, 0, 0)), lx(v(0, 1, 0), v(1, 1, 0))
+    c01, c11 = lx(v(0, 0, 1), v(1, 0, 1)), lx(v(0, 1, 1), v(1, 1, 1))
+    ly = lambda a, b: (1 - d[:, 1]) * a + d[:, 1] * b
+    return np.maximum(0.0, (1 - d[:, 2]) * ly(c00, c10) + d[:, 2] * ly(c01, c11))
+
+
+def test_nanovdb_fog_sphere_and_its_index_space_voxels(oracle):
+    """A NanoVDB fog sphere written with NanoVDB's tools and loaded by the reference (as its
+    tests/test_media.cpp:134-148 does): density 1 at the centre (2 %), 0 outside; and the grid
+    densified at its voxel centres (the form the device takes) reproduces the reference field's
+    trilinear lookups at random points to 1e-5."""
+    import render_util as ru
+
+    vs = 0.05
+    path, s = ru.nvdb_scene_file("nvdb_pin", radius=1.0, voxel_size=vs, seed=0, width=8, height=8)
+    rs = oracle.RefScene(path)
+    (name, b), = rs.grid_media()
+    assert name == "smoke" and np.all(b[0] <= -0.9) and np.all(b[1] >= 0.9)
+    d0, d1 = rs.grid_density(0, np.array([[0, 0, 0], [1.5, 0, 0]], np.float32))
+    assert abs(d0 - 1.0) <= 0.02 and d1 == 0.0
+    dens, org, ib = ru.densify_index_grid(rs, 0, vs)
+    assert dens.max() <= 1.0 + 1e-6 and dens.min() >= 0.0
+    rng = np.random.default_rng(7)
+    p = rng.uniform(b[0] * 0.98, b[1] * 0.98, size=(20000, 3)).astype(np.float32)
+    want = rs.grid_density(0, p)
+    got = _trilinear_index(dens, org, p.astype(np.float64) / vs)
+    assert np.abs(got - want).max() <= 1e-5, np.abs(got - want).max()

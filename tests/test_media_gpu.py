@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 import render_util as ru
-from prgpu import render, scenes
+from prgpu import abi, render, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -73,6 +73,33 @@ def test_noise_medium_agrees_with_reference_path_tracer(gpu, oracle, falloff):
     assert abs(ye / yc - 1) > 0.05, f"empty field mean Y {ye}, smoke {yc}"
 
 
+def test_nanovdb_medium_agrees_with_reference_path_tracer(gpu, oracle):
+    """The smoke room with a NanoVDB fog sphere (written with NanoVDB's tools, loaded by the
+    reference's LoadNanoVDB; pr::NanoVDBField, nanovdb_field.cpp:17-96), handed to the device as
+    its index-space voxels: the same z statistics as the voxel smoke; with the voxels zeroed the
+    room renders visibly differently."""
+    w = h = 32
+    vs = 0.04
+    path, s = ru.nvdb_scene_file("nvdb_smoke", radius=0.8, voxel_size=vs, seed=0, width=w, height=h)
+    rs = oracle.RefScene(path)
+    sd, ext = ru.grid_scene_inputs(rs, s, indexed_voxel=vs)
+    g = _gpu_seeds(sd, ext, w, h, 128, 16, 8)
+    c = _cpu_seeds(rs, 128, 16, 8)
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    yg, yc = g[..., 1].mean(), c[..., 1].mean()
+    print(f"nanovdb medium: frac {frac:.4f}, mean Y gpu {yg:.5f} cpu {yc:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(yg / yc - 1) < 0.02, f"mean Y gpu {yg} cpu {yc}"
+    grid = ext._keep[-1][0]
+    zero = abi.GridMediumDesc.from_buffer_copy(grid)
+    empty = np.zeros((grid.nz, grid.ny, grid.nx), np.float32)
+    zero.density = empty.ctypes.data
+    eext = render.make_ext(grid_media=[zero])
+    ye = _gpu_seeds(sd, eext, w, h, 64, 2, 8)[..., 1].mean()
+    assert abs(ye / yc - 1) > 0.05, f"empty grid mean Y {ye}, fog {yc}"
+
+
 def test_constant_grid_equals_homogeneous_medium(gpu, oracle):
     """A grid of constant density 0.7 covering the whole interface box is the homogeneous medium of
     sigma * 0.7: spectral/ratio tracking on one side, hero-wavelength free flight and Beer-Lambert
@@ -130,4 +157,4 @@ def test_grid_medium_input_validation(gpu, oracle):
     # The scene references medium index mediumCount + 0; without the extension it is out of range.
     with pytest.raises(abi.PrgpuError, match="(?i)medium"):
         render.render_ex(sd, w, h, 1)
-    assert C.sizeof(abi.GridMediumDesc) == 152
+    assert C.sizeof(abi.GridMediumDesc) == 160
