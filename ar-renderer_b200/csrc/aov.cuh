@@ -68,7 +68,7 @@ __device__ ChainEnd follow_chain(const DevScene &s, V3 o, V3 d, Hit h, bool thro
         if (full_material(m)) {
             FullBsdf fb;
             make_full(s, m, sf.u, sf.v, lam, &fb);
-            if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, fb.layered ? &fb.lay.bottom : &fb.base);
+            textured_full(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &fb);
             if (fb.black || full_non_specular(fb)) {
                 e.valid = true;
                 return e;
@@ -182,8 +182,7 @@ __global__ void __launch_bounds__(128) k_aov(const DevScene *sp, AovArgs a, floa
                             if (full_material(m)) {
                                 FullBsdf fb;
                                 make_full(s, m, e.sf.u, e.sf.v, lam, &fb);
-                                Lobe &base = fb.layered ? fb.lay.bottom : fb.base;
-                                if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{e.sf.p, e.sf.u, e.sf.v}, lam, &base);
+                                textured_full(s, int(&m - s.mats), TexCtx{e.sf.p, e.sf.u, e.sf.v}, lam, &fb);
                                 bool prop;
                                 ok = wol.z != 0.f && full_sample(fb, wol, uc, u0, u1, &bs, &prop);
                             } else {

@@ -137,8 +137,9 @@ struct DevScene {
     int deltaCount;
     // Image textures and procedural texture trees; matTex is null unless a material uses one.
     const DevTex *textures;
-    // per material three entries: (reflectance texture, normal map, strength bits, flip green),
-    // (bump map, channel, scale bits, reflectance tree) and (bump tree, roughness trees u, v, 0)
+    // per material four entries: (reflectance texture, normal map, strength bits, flip green),
+    // (bump map, channel, scale bits, reflectance tree), (bump tree, roughness trees u, v, sheen
+    // roughness tree) and (coat roughness, thickness, coat albedo, sheen colour trees)
     const int4 *matTex;
     const prgpu::TextureNode *texNodes;
     const float *rgbZ, *rgbCoeffs;

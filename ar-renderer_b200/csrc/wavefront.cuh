@@ -418,7 +418,7 @@ __device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
 __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l) {
     if (!s.matTex) return;
     if (l->kind == kLobeDiffuse) {
-        const int tree = s.matTex[3 * mi + 1].w, img = s.matTex[3 * mi].x;
+        const int tree = s.matTex[4 * mi + 1].w, img = s.matTex[4 * mi].x;
         if (tree >= 0) {
             SS r = spectrum_texture(s, tree, c, lam);
 #pragma unroll
@@ -430,7 +430,7 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
             l->R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
         }
     } else if (l->kind == kLobeConductor || l->kind == kLobeDielectric) {
-        const int4 m2 = s.matTex[3 * mi + 2];
+        const int4 m2 = s.matTex[4 * mi + 2];
         if (m2.y < 0 && m2.z < 0) return;
         const prgpu::Material &m = s.mats[mi];
         float ax = m.alphaX, ay = m.alphaY;
@@ -493,8 +493,8 @@ __device__ __forceinline__ float height_at(const DevTex &t, int channel, float u
 // hemisphere and the shading dp/du follows it.
 __device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
     if (!s.matTex) return;
-    const int4 mt = s.matTex[3 * mi], bt = s.matTex[3 * mi + 1];
-    const int bumpTree = s.matTex[3 * mi + 2].x;
+    const int4 mt = s.matTex[4 * mi], bt = s.matTex[4 * mi + 1];
+    const int bumpTree = s.matTex[4 * mi + 2].x;
     if (mt.y < 0 && bt.x < 0 && bumpTree < 0) return;
     V3 dpdu, dpdv;
     surface_dpduv(pr, *sf, &dpdu, &dpdv);
@@ -609,6 +609,39 @@ __device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material 
         sh.weight = clampf(m.sheenWeight, 0.f, 1.f);
         sh.colorMax = clampf(max_c(sh.color), 0.f, 1.f);
         sh.table = s.sheenTable;
+    }
+}
+
+// The textured parameters of a coated / sheen BSDF: its base lobe (textured_lobe), the coat's
+// roughness, thickness and medium albedo (MakeCoatTop, material.cpp:119-130) and the sheen's colour
+// and roughness (Material::GetBSDF, material.cpp:5-14; SheenBxDF clamps, bxdf.cpp:568-571).
+__device__ void textured_full(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, FullBsdf *b) {
+    if (!s.matTex || b->black) return;
+    textured_lobe(s, mi, c, lam, b->layered ? &b->lay.bottom : &b->base);
+    const int4 m2 = s.matTex[4 * mi + 2], m3 = s.matTex[4 * mi + 3];
+    if (b->layered) {
+        Layered &L = b->lay;
+        if (m3.x >= 0) {
+            const float r = clampf(float_texture(s, m3.x, c), 0.f, 1.f);
+            L.top.mf = make_ggx(r * r, r * r);
+        }
+        if (m3.y >= 0) L.thickness = fmaxf(float_texture(s, m3.y, c), 1.17549435e-38f);
+        if (m3.z >= 0) {
+            L.albedo = spectrum_texture(s, m3.z, c, lam);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) L.albedo.v[i] = fmaxf(0.f, L.albedo.v[i]);
+            L.hasAlbedo = nonzero(L.albedo);
+        }
+    }
+    if (b->sheen) {
+        Sheen &sh = b->sh;
+        if (m3.w >= 0) {
+            sh.color = spectrum_texture(s, m3.w, c, lam);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) sh.color.v[i] = fmaxf(0.f, sh.color.v[i]);
+            sh.colorMax = clampf(max_c(sh.color), 0.f, 1.f);
+        }
+        if (m2.w >= 0) sh.alpha = clampf(float_texture(s, m2.w, c), 0.05f, 1.f);
     }
 }
 
@@ -1439,8 +1472,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     FullBsdf fb;
                     make_full(s, m, sf.u, sf.v, lam, &fb);
                     if constexpr (kDelta) {
-                        Lobe &base = fb.layered ? fb.lay.bottom : fb.base;
-                        if (!fb.black) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &base);
+                        textured_full(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &fb);
                     }
                     if (full_non_specular(fb))
                         nee(sf.p, sf.n, nullptr, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside, nullptr, &fb);

@@ -331,7 +331,10 @@ struct TextureNode {
 // multiplier in all three rgbScale components. The *Node fields name TextureNode trees instead
 // (-1 none); a reflectance or bump tree takes precedence over the image of the same slot, and the
 // roughness trees replace the GGX roughness (alpha = clamp(r, 0, 1)^2) of conductor, rough
-// dielectric and coated-conductor base lobes, each direction separately.
+// dielectric and coated-conductor base lobes, each direction separately. The coat trees replace
+// the coat's roughness, thickness and medium albedo (coated materials, MakeCoatTop,
+// material.cpp:119-130) and the sheen trees its colour and roughness (Material::GetBSDF,
+// material.cpp:5-14).
 struct MaterialTextures {
     int32_t reflectance;
     int32_t normalMap;
@@ -344,7 +347,11 @@ struct MaterialTextures {
     int32_t bumpNode;
     int32_t roughnessNodeU;
     int32_t roughnessNodeV;
-    uint32_t pad;
+    int32_t coatRoughnessNode;
+    int32_t thicknessNode;
+    int32_t coatAlbedoNode;     // spectrum tree
+    int32_t sheenColorNode;     // spectrum tree
+    int32_t sheenRoughnessNode;
 };
 
 struct SceneExt {

@@ -323,3 +323,68 @@ def test_procedural_textures_agree_with_reference(gpu, oracle):
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
+
+
+def test_textured_coats_and_sheen_agree_with_reference(gpu, oracle):
+    """Texture trees in the coat and sheen slots: a coated-diffuse ground whose coat roughness (uv
+    noise blend), thickness (float checker) and scattering albedo (world noise blend of two colours)
+    are textured; a diffuse sphere under a sheen with a checker colour and noise roughness; a coated
+    gold sphere with noise base and coat roughness. The same z statistics as above."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    pfm = os.path.join(d, "unused_tex.pfm")
+    _write_pfm(pfm, _texture())
+    doc = ru_outdoor_doc(w, h, pfm)
+    ca, cb, sa, sb = [0.9, 0.5, 0.3], [0.2, 0.6, 0.9], [1.0, 0.8, 0.9], [0.3, 0.9, 0.4]
+    doc["textures"] = {
+        "crough": {"type": "noise", "a": 0.0, "b": 0.4, "frequency": 5.0, "octaves": 3, "space": "uv"},
+        "thick": {"type": "checker", "a": 0.01, "b": 0.3, "uv_scale": [3.0, 3.0]},
+        "calb": {"type": "noise", "a": ca, "b": cb, "frequency": 2.0, "octaves": 4},
+        "scol": {"type": "checker", "a": sa, "b": sb, "uv_scale": [4.0, 4.0]},
+        "srough": {"type": "noise", "a": 0.1, "b": 0.8, "frequency": 6.0, "octaves": 3, "space": "uv"},
+        "broug": {"type": "noise", "a": 0.05, "b": 0.5, "frequency": 3.0, "octaves": 2},
+    }
+    doc["materials"] = {
+        "ground": {"type": "coated_diffuse", "reflectance": [0.6, 0.55, 0.5], "coat_roughness": {"texture": "crough"},
+                   "thickness": {"texture": "thick"}, "albedo": {"texture": "calb"}, "g": 0.3},
+        "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15],
+                "sheen": {"color": {"texture": "scol"}, "roughness": {"texture": "srough"}, "weight": 1.0}},
+        "tex_coat": {"type": "coated_conductor", "metal": "Au", "roughness": {"texture": "broug"},
+                     "coat_roughness": {"texture": "crough"}},
+    }
+    path = os.path.join(d, "textured_coats.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    sd, (ia, ib, isa, isb) = _with_albedo_spectra(rs, [ca, cb, sa, sb])
+    T = render.texture_node
+    nodes = [T(abi.TEX_CONSTANT, value=0.0), T(abi.TEX_CONSTANT, value=0.4),
+             T(abi.TEX_NOISE, frequency=5.0, octaves=3, world_space=False), T(abi.TEX_MIX, a=0, b=1, t=2),
+             T(abi.TEX_CONSTANT, value=0.01), T(abi.TEX_CONSTANT, value=0.3), T(abi.TEX_CHECKER, a=4, b=5, uv_scale=(3.0, 3.0)),
+             T(abi.TEX_CONSTANT, a=ia), T(abi.TEX_CONSTANT, a=ib), T(abi.TEX_NOISE, frequency=2.0, octaves=4),
+             T(abi.TEX_MIX, a=7, b=8, t=9),
+             T(abi.TEX_CONSTANT, a=isa), T(abi.TEX_CONSTANT, a=isb), T(abi.TEX_CHECKER, a=11, b=12, uv_scale=(4.0, 4.0)),
+             T(abi.TEX_CONSTANT, value=0.1), T(abi.TEX_CONSTANT, value=0.8),
+             T(abi.TEX_NOISE, frequency=6.0, octaves=3, world_space=False), T(abi.TEX_MIX, a=14, b=15, t=16),
+             T(abi.TEX_CONSTANT, value=0.05), T(abi.TEX_CONSTANT, value=0.5), T(abi.TEX_NOISE, frequency=3.0, octaves=2),
+             T(abi.TEX_MIX, a=18, b=19, t=20)]
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    slots = {"ground": {"coatRoughnessNode": 3, "thicknessNode": 6, "coatAlbedoNode": 10},
+             "red": {"sheenColorNode": 13, "sheenRoughnessNode": 17},
+             "tex_coat": {"roughnessNodeU": 21, "roughnessNodeV": 21, "coatRoughnessNode": 3}}
+    ext = render.make_ext(material_textures=[slots.get(n, {}) for n in used], texture_nodes=nodes)
+    g = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"textured coats and sheen: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
