@@ -351,10 +351,45 @@ __device__ __forceinline__ void cswap(float &ta, int &ra, float &tb, int &rb) {
 
 // kSkipTransparent: primitives whose class byte (cls) has kTransparentBit do not count as hits;
 // intersecting one sets s.crossed.
-template <bool kAny, bool kSpheres, bool kSkipTransparent = false>
-__device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
-                                               const TraceRay &r, TravState &s, int *stackRef, float *stackT,
-                                               bool *overflow, const uint8_t *__restrict__ cls = nullptr) {
+// The traversal stack as two per-thread arrays (local memory).
+struct LocalStack {
+    int *ref;
+    float *t;
+    __device__ __forceinline__ void put(int i, int r, float d) {
+        ref[i] = r;
+        t[i] = d;
+    }
+    __device__ __forceinline__ float dist(int i) const { return t[i]; }
+    __device__ __forceinline__ int node(int i) const { return ref[i]; }
+};
+
+// The bottom kShort entries of a thread's stack in shared memory, the rest in local memory. `sh`
+// points at the thread's column of its block's [kShort][kThreads] array, so that the lanes of a
+// warp touch consecutive words (no bank conflicts); traversals rarely go deeper than kShort, so
+// the local-memory part, which shares the L1 with the node and leaf loads, is rarely touched.
+template <int kShort, int kThreads>
+struct HybridStack {
+    int2 *sh;
+    int ref[kStackSize - kShort];
+    float t[kStackSize - kShort];
+    __device__ __forceinline__ void put(int i, int r, float d) {
+        if (i < kShort) {
+            sh[i * kThreads] = make_int2(r, __float_as_int(d));
+        } else {
+            ref[i - kShort] = r;
+            t[i - kShort] = d;
+        }
+    }
+    __device__ __forceinline__ float dist(int i) const {
+        return i < kShort ? __int_as_float(sh[i * kThreads].y) : t[i - kShort];
+    }
+    __device__ __forceinline__ int node(int i) const { return i < kShort ? sh[i * kThreads].x : ref[i - kShort]; }
+};
+
+template <bool kAny, bool kSpheres, bool kSkipTransparent = false, class Stack>
+__device__ __forceinline__ bool traverse4_step_st(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
+                                                  const TraceRay &r, TravState &s, Stack &stack, bool *overflow,
+                                                  const uint8_t *__restrict__ cls = nullptr) {
     if (s.ref >= 0) {
         const QNode *n = nodes + s.ref;
         const float4 lx = __ldg(&n->lox), ly = __ldg(&n->loy), lz = __ldg(&n->loz);
@@ -386,18 +421,9 @@ __device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, 
                 *overflow = true;
                 return true;
             }
-            if (t3 < inf) {
-                stackRef[s.sp] = r3;
-                stackT[s.sp++] = t3;
-            }
-            if (t2 < inf) {
-                stackRef[s.sp] = r2;
-                stackT[s.sp++] = t2;
-            }
-            if (t1 < inf) {
-                stackRef[s.sp] = r1;
-                stackT[s.sp++] = t1;
-            }
+            if (t3 < inf) stack.put(s.sp++, r3, t3);
+            if (t2 < inf) stack.put(s.sp++, r2, t2);
+            if (t1 < inf) stack.put(s.sp++, r1, t1);
             s.ref = r0;
             return false;
         }
@@ -429,12 +455,20 @@ __device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, 
     }
     while (s.sp > 0) {
         --s.sp;
-        if (stackT[s.sp] < s.tMax) {
-            s.ref = stackRef[s.sp];
+        if (stack.dist(s.sp) < s.tMax) {
+            s.ref = stack.node(s.sp);
             return false;
         }
     }
     return true;
+}
+
+template <bool kAny, bool kSpheres, bool kSkipTransparent = false>
+__device__ __forceinline__ bool traverse4_step(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
+                                               const TraceRay &r, TravState &s, int *stackRef, float *stackT,
+                                               bool *overflow, const uint8_t *__restrict__ cls = nullptr) {
+    LocalStack st{stackRef, stackT};
+    return traverse4_step_st<kAny, kSpheres, kSkipTransparent>(nodes, prims, r, s, st, overflow, cls);
 }
 
 } // namespace prb
