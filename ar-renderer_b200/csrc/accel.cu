@@ -14,11 +14,6 @@ namespace prb {
 // atomic per warp and refill), then the lanes advance their traversals one node or leaf per
 // iteration. Incoherent rays end after very different numbers of steps; refilling keeps the
 // lanes of a warp busy instead of idling until the warp's longest ray ends.
-// Stack entries per thread in shared memory for the 4-wide traversal: 16 x 8 B x 256 threads =
-// 32 KiB per block, 128 KiB per SM at 4 resident blocks (measured: 4 -> 3.27, 8 -> 3.53, 16 -> 3.83
-// Grays/s against 3.36 with the whole stack in local memory).
-constexpr int kShortStack = 16;
-
 template <bool kAny, bool kWide>
 __global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ nodes,
                                                        const LeafPrim *__restrict__ prims, RootInfo root,

@@ -368,6 +368,15 @@ struct LocalStack {
 // warp touch consecutive words (no bank conflicts); traversals rarely go deeper than kShort, so
 // the local-memory part, which shares the L1 with the node and leaf loads, is rarely touched.
 template <int kShort, int kThreads>
+struct HybridStack;
+
+// Stack entries per thread in shared memory for the 4-wide traversals: 16 x 8 B x 256 threads =
+// 32 KiB per block, 128 KiB per SM at 4 resident blocks (measured on the ray-query benchmark:
+// 4 -> 3.27, 8 -> 3.53, 16 -> 3.83, 24 -> 3.79 Grays/s, against 3.36 with the whole stack in local
+// memory).
+constexpr int kShortStack = 16;
+
+template <int kShort, int kThreads>
 struct HybridStack {
     int2 *sh;
     int ref[kStackSize - kShort];

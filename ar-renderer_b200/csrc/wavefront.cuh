@@ -1114,8 +1114,9 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n = counters[kCntActive];
-    int stackRef[kStackSize];
-    float stackT[kStackSize];
+    __shared__ int2 shortStack[kShortStack * 256];
+    HybridStack<kShortStack, 256> hs;
+    hs.sh = shortStack + threadIdx.x;
     TraceRay r;
     TravState st;
     st.ref = 0;
@@ -1157,7 +1158,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
                 }
             }
         }
-        if (active && traverse4_step<false, kSpheres>(nodes, leaves, r, st, stackRef, stackT, &overflow)) {
+        if (active && traverse4_step_st<false, kSpheres>(nodes, leaves, r, st, hs, &overflow)) {
             active = false;
             P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
         }
@@ -1629,8 +1630,9 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n = counters[kCntShadow];
-    int stackRef[kStackSize];
-    float stackT[kStackSize];
+    __shared__ int2 shortStack[kShortStack * 256];
+    HybridStack<kShortStack, 256> hs;
+    hs.sh = shortStack + threadIdx.x;
     TraceRay r;
     TravState st;
     st.ref = 0;
@@ -1675,7 +1677,7 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                 }
             }
         }
-        if (active && traverse4_step<true, kSpheres, kWalls>(nodes, leaves, r, st, stackRef, stackT, &overflow, cls)) {
+        if (active && traverse4_step_st<true, kSpheres, kWalls>(nodes, leaves, r, st, hs, &overflow, cls)) {
             active = false;
             if (!st.found) {
                 if (kWalls && st.crossed) toWalk = true;
