@@ -51,7 +51,7 @@ TRIS_PER_RAY = 2.21
 BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
 # DRAM bytes per closest-hit launch from ncu (profiles/trace_closest_soup1m.md): read + write of a
 # 2^22-ray capture of the same kernel, scaled by the rays of a full 2^24-ray launch.
-NCU_TRAFFIC_PER_LAUNCH = (798.266880e6 + 87.654400e6) * 4
+NCU_TRAFFIC_PER_LAUNCH = (565.865472e6 + 46.270720e6) * 4
 
 
 def _peaks():
