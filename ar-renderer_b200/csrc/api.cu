@@ -68,7 +68,7 @@ static_assert(sizeof(prgpu::SceneExt) == 128 && offsetof(prgpu::SceneExt, gridMe
               offsetof(prgpu::SceneExt, sun) == 56 && offsetof(prgpu::SceneExt, deltaLights) == 72 &&
               offsetof(prgpu::SceneExt, rgbToSpectrum) == 104 && offsetof(prgpu::SceneExt, textureNodes) == 112);
 static_assert(sizeof(prgpu::TextureNode) == 64);
-static_assert(sizeof(prgpu::ImageTextureDesc) == 56 && sizeof(prgpu::MaterialTextures) == 64);
+static_assert(sizeof(prgpu::ImageTextureDesc) == 56 && sizeof(prgpu::MaterialTextures) == 72);
 static_assert(sizeof(prgpu::DeltaLightDesc) == 104 && offsetof(prgpu::DeltaLightDesc, frame) == 48 &&
               offsetof(prgpu::DeltaLightDesc, profile) == 96);
 static_assert(sizeof(prgpu::EnvMapDesc) == 32 && sizeof(prgpu::SunDesc) == 28);

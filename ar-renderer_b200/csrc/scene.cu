@@ -199,11 +199,13 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
             !texture_tree_ok(ext, sd, x.roughnessNodeU, false, 0) || !texture_tree_ok(ext, sd, x.roughnessNodeV, false, 0) ||
             !texture_tree_ok(ext, sd, x.coatRoughnessNode, false, 0) || !texture_tree_ok(ext, sd, x.thicknessNode, false, 0) ||
             !texture_tree_ok(ext, sd, x.coatAlbedoNode, true, 0) || !texture_tree_ok(ext, sd, x.sheenColorNode, true, 0) ||
-            !texture_tree_ok(ext, sd, x.sheenRoughnessNode, false, 0))
+            !texture_tree_ok(ext, sd, x.sheenRoughnessNode, false, 0) || !texture_tree_ok(ext, sd, x.etaNode, true, 0) ||
+            !texture_tree_ok(ext, sd, x.kNode, true, 0) || ((x.etaNode >= 0) != (x.kNode >= 0)))
             return fail("bad texture tree (index out of range, deeper than 8 nodes, or a node of the wrong kind)");
         if (!ext->rgbToSpectrum && (texture_tree_has_image(ext, x.reflectanceNode, 0) ||
                                     texture_tree_has_image(ext, x.coatAlbedoNode, 0) ||
-                                    texture_tree_has_image(ext, x.sheenColorNode, 0)))
+                                    texture_tree_has_image(ext, x.sheenColorNode, 0) ||
+                                    texture_tree_has_image(ext, x.etaNode, 0) || texture_tree_has_image(ext, x.kNode, 0)))
             return fail("textured materials need the RGB -> spectrum table");
         if (!std::isfinite(x.bumpScale)) return fail("bad bump map scale");
     }
@@ -400,7 +402,7 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         used = used || (n > 0 && (x.reflectance >= 0 || x.normalMap >= 0 || x.bumpMap >= 0)) ||
                (nn > 0 && (x.reflectanceNode >= 0 || x.bumpNode >= 0 || x.roughnessNodeU >= 0 || x.roughnessNodeV >= 0 ||
                            x.coatRoughnessNode >= 0 || x.thicknessNode >= 0 || x.coatAlbedoNode >= 0 ||
-                           x.sheenColorNode >= 0 || x.sheenRoughnessNode >= 0));
+                           x.sheenColorNode >= 0 || x.sheenRoughnessNode >= 0 || x.etaNode >= 0));
     }
     if (!used) return;
     size_t total = 0;
@@ -422,7 +424,7 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         g.scale[0] = x.rgbScale[0], g.scale[1] = x.rgbScale[1], g.scale[2] = x.rgbScale[2];
         off += m;
     }
-    std::vector<int4> mt(static_cast<size_t>(4 * nm));
+    std::vector<int4> mt(static_cast<size_t>(5 * nm));
     for (int32_t i = 0; i < nm; ++i) {
         const prgpu::MaterialTextures &x = ext->materialTextures[i];
         int sbits, bbits;
@@ -430,12 +432,13 @@ void upload_textures(const prgpu::SceneExt *ext, SceneCache &cache, DevScene &d,
         std::memcpy(&bbits, &x.bumpScale, sizeof(bbits));
         const bool img = n > 0, trees = nn > 0;
         auto tree = [&](int32_t v) { return trees ? v : -1; };
-        mt[size_t(4 * i)] = make_int4(img ? x.reflectance : -1, img ? x.normalMap : -1, sbits, x.normalFlipGreen ? 1 : 0);
-        mt[size_t(4 * i + 1)] = make_int4(img ? x.bumpMap : -1, x.bumpChannel, bbits, tree(x.reflectanceNode));
-        mt[size_t(4 * i + 2)] = make_int4(tree(x.bumpNode), tree(x.roughnessNodeU), tree(x.roughnessNodeV),
+        mt[size_t(5 * i)] = make_int4(img ? x.reflectance : -1, img ? x.normalMap : -1, sbits, x.normalFlipGreen ? 1 : 0);
+        mt[size_t(5 * i + 1)] = make_int4(img ? x.bumpMap : -1, x.bumpChannel, bbits, tree(x.reflectanceNode));
+        mt[size_t(5 * i + 2)] = make_int4(tree(x.bumpNode), tree(x.roughnessNodeU), tree(x.roughnessNodeV),
                                           tree(x.sheenRoughnessNode));
-        mt[size_t(4 * i + 3)] = make_int4(tree(x.coatRoughnessNode), tree(x.thicknessNode), tree(x.coatAlbedoNode),
+        mt[size_t(5 * i + 3)] = make_int4(tree(x.coatRoughnessNode), tree(x.thicknessNode), tree(x.coatAlbedoNode),
                                           tree(x.sheenColorNode));
+        mt[size_t(5 * i + 4)] = make_int4(tree(x.etaNode), tree(x.kNode), 0, 0);
     }
     if (n > 0) put(cache.textures, t.data(), t.size(), s);
     put(cache.matTex, mt.data(), mt.size(), s);

@@ -374,7 +374,9 @@ __device__ __forceinline__ void walk_texture(const DevScene &s, int root, const 
 
 // A spectrum tree as an albedo at the 4 wavelengths (constants from the spectrum table, images
 // uplifted through the RGB -> spectrum table).
-__device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, const Lambda &lam) {
+__device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam);
+
+__device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, const Lambda &lam, bool unbounded = false) {
     SS acc = splat(0.f);
     walk_texture(s, root, c, [&](const prgpu::TextureNode &n, float w) {
         SS v;
@@ -383,7 +385,7 @@ __device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, con
         } else if (n.type == prgpu::TexImage) {
             float rgb[3];
             tex_rgb(s.textures[n.a], c.u, c.v, rgb);
-            v = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
+            v = unbounded ? rgb_unbounded(s, rgb[0], rgb[1], rgb[2], lam) : rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
         } else {
             return;
         }
@@ -415,10 +417,11 @@ __device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
 // a diffuse lobe (a tree, else an image; clamped to [0, 1] as DiffuseMaterial::GetBxDF,
 // material.cpp:73-77) and the roughness of conductor and rough dielectric lobes (trees; alpha =
 // clamp(r, 0, 1)^2, material.cpp:80-85, 110-116, 151-154).
-__device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l) {
+__device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l,
+                              float etaScale = 1.f) {
     if (!s.matTex) return;
     if (l->kind == kLobeDiffuse) {
-        const int tree = s.matTex[4 * mi + 1].w, img = s.matTex[4 * mi].x;
+        const int tree = s.matTex[5 * mi + 1].w, img = s.matTex[5 * mi].x;
         if (tree >= 0) {
             SS r = spectrum_texture(s, tree, c, lam);
 #pragma unroll
@@ -430,7 +433,12 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
             l->R = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
         }
     } else if (l->kind == kLobeConductor || l->kind == kLobeDielectric) {
-        const int4 m2 = s.matTex[4 * mi + 2];
+        const int4 m4 = s.matTex[5 * mi + 4];
+        if (l->kind == kLobeConductor && m4.x >= 0 && m4.y >= 0) {
+            l->eta = spectrum_texture(s, m4.x, c, lam, true) * (1.f / etaScale);
+            l->k = spectrum_texture(s, m4.y, c, lam, true) * (1.f / etaScale);
+        }
+        const int4 m2 = s.matTex[5 * mi + 2];
         if (m2.y < 0 && m2.z < 0) return;
         const prgpu::Material &m = s.mats[mi];
         float ax = m.alphaX, ay = m.alphaY;
@@ -444,6 +452,17 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
         }
         l->mf = make_ggx(ax, ay);
     }
+}
+
+// RGBUnboundedSpectrum (rgb2spec.cpp:328-336): the sigmoid polynomial of the colour divided by
+// scale = 2 max(r, g, b), times that scale.
+__device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam) {
+    const float m = fmaxf(r, fmaxf(g, b));
+    const float scale = 2.f * m;
+    SS v = scale > 0.f ? rgb_albedo(s, r / scale, g / scale, b / scale, lam) : rgb_albedo(s, 0.f, 0.f, 0.f, lam);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v.v[i] *= scale;
+    return v;
 }
 
 // dp/du and dp/dv of the parameterization at a hit (Sphere / Triangle::Intersect, shape.cpp:75-82,
@@ -493,8 +512,8 @@ __device__ __forceinline__ float height_at(const DevTex &t, int channel, float u
 // hemisphere and the shading dp/du follows it.
 __device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
     if (!s.matTex) return;
-    const int4 mt = s.matTex[4 * mi], bt = s.matTex[4 * mi + 1];
-    const int bumpTree = s.matTex[4 * mi + 2].x;
+    const int4 mt = s.matTex[5 * mi], bt = s.matTex[5 * mi + 1];
+    const int bumpTree = s.matTex[5 * mi + 2].x;
     if (mt.y < 0 && bt.x < 0 && bumpTree < 0) return;
     V3 dpdu, dpdv;
     surface_dpduv(pr, *sf, &dpdu, &dpdv);
@@ -617,8 +636,9 @@ __device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material 
 // and roughness (Material::GetBSDF, material.cpp:5-14; SheenBxDF clamps, bxdf.cpp:568-571).
 __device__ void textured_full(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, FullBsdf *b) {
     if (!s.matTex || b->black) return;
-    textured_lobe(s, mi, c, lam, b->layered ? &b->lay.bottom : &b->base);
-    const int4 m2 = s.matTex[4 * mi + 2], m3 = s.matTex[4 * mi + 3];
+    // A coated conductor's n, k are relative to the coat's IOR.
+    textured_lobe(s, mi, c, lam, b->layered ? &b->lay.bottom : &b->base, b->layered ? b->lay.top.etaD : 1.f);
+    const int4 m2 = s.matTex[5 * mi + 2], m3 = s.matTex[5 * mi + 3];
     if (b->layered) {
         Layered &L = b->lay;
         if (m3.x >= 0) {

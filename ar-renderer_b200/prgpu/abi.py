@@ -151,7 +151,7 @@ class MaterialTextures(C.Structure):
                 ("bumpScale", C.c_float), ("reflectanceNode", C.c_int32), ("bumpNode", C.c_int32),
                 ("roughnessNodeU", C.c_int32), ("roughnessNodeV", C.c_int32), ("coatRoughnessNode", C.c_int32),
                 ("thicknessNode", C.c_int32), ("coatAlbedoNode", C.c_int32), ("sheenColorNode", C.c_int32),
-                ("sheenRoughnessNode", C.c_int32)]
+                ("sheenRoughnessNode", C.c_int32), ("etaNode", C.c_int32), ("kNode", C.c_int32)]
 
 
 TEX_CONSTANT, TEX_IMAGE, TEX_CHECKER, TEX_NOISE, TEX_MIX = 0, 1, 2, 3, 4
@@ -211,7 +211,7 @@ class RenderStats(C.Structure):
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
 assert C.sizeof(GridMediumDesc) == 160 and C.sizeof(SceneExt) == 128 and C.sizeof(DeltaLightDesc) == 104
-assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 64 and C.sizeof(TextureNode) == 64
+assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 72 and C.sizeof(TextureNode) == 64
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
 assert C.sizeof(BatchItem) == 48 and C.sizeof(BatchConfig) == 16 and C.sizeof(BatchStats) == 72

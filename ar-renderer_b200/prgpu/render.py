@@ -108,7 +108,7 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
             mt[i].normalStrength, mt[i].normalFlipGreen = float(v[2]), 1 if v[3] else 0
             mt[i].bumpMap, mt[i].bumpChannel, mt[i].bumpScale = int(v[4]), int(v[5]), float(v[6])
             for k in ("reflectanceNode", "bumpNode", "roughnessNodeU", "roughnessNodeV", "coatRoughnessNode",
-                      "thicknessNode", "coatAlbedoNode", "sheenColorNode", "sheenRoughnessNode"):
+                      "thicknessNode", "coatAlbedoNode", "sheenColorNode", "sheenRoughnessNode", "etaNode", "kNode"):
                 setattr(mt[i], k, -1)
         e.materialTextureCount = len(mt)
         e.materialTextures = C.cast(mt, C.c_void_p)
@@ -129,7 +129,8 @@ def make_ext(light_bvh: np.ndarray | None = None, light_bvh_prob: float = 1.0, w
 MATERIAL_TEXTURES_DEFAULT = {"reflectance": -1, "normalMap": -1, "normalStrength": 1.0, "normalFlipGreen": 0,
                              "bumpMap": -1, "bumpChannel": -1, "bumpScale": 0.01, "reflectanceNode": -1,
                              "bumpNode": -1, "roughnessNodeU": -1, "roughnessNodeV": -1, "coatRoughnessNode": -1,
-                             "thicknessNode": -1, "coatAlbedoNode": -1, "sheenColorNode": -1, "sheenRoughnessNode": -1}
+                             "thicknessNode": -1, "coatAlbedoNode": -1, "sheenColorNode": -1, "sheenRoughnessNode": -1,
+                             "etaNode": -1, "kNode": -1}
 
 
 def texture_node(kind: int, a: int = -1, b: int = -1, t: int = -1, channel: int = -1, value: float = 0.0,

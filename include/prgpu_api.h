@@ -352,6 +352,11 @@ struct MaterialTextures {
     int32_t coatAlbedoNode;     // spectrum tree
     int32_t sheenColorNode;     // spectrum tree
     int32_t sheenRoughnessNode;
+    // Conductor n and k (conductor and coated-conductor base; ConductorMaterial::MakeBxDF,
+    // material.cpp:80-92) as spectrum trees of unbounded spectra: their image leaves are uplifted
+    // as RGBUnboundedSpectrum (2 max(r, g, b) times the sigmoid of the colour over that scale).
+    int32_t etaNode;
+    int32_t kNode;
 };
 
 struct SceneExt {

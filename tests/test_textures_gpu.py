@@ -235,9 +235,9 @@ def test_bump_maps_agree_with_reference(gpu, oracle):
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
 
 
-def _with_albedo_spectra(rs, rgbs):
-    """The exported scene with the RGBAlbedoSpectrum of each colour appended to its spectra; the
-    appended rows' indices."""
+def _with_albedo_spectra(rs, rgbs, kinds=None):
+    """The exported scene with the RGBAlbedoSpectrum of each colour (kind 1: RGBUnboundedSpectrum)
+    appended to its spectra; the appended rows' indices."""
     import ctypes as C
 
     import ref as oracle_ref
@@ -249,9 +249,10 @@ def _with_albedo_spectra(rs, rgbs):
     old = np.ctypeslib.as_array((C.c_float * (95 * base.spectrumCount)).from_address(base.spectra)).reshape(-1, 95)
     lam = spectra.LAMBDA.astype(np.float32)
     rows = []
-    for rgb in rgbs:
+    for j, rgb in enumerate(rgbs):
         out = np.zeros(95, np.float32)
-        assert oracle_ref.ref_lib().prref_spectrum(0, *[float(v) for v in rgb], None, 95, oracle_ref._p(lam),
+        kind = 0 if kinds is None else kinds[j]
+        assert oracle_ref.ref_lib().prref_spectrum(kind, *[float(v) for v in rgb], None, 95, oracle_ref._p(lam),
                                                    oracle_ref._p(out)) == 0
         rows.append(out)
     table = np.ascontiguousarray(np.concatenate([old, np.stack(rows)]), np.float32)
@@ -384,6 +385,58 @@ def test_textured_coats_and_sheen_agree_with_reference(gpu, oracle):
     mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
     se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
     print(f"textured coats and sheen: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
+
+
+def test_textured_conductor_n_k_agree_with_reference(gpu, oracle):
+    """Conductor n and k from texture trees of unbounded spectra: a rough conductor sphere whose n and
+    k are checkers of two colours each, and a coated-conductor ground whose n and k are world-space
+    noise blends (relative to the coat's IOR on the device, as the reference divides them). The
+    same z statistics as above."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    pfm = os.path.join(d, "unused_tex2.pfm")
+    _write_pfm(pfm, _texture())
+    doc = ru_outdoor_doc(w, h, pfm)
+    ea, eb, ka, kb = [0.2, 0.4, 1.2], [1.5, 1.0, 0.5], [3.5, 2.7, 2.2], [2.0, 2.5, 3.0]
+    doc["textures"] = {
+        "eta_chk": {"type": "checker", "a": ea, "b": eb, "uv_scale": [4.0, 4.0]},
+        "k_chk": {"type": "checker", "a": ka, "b": kb, "uv_scale": [4.0, 4.0]},
+        "eta_nz": {"type": "noise", "a": ea, "b": eb, "frequency": 2.0, "octaves": 3},
+        "k_nz": {"type": "noise", "a": ka, "b": kb, "frequency": 2.0, "octaves": 3},
+    }
+    doc["materials"] = {
+        "ground": {"type": "coated_conductor", "eta": {"texture": "eta_nz"}, "k": {"texture": "k_nz"},
+                   "roughness": 0.2, "coat_roughness": 0.1},
+        "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+        "tex_coat": {"type": "conductor", "eta": {"texture": "eta_chk"}, "k": {"texture": "k_chk"}, "roughness": 0.3},
+    }
+    path = os.path.join(d, "textured_nk.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    sd, (iea, ieb, ika, ikb) = _with_albedo_spectra(rs, [ea, eb, ka, kb], kinds=[1, 1, 1, 1])
+    T = render.texture_node
+    nodes = [T(abi.TEX_CONSTANT, a=iea), T(abi.TEX_CONSTANT, a=ieb), T(abi.TEX_CHECKER, a=0, b=1, uv_scale=(4.0, 4.0)),
+             T(abi.TEX_CONSTANT, a=ika), T(abi.TEX_CONSTANT, a=ikb), T(abi.TEX_CHECKER, a=3, b=4, uv_scale=(4.0, 4.0)),
+             T(abi.TEX_NOISE, frequency=2.0, octaves=3), T(abi.TEX_MIX, a=0, b=1, t=6), T(abi.TEX_MIX, a=3, b=4, t=6)]
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    slots = {"ground": {"etaNode": 7, "kNode": 8}, "tex_coat": {"etaNode": 2, "kNode": 5}}
+    ext = render.make_ext(material_textures=[slots.get(n, {}) for n in used], texture_nodes=nodes)
+    g = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"textured n, k: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
     assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
