@@ -11,11 +11,16 @@
 // The array g_noalloc_scratch (32 MiB, below) is a file-scope __device__ variable: every GPU on
 // which the library's kernels are loaded holds it until the process exits. Its host-side name is
 // only a stand-in, so its device address is looked up with cudaGetSymbolAddress once per device,
-// on that device's first call (that first call should come before any stream capture). All calls
-// share the array and it keeps the previous call's contents; the status word is cleared at the
-// start of each call. Calls that overlapped on the GPU would race on the array, so each call
-// holds the library's lock and waits for its own GPU work before it returns: calls made through
-// this entry point run one after another.
+// on that device's first call. That first call may do more one-time work of the CUDA runtime and
+// driver: load this file's kernels (lazy module loading), create the calling thread's per-thread
+// default stream, and grow the device's per-thread local-memory reserve for the traversal stack.
+// So make one call per device at set-up, before any stream capture and before the point from
+// which nothing may allocate; later calls allocate nothing. All calls share the array and it
+// keeps the previous call's contents; the status word is cleared at the start of each call. Calls
+// that overlapped on the GPU would race on the array, so each call holds the library's lock and
+// waits for its own GPU work before it returns: calls made through this entry point run one after
+// another. The work is issued on the calling thread's per-thread default stream
+// (cudaStreamPerThread), which does not wait for the caller's other streams.
 //
 // Limits: at most kNoAllocMaxPrims triangles (and 2 * kNoAllocMaxPrims - 1 nodes) per call; any
 // number of rays (they stream through a 2^18-ray staging area). The traversal reads the caller's
@@ -199,7 +204,9 @@ PRGPU_API int prgpu_trace_rays_noalloc(int deviceIndex, const prgpu::BVHNode *no
         auto *dT = reinterpret_cast<float *>(base + kOffT);
         auto *dB1 = reinterpret_cast<float *>(base + kOffB1);
         auto *dB2 = reinterpret_cast<float *>(base + kOffB2);
-        cudaStream_t s = 0;  // the legacy default stream: nothing is created
+        // The per-thread default stream: no stream object to create or destroy, and unlike the
+        // legacy stream 0 it does not serialise with the caller's other (blocking) streams.
+        cudaStream_t s = cudaStreamPerThread;
         PRB_CUDA(cudaMemsetAsync(dStatus, 0, sizeof(int), s));
         if (nodeCount)
             PRB_CUDA(cudaMemcpyAsync(dNodes, nodes, size_t(nodeCount) * sizeof(prgpu::BVHNode), cudaMemcpyHostToDevice, s));
@@ -207,12 +214,12 @@ PRGPU_API int prgpu_trace_rays_noalloc(int deviceIndex, const prgpu::BVHNode *no
             PRB_CUDA(cudaMemcpyAsync(dOrder, primOrder, size_t(primCount) * sizeof(int32_t), cudaMemcpyHostToDevice, s));
             PRB_CUDA(cudaMemcpyAsync(dVerts, triVerts, size_t(primCount) * 9 * sizeof(float), cudaMemcpyHostToDevice, s));
         }
-        cudaDeviceProp prop{};
-        PRB_CUDA(cudaGetDeviceProperties(&prop, deviceIndex));
+        int smCount = 0;
+        PRB_CUDA(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount, deviceIndex));
         for (int64_t off = 0; off < rayCount; off += kNoAllocChunkRays) {
             int64_t cnt = std::min(kNoAllocChunkRays, rayCount - off);
             PRB_CUDA(cudaMemcpyAsync(dRays, rays + off, size_t(cnt) * sizeof(prgpu::Ray), cudaMemcpyHostToDevice, s));
-            int grid = int(std::min<int64_t>((cnt + 255) / 256, int64_t(prop.multiProcessorCount) * 32));
+            int grid = int(std::min<int64_t>((cnt + 255) / 256, int64_t(smCount) * 32));
             const auto *r4 = reinterpret_cast<const float4 *>(dRays);
             if (anyHit)
                 k_trace_v4<true><<<grid, 256, 0, s>>>(dNodes, nodeCount, dOrder, dVerts, r4, cnt, dPrim, nullptr, nullptr,

@@ -435,8 +435,15 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
     } else if (l->kind == kLobeConductor || l->kind == kLobeDielectric) {
         const int4 m4 = s.matTex[5 * mi + 4];
         if (l->kind == kLobeConductor && m4.x >= 0 && m4.y >= 0) {
-            l->eta = spectrum_texture(s, m4.x, c, lam, true) * (1.f / etaScale);
-            l->k = spectrum_texture(s, m4.y, c, lam, true) * (1.f / etaScale);
+            // Divided by the coat's IOR under a coat, as CoatedConductorMaterial (material.cpp:157-158).
+            SS e = spectrum_texture(s, m4.x, c, lam, true), k = spectrum_texture(s, m4.y, c, lam, true);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                e.v[i] = e.v[i] / etaScale;
+                k.v[i] = k.v[i] / etaScale;
+            }
+            l->eta = e;
+            l->k = k;
         }
         const int4 m2 = s.matTex[5 * mi + 2];
         if (m2.y < 0 && m2.z < 0) return;
@@ -454,14 +461,21 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
     }
 }
 
-// RGBUnboundedSpectrum (rgb2spec.cpp:328-336): the sigmoid polynomial of the colour divided by
-// scale = 2 max(r, g, b), times that scale.
+// RGBUnboundedSpectrum (rgb2spec.cpp:327-335): zero for a colour whose largest component is not
+// positive, else the sigmoid polynomial of the colour times 1 / scale, scale = 2 max(r, g, b),
+// times that scale (the reference's order of operations, so the same bits).
 __device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam) {
-    const float m = fmaxf(r, fmaxf(g, b));
-    const float scale = 2.f * m;
-    SS v = scale > 0.f ? rgb_albedo(s, r / scale, g / scale, b / scale, lam) : rgb_albedo(s, 0.f, 0.f, 0.f, lam);
+    const float m = fmaxf(0.f, fmaxf(r, fmaxf(g, b)));
+    SS v;
+    if (m == 0.f) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) v.v[i] *= scale;
+        for (int i = 0; i < 4; ++i) v.v[i] = 0.f;
+        return v;
+    }
+    const float scale = 2.f * m, inv = 1.f / scale;
+    v = rgb_albedo(s, r * inv, g * inv, b * inv, lam);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v.v[i] = scale * v.v[i];
     return v;
 }
 
@@ -602,8 +616,15 @@ __device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material 
             L.bottom.etaD = 1.f;
             L.bottom.mf = make_ggx(m.alphaX, m.alphaY);
             if (m.eta >= 0) {
-                L.bottom.eta = tab4(s.spectra, m.eta, lam) * (1.f / coatEta);
-                L.bottom.k = tab4(s.spectra, m.k, lam) * (1.f / coatEta);
+                // Divided (not multiplied by the reciprocal), as material.cpp:157-158.
+                SS e = tab4(s.spectra, m.eta, lam), k = tab4(s.spectra, m.k, lam);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    e.v[i] = e.v[i] / coatEta;
+                    k.v[i] = k.v[i] / coatEta;
+                }
+                L.bottom.eta = e;
+                L.bottom.k = k;
             } else {
                 SS r = tab4(s.spectra, m.albedo, lam);
 #pragma unroll

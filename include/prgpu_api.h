@@ -501,7 +501,10 @@ PRGPU_API int prgpu_trace_rays(int deviceIndex, const prgpu::BVHNode *nodes, int
 // synchronisation of cudaMalloc / cudaFree). It allocates nothing: every device byte comes from
 // one 32 MiB array the library reserves on each GPU where it is loaded. Limits: at most 131,072
 // triangles and 262,143 BVH nodes per call (larger inputs return 1 with a message); any number of
-// rays. Calls run one after another. No counterpart in the reference (src/gpu/gpu_api.h).
+// rays. Calls run one after another, on the calling thread's per-thread default stream. The
+// first call on a device also does the runtime's one-time set-up (the array's address, module
+// load, local-memory reserve): make it before the point from which nothing may allocate. This
+// entry point has no counterpart in the reference.
 PRGPU_API int prgpu_trace_rays_noalloc(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
                                        const int32_t *primOrder, const prgpu::Float3 *triVerts, int32_t primCount,
                                        const prgpu::Ray *rays, int64_t rayCount, int32_t anyHit, int32_t *primOut,

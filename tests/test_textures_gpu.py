@@ -437,7 +437,7 @@ def test_textured_conductor_n_k_agree_with_reference(gpu, oracle):
     mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
     se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
     print(f"textured n, k: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
-    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert frac >= 0.998, f"only {frac:.4f} of values within |z| < 4"
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95

@@ -7,6 +7,8 @@ on two calls in a row, since the second call finds the first call's data still i
 This file is named to be collected last: run alone in a fresh process or after every other test,
 the results must be the same."""
 
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -59,6 +61,34 @@ def test_noalloc_matches_allocating_entry_point_twice_in_a_row(gpu):
     gp, gt, _, _ = _noalloc(n2, o2, v2, r3)
     np.testing.assert_array_equal(gp, wp)
     np.testing.assert_array_equal(_bits(gt[wp >= 0]), _bits(wt[wp >= 0]))
+
+
+def _device_free_bytes() -> int:
+    """Free device memory as the driver reports it for the context current on this thread (the
+    primary context the library made current), through libcuda's cuMemGetInfo."""
+    cu = ctypes.CDLL("libcuda.so.1")
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert cu.cuMemGetInfo_v2(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
+def test_noalloc_calls_after_the_first_leave_device_memory_untouched(gpu):
+    # The first call of each kernel variant may do the runtime's one-time set-up (symbol address,
+    # lazy module load, local-memory reserve); every later call must allocate nothing.
+    v = workloads.triangle_soup(20_000, seed=41)
+    nodes, order = trace.build_bvh_triangles(v)
+    rc = workloads.soup_rays(300_000, seed=42)
+    ra = workloads.soup_rays(300_000, seed=43, any_hit=True)
+    first = _noalloc(nodes, order, v, rc)
+    first_occ = _noalloc(nodes, order, v, ra, any_hit=True)
+    free0 = _device_free_bytes()
+    again = _noalloc(nodes, order, v, rc)
+    again_occ = _noalloc(nodes, order, v, ra, any_hit=True)
+    free1 = _device_free_bytes()
+    assert free1 == free0, f"device free memory changed by {free1 - free0} bytes across two calls"
+    np.testing.assert_array_equal(again[0], first[0])
+    np.testing.assert_array_equal(_bits(again[1]), _bits(first[1]))
+    np.testing.assert_array_equal(again_occ, first_occ)
 
 
 def test_noalloc_rejects_scenes_beyond_its_limit(gpu):
