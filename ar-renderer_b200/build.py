@@ -14,6 +14,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
@@ -56,6 +57,26 @@ def _sources(d: str, exts) -> list[str]:
     return sorted(os.path.join(d, f) for f in os.listdir(d) if f.endswith(exts))
 
 
+def _local_includes(path: str, seen: set | None = None) -> set:
+    """The file and every header it includes with quotes, transitively (resolved beside the
+    including file, then in include/)."""
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path, errors="replace") as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include \""):
+                name = line.split('"')[1]
+                for base in (os.path.dirname(path), INCLUDE):
+                    cand = os.path.normpath(os.path.join(base, name))
+                    if os.path.exists(cand):
+                        _local_includes(cand, seen)
+                        break
+    return seen
+
+
 def _run(cmd: list[str]) -> None:
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -73,10 +94,17 @@ def build_gpu(force: bool = False, verbose: bool = False) -> str:
 
     def compile_one(src: str) -> str:
         obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        # An object is current when it is newer than its source and the headers that source reaches.
+        if not force and not verbose and os.path.exists(obj) and \
+                os.path.getmtime(obj) >= _newest(_local_includes(src)) and os.path.getmtime(obj) >= os.path.getmtime(__file__):
+            return obj
         cmd = [nvcc, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), "-c", src, "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
+        started = time.time()
         _run(cmd)
+        # Date the object at the start of its compile, so a source edited meanwhile is newer.
+        os.utime(obj, (started, started))
         return obj
 
     with ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:

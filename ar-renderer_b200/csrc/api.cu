@@ -64,7 +64,7 @@ static_assert(sizeof(prgpu::Light) == 48 && offsetof(prgpu::Light, position) == 
 static_assert(sizeof(prgpu::Camera) == 80 && offsetof(prgpu::Camera, width) == 64);
 static_assert(sizeof(prgpu::GridMediumDesc) == 160 && offsetof(prgpu::GridMediumDesc, density) == 104 &&
               offsetof(prgpu::GridMediumDesc, field) == 112);
-static_assert(sizeof(prgpu::SceneExt) == 128 && offsetof(prgpu::SceneExt, gridMedia) == 40 &&
+static_assert(sizeof(prgpu::SceneExt) == 144 && offsetof(prgpu::SceneExt, rayTap) == 128 && offsetof(prgpu::SceneExt, gridMedia) == 40 &&
               offsetof(prgpu::SceneExt, sun) == 56 && offsetof(prgpu::SceneExt, deltaLights) == 72 &&
               offsetof(prgpu::SceneExt, rgbToSpectrum) == 104 && offsetof(prgpu::SceneExt, textureNodes) == 112);
 static_assert(sizeof(prgpu::TextureNode) == 64);

@@ -283,7 +283,8 @@ __host__ __device__ constexpr uint32_t dw_col(int l) { return 64 + 64 * uint32_t
 __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict__ features,
                                                         const GuideSample *__restrict__ samples, const int *count,
                                                         const __half *__restrict__ packed, float *grad,
-                                                        float *lossSum, int *status, const float *wnorm) {
+                                                        float *lossSum, int *status, const float *wnorm,
+                                                        GuideOpts opts) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     GuideSmemTrain &S = *reinterpret_cast<GuideSmemTrain *>(smraw);
     const int n = *count;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict
                 if (valid) {
                     const GuideSample sm = samples[row];
                     lossAcc += guide_loss_grad(z, mk(sm.wi[0], sm.wi[1], sm.wi[2]), mk(sm.n[0], sm.n[1], sm.n[2]),
-                                               sm.pb, sm.w * wscale, gout);
+                                               sm.pb, sm.w * wscale, gout, opts);
                 } else {
 #pragma unroll
                     for (int k = 0; k < kGuideOut; ++k) gout[k] = 0.f;
@@ -440,6 +441,7 @@ struct GuideState {
     bool ready = false;
     int sms = 0;
     float lr = 1e-3f;      // online learning rate (Adam)
+    GuideOpts opts;        // sampling and training settings
 };
 
 GuideState gGuide[64];
@@ -490,7 +492,7 @@ void guide_train(cudaStream_t st, GuideState &g, const __half *features, const G
     PRB_CUDA(cudaMemsetAsync(g.grad.ptr, 0, kGuideParams * sizeof(float), st));
     PRB_CUDA(cudaMemsetAsync(g.loss.ptr, 0, sizeof(float), st));
     k_guide_train<<<grid, 128, train_smem(), st>>>(features, samples, dcount, g.packed.as<__half>(), g.grad.as<float>(),
-                                                   g.loss.as<float>(), g.status.as<int>(), nullptr);
+                                                   g.loss.as<float>(), g.status.as<int>(), nullptr, g.opts);
     count_launch();
 }
 
@@ -580,6 +582,8 @@ bool guide_failed(DeviceState &ds, int device) {
     return s != 0;
 }
 
+GuideOpts guide_options(int device) { return gGuide[device].opts; }
+
 void guide_infer_rows(cudaStream_t st, int device, const __half *features, const int *dcount, int maxRows, float *out) {
     guide_forward(st, gGuide[device], features, dcount, maxRows, out);
 }
@@ -603,7 +607,8 @@ void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs,
     PRB_CUDA(cudaMemsetAsync(g.grad.ptr, 0, kGuideParams * sizeof(float), st));
     PRB_CUDA(cudaMemsetAsync(g.loss.ptr, 0, sizeof(float), st));
     k_guide_train<<<std::max(1, std::min(tiles, g.sms)), 128, train_smem(), st>>>(
-        feat, smp, rows, g.packed.as<__half>(), g.grad.as<float>(), g.loss.as<float>(), g.status.as<int>(), wnorm);
+        feat, smp, rows, g.packed.as<__half>(), g.grad.as<float>(), g.loss.as<float>(), g.status.as<int>(), wnorm,
+        g.opts);
     ++g.step;
     k_guide_adam<<<64, 256, 0, st>>>(g.master.as<float>(), g.m.as<float>(), g.v.as<float>(), g.grad.as<float>(), 0.f,
                                      scale, lr, 0.9f, 0.999f, 1e-8f, g.step);
@@ -753,6 +758,45 @@ PRGPU_API int prgpu_guide_set_learning_rate(int deviceIndex, float learningRate,
             return 1;
         }
         gGuide[deviceIndex].lr = learningRate;
+        return 0;
+    });
+}
+
+PRGPU_API int prgpu_guide_set_options(int deviceIndex, const prgpu::GuideOptions *opts, char *err, int errLen) {
+    return guarded(err, errLen, [&]() {
+        if (deviceIndex < 0 || deviceIndex >= 64) {
+            set_err(err, errLen, "bad device");
+            return 1;
+        }
+        GuideOpts o;  // null: the defaults
+        if (opts) {
+            if (!(opts->maxSelect > 0.f && opts->maxSelect <= 0.99f) || !(opts->logKappaMax >= 0.f && opts->logKappaMax <= 8.f) ||
+                (opts->selectLoss != 0 && opts->selectLoss != 1) || opts->trainPasses < 1 || opts->trainPasses > 64) {
+                set_err(err, errLen, "guide options out of range (0 < maxSelect <= 0.99, 0 <= logKappaMax <= 8, "
+                                     "selectLoss 0 or 1, 1 <= trainPasses <= 64)");
+                return 1;
+            }
+            o.maxSelect = opts->maxSelect;
+            o.logKappaMax = opts->logKappaMax;
+            o.selectLoss = opts->selectLoss;
+            o.trainPasses = opts->trainPasses;
+        }
+        gGuide[deviceIndex].opts = o;
+        return 0;
+    });
+}
+
+PRGPU_API int prgpu_guide_get_options(int deviceIndex, prgpu::GuideOptions *out, char *err, int errLen) {
+    return guarded(err, errLen, [&]() {
+        if (deviceIndex < 0 || deviceIndex >= 64 || !out) {
+            set_err(err, errLen, "bad arguments");
+            return 1;
+        }
+        const GuideOpts &o = gGuide[deviceIndex].opts;
+        out->maxSelect = o.maxSelect;
+        out->logKappaMax = o.logKappaMax;
+        out->selectLoss = o.selectLoss;
+        out->trainPasses = o.trainPasses;
         return 0;
     });
 }

@@ -34,8 +34,16 @@ constexpr int kGuideBands = 12, kGuideConstIn = 81, kGuideConstHid = 63;
 __host__ __device__ constexpr int guide_layer_in(int l) { return l == 0 ? kGuideIn : kGuideHid; }
 __host__ __device__ constexpr int guide_layer_out(int l) { return l == kGuideLayers - 1 ? kGuideOut : kGuideHid; }
 constexpr int kGuideParams = kGuideHid * kGuideIn + 3 * kGuideHid * kGuideHid + kGuideOut * kGuideHid;  // 23,552
-constexpr float kGuideMaxSelect = 0.9f;
 constexpr int kGuideVertices = 4;  // diffuse vertices per path that are guided and recorded
+
+// Settings of sampling and training (prgpu_guide_set_options). The defaults are the network's
+// original form: c = 0.9 sigmoid, log kappa clamped to [-4, 8], c trained on the KL objective.
+struct GuideOpts {
+    float maxSelect = 0.9f;    // c = maxSelect * sigmoid(output 40)
+    float logKappaMax = 8.f;   // upper clamp of log kappa
+    int selectLoss = 0;        // c's objective: 0 = -w log p_mix, 1 = second moment w^2 / p_mix
+    int trainPasses = 1;       // passes over each chunk's recorded samples (online training)
+};
 
 __host__ __device__ constexpr int guide_weight_offset(int l) {
     return l == 0 ? 0 : kGuideHid * kGuideIn + (l - 1) * kGuideHid * kGuideHid;
@@ -72,7 +80,7 @@ struct GuideMix {
 
 __device__ __forceinline__ float guide_sigmoid(float x) { return 1.f / (1.f + expf(-x)); }
 
-__device__ __forceinline__ GuideMix guide_decode(const float *o) {
+__device__ __forceinline__ GuideMix guide_decode(const float *o, const GuideOpts &op) {
     GuideMix m;
     float mx = -1e30f;
 #pragma unroll
@@ -83,13 +91,13 @@ __device__ __forceinline__ GuideMix guide_decode(const float *o) {
         V3 v = mk(o[5 * k], o[5 * k + 1], o[5 * k + 2]);
         float l = sqrtf(dot(v, v));
         m.mu[k] = l > 1e-6f ? v * (1.f / l) : mk(0.f, 0.f, 1.f);
-        m.kappa[k] = expf(fminf(fmaxf(o[5 * k + 3], -4.f), 8.f));
+        m.kappa[k] = expf(fminf(fmaxf(o[5 * k + 3], -4.f), op.logKappaMax));
         m.pi[k] = expf(o[5 * k + 4] - mx);
         sum += m.pi[k];
     }
 #pragma unroll
     for (int k = 0; k < kGuideLobes; ++k) m.pi[k] /= sum;
-    m.c = kGuideMaxSelect * guide_sigmoid(o[40]);
+    m.c = op.maxSelect * guide_sigmoid(o[40]);
     return m;
 }
 
@@ -161,10 +169,15 @@ __device__ __forceinline__ void guide_features_n(const float *xn, V3 n, V3 wo, f
 // from -w log q_n, the selection output from -w log(c q_n + (1 - c) pb) with q_n fixed. wi lies on
 // the side of n the sample came from, so q_n(wi) = q(wi) + q(mirror(wi)). Returns the sum of both
 // parts; g receives the gradient (zero for the unused outputs 41..47).
-__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, V3 n, float pb, float w, float *g) {
+// With op.selectLoss = 1 the selection output instead descends the second moment of the one-sample
+// estimator f Li / p_mix, E[(f Li)^2 / p_mix]: its derivative in c, estimated from a sample drawn
+// from p_mix with w = f Li / p_mix, is -w^2 (q_n - pb) / p_mix (the variance-optimal selection
+// rather than the KL-optimal one).
+__device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, V3 n, float pb, float w, float *g,
+                                                 const GuideOpts &op) {
 #pragma unroll
     for (int i = 0; i < kGuideOut; ++i) g[i] = 0.f;
-    GuideMix m = guide_decode(o);
+    GuideMix m = guide_decode(o, op);
     const V3 wr = guide_mirror(wi, n);
     float v1[kGuideLobes], v2[kGuideLobes];
     float q = 0.f;
@@ -176,11 +189,14 @@ __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, V3 n, fl
     }
     float p = m.c * q + (1.f - m.c) * pb;
     if (!(p > 0.f) || !(q > 0.f) || !(w > 0.f)) return 0.f;
-    float loss = -w * logf(q) - w * logf(p);
+    // The selection term's weight: w (KL), or w^2 for the second moment (the surrogate
+    // -w w' log p with w' = w held fixed, whose c-derivative is -w^2 (q_n - pb) / p).
+    const float ws = op.selectLoss == 1 ? w * w : w;
+    float loss = -w * logf(q) - ws * logf(p);
     float dq = -w / q;                             // d(-w log q_n)/dq_n
-    float dc = -w * (q - pb) / p;                  // d(-w log p)/dc at fixed q_n
+    float dc = -ws * (q - pb) / p;                 // d(-ws log p)/dc at fixed q_n
     float s = guide_sigmoid(o[40]);
-    g[40] = dc * kGuideMaxSelect * s * (1.f - s);
+    g[40] = dc * op.maxSelect * s * (1.f - s);
     float sumPiG = 0.f;
 #pragma unroll
     for (int k = 0; k < kGuideLobes; ++k) sumPiG += m.pi[k] * dq * (v1[k] + v2[k]);
@@ -191,7 +207,7 @@ __device__ __forceinline__ float guide_loss_grad(const float *o, V3 wi, V3 n, fl
         const float d1 = dq * m.pi[k] * v1[k], d2 = dq * m.pi[k] * v2[k];  // dL/d(log vmf_k) at wi, wr
         const float kap = m.kappa[k];
         const float raw = o[5 * k + 3];
-        if (raw > -4.f && raw < 8.f && kap >= 1e-4f) {
+        if (raw > -4.f && raw < op.logKappaMax && kap >= 1e-4f) {
             // d log vmf / d kappa = 1/kappa - 2 e^{-2k} / (1 - e^{-2k}) + (mu.w - 1); d kappa / d raw = kappa
             const float base = 1.f / kap - 2.f * expf(-2.f * kap) / (-expm1f(-2.f * kap));
             g[5 * k + 3] = (d1 * (base + dot(m.mu[k], wi) - 1.f) + d2 * (base + dot(m.mu[k], wr) - 1.f)) * kap;

@@ -70,6 +70,34 @@ __global__ void __launch_bounds__(256) k_guide_collect(Paths P, float4 *rec, int
     }
 }
 
+// Measurement tap: the closest-hit rays of queued paths in slots [0, paths), then (before the
+// shadow pass) the shadow rays, as 8-float records (origin, tMax, direction, 1) at bounce b.
+__global__ void __launch_bounds__(256) k_tap_closest(Paths P, const int *counters, const int *queue, float4 *tap,
+                                                     int paths, int bounce) {
+    const int n = counters[kCntActive];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int j = queue[q];
+        if (j >= paths) continue;
+        const float4 o = P.o[j], d = P.d[j];
+        float4 *r = tap + 2 * (size_t(bounce) * paths + j);
+        r[0] = make_float4(o.x, o.y, o.z, kInf);
+        r[1] = make_float4(d.x, d.y, d.z, 1.f);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_tap_shadow(Shadows S, const int *counters, float4 *tap, int paths,
+                                                    int bounces, int bounce) {
+    const int n = counters[kCntShadow];
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const float4 o = S.o[q], d = S.d[q];
+        const int j = __float_as_int(d.w);
+        if (j < 0 || j >= paths) continue;
+        float4 *r = tap + 2 * ((size_t(bounces) + bounce) * paths + j);
+        r[0] = make_float4(o.x, o.y, o.z, 1.f - kShadowEps);
+        r[1] = make_float4(d.x, d.y, d.z, 1.f);
+    }
+}
+
 constexpr int kGuideBatch = 1 << 16;    // training samples per online step
 constexpr int kGuideRecords = 1 << 18;  // samples kept per chunk: up to 4 steps
 
@@ -80,6 +108,7 @@ struct RenderState {
     DevBuf pathBuf, shadowBuf, queues, classQueues, counters, stats, film;
     DevBuf guideFeat, guideOut, guideRec, guideTrain;  // guided form (allocated on first use)
     DevBuf sceneTable;  // the render's DevScene in device memory, for the shading kernels
+    DevBuf tap;         // measurement tap (allocated on first use)
     int guideCap = 0;
     int capacity = 0;
     Paths P{};
@@ -211,8 +240,10 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     const int guideMode = gflags & 3;
     GuideTrainRec *trainRecs = nullptr;
     int *trainCount = nullptr;
+    GuideOpts gopts;
     if (guideMode) {
         guide_prepare(ds, ds.device, (gflags & 4) != 0, rp.seed);
+        gopts = guide_options(ds.device);
         if (rs.guideCap < rs.capacity) {
             rs.guideFeat.ensure(size_t(rs.capacity) * kGuideIn * sizeof(__half));
             rs.guideOut.ensure(size_t(rs.capacity) * kGuideOut * sizeof(float));
@@ -225,6 +256,15 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
         trainRecs = rs.guideTrain.as<GuideTrainRec>();
         trainCount = reinterpret_cast<int *>(rs.guideTrain.as<unsigned char>() + size_t(kGuideRecords) * sizeof(GuideTrainRec));
     }
+    // Measurement tap of the first chunk's rays (SceneExt::rayTap).
+    const int tapPaths = (ext && ext->rayTap) ? std::max(0, ext->rayTapPaths) : 0;
+    const int tapBounces = tapPaths > 0 ? std::max(0, ext->rayTapBounces) : 0;
+    const size_t tapBytes = size_t(2) * tapBounces * tapPaths * 8 * sizeof(float);
+    if (tapBytes) {
+        rs.tap.ensure(tapBytes);
+        PRB_CUDA(cudaMemsetAsync(rs.tap.ptr, 0, tapBytes, st));
+    }
+    int bounceIndex = 0;
     PRB_CUDA(cudaMemsetAsync(cnt, 0, kCntSlots * sizeof(int), st));
     PRB_CUDA(cudaMemsetAsync(dstats, 0, kStatSlots * sizeof(unsigned long long), st));
     for (int64_t pix0 = 0; pix0 < npix; pix0 += npixChunk) {
@@ -243,6 +283,11 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
             int *qin = qa, *qout = qb;
             for (;;) {
                 for (int b = 0; b < kBouncesPerPoll; ++b) {
+                    const bool tapNow = tapBytes && pix0 == 0 && s0 == 0 && bounceIndex < tapBounces;
+                    if (tapNow) {
+                        k_tap_closest<<<gShade, 256, 0, st>>>(rs.P, cnt, qin, rs.tap.as<float4>(), tapPaths, bounceIndex);
+                        ++launches;
+                    }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b], st));
                     if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     else k_extend<false><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
@@ -256,7 +301,8 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     }
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 1], st));
                     ShadeArgs sa{scene, rs.sceneTable.as<DevScene>(), rs.P, rs.S, cq, rs.capacity, qout, cnt,
-                                 rp.maxDepth, 0, rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin};
+                                 rp.maxDepth, 0, rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin,
+                                 gopts};
                     const bool dl = scene.deltaCount > 0 || scene.matTex != nullptr;
                     if (guideMode) {
                         if (dl) k_shade<false, true, false, true><<<gShade, 256, 0, st>>>(sa);
@@ -270,6 +316,12 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                         else k_shade<false, false, true><<<gShade, 256, 0, st>>>(sa);
                         ++launches;
                     }
+                    if (tapNow) {
+                        k_tap_shadow<<<gShade, 256, 0, st>>>(rs.S, cnt, rs.tap.as<float4>(), tapPaths, tapBounces,
+                                                             bounceIndex);
+                        ++launches;
+                    }
+                    ++bounceIndex;
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b + 2], st));
                     shadowAny<<<gShadow, 256, 0, st>>>(scene, nullptr, rs.P, rs.S, cnt);
                     if (scene.hasInterfaces) {
@@ -305,9 +357,10 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                 PRB_CUDA(cudaMemsetAsync(trainCount, 0, sizeof(int), st));
                 k_guide_collect<<<grid_for(ds, total), 256, 0, st>>>(rs.P, rs.guideRec.as<float4>(), total, trainRecs,
                                                                      trainCount, kGuideRecords);
-                for (int k = 0; k < kGuideRecords / kGuideBatch; ++k)
-                    guide_train_records(st, ds.device, trainRecs, trainCount, k * kGuideBatch, kGuideBatch, 0.f);
-                launches += 1 + (kGuideRecords / kGuideBatch) * kGuideTrainLaunches;
+                for (int pass = 0; pass < gopts.trainPasses; ++pass)
+                    for (int k = 0; k < kGuideRecords / kGuideBatch; ++k)
+                        guide_train_records(st, ds.device, trainRecs, trainCount, k * kGuideBatch, kGuideBatch, 0.f);
+                launches += 1 + gopts.trainPasses * (kGuideRecords / kGuideBatch) * kGuideTrainLaunches;
             }
             if (timing) {
                 PRB_CUDA(cudaEventRecord(rs.ev[4 * kBouncesPerPoll + 1], st));
@@ -323,6 +376,7 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
     unsigned long long hs[kStatSlots] = {};
     PRB_CUDA(cudaMemcpyAsync(&status, cnt + kCntStatus, sizeof(int), cudaMemcpyDeviceToHost, st));
     PRB_CUDA(cudaMemcpyAsync(hs, dstats, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    if (tapBytes) PRB_CUDA(cudaMemcpyAsync(ext->rayTap, rs.tap.ptr, tapBytes, cudaMemcpyDeviceToHost, st));
     PRB_CUDA(cudaStreamSynchronize(st));
     count_launch(launches);
     if (stats) {

@@ -1227,6 +1227,7 @@ struct ShadeArgs {
     // Paths that reached a coated / sheen surface, deferred by the main pass to the kFull pass
     // (the ping-pong queue being consumed, free while shading runs).
     int *fullQ;
+    GuideOpts guideOpts;     // guided form: the decoding settings of the network outputs
 };
 
 // One bounce of PathIntegrator::Li for every active path (path.cpp:155-236). The main pass
@@ -1536,7 +1537,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     const bool guided = (a.guideMode & 1) && inRange;
                     const int recIndex = gcount;
                     if (inRange) ++gcount;
-                    if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut);
+                    if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut, a.guideOpts);
                     if (lobe.non_specular())
                         nee(sf.p, sf.n, &lobe, &fr, sf.ns, wo, 0.f, pr.mediumInside, pr.mediumOutside,
                             guided ? &gm : nullptr);

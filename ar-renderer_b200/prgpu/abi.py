@@ -172,7 +172,8 @@ class SceneExt(C.Structure):
                 ("envMap", C.c_void_p), ("sun", C.c_void_p), ("deltaLightCount", C.c_int32), ("pad", C.c_int32),
                 ("deltaLights", C.c_void_p), ("textureCount", C.c_int32), ("materialTextureCount", C.c_int32),
                 ("textures", C.c_void_p), ("materialTextures", C.c_void_p), ("rgbToSpectrum", C.c_void_p),
-                ("textureNodes", C.c_void_p), ("textureNodeCount", C.c_int32), ("pad2", C.c_int32)]
+                ("textureNodes", C.c_void_p), ("textureNodeCount", C.c_int32), ("pad2", C.c_int32),
+                ("rayTap", C.c_void_p), ("rayTapPaths", C.c_int32), ("rayTapBounces", C.c_int32)]
 
 
 class BatchItem(C.Structure):
@@ -201,6 +202,11 @@ class BatchStats(C.Structure):
                 ("graphBuilt", C.c_int32), ("tuned", C.c_int32)]
 
 
+class GuideOptions(C.Structure):
+    _fields_ = [("maxSelect", C.c_float), ("logKappaMax", C.c_float), ("selectLoss", C.c_int32),
+                ("trainPasses", C.c_int32)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("pathSamples", C.c_uint64), ("closestRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("bounces", C.c_uint64), ("kernelLaunches", C.c_uint64), ("deviceMs", C.c_double),
@@ -210,7 +216,7 @@ class RenderStats(C.Structure):
 
 assert C.sizeof(Camera) == 80 and C.sizeof(Filter) == 276 and C.sizeof(SceneDesc) == 520
 assert C.sizeof(RenderParams) == 24 and C.sizeof(DeviceInfo) == 304
-assert C.sizeof(GridMediumDesc) == 160 and C.sizeof(SceneExt) == 128 and C.sizeof(DeltaLightDesc) == 104
+assert C.sizeof(GridMediumDesc) == 160 and C.sizeof(SceneExt) == 144 and C.sizeof(DeltaLightDesc) == 104
 assert C.sizeof(ImageTextureDesc) == 56 and C.sizeof(MaterialTextures) == 72 and C.sizeof(TextureNode) == 64
 assert C.sizeof(AovParams) == 96
 assert C.sizeof(EnvMapDesc) == 32 and C.sizeof(SunDesc) == 28
@@ -257,6 +263,8 @@ def gpu_lib() -> C.CDLL:
         _bind(lib, "prgpu_guide_adam_step", [C.c_int, C.c_float, C.c_float, *_ERR], C.c_int)
         _bind(lib, "prgpu_guide_stats", [C.c_int, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_guide_set_learning_rate", [C.c_int, C.c_float, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_set_options", [C.c_int, _P, *_ERR], C.c_int)
+        _bind(lib, "prgpu_guide_get_options", [C.c_int, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64, C.c_int32,
                                         _P, _P, _P, _P, *_ERR], C.c_int)
         _bind(lib, "prgpu_trace_rays_noalloc", [C.c_int, _P, C.c_int32, _P, _P, C.c_int32, _P, C.c_int64,
@@ -291,6 +299,12 @@ def host_lib() -> C.CDLL:
         lib.prhost_build_bvh_triangles.restype = C.c_int64
         lib.prhost_build_light_bvh.argtypes = [_P, C.c_int32, _P]
         lib.prhost_build_light_bvh.restype = C.c_int32
+        lib.prhost_preetham_sky.argtypes = [_P, C.c_float, C.c_float, C.c_int32, C.c_int32, _P]
+        lib.prhost_preetham_sky.restype = C.c_int
+        lib.prhost_sun_radiance.argtypes = [_P, C.c_float, C.c_float, C.c_int64, _P, _P]
+        lib.prhost_sun_radiance.restype = C.c_int
+        lib.prhost_rgb_to_sigmoid.argtypes = [C.c_int64, _P, _P, C.c_int32, _P]
+        lib.prhost_rgb_to_sigmoid.restype = C.c_int
         lib.prhost_checkpoint_write.argtypes = [C.c_char_p, _P, _P, C.c_uint64, _P, C.c_uint64, C.c_char_p, C.c_int]
         lib.prhost_checkpoint_write.restype = C.c_int
         lib.prhost_checkpoint_read.argtypes = [C.c_char_p, _P, _P, C.c_uint64, _P, C.c_uint64, C.POINTER(C.c_uint64),

@@ -71,3 +71,24 @@ def set_learning_rate(lr: float, device: int = 0) -> None:
     err = abi.err_buf()
     abi.check(abi.gpu_lib().prgpu_guide_set_learning_rate(device, lr, err, len(err)), err,
               "prgpu_guide_set_learning_rate")
+
+
+DEFAULT_OPTIONS = dict(max_select=0.9, log_kappa_max=8.0, select_loss=0, train_passes=1)
+
+
+def set_options(max_select: float = 0.9, log_kappa_max: float = 8.0, select_loss: int = 0, train_passes: int = 1,
+                device: int = 0) -> None:
+    """Sampling and training settings of the guide (prgpu_guide_set_options): the cap of the
+    selection probability c, the cap of log kappa, c's objective (0 KL, 1 second moment of the
+    one-sample estimator) and the online training passes over each chunk's samples."""
+    o = abi.GuideOptions(max_select, log_kappa_max, select_loss, train_passes)
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_set_options(device, C.byref(o), err, len(err)), err, "prgpu_guide_set_options")
+
+
+def get_options(device: int = 0) -> dict:
+    o = abi.GuideOptions()
+    err = abi.err_buf()
+    abi.check(abi.gpu_lib().prgpu_guide_get_options(device, C.byref(o), err, len(err)), err, "prgpu_guide_get_options")
+    return dict(max_select=o.maxSelect, log_kappa_max=o.logKappaMax, select_loss=o.selectLoss,
+                train_passes=o.trainPasses)

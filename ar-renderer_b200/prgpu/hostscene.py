@@ -308,6 +308,8 @@ METALS = ("Au", "Ag", "Cu", "Al")
 CLOUD_TO_WORLD = np.array([[25, 0, 0, 0], [0, 6, 0, 22], [0, 0, 25, -5], [0, 0, 0, 1]], np.float64)
 CLOUD_BOX = (np.array([-25.0, 16.0, -30.0]), np.array([25.0, 28.0, 20.0]))
 SUN_ELEVATION, SUN_AZIMUTH = 20.0, math.degrees(0.6)
+SUN_RADIUS_DEG = 0.2665     # the loader's sun radius (scene_loader.cpp:986)
+SUN_SKY_INTENSITY = 0.03    # the loader's default sun_sky intensity (scene_loader.cpp:985)
 CAMERA = dict(cam_pos=(0.0, 14.0, 45.0), cam_target=(0.0, 6.0, 0.0), fov_y=45.0)
 
 
@@ -335,15 +337,19 @@ def large_scene_layout(terrain_res: int = 4096, cloud_res: int = 256, spheres: i
 
 
 def build_large_scene(width: int = 3840, height: int = 2160, terrain_res: int = 4096, cloud_res: int = 256,
-                      spheres: int = 200, seed: int = 0):
+                      spheres: int = 200, seed: int = 0, turbidity: float = 3.0, sky_resolution: int = 512):
     """The large outdoor scene: a terrain_res^2 fBm heightfield (8 octaves, 2 (res - 1)^2 triangles,
     Lambert 0.3) over [-50, 50]^2, a cloud_res^3 fBm cloud density grid above it (max density 4,
     albedo 0.95, Henyey-Greenstein g = 0.8, spectral / ratio tracking inside an interface box),
     `spheres` analytic GGX conductor spheres (Au / Ag / Cu / Al, alpha uniform in [0.05, 0.5]) on
-    the terrain, a sun 20 degrees above the horizon and a sky. Lighting stand-ins: the sun is a
-    5,800 K blackbody cone of the reference's angular radius and the sky an importance-sampled
-    equirect map with a zenith-to-horizon gradient of an 8,000 K blackbody (the reference builds a
-    Preetham sky on the host, which this builder does not restate).
+    the terrain, lit as PRender lights a "sun_sky" light (scene_loader.cpp:977-996): the sun 20
+    degrees above the horizon with the spectral radiance of pr::MakeSunRadiance, the Preetham sky
+    of pr::MakePreethamSky (turbidity 3, ground albedo 0.3, a sky_resolution x sky_resolution / 2
+    equirect map, importance-sampled), both at the loader's intensity 0.03 and picked with
+    probability 1/2 each, both from the host library (prhost_sun_radiance, prhost_preetham_sky).
+    The sky texels are fitted to sigmoid polynomials under a 6504 K blackbody of unit luminance,
+    which stands in for the reference's tabulated CIE D65 (same luminance and white point to
+    within the fit; the reference interpolates its precomputed table of fits under D65).
     Returns (HostScene, SceneExt)."""
     from . import media, render
 
@@ -361,8 +367,10 @@ def build_large_scene(width: int = 3840, height: int = 2160, terrain_res: int = 
         h.spheres([c for c, _, _, _ in lay["spheres"]], [r for _, r, _, _ in lay["spheres"]], ms)
     absorb = h.spectrum(spectra.constant(0.05))
     scatter = h.spectrum(spectra.constant(0.95))
-    sky_ill = h.spectrum(spectra.blackbody(8000.0) / spectra.blackbody(8000.0).max())
-    sun_spec = h.spectrum(spectra.blackbody(5800.0) / spectra.blackbody(5800.0).max())
+    sun_dir = scenes.sun_direction(SUN_ELEVATION, SUN_AZIMUTH)
+    white = spectra.blackbody(6504.0)  # unit luminance: the D65 stand-in
+    sky_ill = h.spectrum(white)
+    sun_spec = h.spectrum(spectra.sun_radiance(sun_dir, turbidity, SUN_RADIUS_DEG))
     grid = media.grid_desc(absorb, scatter, lay["density"], [[-1, -1, -1], [1, 1, 1]], scale=1.0, g=0.8,
                            world_to_medium=media.affine_inverse(CLOUD_TO_WORLD))
     # The cloud's interface box, outward-facing: rays that cross it enter and leave grid medium 0
@@ -370,22 +378,20 @@ def build_large_scene(width: int = 3840, height: int = 2160, terrain_res: int = 
     bverts, bidx = box_mesh(*CLOUD_BOX)
     h.mesh(bverts, bidx, h.material(type=abi.MAT_INTERFACE), medium_inside=len(h.media), medium_outside=-1)
     h.finish(width=width, height=height, max_leaf=4, **CAMERA)
-    # Sky: a 256 x 128 equirect map of flat sigmoid-polynomial texels (c0 = c1 = c2 = 0, so the
-    # spectrum is scale / 2 x the illuminant) with a zenith-to-horizon gradient and a dark ground.
-    sw, sh = 256, 128
-    cos_t = np.cos((np.arange(sh, dtype=np.float32) + 0.5) / sh * np.pi)
-    lum = np.where(cos_t > 0, 0.35 + 0.65 * (1 - cos_t) ** 2, 0.05)
-    texels = np.zeros((sh, sw, 4), np.float32)
-    texels[:, :, 3] = 2.0 * lum[:, None]
+    # Sky: the Preetham map, its RGB texels uplifted to sigmoid-polynomial spectra times the
+    # illuminant (the reference's RGBIlluminantSpectrum texels, light.cpp:243-265).
+    sw, sh = sky_resolution, sky_resolution // 2
+    sky = spectra.preetham_sky(sun_dir, turbidity, 0.3, sw, sh)
+    texels = np.ascontiguousarray(spectra.rgb_to_sigmoid(sky.reshape(-1, 3), white).reshape(sh, sw, 4))
     env = abi.EnvMapDesc()
     env.width, env.height = sw, sh
     env.texels = texels.ctypes.data
-    env.illuminant, env.scale, env.rotationDeg, env.pmf = sky_ill, 1.0, 0.0, 0.5
+    env.illuminant, env.scale, env.rotationDeg, env.pmf = sky_ill, SUN_SKY_INTENSITY, 0.0, 0.5
     sd = abi.SunDesc()
-    for i, v in enumerate(scenes.sun_direction(SUN_ELEVATION, SUN_AZIMUTH)):
+    for i, v in enumerate(sun_dir):
         sd.direction[i] = float(v)
-    sd.cosThetaMax = math.cos(math.radians(0.2665))
-    sd.spectrum, sd.scale, sd.pmf = sun_spec, 2.0e4, 0.5
+    sd.cosThetaMax = math.cos(math.radians(SUN_RADIUS_DEG))
+    sd.spectrum, sd.scale, sd.pmf = sun_spec, SUN_SKY_INTENSITY, 0.5
     ext = render.make_ext(grid_media=[grid])
     ext.envMap = C.addressof(env)
     ext.sun = C.addressof(sd)

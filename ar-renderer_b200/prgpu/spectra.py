@@ -146,3 +146,40 @@ def rgb_albedo(rgb) -> np.ndarray:
 
 def constant(v: float) -> np.ndarray:
     return np.full(95, v, np.float32)
+
+
+def preetham_sky(sun_dir, turbidity: float = 3.0, ground_albedo: float = 0.3, width: int = 512,
+                 height: int = 256) -> np.ndarray:
+    """The Preetham sky map (height, width, 3) linear sRGB from the host library
+    (prhost_preetham_sky, the daylight PRender builds for a sun_sky light)."""
+    from . import abi
+
+    d = np.ascontiguousarray(sun_dir, np.float32)
+    out = np.zeros((height, width, 3), np.float32)
+    assert abi.host_lib().prhost_preetham_sky(abi.ptr(d), turbidity, ground_albedo, width, height, abi.ptr(out)) == 0
+    return out
+
+
+def sun_radiance(sun_dir, turbidity: float = 3.0, radius_deg: float = 0.2665, lam: np.ndarray = LAMBDA) -> np.ndarray:
+    """The sun's spectral radiance at wavelengths lam (prhost_sun_radiance)."""
+    from . import abi
+
+    d = np.ascontiguousarray(sun_dir, np.float32)
+    lam = np.ascontiguousarray(lam, np.float32)
+    out = np.zeros(lam.shape, np.float32)
+    assert abi.host_lib().prhost_sun_radiance(abi.ptr(d), turbidity, radius_deg, lam.size, abi.ptr(lam),
+                                              abi.ptr(out)) == 0
+    return out
+
+
+def rgb_to_sigmoid(rgb: np.ndarray, illuminant: np.ndarray) -> np.ndarray:
+    """Environment-map texels (n, 4) = (c0, c1, c2, scale) of unbounded RGBs (prhost_rgb_to_sigmoid)
+    fitted under the given 95-sample illuminant."""
+    from . import abi
+
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    ill = np.ascontiguousarray(illuminant, np.float32)
+    assert ill.size == 95
+    out = np.zeros((rgb.shape[0], 4), np.float32)
+    assert abi.host_lib().prhost_rgb_to_sigmoid(rgb.shape[0], abi.ptr(rgb), abi.ptr(ill), 0, abi.ptr(out)) == 0
+    return out

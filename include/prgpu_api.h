@@ -386,6 +386,15 @@ struct SceneExt {
     const TextureNode *textureNodes;
     int32_t textureNodeCount;
     int32_t pad2;
+    // Measurement tap (null = off): the rays traced for the paths in wavefront slots
+    // [0, rayTapPaths) of the call's first chunk (slot = pixel + pixels-per-chunk * sample), for
+    // their first rayTapBounces bounces, copied to HOST memory at rayTap as 2 x rayTapBounces x
+    // rayTapPaths records of 8 floats (origin, tMax, direction, 1): the closest-hit rays, then the
+    // shadow rays (tMax in units of the direction's length); a record stays zero where its path
+    // traced no such ray. For per-ray work counts (nodes and triangles visited), not for renders.
+    float *rayTap;
+    int32_t rayTapPaths;
+    int32_t rayTapBounces;
 };
 
 // Parameters of prgpu_render_aov (pr::RenderAOV, src/integrators/aov.h:10-21).
@@ -445,6 +454,16 @@ struct RenderStats {
     double shadowMs;           // device time in the shadow kernel
     double shadeMs;            // device time in the shading kernel
     double filmMs;             // device time in the film kernel
+};
+
+// Settings of the path-guiding network's sampling and online training (prgpu_guide_set_options;
+// defaults in brackets).
+struct GuideOptions {
+    float maxSelect;           // [0.9] cap of the probability c of sampling the guide (0 < x <= 0.99)
+    float logKappaMax;         // [8] upper clamp of the lobes' log concentration (0 <= x <= 8)
+    int32_t selectLoss;        // [0] c trained on the mixture's KL divergence (0) or on the second
+                               //     moment of the one-sample estimator (1)
+    int32_t trainPasses;       // [1] online training passes over each chunk's samples (1..64)
 };
 
 } // namespace prgpu
@@ -577,6 +596,10 @@ PRGPU_API int prgpu_guide_set_learning_rate(int deviceIndex, float learningRate,
 PRGPU_API int prgpu_guide_stats(int deviceIndex, float *out4, char *err, int errLen);
 // Adam step (beta 0.9 / 0.999, eps 1e-8) on the last gradient times gradScale.
 PRGPU_API int prgpu_guide_adam_step(int deviceIndex, float gradScale, float learningRate, char *err, int errLen);
+// Sampling and training settings of the guide on a device (null: the defaults); out-of-range
+// values return 1 with a message. They apply to later renders, gradients and training steps.
+PRGPU_API int prgpu_guide_set_options(int deviceIndex, const prgpu::GuideOptions *opts, char *err, int errLen);
+PRGPU_API int prgpu_guide_get_options(int deviceIndex, prgpu::GuideOptions *out, char *err, int errLen);
 
 // Number of kernel launches this library has issued since load (for launch accounting).
 PRGPU_API uint64_t prgpu_launch_count();

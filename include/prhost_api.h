@@ -68,3 +68,25 @@ PRHOST_API int prhost_checkpoint_write(const char *path, const prhost::Checkpoin
 PRHOST_API int prhost_checkpoint_read(const char *path, const prhost::CheckpointHeader *expected, double *film,
                                       uint64_t filmCount, void *body, uint64_t bodyCapacity, uint64_t *bodySize,
                                       char *err, int errLen);
+
+// Preetham daylight (A. J. Preetham, P. Shirley, B. Smits, SIGGRAPH 1999) as PRender builds it for
+// a "sun_sky" light: an equirect (+y up) map of width x height linear-sRGB texels (rgb: 3 floats
+// each, row 0 at the zenith) for the sun direction sunDir (normalised here), turbidity T (clamped
+// to [1.7, 10]) and a Lambertian ground of groundAlbedo below the horizon. Returns 0, or 1 on bad
+// arguments. Replaces pr::MakePreethamSky (src/lights/sky.cpp:146-205).
+PRHOST_API int prhost_preetham_sky(const float *sunDir, float turbidity, float groundAlbedo, int32_t width,
+                                   int32_t height, float *rgb);
+// The sun's spectral radiance (a 5778 K blackbody at the solar disk's luminance, scaled for an
+// enlarged disk, through the Rayleigh and aerosol optical depth of the air mass) at n wavelengths
+// (nm). Returns 0, or 1 on bad arguments. Replaces pr::MakeSunRadiance (src/lights/sky.cpp:207-233).
+PRHOST_API int prhost_sun_radiance(const float *sunDir, float turbidity, float angularRadiusDeg, int64_t n,
+                                   const float *lambdaNm, float *out);
+// Unbounded RGB -> environment-map texel (prgpu::EnvMapDesc::texels): per colour, out4 = (c0, c1,
+// c2, scale) with the spectrum scale * S(c0 l^2 + c1 l + c2), l in nm, S(x) = 1/2 + x / (2
+// sqrt(1 + x^2)), scale = 2 max(r, g, b) (0 for a colour without a positive component), the
+// coefficients fitted (Gauss-Newton in CIELAB) so that the reflectance S of rgb / scale under
+// illuminant95 (95 samples at 360..830 nm by 5) has the colour's sRGB chromaticity. threads = 0
+// uses all hardware threads. Returns 0, or 1 on bad arguments. The reference interpolates its
+// precomputed table of the same fits under D65 instead (RGBToSpectrumTable, src/core/rgb2spec.cpp).
+PRHOST_API int prhost_rgb_to_sigmoid(int64_t n, const float *rgb, const float *illuminant95, int32_t threads,
+                                     float *out4);

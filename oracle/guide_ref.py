@@ -17,6 +17,12 @@ The renderer folds the mixture onto the hemisphere of the shading normal n that 
 q_n(w) = q(w) + q(w - 2 (w.n) n). Loss per sample, two parts: -w log q_n(wi) trains the lobes,
 -w log(c q_n(wi) + (1 - c) pb) trains the selection output with q_n held fixed (its gradient is
 taken as if q_n were a constant).
+
+Settings (prgpu_guide_set_options; the defaults above): the selection cap (c = max_select
+sigmoid), the upper clamp of log kappa, and c's objective: select_loss = 1 replaces the selection
+term by the surrogate -w w' log(c q_n + (1 - c) pb) with w' = w held fixed, whose derivative in c
+is the sample estimate -w^2 (q_n - pb) / p of the derivative of the one-sample estimator's second
+moment E[(f Li)^2 / p].
 """
 
 from __future__ import annotations
@@ -98,16 +104,16 @@ def forward(params, X, round16=True):
     return A, (W, acts, zs)
 
 
-def decode(o):
+def decode(o, max_select=MAX_SELECT, log_kappa_max=8.0):
     v = o[:, :40].reshape(-1, LOBES, 5)
     d = v[:, :, 0:3]
     l = np.linalg.norm(d, axis=2, keepdims=True)
     mu = np.where(l > 1e-6, d / np.maximum(l, 1e-300), np.array([0.0, 0.0, 1.0]))
-    kappa = np.exp(np.clip(v[:, :, 3], -4.0, 8.0))
+    kappa = np.exp(np.clip(v[:, :, 3], -4.0, log_kappa_max))
     a = v[:, :, 4]
     e = np.exp(a - a.max(1, keepdims=True))
     pi = e / e.sum(1, keepdims=True)
-    c = MAX_SELECT / (1.0 + np.exp(-o[:, 40]))
+    c = max_select / (1.0 + np.exp(-o[:, 40]))
     return mu, kappa, pi, c
 
 
@@ -127,12 +133,12 @@ def mirror(w, n):
     return w - 2.0 * (w * n).sum(1, keepdims=True) * n
 
 
-def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None):
+def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None, max_select=MAX_SELECT, log_kappa_max=8.0, select_loss=0):
     """Loss per sample and its gradient w.r.t. the 48 outputs (FP64, analytic); n: the shading
     normals (folding planes). The mixture part uses q_fixed when given (the value whose gradient
     is stopped), else the current q_n."""
     o = np.asarray(o, np.float64)
-    mu, kappa, pi, c = decode(o)
+    mu, kappa, pi, c = decode(o, max_select, log_kappa_max)
     wr = mirror(wi, n)
     v1 = vmf(mu, kappa, wi)
     v2 = vmf(mu, kappa, wr)
@@ -143,12 +149,13 @@ def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None):
     ok = (p > 0) & (q > 0) & (wgt > 0)
     ps = np.where(ok, p, 1.0)
     qs = np.where(ok, q, 1.0)
-    loss = np.where(ok, -wgt * np.log(qs) - wgt * np.log(ps), 0.0)
+    ws = wgt * wgt if select_loss == 1 else wgt  # the selection term's weight
+    loss = np.where(ok, -wgt * np.log(qs) - ws * np.log(ps), 0.0)
     dq = np.where(ok, -wgt / qs, 0.0)
-    dc = np.where(ok, -wgt * (qm - pb) / ps, 0.0)
+    dc = np.where(ok, -ws * (qm - pb) / ps, 0.0)
     g = np.zeros_like(o)
     s = 1.0 / (1.0 + np.exp(-o[:, 40]))
-    g[:, 40] = dc * MAX_SELECT * s * (1 - s)
+    g[:, 40] = dc * max_select * s * (1 - s)
     gpi = dq[:, None] * vk
     sum_pig = (pi * gpi).sum(1, keepdims=True)
     ga = pi * gpi - pi * sum_pig
@@ -159,7 +166,8 @@ def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None):
     base = 1.0 / kappa - 2 * e / -np.expm1(-2 * kappa)
     t1 = np.einsum("nkc,nc->nk", mu, wi) - 1.0
     t2 = np.einsum("nkc,nc->nk", mu, wr) - 1.0
-    gk = np.where((raw > -4) & (raw < 8) & (kappa >= 1e-4), (d1 * (base + t1) + d2 * (base + t2)) * kappa, 0.0)
+    gk = np.where((raw > -4) & (raw < log_kappa_max) & (kappa >= 1e-4), (d1 * (base + t1) + d2 * (base + t2)) * kappa,
+                  0.0)
     d = o[:, :40].reshape(-1, LOBES, 5)[:, :, 0:3]
     l = np.linalg.norm(d, axis=2, keepdims=True)
     gm = (wi[:, None, :] * d1[:, :, None] + wr[:, None, :] * d2[:, :, None]) * kappa[:, :, None]
@@ -173,19 +181,20 @@ def loss_and_grad_out(o, wi, pb, wgt, n, q_fixed=None):
     return loss, g
 
 
-def mixture_q(o, wi, n):
+def mixture_q(o, wi, n, log_kappa_max=8.0):
     """The folded mixture density q_n(wi) (wi on the side of n it was sampled on)."""
-    mu, kappa, pi, _ = decode(np.asarray(o, np.float64))
+    mu, kappa, pi, _ = decode(np.asarray(o, np.float64), log_kappa_max=log_kappa_max)
     return (pi * (vmf(mu, kappa, wi) + vmf(mu, kappa, mirror(wi, n)))).sum(1)
 
 
-def backward(params, X, wi, pb, wgt, round16=True, n=None):
+def backward(params, X, wi, pb, wgt, round16=True, n=None, **opts):
     """Mean loss over the batch and the gradient of the SUMMED loss w.r.t. the flat weights
-    (n: folding normals, by default the normal inputs X[:, 75:78])."""
+    (n: folding normals, by default the normal inputs X[:, 75:78]; opts: the settings of
+    loss_and_grad_out)."""
     out, (W, acts, zs) = forward(params, X, round16)
     if n is None:
         n = np.asarray(X, np.float64)[:, 75:78]
-    loss, g = loss_and_grad_out(out, wi, pb, wgt, n)
+    loss, g = loss_and_grad_out(out, wi, pb, wgt, n, **opts)
     grads = [None] * 5
     dZ = _r16(g, round16)
     for l in range(4, -1, -1):

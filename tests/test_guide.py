@@ -58,6 +58,34 @@ def test_output_gradient_matches_finite_differences():
         np.testing.assert_allclose(g[:, i], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-7)
 
 
+def test_output_gradient_with_settings_matches_finite_differences():
+    """Selection cap 0.6, log kappa capped at 3 (some lobes beyond it), second-moment selection
+    objective: the analytic output gradient is that of the surrogate loss."""
+    rng = np.random.default_rng(11)
+    n = 6
+    o = rng.normal(0, 1.5, (n, 48))
+    o[:, 3:40:10] += 3.0  # lobes 0, 2, 4, 6 concentrated, some beyond the cap
+    X, wi, pb, w = _batch(n, 12)
+    nrm = X[:, 75:78]
+    wi = np.where((wi * nrm).sum(1, keepdims=True) < 0, G.mirror(wi, nrm), wi)
+    opts = dict(max_select=0.6, log_kappa_max=3.0, select_loss=1)
+    q0 = G.mixture_q(o, wi, nrm, log_kappa_max=3.0)
+    _, g = G.loss_and_grad_out(o, wi, pb, w, nrm, q_fixed=q0, **opts)
+    assert (o[:, :40].reshape(n, 8, 5)[:, :, 3] > 3.0).any()
+    h = 1e-6
+    for i in range(41):
+        d = np.zeros_like(o)
+        d[:, i] = h
+        lp, _ = G.loss_and_grad_out(o + d, wi, pb, w, nrm, q_fixed=q0, **opts)
+        lm, _ = G.loss_and_grad_out(o - d, wi, pb, w, nrm, q_fixed=q0, **opts)
+        np.testing.assert_allclose(g[:, i], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-7)
+    # The selection gradient is -w^2 (q - pb) / p times dc/do40.
+    c = G.decode(o, 0.6, 3.0)[3]
+    p = c * q0 + (1 - c) * pb
+    s = 1 / (1 + np.exp(-o[:, 40]))
+    np.testing.assert_allclose(g[:, 40], -w * w * (q0 - pb) / p * 0.6 * s * (1 - s), rtol=1e-12)
+
+
 def test_weight_gradient_matches_finite_differences():
     p = G.init_params(5).astype(np.float64)
     X, wi, pb, w = _batch(8, 6)

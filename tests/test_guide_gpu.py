@@ -92,6 +92,51 @@ def test_training_gradient_matches_oracle(gpu, n):
         assert not W[l][G.CONST_HID].any()
 
 
+@pytest.fixture
+def default_guide_options(gpu):
+    yield
+    guide.set_options()
+
+
+def test_training_gradient_with_settings_matches_oracle(gpu, default_guide_options):
+    """The same pass with non-default settings (selection cap 0.7, log kappa capped at 2, the
+    second-moment selection objective) against the oracle with those settings."""
+    n = 1000
+    w = _weights(41)
+    guide.set_weights(w)
+    guide.set_options(max_select=0.7, log_kappa_max=2.0, select_loss=1)
+    assert guide.get_options() == dict(max_select=pytest.approx(0.7), log_kappa_max=2.0, select_loss=1,
+                                       train_passes=1)
+    X = _inputs(n, 42)
+    rng = np.random.default_rng(43)
+    wi = rng.normal(size=(n, 3))
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    pb = np.abs(wi[:, 2]) / np.pi + 0.02
+    wt = rng.exponential(1.0, n)
+    loss, g = guide.gradient(X, wi, pb, wt)
+    f64 = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731
+    lref, gref = G.backward(w, X, f64(wi), f64(pb), f64(wt), round16=True, max_select=np.float32(0.7),
+                            log_kappa_max=2.0, select_loss=1)
+    assert abs(loss - lref * n) <= 1e-3 * abs(lref * n)
+    cos = float(g @ gref / (np.linalg.norm(g) * np.linalg.norm(gref)))
+    rel = float(np.linalg.norm(g - gref) / np.linalg.norm(gref))
+    assert cos > 0.999 and rel < 3e-2, (cos, rel)
+    # Defaults give a different gradient (the settings reached the kernel).
+    guide.set_options()
+    _, g0 = guide.gradient(X, wi, pb, wt)
+    assert float(np.linalg.norm(g0 - g) / np.linalg.norm(g)) > 0.05
+
+
+def test_guide_options_are_validated(gpu, default_guide_options):
+    from prgpu import abi
+
+    for bad in (dict(max_select=0.0), dict(max_select=1.0), dict(log_kappa_max=9.0), dict(select_loss=2),
+                dict(train_passes=0)):
+        with pytest.raises(abi.PrgpuError, match="out of range"):
+            guide.set_options(**bad)
+    assert guide.get_options()["max_select"] == pytest.approx(0.9)
+
+
 def test_adam_steps_reduce_the_training_loss(gpu):
     w = _weights(41)
     guide.set_weights(w)

@@ -46,3 +46,26 @@ def test_host_built_large_scene_renders(gpu):
     assert np.isfinite(a).all() and (a >= 0).all()
     assert np.array_equal(a, b)
     assert a[..., 1].mean() > 0
+
+
+def test_host_built_sun_and_sky_agree_with_reference(gpu, oracle):
+    """The host-built form with the host library's Preetham sky and sun radiance (a 64 x 32 sky map)
+    against the reference rendering the same layout from its JSON form (its own sun_sky light):
+    48 x 27, depth 64, 16 renders of 64 spp each side. The host fits the sky texels under a 6504 K
+    blackbody of unit luminance where the reference uses its D65 table, so the bar is |z| < 4 on
+    >= 99% of values and mean luminance within 4 standard errors or 1 %."""
+    w, h = 48, 27
+    path = hostscene.write_large_scene_json(os.path.join(tempfile.gettempdir(), "prb_scenes", "large_small_sky.prscene.json"),
+                                            w, h, terrain_res=48, cloud_res=24, spheres=12, sky_resolution=64)
+    rs = oracle.RefScene(path)
+    hs, ext = hostscene.build_large_scene(w, h, terrain_res=48, cloud_res=24, spheres=12, sky_resolution=64)
+    desc = hs.desc()
+    g = np.stack([render.render_ex(desc, w, h, 64, seed=1000 + k, max_depth=64, ext=ext) / 64 for k in range(16)])
+    c = np.stack([rs.render(64, 2000 + k, 64)[0].astype(np.float64) / 64 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"host-built sun and sky: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.99, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < max(4 * se, 0.01 * mc.mean()), f"mean Y gpu {mg.mean()} cpu {mc.mean()}"

@@ -66,7 +66,7 @@ def test_grid_desc_layout_and_ext():
     assert list(g.worldToMedium) == [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0]
     assert g.density == d.ctypes.data
     e = render.make_ext(grid_media=[g, g])
-    assert e.gridMediumCount == 2 and e.structSize == C.sizeof(abi.SceneExt) == 128
+    assert e.gridMediumCount == 2 and e.structSize == C.sizeof(abi.SceneExt) == 144
     arr = (abi.GridMediumDesc * 2).from_address(e.gridMedia)
     assert arr[1].nx == 4 and arr[1].density == d.ctypes.data
     assert abi.GridMediumDesc.density.offset == 104 and abi.SceneExt.gridMedia.offset == 40
