@@ -37,7 +37,7 @@ NVCC_FLAGS = [
 # Shading and the verification kernels round every product before it is added (no FMA
 # contraction), as the reference's ISO C++ build does, so BxDF / phase / medium values agree
 # with it to a few ulps even where the formulas cancel.
-PER_FILE_FLAGS = {"render.cu": ["--fmad=false"], "funcs.cu": ["--fmad=false"]}
+PER_FILE_FLAGS = {"render.cu": ["--fmad=false"], "batch.cu": ["--fmad=false"], "funcs.cu": ["--fmad=false"]}
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-fvisibility=hidden", "-ffp-contract=off", "-I", INCLUDE,
              "-pthread"]
 

@@ -329,8 +329,9 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict
                 float gout[kGuideOut];
                 if (valid) {
                     const GuideSample sm = samples[row];
+                    const float wn = opts.weightClamp > 0.f ? fminf(sm.w * wscale, opts.weightClamp) : sm.w * wscale;
                     lossAcc += guide_loss_grad(z, mk(sm.wi[0], sm.wi[1], sm.wi[2]), mk(sm.n[0], sm.n[1], sm.n[2]),
-                                               sm.pb, sm.w * wscale, gout, opts);
+                                               sm.pb, wn, gout, opts);
                 } else {
 #pragma unroll
                     for (int k = 0; k < kGuideOut; ++k) gout[k] = 0.f;
@@ -411,13 +412,17 @@ __global__ void k_guide_pack(const float *master, __half *packed) {
     }
 }
 
+// Adam on the gradient times scale (or *scaleDev: 0 = an empty online batch, no step). The step
+// count for the bias correction lives on the device (*stepDev, advanced before this kernel by
+// k_guide_norm or k_guide_bump), so captured graphs that replay training stay correct.
 __global__ void k_guide_adam(float *master, float *m, float *v, const float *grad, float scale, const float *scaleDev,
-                             float lr, float b1, float b2, float eps, int step) {
-    const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
+                             float lr, float b1, float b2, float eps, const int *stepDev) {
     if (scaleDev) {
         scale = *scaleDev;
-        if (scale == 0.f) return;  // empty online batch: no step
+        if (scale == 0.f) return;
     }
+    const int step = *stepDev;
+    const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGuideParams; i += gridDim.x * blockDim.x) {
         float g = grad[i] * scale;
         float mi = b1 * m[i] + (1.f - b1) * g;
@@ -428,6 +433,8 @@ __global__ void k_guide_adam(float *master, float *m, float *v, const float *gra
     }
 }
 
+__global__ void k_guide_bump(int *stepDev) { ++*stepDev; }
+
 __global__ void k_guide_to_half(const float *in, __half *out, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = __float2half_rn(in[i]);
 }
@@ -437,7 +444,7 @@ __global__ void k_guide_to_half(const float *in, __half *out, int n) {
 
 struct GuideState {
     DevBuf master, m, v, grad, packed, scratch, loss, status, train;
-    int step = 0;
+    DevBuf stepDev;        // Adam steps taken (int, device)
     bool ready = false;
     int sms = 0;
     float lr = 1e-3f;      // online learning rate (Adam)
@@ -458,6 +465,8 @@ void guide_setup(DeviceState &ds, GuideState &g) {
     g.packed.ensure(kWTotalBytes);
     g.loss.ensure(sizeof(float) * 4);
     g.status.ensure(sizeof(int) * 4);
+    g.stepDev.ensure(sizeof(int));
+    PRB_CUDA(cudaMemsetAsync(g.stepDev.ptr, 0, sizeof(int), ds.stream));
     PRB_CUDA(cudaMemsetAsync(g.master.ptr, 0, kGuideParams * sizeof(float), ds.stream));
     PRB_CUDA(cudaMemsetAsync(g.m.ptr, 0, kGuideParams * sizeof(float), ds.stream));
     PRB_CUDA(cudaMemsetAsync(g.v.ptr, 0, kGuideParams * sizeof(float), ds.stream));
@@ -472,7 +481,7 @@ void guide_set_weights(DeviceState &ds, GuideState &g, const float *host) {
     PRB_CUDA(cudaMemcpyAsync(g.master.ptr, host, kGuideParams * sizeof(float), cudaMemcpyHostToDevice, ds.stream));
     PRB_CUDA(cudaMemsetAsync(g.m.ptr, 0, kGuideParams * sizeof(float), ds.stream));
     PRB_CUDA(cudaMemsetAsync(g.v.ptr, 0, kGuideParams * sizeof(float), ds.stream));
-    g.step = 0;
+    PRB_CUDA(cudaMemsetAsync(g.stepDev.ptr, 0, sizeof(int), ds.stream));
     k_guide_pack<<<64, 256, 0, ds.stream>>>(g.master.as<float>(), g.packed.as<__half>());
     count_launch();
 }
@@ -497,17 +506,17 @@ void guide_train(cudaStream_t st, GuideState &g, const __half *features, const G
 }
 
 void guide_adam(cudaStream_t st, GuideState &g, float scale, float lr) {
-    ++g.step;
+    k_guide_bump<<<1, 1, 0, st>>>(g.stepDev.as<int>());
     k_guide_adam<<<64, 256, 0, st>>>(g.master.as<float>(), g.m.as<float>(), g.v.as<float>(), g.grad.as<float>(), scale,
-                                     nullptr, lr, 0.9f, 0.999f, 1e-8f, g.step);
+                                     nullptr, lr, 0.9f, 0.999f, 1e-8f, g.stepDev.as<int>());
     k_guide_pack<<<64, 256, 0, st>>>(g.master.as<float>(), g.packed.as<__half>());
-    count_launch(2);
+    count_launch(3);
 }
 
 // Online training: recorded samples -> FP16 features and loss inputs for up to maxRows rows, the
 // batch's weight sum, then the normalisation (weights to mean 1) and the Adam scale (1 / rows).
 __global__ void k_guide_prep(const GuideTrainRec *recs, const int *count, int offset, int maxRows, __half *features,
-                             GuideSample *samples, int *rows, float *wsum) {
+                             GuideSample *samples, int *rows, float *wsum, int bands) {
     const int n = max(0, min(*count - offset, maxRows));
     recs += offset;
     if (blockIdx.x == 0 && threadIdx.x == 0) *rows = n;
@@ -516,7 +525,7 @@ __global__ void k_guide_prep(const GuideTrainRec *recs, const int *count, int of
         float f[kGuideIn];
 #pragma unroll
         for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
-        guide_features_n(r.xn, mk(r.n[0], r.n[1], r.n[2]), mk(r.wo[0], r.wo[1], r.wo[2]), f);
+        guide_features_n(r.xn, mk(r.n[0], r.n[1], r.n[2]), mk(r.wo[0], r.wo[1], r.wo[2]), f, bands);
         __half2 *dst = reinterpret_cast<__half2 *>(features + size_t(i) * kGuideIn);
 #pragma unroll
         for (int k = 0; k < kGuideIn / 2; ++k) dst[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
@@ -525,11 +534,12 @@ __global__ void k_guide_prep(const GuideTrainRec *recs, const int *count, int of
     }
 }
 
-__global__ void k_guide_norm(const int *rows, const float *wsum, float *wnorm, float *scale) {
+__global__ void k_guide_norm(const int *rows, const float *wsum, float *wnorm, float *scale, int *stepDev) {
     const int n = *rows;
     const float s = *wsum;
     *wnorm = (n > 0 && s > 0.f) ? float(n) / s : 0.f;
     *scale = n > 0 ? 1.f / float(n) : 0.f;
+    if (n > 0) ++*stepDev;  // this batch's Adam step
 }
 
 int guide_status(DeviceState &ds, GuideState &g) {
@@ -583,6 +593,14 @@ bool guide_failed(DeviceState &ds, int device) {
 }
 
 GuideOpts guide_options(int device) { return gGuide[device].opts; }
+float guide_learning_rate(int device) { return gGuide[device].lr; }
+
+size_t guide_training_bytes(int maxRows) {
+    const size_t fb = size_t(maxRows) * kGuideIn * sizeof(__half), sb = size_t(maxRows) * sizeof(GuideSample);
+    return ((fb + 255) & ~size_t(255)) + ((sb + 255) & ~size_t(255)) + 256;
+}
+void guide_reserve_training(int device, int maxRows) { gGuide[device].train.ensure(guide_training_bytes(maxRows)); }
+const void *guide_training_buffer(int device) { return gGuide[device].train.ptr; }
 
 void guide_infer_rows(cudaStream_t st, int device, const __half *features, const int *dcount, int maxRows, float *out) {
     guide_forward(st, gGuide[device], features, dcount, maxRows, out);
@@ -593,7 +611,7 @@ void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs,
     GuideState &g = gGuide[device];
     if (lr <= 0.f) lr = g.lr;
     const size_t fb = size_t(maxRows) * kGuideIn * sizeof(__half), sb = size_t(maxRows) * sizeof(GuideSample);
-    g.train.ensure(((fb + 255) & ~size_t(255)) + ((sb + 255) & ~size_t(255)) + 256);
+    g.train.ensure(guide_training_bytes(maxRows));
     auto *feat = g.train.as<__half>();
     auto *smp = reinterpret_cast<GuideSample *>(g.train.as<unsigned char>() + ((fb + 255) & ~size_t(255)));
     auto *stats = reinterpret_cast<float *>(g.train.as<unsigned char>() + ((fb + 255) & ~size_t(255)) +
@@ -601,17 +619,16 @@ void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs,
     int *rows = reinterpret_cast<int *>(stats);
     float *wsum = stats + 1, *wnorm = stats + 2, *scale = stats + 3;
     PRB_CUDA(cudaMemsetAsync(stats, 0, 16, st));
-    k_guide_prep<<<g.sms * 4, 128, 0, st>>>(recs, dcount, offset, maxRows, feat, smp, rows, wsum);
-    k_guide_norm<<<1, 1, 0, st>>>(rows, wsum, wnorm, scale);
+    k_guide_prep<<<g.sms * 4, 128, 0, st>>>(recs, dcount, offset, maxRows, feat, smp, rows, wsum, g.opts.bands);
+    k_guide_norm<<<1, 1, 0, st>>>(rows, wsum, wnorm, scale, g.stepDev.as<int>());
     const int tiles = (maxRows + kTileRows - 1) / kTileRows;
     PRB_CUDA(cudaMemsetAsync(g.grad.ptr, 0, kGuideParams * sizeof(float), st));
     PRB_CUDA(cudaMemsetAsync(g.loss.ptr, 0, sizeof(float), st));
     k_guide_train<<<std::max(1, std::min(tiles, g.sms)), 128, train_smem(), st>>>(
         feat, smp, rows, g.packed.as<__half>(), g.grad.as<float>(), g.loss.as<float>(), g.status.as<int>(), wnorm,
         g.opts);
-    ++g.step;
     k_guide_adam<<<64, 256, 0, st>>>(g.master.as<float>(), g.m.as<float>(), g.v.as<float>(), g.grad.as<float>(), 0.f,
-                                     scale, lr, 0.9f, 0.999f, 1e-8f, g.step);
+                                     scale, lr, 0.9f, 0.999f, 1e-8f, g.stepDev.as<int>());
     k_guide_pack<<<64, 256, 0, st>>>(g.master.as<float>(), g.packed.as<__half>());
     count_launch(5);
 }
@@ -771,15 +788,18 @@ PRGPU_API int prgpu_guide_set_options(int deviceIndex, const prgpu::GuideOptions
         GuideOpts o;  // null: the defaults
         if (opts) {
             if (!(opts->maxSelect > 0.f && opts->maxSelect <= 0.99f) || !(opts->logKappaMax >= 0.f && opts->logKappaMax <= 8.f) ||
-                (opts->selectLoss != 0 && opts->selectLoss != 1) || opts->trainPasses < 1 || opts->trainPasses > 64) {
+                (opts->selectLoss != 0 && opts->selectLoss != 1) || opts->trainPasses < 1 || opts->trainPasses > 64 ||
+                opts->bands < 0 || opts->bands > kGuideBandsMax || !(opts->weightClamp >= 0.f)) {
                 set_err(err, errLen, "guide options out of range (0 < maxSelect <= 0.99, 0 <= logKappaMax <= 8, "
-                                     "selectLoss 0 or 1, 1 <= trainPasses <= 64)");
+                                     "selectLoss 0 or 1, 1 <= trainPasses <= 64, 0 <= bands <= 12, weightClamp >= 0)");
                 return 1;
             }
             o.maxSelect = opts->maxSelect;
             o.logKappaMax = opts->logKappaMax;
             o.selectLoss = opts->selectLoss;
             o.trainPasses = opts->trainPasses;
+            o.bands = opts->bands;
+            o.weightClamp = opts->weightClamp;
         }
         gGuide[deviceIndex].opts = o;
         return 0;
@@ -797,6 +817,8 @@ PRGPU_API int prgpu_guide_get_options(int deviceIndex, prgpu::GuideOptions *out,
         out->logKappaMax = o.logKappaMax;
         out->selectLoss = o.selectLoss;
         out->trainPasses = o.trainPasses;
+        out->bands = o.bands;
+        out->weightClamp = o.weightClamp;
         return 0;
     });
 }
@@ -810,7 +832,9 @@ PRGPU_API int prgpu_guide_stats(int deviceIndex, float *out4, char *err, int err
         DeviceState &ds = device_state(deviceIndex);
         GuideState &g = gGuide[deviceIndex];
         float loss = 0.f, tr[4] = {0.f, 0.f, 0.f, 0.f};
+        int steps = 0;
         PRB_CUDA(cudaMemcpyAsync(&loss, g.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, ds.stream));
+        PRB_CUDA(cudaMemcpyAsync(&steps, g.stepDev.ptr, sizeof(int), cudaMemcpyDeviceToHost, ds.stream));
         if (g.train.ptr) {
             // rows (int bits), weight sum of the last online batch: the stats block after the samples
             const size_t fb = size_t(1 << 16) * kGuideIn * sizeof(__half), sb = size_t(1 << 16) * sizeof(GuideSample);
@@ -825,7 +849,7 @@ PRGPU_API int prgpu_guide_stats(int deviceIndex, float *out4, char *err, int err
         out4[0] = loss;
         out4[1] = float(rows);
         out4[2] = tr[1];
-        out4[3] = float(g.step);
+        out4[3] = float(steps);
         return 0;
     });
 }

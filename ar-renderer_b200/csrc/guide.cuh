@@ -29,7 +29,7 @@
 namespace prb {
 
 constexpr int kGuideIn = 128, kGuideHid = 64, kGuideOut = 48, kGuideLayers = 5, kGuideLobes = 8;
-constexpr int kGuideBands = 12, kGuideConstIn = 81, kGuideConstHid = 63;
+constexpr int kGuideBands = 12, kGuideBandsMax = 12, kGuideConstIn = 81, kGuideConstHid = 63;
 // Weight matrix l is [out_l x in_l]; the flattened FP32 master array keeps them in order, row-major.
 __host__ __device__ constexpr int guide_layer_in(int l) { return l == 0 ? kGuideIn : kGuideHid; }
 __host__ __device__ constexpr int guide_layer_out(int l) { return l == kGuideLayers - 1 ? kGuideOut : kGuideHid; }
@@ -43,14 +43,18 @@ struct GuideOpts {
     float logKappaMax = 8.f;   // upper clamp of log kappa
     int selectLoss = 0;        // c's objective: 0 = -w log p_mix, 1 = second moment w^2 / p_mix
     int trainPasses = 1;       // passes over each chunk's recorded samples (online training)
+    int bands = kGuideBandsMax;  // position encoding bands in use (the rest of the inputs zero)
+    float weightClamp = 0.f;   // > 0: training weights (normalised to mean 1 per batch) clamped to it
 };
 
 __host__ __device__ constexpr int guide_weight_offset(int l) {
     return l == 0 ? 0 : kGuideHid * kGuideIn + (l - 1) * kGuideHid * kGuideHid;
 }
 
-// Input features (FP32) of a shading point; bmin / bext: scene bounds and extent.
-__device__ __forceinline__ void guide_features(V3 x, V3 n, V3 wo, const float *bmin, const float *bext, float *f) {
+// Input features (FP32) of a shading point; bmin / bext: scene bounds and extent; bands: the
+// encoding bands in use (higher bands' inputs are zero).
+__device__ __forceinline__ void guide_features(V3 x, V3 n, V3 wo, const float *bmin, const float *bext, float *f,
+                                               int bands = kGuideBands) {
     float xn[3] = {(x.x - bmin[0]) / bext[0], (x.y - bmin[1]) / bext[1], (x.z - bmin[2]) / bext[2]};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -63,8 +67,8 @@ __device__ __forceinline__ void guide_features(V3 x, V3 n, V3 wo, const float *b
         for (int a = 0; a < 3; ++a) {
             float s, c;
             sincospif(xn[a] * float(1 << b), &s, &c);
-            f[3 + 6 * b + 2 * a] = s;
-            f[3 + 6 * b + 2 * a + 1] = c;
+            f[3 + 6 * b + 2 * a] = b < bands ? s : 0.f;
+            f[3 + 6 * b + 2 * a + 1] = b < bands ? c : 0.f;
         }
     f[75] = n.x, f[76] = n.y, f[77] = n.z;
     f[78] = wo.x, f[79] = wo.y, f[80] = wo.z;
@@ -160,9 +164,9 @@ struct GuideTrainRec {
 };
 
 // Input features from a normalised position (x already in [0,1]^3).
-__device__ __forceinline__ void guide_features_n(const float *xn, V3 n, V3 wo, float *f) {
+__device__ __forceinline__ void guide_features_n(const float *xn, V3 n, V3 wo, float *f, int bands = kGuideBands) {
     const float zero[3] = {0.f, 0.f, 0.f}, one[3] = {1.f, 1.f, 1.f};
-    guide_features(mk(xn[0], xn[1], xn[2]), n, wo, zero, one, f);
+    guide_features(mk(xn[0], xn[1], xn[2]), n, wo, zero, one, f, bands);
 }
 
 // Gradient of the two-part loss above with respect to the 48 raw outputs (FP32): lobe outputs

@@ -19,8 +19,13 @@ void guide_infer_rows(cudaStream_t st, int device, const __half *features, const
 // recorded samples (count on the device); weights are normalised to mean 1 within the batch.
 void guide_train_records(cudaStream_t st, int device, const GuideTrainRec *recs, const int *dcount, int offset,
                          int maxRows, float lr);
-// The device's sampling and training settings (prgpu_guide_set_options).
+// The device's sampling and training settings (prgpu_guide_set_options) and learning rate.
 GuideOpts guide_options(int device);
+float guide_learning_rate(int device);
+// Allocates the staging buffers of guide_train_records for batches of up to maxRows, so that its
+// launches can be captured into a graph (no allocation during capture); their address.
+void guide_reserve_training(int device, int maxRows);
+const void *guide_training_buffer(int device);
 // True (and cleared) when a guide kernel gave up waiting for its tensor-core work.
 bool guide_failed(DeviceState &ds, int device);
 // Launch bookkeeping: kernels per inference / training step.

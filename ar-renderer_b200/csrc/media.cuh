@@ -35,7 +35,7 @@ __device__ __forceinline__ float lerpf(float t, float a, float b) { return (1.f 
 
 // pr::NoiseField::Density (medium.cpp:168-177) at a medium-space point inside the bounds: the
 // remapped fBm, faded towards the bounds' inscribed ellipsoid, thresholded and sharpened.
-__device__ __noinline__ float noise_field_density(const DevGrid &g, V3 p) {
+static __device__ __noinline__ float noise_field_density(const DevGrid &g, V3 p) {
     const V3 q = (p + mk(g.noiseOffset[0], g.noiseOffset[1], g.noiseOffset[2])) * g.noiseFrequency;
     float n = 0.5f + 0.5f * fbm_noise(q, g.noiseOctaves, false) * 1.4f;
     if (g.noiseFalloff) {
@@ -50,7 +50,7 @@ __device__ __noinline__ float noise_field_density(const DevGrid &g, V3 p) {
 // Density of an index-space grid (a densified NanoVDB grid; NanoVDBField::Density,
 // nanovdb_field.cpp:27-39): trilinear between voxel centres at integer coordinates, the background
 // 0 beyond the array, clamped at 0.
-__device__ __noinline__ float indexed_density(const DevGrid &g, V3 p) {
+static __device__ __noinline__ float indexed_density(const DevGrid &g, V3 p) {
     const float x = p.x - float(g.org[0]), y = p.y - float(g.org[1]), z = p.z - float(g.org[2]);
     const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
     const int x0 = int(fx), y0 = int(fy), z0 = int(fz);
@@ -188,7 +188,7 @@ __device__ __forceinline__ void majorant_walk(const DevGrid &g, V3 mo, V3 md, fl
 
 // Ratio-tracking transmittance over [0, dist) along the unit direction d, Russian roulette once
 // the largest channel drops below 0.1 (unbiased). rng: a stream for this segment.
-__device__ SS grid_tr(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float dist, Pcg &rng) {
+static __device__ SS grid_tr(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float dist, Pcg &rng) {
     V3 mo, md;
     float t0, t1;
     if (!isfinite(dist) || !grid_clip(g, o, d, dist, &mo, &md, &t0, &t1)) return splat(1.f);
@@ -230,7 +230,7 @@ __device__ __forceinline__ SS medium_transmittance(const DevScene &s, int m, con
 // live wavelengths, per-wavelength weights sigma_e / (mu P_e)). Returns 1 on a real scattering
 // event at *tOut, 2 on absorption, 0 when the segment [0, tMax) is crossed; *weight multiplies
 // the throughput in every case.
-__device__ int grid_sample(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float tMax, Pcg &rng,
+static __device__ int grid_sample(const DevScene &s, const DevGrid &g, const Lambda &lam, V3 o, V3 d, float tMax, Pcg &rng,
                            float *tOut, SS *weight) {
     *weight = splat(1.f);
     *tOut = tMax;

@@ -32,7 +32,7 @@ __device__ __forceinline__ float perlin_grad(int h, float x, float y, float z) {
 }
 __device__ __forceinline__ float perlin_lerp(float t, float a, float b) { return (1.f - t) * a + t * b; }
 
-__device__ float perlin_noise(V3 p) {
+static __device__ float perlin_noise(V3 p) {
     const float fx = floorf(p.x), fy = floorf(p.y), fz = floorf(p.z);
     const int X = int(fx) & 255, Y = int(fy) & 255, Z = int(fz) & 255;
     const float x = p.x - fx, y = p.y - fy, z = p.z - fz;
@@ -52,7 +52,7 @@ __device__ float perlin_noise(V3 p) {
 
 // Fractional Brownian motion: octaves of noise at doubling frequency and halving amplitude,
 // normalised by the amplitude sum; |noise| per octave for turbulence.
-__device__ float fbm_noise(V3 p, int octaves, bool turbulence) {
+static __device__ float fbm_noise(V3 p, int octaves, bool turbulence) {
     float sum = 0.f, amp = 0.5f, freq = 1.f, norm = 0.f;
     const int n = max(1, octaves);
     for (int i = 0; i < n; ++i) {

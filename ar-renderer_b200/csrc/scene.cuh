@@ -148,6 +148,7 @@ struct DevScene {
     int maxDepth;            // <= 0: unlimited
     float clampY;            // 0: off
     double *film;            // the render's device FP64 film, 3 doubles per pixel
+    int guideMode;           // the render's guide flags (bit 0 sample with the guide, bit 1 train it)
 };
 
 struct SceneCache {

@@ -94,7 +94,7 @@ __device__ __forceinline__ int warp_append(int *counter) {
 // Pixel filter importance sampling (src/gpu/prender_gpu.cpp:1465-1494; the host builds the CDF
 // as src/integrators/gpu_path.cpp:431-456)
 
-__device__ float filter_eval_1d(const DevScene &s, float x) {
+static __device__ float filter_eval_1d(const DevScene &s, float x) {
     x = fabsf(x);
     if (x > s.filterRadius) return 0.f;
     switch (s.filterType) {
@@ -111,7 +111,7 @@ __device__ float filter_eval_1d(const DevScene &s, float x) {
     }
 }
 
-__device__ float filter_sample_1d(const DevScene &s, float u, float *pdf) {
+static __device__ float filter_sample_1d(const DevScene &s, float u, float *pdf) {
     int lo = 0, hi = prgpu::kFilterBins;
     while (hi - lo > 1) {
         int mid = (lo + hi) >> 1;
@@ -134,7 +134,7 @@ struct Surf {
     float u, v;
 };
 
-__device__ Surf shade_point(const DevScene &s, const prgpu::Primitive &pr, float t, float b1, float b2, V3 o, V3 d) {
+static __device__ Surf shade_point(const DevScene &s, const prgpu::Primitive &pr, float t, float b1, float b2, V3 o, V3 d) {
     Surf sf;
     if (pr.type == prgpu::PrimSphere) {
         V3 c = f3(pr.p0);
@@ -182,7 +182,7 @@ __device__ Surf shade_point(const DevScene &s, const prgpu::Primitive &pr, float
 // ---------------------------------------------------------------------------------------------
 // Materials (src/materials/material.cpp:73-117; src/gpu/prender_gpu.cpp:1136-1226)
 
-__device__ Ggx make_ggx(float ax, float ay) {
+static __device__ Ggx make_ggx(float ax, float ay) {
     Ggx g{ax, ay};
     if (!g.smooth()) {
         g.ax = fmaxf(g.ax, 1e-4f);
@@ -191,7 +191,7 @@ __device__ Ggx make_ggx(float ax, float ay) {
     return g;
 }
 
-__device__ SS diffuse_albedo(const DevScene &s, const prgpu::Material &m, float u, float v, const Lambda &lam) {
+static __device__ SS diffuse_albedo(const DevScene &s, const prgpu::Material &m, float u, float v, const Lambda &lam) {
     int id = m.albedo;
     if (m.albedoB >= 0 && m.checkerScale > 0.f) {
         int odd = (int(floorf(u * m.checkerScale)) + int(floorf(v * m.checkerScale))) & 1;
@@ -204,7 +204,7 @@ __device__ SS diffuse_albedo(const DevScene &s, const prgpu::Material &m, float 
 }
 
 // Builds the lobe of material m at the hit; may terminate the secondary wavelengths.
-__device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam) {
+static __device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam) {
     Lobe l;
     l.kind = kLobeNone;
     l.etaD = 1.f;
@@ -259,7 +259,7 @@ __device__ __forceinline__ int tex_wrap(int v, int n, int mode) {
     return v < 0 ? v + n : v;
 }
 
-__device__ void tex_rgb(const DevTex &t, float u, float v, float rgb[3]) {
+static __device__ void tex_rgb(const DevTex &t, float u, float v, float rgb[3]) {
     u = u * t.su + t.ou;
     v = v * t.sv + t.ov;
     if (t.flipV) v = 1.f - v;
@@ -276,7 +276,7 @@ __device__ void tex_rgb(const DevTex &t, float u, float v, float rgb[3]) {
 }
 
 // Sigmoid-polynomial reflectance of an sRGB triple at the 4 wavelengths (RGBAlbedoSpectrum).
-__device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lambda &lam) {
+static __device__ SS rgb_albedo(const DevScene &s, float r, float g, float b, const Lambda &lam) {
     float rgb[3] = {clampf(r, 0.f, 1.f), clampf(g, 0.f, 1.f), clampf(b, 0.f, 1.f)};
     float c[3];
     if (rgb[0] == rgb[1] && rgb[1] == rgb[2]) {
@@ -327,7 +327,7 @@ struct TexCtx {
     float u, v;
 };
 
-__device__ float noise_node(const prgpu::TextureNode &n, const TexCtx &c) {
+static __device__ float noise_node(const prgpu::TextureNode &n, const TexCtx &c) {
     V3 p = (n.flags & prgpu::TexNoiseWorldSpace) ? c.p : mk(c.u, c.v, 0.f);
     p = (p + mk(n.offset[0], n.offset[1], n.offset[2])) * n.frequency;
     const bool turb = (n.flags & prgpu::TexNoiseTurbulence) != 0;
@@ -374,9 +374,9 @@ __device__ __forceinline__ void walk_texture(const DevScene &s, int root, const 
 
 // A spectrum tree as an albedo at the 4 wavelengths (constants from the spectrum table, images
 // uplifted through the RGB -> spectrum table).
-__device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam);
+static __device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam);
 
-__device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, const Lambda &lam, bool unbounded = false) {
+static __device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, const Lambda &lam, bool unbounded = false) {
     SS acc = splat(0.f);
     walk_texture(s, root, c, [&](const prgpu::TextureNode &n, float w) {
         SS v;
@@ -395,7 +395,7 @@ __device__ SS spectrum_texture(const DevScene &s, int root, const TexCtx &c, con
     return acc;
 }
 
-__device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
+static __device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
     float acc = 0.f;
     walk_texture(s, root, c, [&](const prgpu::TextureNode &n, float w) {
         float v = 0.f;
@@ -417,7 +417,7 @@ __device__ float float_texture(const DevScene &s, int root, const TexCtx &c) {
 // a diffuse lobe (a tree, else an image; clamped to [0, 1] as DiffuseMaterial::GetBxDF,
 // material.cpp:73-77) and the roughness of conductor and rough dielectric lobes (trees; alpha =
 // clamp(r, 0, 1)^2, material.cpp:80-85, 110-116, 151-154).
-__device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l,
+static __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, Lobe *l,
                               float etaScale = 1.f) {
     if (!s.matTex) return;
     if (l->kind == kLobeDiffuse) {
@@ -464,7 +464,7 @@ __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c, const 
 // RGBUnboundedSpectrum (rgb2spec.cpp:327-335): zero for a colour whose largest component is not
 // positive, else the sigmoid polynomial of the colour times 1 / scale, scale = 2 max(r, g, b),
 // times that scale (the reference's order of operations, so the same bits).
-__device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam) {
+static __device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const Lambda &lam) {
     const float m = fmaxf(0.f, fmaxf(r, fmaxf(g, b)));
     SS v;
     if (m == 0.f) {
@@ -481,7 +481,7 @@ __device__ SS rgb_unbounded(const DevScene &s, float r, float g, float b, const 
 
 // dp/du and dp/dv of the parameterization at a hit (Sphere / Triangle::Intersect, shape.cpp:75-82,
 // 237-251): the sphere's scaled by 2 pi and pi, a coordinate system where they degenerate.
-__device__ void surface_dpduv(const prgpu::Primitive &pr, const Surf &sf, V3 *dpdu, V3 *dpdv) {
+static __device__ void surface_dpduv(const prgpu::Primitive &pr, const Surf &sf, V3 *dpdu, V3 *dpdv) {
     if (pr.type == prgpu::PrimSphere) {
         V3 rel = sf.p - f3(pr.p0);
         float cosT = clampf(rel.y / pr.r, -1.f, 1.f), sinT = safe_sqrt(1.f - cosT * cosT);
@@ -524,7 +524,7 @@ __device__ __forceinline__ float height_at(const DevTex &t, int channel, float u
 // the normal map's colour is a direction in the frame of the shading dp/du and normal (the
 // bitangent along dp/dv), scaled in the tangent plane; the result stays in the geometric
 // hemisphere and the shading dp/du follows it.
-__device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
+static __device__ void perturb_shading(const DevScene &s, int mi, const prgpu::Primitive &pr, Surf *sf) {
     if (!s.matTex) return;
     const int4 mt = s.matTex[5 * mi], bt = s.matTex[5 * mi + 1];
     const int bumpTree = s.matTex[5 * mi + 2].x;
@@ -584,7 +584,7 @@ __device__ __forceinline__ bool full_material(const prgpu::Material &m) {
 // Builds the coated / sheen BSDF of material m (the reference's CoatedDiffuseMaterial,
 // CoatedConductorMaterial and Material::GetBSDF sheen wrapper, material.cpp:5-14, 117-166); may
 // terminate the secondary wavelengths (dispersive coat).
-__device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam,
+static __device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material &m, float u, float v, Lambda &lam,
                                        FullBsdf *b) {
     b->layered = b->sheen = b->black = false;
     if (m.type == prgpu::MatCoatedDiffuse || m.type == prgpu::MatCoatedConductor) {
@@ -655,7 +655,7 @@ __device__ __noinline__ void make_full(const DevScene &s, const prgpu::Material 
 // The textured parameters of a coated / sheen BSDF: its base lobe (textured_lobe), the coat's
 // roughness, thickness and medium albedo (MakeCoatTop, material.cpp:119-130) and the sheen's colour
 // and roughness (Material::GetBSDF, material.cpp:5-14; SheenBxDF clamps, bxdf.cpp:568-571).
-__device__ void textured_full(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, FullBsdf *b) {
+static __device__ void textured_full(const DevScene &s, int mi, const TexCtx &c, const Lambda &lam, FullBsdf *b) {
     if (!s.matTex || b->black) return;
     // A coated conductor's n, k are relative to the coat's IOR.
     textured_lobe(s, mi, c, lam, b->layered ? &b->lay.bottom : &b->base, b->layered ? b->lay.top.etaD : 1.f);
@@ -689,7 +689,7 @@ __device__ void textured_full(const DevScene &s, int mi, const TexCtx &c, const 
 // ---------------------------------------------------------------------------------------------
 // Lights
 
-__device__ SS emitted(const DevScene &s, const prgpu::Light &l, V3 n, V3 w, const Lambda &lam) {
+static __device__ SS emitted(const DevScene &s, const prgpu::Light &l, V3 n, V3 w, const Lambda &lam) {
     float c = dot(n, w);
     if (!l.twoSided && c <= 0.f) return splat(0.f);
     float prof = l.cosPower > 0.f ? powf(fabsf(c), l.cosPower) : 1.f;
@@ -697,7 +697,7 @@ __device__ SS emitted(const DevScene &s, const prgpu::Light &l, V3 n, V3 w, cons
 }
 
 // Solid-angle density of sampling point p (normal n) on area light l from ref (uniform area).
-__device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
+static __device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
     V3 d = p - ref;
     float d2 = len2(d);
     float c = fabsf(dot(n, d * rsqrtf(d2)));
@@ -707,7 +707,7 @@ __device__ float area_pdf(const prgpu::Light &l, V3 ref, V3 p, V3 n) {
 
 // Probability that NEE at (p, n) picks light li: the light-BVH pmf when the scene has one (the
 // exact leaf-to-root walk), the power pmf otherwise.
-__device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
+static __device__ float light_pmf(const DevScene &s, int li, V3 p, V3 n) {
     if (s.lbvhCount == 0) return s.lights[li].pmf;
     return lbvh_pmf(LightTree{s.lbvh, s.lbvhCount, s.lbvhProb, s.lightLeaf}, li, p, n);
 }
@@ -738,7 +738,7 @@ __device__ __forceinline__ float texel_at(const float4 &t, float l) {
 
 // Radiance of the map towards world direction d: bilinear texel spectra with horizontal wrap
 // (EnvironmentLight::Lookup, light.cpp:238-261), times the illuminant and the scale.
-__device__ SS env_lookup(const DevScene &s, V3 d, const Lambda &lam) {
+static __device__ SS env_lookup(const DevScene &s, V3 d, const Lambda &lam) {
     const DevEnvMap &m = s.envMap;
     float u, v;
     dir_to_equirect(normalize(env_to_light(m, d)), &u, &v);
@@ -776,7 +776,7 @@ __device__ __forceinline__ float dist1d_sample(const float *cdf, int n, float u,
 }
 
 // Direction and solid-angle pdf from the map's 2D distribution (EnvironmentLight::SampleLi).
-__device__ bool env_sample(const DevScene &s, float u0, float u1, V3 *wi, float *pdf) {
+static __device__ bool env_sample(const DevScene &s, float u0, float u1, V3 *wi, float *pdf) {
     const DevEnvMap &m = s.envMap;
     if (!(m.margInt > 0.f)) return false;
     int iv, iu;
@@ -794,7 +794,7 @@ __device__ bool env_sample(const DevScene &s, float u0, float u1, V3 *wi, float 
 }
 
 // Solid-angle pdf of sampling world direction d (EnvironmentLight::PDF_Li).
-__device__ float env_pdf(const DevScene &s, V3 d) {
+static __device__ float env_pdf(const DevScene &s, V3 d) {
     const DevEnvMap &m = s.envMap;
     if (!(m.margInt > 0.f)) return 0.f;
     float u, v;
@@ -838,7 +838,7 @@ __device__ __forceinline__ int find_interval(const float *v, int n, float x) {
 // Relative intensity of a type C IES profile towards the profile-frame direction w
 // (IESProfile::Evaluate / EvaluateAngles, ies.cpp:79-109): theta from the nadir axis, phi folded
 // by the symmetry the last horizontal angle implies, then linear in theta and in phi.
-__device__ float ies_eval(const DevDelta &l, V3 w) {
+static __device__ float ies_eval(const DevDelta &l, V3 w) {
     const float *va = l.profile, *ha = l.profile + l.nV, *cd = l.profile + l.nV + l.nH;
     const float deg = 57.295779513082320876f;
     float theta = acosf(clampf(w.z, -1.f, 1.f)) * deg;
@@ -901,7 +901,7 @@ __device__ __forceinline__ LightSample sample_delta_light(const DevScene &s, con
     return ls;
 }
 
-__device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
+static __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda &lam, float ul, float u0, float u1) {
     LightSample ls;
     ls.ok = false;
     ls.delta = false;
@@ -1014,7 +1014,7 @@ __device__ LightSample sample_light(const DevScene &s, V3 p, V3 n, const Lambda 
 }
 
 // Transmittance of the shadow segment o -> o + dd (length len(dd)) in the given medium.
-__device__ SS segment_tr(const DevScene &s, int medium, const Lambda &lam, V3 o, V3 dd, float frac) {
+static __device__ SS segment_tr(const DevScene &s, int medium, const Lambda &lam, V3 o, V3 dd, float frac) {
     float l = len(dd);
     float dist = frac * l;
     if (!is_grid(s, medium)) return homogeneous_tr(s, medium, lam, dist);
@@ -1107,7 +1107,7 @@ __device__ __forceinline__ void raygen_path(const DevScene &s, const Paths &P, i
     }
 }
 
-__global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo ci, int *counters, int *queue) {
+static __global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, ChunkInfo ci, int *counters, int *queue) {
     int total = ci.npix * ci.samples;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x) {
         int sIdx = j / ci.npix, pl = j - sIdx * ci.npix;
@@ -1275,7 +1275,9 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         int iters = __float_as_int(pn4.w) + (kFull ? 0 : 1);
         int prim = __float_as_int(hit.w);
         bool alive = true, deferred = false;
-        if constexpr (kGuide && !kFull) if (a.guideMode & 2) {
+        // Guide mode of this path: the call's, restricted in the batched form to its render's flags.
+        const int gmode = kBatch ? (a.guideMode & s.guideMode) : a.guideMode;
+        if constexpr (kGuide && !kFull) if (gmode & 2) {
             // A record taken at this path's previous vertex: its radiance snapshot is the sum so far
             // (that vertex's NEE included, nothing from here on), so the final sum minus it is the
             // light that came along the sampled direction.
@@ -1534,7 +1536,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     // vertices of each path.
                     const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse;
                     const bool inRange = diffuseVertex && gcount < kGuideVertices;
-                    const bool guided = (a.guideMode & 1) && inRange;
+                    const bool guided = (gmode & 1) && inRange;
                     const int recIndex = gcount;
                     if (inRange) ++gcount;
                     if (guided) gm = guide_decode(a.guideOut + size_t(q - first) * kGuideOut, a.guideOpts);
@@ -1570,7 +1572,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     ok = ok && nonzero(bs.f) && bs.pdf > 0.f && isfinite(bs.pdf) && bs.wi.z != 0.f &&
                          isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
                     float4 *rec = a.guideRec + 4 * (size_t(j) * kGuideVertices + recIndex);
-                    if (ok && (a.guideMode & 2) && inRange) {
+                    if (ok && (gmode & 2) && inRange) {
                         // First diffuse vertex of the path: record (x, n, wo, wi, p_bsdf, mean beta).
                         const float *bmin = s.root.box, *bmax = s.root.box + 3;
                         V3 xn = mk((sf.p.x - bmin[0]) / fmaxf(bmax[0] - bmin[0], 1e-20f),
@@ -1743,7 +1745,7 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
 
 // Moves the survivors' queue into place for the next bounce and accumulates statistics (one
 // thread; keeps the bounce loop free of host round trips).
-__global__ void k_advance(int *counters, unsigned long long *stats) {
+static __global__ void k_advance(int *counters, unsigned long long *stats) {
     stats[kStatClosest] += (unsigned long long)counters[kCntActive];
     stats[kStatShadow] += (unsigned long long)counters[kCntShadow];
     stats[kStatBounces] += counters[kCntActive] > 0 ? 1ull : 0ull;
@@ -1892,7 +1894,7 @@ __device__ __forceinline__ void film_pixel(const DevScene &s, const Paths &P, in
     film3[2] = Z;
 }
 
-__global__ void __launch_bounds__(256) k_film(DevScene s, Paths P, ChunkInfo ci, float clampY, double *film) {
+static __global__ void __launch_bounds__(256) k_film(DevScene s, Paths P, ChunkInfo ci, float clampY, double *film) {
     for (int pl = blockIdx.x * blockDim.x + threadIdx.x; pl < ci.npix; pl += gridDim.x * blockDim.x)
         film_pixel(s, P, 0, ci.npix, pl, ci.samples, clampY, film + 3 * size_t(ci.pixBegin + pl));
 }

@@ -157,7 +157,6 @@ constexpr float kXYZToSRGB[3][3] = {{3.2404542f, -1.5371385f, -0.4985314f},
 
 struct FitTables {
     std::vector<double> w[3];  // illuminant x CIE xyz at the quadrature wavelengths, Y of white = 1
-    double white[3];
 };
 
 double lab_f(double t) {
@@ -211,15 +210,17 @@ bool solve3(double A[3][3], double *b) {
 void fit_one(const FitTables &T, const double rgb[3], double *c) {
     const double M[3][3] = {{0.4124564, 0.3575761, 0.1804375}, {0.2126729, 0.7151522, 0.0721750},
                             {0.0193339, 0.1191920, 0.9503041}};
-    // Target XYZ: the colour's share of the white point's XYZ, channel by channel.
-    double wsum[3] = {M[0][0] + M[0][1] + M[0][2], M[1][0] + M[1][1] + M[1][2], M[2][0] + M[2][1] + M[2][2]};
+    // Target: the colour's XYZ with the sRGB (D65) white point, in CIELAB relative to that white;
+    // the reflectance's XYZ under the fit illuminant (unit luminance) is compared in the same
+    // space, so an illuminant whose white differs from D65 is corrected for, not inherited.
+    const double white[3] = {M[0][0] + M[0][1] + M[0][2], M[1][0] + M[1][1] + M[1][2], M[2][0] + M[2][1] + M[2][2]};
     double xyz[3], target[3];
-    for (int i = 0; i < 3; ++i) xyz[i] = (M[i][0] * rgb[0] + M[i][1] * rgb[1] + M[i][2] * rgb[2]) * T.white[i] / wsum[i];
-    to_lab(xyz, T.white, target);
+    for (int i = 0; i < 3; ++i) xyz[i] = M[i][0] * rgb[0] + M[i][1] * rgb[1] + M[i][2] * rgb[2];
+    to_lab(xyz, white, target);
     for (int it = 0; it < 40; ++it) {
         double cur[3], lab[3], r[3];
         fit_xyz(T, c, cur);
-        to_lab(cur, T.white, lab);
+        to_lab(cur, white, lab);
         for (int i = 0; i < 3; ++i) r[i] = target[i] - lab[i];
         if (r[0] * r[0] + r[1] * r[1] + r[2] * r[2] < 1e-10) break;
         double J[3][3];
@@ -230,8 +231,8 @@ void fit_one(const FitTables &T, const double rgb[3], double *c) {
             double xp[3], xm[3], lp[3], lm[3];
             fit_xyz(T, cp, xp);
             fit_xyz(T, cm, xm);
-            to_lab(xp, T.white, lp);
-            to_lab(xm, T.white, lm);
+            to_lab(xp, white, lp);
+            to_lab(xm, white, lm);
             for (int i = 0; i < 3; ++i) J[i][k] = -(lp[i] - lm[i]) / 2e-5;  // d residual / d c
         }
         double step[3] = {r[0], r[1], r[2]};
@@ -339,13 +340,8 @@ PRHOST_API int prhost_rgb_to_sigmoid(int64_t n, const float *rgb, const float *i
     double ysum = 0;
     for (double v : T.w[1]) ysum += v;
     if (!(ysum > 0)) return 1;
-    for (int k = 0; k < 3; ++k) {
-        T.white[k] = 0;
-        for (double &v : T.w[k]) {
-            v /= ysum;
-            T.white[k] += v;
-        }
-    }
+    for (int k = 0; k < 3; ++k)
+        for (double &v : T.w[k]) v /= ysum;
     int nt = threads > 0 ? threads : int(std::max(1u, std::thread::hardware_concurrency()));
     nt = int(std::min<int64_t>(nt, std::max<int64_t>(1, n / 256)));
     auto work = [&](int64_t b, int64_t e) {

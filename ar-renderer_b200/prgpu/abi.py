@@ -204,7 +204,7 @@ class BatchStats(C.Structure):
 
 class GuideOptions(C.Structure):
     _fields_ = [("maxSelect", C.c_float), ("logKappaMax", C.c_float), ("selectLoss", C.c_int32),
-                ("trainPasses", C.c_int32)]
+                ("trainPasses", C.c_int32), ("bands", C.c_int32), ("weightClamp", C.c_float)]
 
 
 class RenderStats(C.Structure):

@@ -73,15 +73,16 @@ def set_learning_rate(lr: float, device: int = 0) -> None:
               "prgpu_guide_set_learning_rate")
 
 
-DEFAULT_OPTIONS = dict(max_select=0.9, log_kappa_max=8.0, select_loss=0, train_passes=1)
+DEFAULT_OPTIONS = dict(max_select=0.9, log_kappa_max=8.0, select_loss=0, train_passes=1, bands=12, weight_clamp=0.0)
 
 
 def set_options(max_select: float = 0.9, log_kappa_max: float = 8.0, select_loss: int = 0, train_passes: int = 1,
-                device: int = 0) -> None:
+                bands: int = 12, weight_clamp: float = 0.0, device: int = 0) -> None:
     """Sampling and training settings of the guide (prgpu_guide_set_options): the cap of the
     selection probability c, the cap of log kappa, c's objective (0 KL, 1 second moment of the
-    one-sample estimator) and the online training passes over each chunk's samples."""
-    o = abi.GuideOptions(max_select, log_kappa_max, select_loss, train_passes)
+    one-sample estimator), the online training passes over each chunk's samples, the position
+    encoding bands in use and the clamp of the batch-normalised training weights (0 off)."""
+    o = abi.GuideOptions(max_select, log_kappa_max, select_loss, train_passes, bands, weight_clamp)
     err = abi.err_buf()
     abi.check(abi.gpu_lib().prgpu_guide_set_options(device, C.byref(o), err, len(err)), err, "prgpu_guide_set_options")
 
@@ -91,4 +92,4 @@ def get_options(device: int = 0) -> dict:
     err = abi.err_buf()
     abi.check(abi.gpu_lib().prgpu_guide_get_options(device, C.byref(o), err, len(err)), err, "prgpu_guide_get_options")
     return dict(max_select=o.maxSelect, log_kappa_max=o.logKappaMax, select_loss=o.selectLoss,
-                train_passes=o.trainPasses)
+                train_passes=o.trainPasses, bands=o.bands, weight_clamp=o.weightClamp)

@@ -49,9 +49,18 @@ TRIS_PER_RAY = 2.21
 # Algorithmic bytes per closest-hit ray: every visited node (32 B in the reference layout) and
 # every tested triangle (36 B) read once, the 32-byte ray read and an 8-byte hit written.
 BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
-# DRAM bytes per closest-hit launch from ncu (profiles/trace_closest_soup1m.md): read + write of a
-# 2^22-ray capture of the same kernel, scaled by the rays of a full 2^24-ray launch.
+# DRAM bytes per closest-hit launch: dram__bytes_read.sum + dram__bytes_write.sum of this kernel
+# in one ncu capture of a 2^22-ray launch of this workload (a full 2^24-ray launch is too large to
+# capture), scaled by the rays of a full launch. Not measured by this run; the JSON says so.
 NCU_TRAFFIC_PER_LAUNCH = (565.865472e6 + 46.270720e6) * 4
+# Plain path tracer (box scene, 256^2, depth 8): algorithmic bytes per path sample,
+# N_closest B_ray + N_shadow B_shadow + 24 B of film, with the reference traversal's per-ray node
+# and triangle counts on the rays the GPU traces for a seeded 2^16-path subset
+# (oracle/measure_path_work.py): 4.266 closest rays of 1,567 B and 2.805 shadow rays of 755 B.
+PT_BYTES_PER_SAMPLE = 4.266 * 1567.27 + 2.805 * 754.97 + 24
+# L2 hit rate of the path tracer's closest-hit kernel on that scene (ncu lts__t_sector_hit_rate of
+# k_extend, first bounce of a 128^2 x 64 spp render): the scene (about 9 MB) stays in L2.
+PT_L2_HIT_RATE = 0.708
 
 
 def _peaks():
@@ -169,6 +178,13 @@ def path_tracer_bench(args, device: int, cpu: bool):
         "e2e": {"value": samples / e2e_s, "unit": "path samples/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": int(w * hh * 3 * 8)},
     }
+    peak, peak_kind = _peaks()
+    achieved = PT_BYTES_PER_SAMPLE * out["value"] / 1e9
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "peak_source": peak_kind, "bytes_per_path_sample": PT_BYTES_PER_SAMPLE,
+                       "l2_hit_rate_closest": PT_L2_HIT_RATE,
+                       "note": "algorithmic bytes of the reference traversal's node / triangle visits per path sample; "
+                               "the scene is L2-resident, so DRAM moves far less"}
     if cpu:
         import tempfile
 
@@ -518,7 +534,9 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "kernel": "k_trace<closest>",
                      "bytes_per_ray": BYTES_PER_RAY, "launch_ms": closest_ms,
-                     "traffic": NCU_TRAFFIC_PER_LAUNCH},
+                     "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                     "traffic_source": "ncu dram read + write of this kernel on a 2^22-ray launch of this workload, "
+                                       "scaled x4; not measured in this run"},
         "cpu_baseline": cpu,
         "clocks": clocks.summary(),
         "gpu_launches": launches,

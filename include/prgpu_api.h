@@ -464,6 +464,8 @@ struct GuideOptions {
     int32_t selectLoss;        // [0] c trained on the mixture's KL divergence (0) or on the second
                                //     moment of the one-sample estimator (1)
     int32_t trainPasses;       // [1] online training passes over each chunk's samples (1..64)
+    int32_t bands;             // [12] position-encoding bands in use (0..12; the others input 0)
+    float weightClamp;         // [0 = off] training weights, normalised to mean 1 per batch, clamped
 };
 
 } // namespace prgpu

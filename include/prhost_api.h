@@ -84,8 +84,9 @@ PRHOST_API int prhost_sun_radiance(const float *sunDir, float turbidity, float a
 // Unbounded RGB -> environment-map texel (prgpu::EnvMapDesc::texels): per colour, out4 = (c0, c1,
 // c2, scale) with the spectrum scale * S(c0 l^2 + c1 l + c2), l in nm, S(x) = 1/2 + x / (2
 // sqrt(1 + x^2)), scale = 2 max(r, g, b) (0 for a colour without a positive component), the
-// coefficients fitted (Gauss-Newton in CIELAB) so that the reflectance S of rgb / scale under
-// illuminant95 (95 samples at 360..830 nm by 5) has the colour's sRGB chromaticity. threads = 0
+// coefficients fitted (Gauss-Newton in CIELAB, D65 white) so that the reflectance S of rgb / scale
+// under illuminant95 (95 samples at 360..830 nm by 5, scaled to unit luminance) has the colour's
+// sRGB XYZ. threads = 0
 // uses all hardware threads. Returns 0, or 1 on bad arguments. The reference interpolates its
 // precomputed table of the same fits under D65 instead (RGBToSpectrumTable, src/core/rgb2spec.cpp).
 PRHOST_API int prhost_rgb_to_sigmoid(int64_t n, const float *rgb, const float *illuminant95, int32_t threads,

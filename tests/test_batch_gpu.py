@@ -108,3 +108,74 @@ def test_batch_input_validation(gpu):
     with pytest.raises(abi.PrgpuError, match="batch size"):
         render.render_batch([], config=render.batch_config(4096, 128))
     assert not film.any()
+
+
+def _guide_weights(seed):
+    """Fixed random weights with peaked, badly placed lobes (the unbiasedness tests' stress case)."""
+    import guide_ref as G
+
+    p = G.init_params(seed).astype(np.float64)
+    rng = np.random.default_rng(seed + 1)
+    W = G.split(p)
+    W[0][:, G.CONST_IN] = rng.normal(0, 0.5, W[0].shape[0])
+    for l in range(1, 5):
+        W[l][:, G.CONST_HID] = rng.normal(0, 0.5, W[l].shape[0])
+    for l in range(4):
+        W[l][G.CONST_HID, :] = 0
+    W[4][41:, :] = 0
+    W[4][40, G.CONST_HID] = 1.5
+    return p.astype(np.float32)
+
+
+def test_guided_batch_matches_guided_single_renders_bit_for_bit(gpu):
+    """The guided, batched form with fixed weights: per-render guide flags (two renders sampling with
+    the guide, one plain) in one graph launch give exactly the films of one prgpu_render_ex per
+    render -- the network's inference per bounce runs inside the batch's graph on the shared
+    diffuse queue, and a path's decision depends only on its own row."""
+    from prgpu import guide
+
+    guide.set_weights(_guide_weights(11))
+    specs = [(0, 40, 24, 6, 8, render.GUIDE_SAMPLE), (1, 32, 32, 5, 8, 0), (2, 24, 40, 7, 6, render.GUIDE_SAMPLE)]
+    items, alone = [], []
+    for seed, w, h, spp, depth, flags in specs:
+        hs = hostscene.build_box_scene(scenes.box_scene(seed=seed, width=w, height=h, medium=bool(seed % 2)))
+        ext = render.make_ext(guide=flags) if flags else None
+        p = dict(spp=spp, seed=300 + seed, max_depth=depth)
+        alone.append(render.render_ex(hs.desc(), w, h, spp, seed=p["seed"], max_depth=depth, ext=ext))
+        items.append((hs.desc(), ext, p, np.zeros((h, w, 3))))
+    for capacity in (2048, 1 << 20):
+        films = [np.zeros_like(f) for *_, f in items]
+        render.render_batch([(d, e, p, f) for (d, e, p, _), f in zip(items, films)],
+                            config=render.batch_config(capacity, 128))
+        for k, (a, b) in enumerate(zip(films, alone)):
+            assert np.array_equal(a, b), f"capacity {capacity}, render {k} differs (max |d| {np.abs(a - b).max()})"
+
+
+def test_guided_batch_trains_online_and_stays_unbiased(gpu, oracle):
+    """Guided renders that also train the network online inside the batch's graph (collect + Adam
+    steps after every filmed wave): the weights move, Adam steps are taken, and the trained-on-the-fly
+    image agrees with the reference PathIntegrator (16 batch items of 256 spp, |z| < 4 on >= 99.5%
+    of values, mean luminance within 1.5%)."""
+    from prgpu import guide
+
+    w = h = 32
+    rs = oracle.RefScene(ru.scene_file("guided_batch_box", seed=0, width=w, height=h))
+    desc = rs.export()
+    guide.set_weights(_guide_weights(7))
+    before = guide.get_weights()
+    steps0 = guide.stats()["steps"]
+    ext = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN)
+    films = [np.zeros((h, w, 3)) for _ in range(16)]
+    render.render_batch([(desc, ext, dict(spp=256, seed=1000 + k, max_depth=8), f) for k, f in enumerate(films)],
+                        config=render.batch_config(1 << 16, 128))
+    assert not np.array_equal(guide.get_weights(), before)
+    assert guide.stats()["steps"] > steps0
+    g = np.stack(films) / 256
+    c = np.stack([rs.render(256, 2000 + k, 8)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    yg, yc = g[..., 1].mean(), c[..., 1].mean()
+    print(f"guided batch, online training: frac {frac:.4f}, mean Y {yg:.5f} vs {yc:.5f}, "
+          f"{guide.stats()['steps'] - steps0} Adam steps")
+    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(yg / yc - 1) < 0.015, f"mean Y guided batch {yg} reference {yc}"

@@ -5,11 +5,13 @@ both sides, as tests/test_quality.cpp:146-173 of the reference estimates them; t
 |z| < 4 on >= 99.9% of values (all three XYZ channels of every pixel) and mean luminance within
 0.5%."""
 
+import os
+
 import numpy as np
 import pytest
 
 import render_util as ru
-from prgpu import render
+from prgpu import hostscene, render, scenes
 
 pytestmark = [pytest.mark.gpu, pytest.mark.slow]
 
@@ -28,5 +30,32 @@ def test_plain_path_tracer_is_unbiased_against_65536_spp_reference(gpu, oracle, 
     z = ru.z_scores(g, c)
     frac = np.mean(np.abs(z) < 4)
     yg, yc = g[..., 1].mean(), c[..., 1].mean()
+    assert frac >= 0.999, f"only {frac:.5f} of values within |z| < 4 (max |z| {np.abs(z).max():.2f})"
+    assert abs(yg / yc - 1) < 0.005, f"mean Y gpu {yg} cpu {yc} ({yg / yc - 1:+.4%})"
+
+
+GATE_FIXTURE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "gate_c0.npz")
+
+
+def test_c0_image_is_unbiased_against_65536_spp_reference_fixture(gpu):
+    """The gate at the benchmark's own configuration: the box-and-spheres scene at 256 x 256, depth 8,
+    built by the library's host side exactly as the benchmark renders it, 16 GPU seeds x 4096 spp,
+    against the reference PathIntegrator's 16 seeds x 4096 spp (65,536 spp) of the same scene,
+    precomputed into tests/golden/gate_c0.npz by tests/golden/make_gate.py (per-pixel mean and
+    across-seed variance). |z| < 4 on >= 99.9% of the 196,608 values and mean luminance within 0.5%."""
+    fx = np.load(GATE_FIXTURE)
+    n, side, depth = int(fx["seeds"]), int(fx["side"]), int(fx["depth"])
+    assert (side, depth, int(fx["spp"])) == (256, 8, SPP)
+    s = scenes.box_scene(seed=0, width=side, height=side, spp=SPP, max_depth=depth)
+    desc = hostscene.build_box_scene(s).desc()
+    g = np.stack([render.render_ex(desc, side, side, SPP, seed=5000 + k, max_depth=depth) / SPP for k in range(SEEDS)])
+    mg, vg = g.mean(0), g.var(0, ddof=1) / SEEDS
+    mc, vc = fx["mean"].astype(np.float64), fx["var"].astype(np.float64) / n
+    den = np.sqrt(vg + vc)
+    z = np.where(den > 0, (mg - mc) / np.where(den > 0, den, 1), np.where(mg == mc, 0.0, np.inf))
+    frac = np.mean(np.abs(z) < 4)
+    yg, yc = mg[..., 1].mean(), float(fx["mean_y"])
+    print(f"C0 gate: frac {frac:.5f} (max |z| {np.abs(z).max():.2f}), mean Y gpu {yg:.6f} cpu {yc:.6f} "
+          f"({yg / yc - 1:+.4%})")
     assert frac >= 0.999, f"only {frac:.5f} of values within |z| < 4 (max |z| {np.abs(z).max():.2f})"
     assert abs(yg / yc - 1) < 0.005, f"mean Y gpu {yg} cpu {yc} ({yg / yc - 1:+.4%})"
