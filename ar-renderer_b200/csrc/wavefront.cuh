@@ -1511,6 +1511,11 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 BSample bs;
                 bool ok;
                 float misPdf;  // the BSDF density for MIS against later light hits
+                // Guided vertices: the sampling density over the BSDF's, folded into etaScale so
+                // that Russian roulette keeps testing the throughput BSDF sampling would have given
+                // (a guide that sends the path towards bright directions lowers beta there by the
+                // same factor; testing beta alone would kill exactly the paths it found).
+                float rrScale = 1.f;
                 if constexpr (kFull) {
                     // Coats and sheen (FullBsdf: stochastic layered walks, out of line); a
                     // proportional sampling pdf takes the estimated density for MIS (path.cpp:219).
@@ -1562,6 +1567,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                         pbGuide = lobe_pdf(lobe, wol, wil);
                         bs.f = lobe_f(lobe, wol, wil);
                         bs.pdf = gm.c * guide_pdf_folded(gm, wiw, sf.ns, side) + (1.f - gm.c) * pbGuide;
+                        if (pbGuide > 0.f) rrScale = fminf(fmaxf(bs.pdf / pbGuide, 1e-3f), 1e3f);
                         bs.wi = wil;
                         bs.flags = kFlagReflection | kFlagDiffuse;
                         bs.eta = 1.f;
@@ -1604,6 +1610,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     prevPdf = misPdf;
                     specular = (bs.flags & kFlagSpecular) != 0u;
                     if (bs.flags & kFlagTransmission) etaScale *= sqr(bs.eta);
+                    etaScale *= rrScale;
                     prevP = sf.p;
                     prevN = sf.n;
                     o = offset_origin(sf.p, sf.n, wi);

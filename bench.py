@@ -266,6 +266,51 @@ def batch_bench(args, device: int, cpu: bool):
     return out
 
 
+def guided_vs_plain_bench(args):
+    """Equal-time relMSE, guided vs plain, on the guided-vs-plain scene (the box with its light
+    behind an occluder with a 0.1-wide slit and 12 subsurface BK7 spheres; 4 hero wavelengths,
+    depth 32) at a reduced size (--gvp-res, default 128^2). The reference image is a 65,536-spp
+    plain render on the GPU. Plain renders --gvp-spp samples per pixel; the guided form starts from
+    fresh weights and trains online (one Adam step per 2^16 recorded samples) while it renders, for
+    as many samples per pixel as fit the plain render's device time (its own per-sample time,
+    training included, measured on a short run first). relMSE is the form of the reference's
+    tests/test_quality.cpp:241-248: mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2).
+    ratio = relMSE plain / relMSE guided (> 1: the guide wins at equal time)."""
+    from prgpu import guide, hostscene, render, scenes
+
+    R, depth = args.gvp_res, 32
+    desc = hostscene.build_box_scene(scenes.slit_scene(seed=0, width=R, height=R, max_depth=depth)).desc()
+    t0 = time.perf_counter()
+    ref_spp = args.gvp_ref_spp
+    ref, rst = render.render_ex(desc, R, R, ref_spp, seed=777, max_depth=depth, stats=True)
+    ref /= ref_spp
+
+    def relmse(img):
+        return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    spp = args.gvp_spp
+    plain, pst = render.render_ex(desc, R, R, spp, seed=11, max_depth=depth, stats=True)
+    plain_ms = pst.deviceMs
+    guide.set_options()
+    train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET, wavefront_paths=65536)
+    _, gst = render.render_ex(desc, R, R, 16, seed=12, max_depth=depth, ext=train, stats=True)
+    per_spp = gst.deviceMs / 16
+    gspp = max(1, int(plain_ms / per_spp))
+    train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET
+    guided, gst2 = render.render_ex(desc, R, R, gspp, seed=13, max_depth=depth, ext=train, stats=True)
+    ep, eg = relmse(plain / spp), relmse(guided / gspp)
+    # Equal sample count, for reference: the guide after that training, sampling only.
+    use = render.make_ext(guide=render.GUIDE_SAMPLE)
+    g_eq, _ = render.render_ex(desc, R, R, spp, seed=14, max_depth=depth, ext=use, stats=True)
+    return {"workload": f"guided vs plain: slit box with 12 subsurface BK7 spheres, {R}x{R}, depth {depth}, "
+                        f"4 hero wavelengths, reference {ref_spp} spp plain (GPU)",
+            "metric": "equal-time relMSE ratio (plain / guided)", "ratio": ep / eg, "unit": "x",
+            "plain": {"spp": spp, "device_ms": plain_ms, "relmse": ep},
+            "guided": {"spp": gspp, "device_ms": gst2.deviceMs, "relmse": eg, "training": "online, fresh weights"},
+            "equal_spp_ratio": ep / relmse(g_eq / spp), "reference_s": time.perf_counter() - t0,
+            "guide_settings": "defaults (selection cap 0.9, 8 lobes, 12 bands, lr 1e-3)"}
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -350,6 +395,66 @@ def large_scene_bench(args, device: int):
     return out
 
 
+def c4_time_to_relmse(args):
+    """The north-star comparison on the large outdoor scene (4096^2 fBm terrain, 256^3 cloud, 200
+    metal spheres, Preetham sun and sky; depth 64) at a reduced film (--c4-width x --c4-height):
+    device time until relMSE <= --c4-target against a plain reference of --c4-ref-spp samples,
+    for the plain path tracer (prgpu_render_ex) and for the guided, batched form (prgpu_render_batch,
+    the guide sampling diffuse vertices and training online after every filmed wave, fresh weights).
+    Both add samples in doubling steps (1, 1, 2, 4, ... spp) onto one film and check relMSE after
+    each step; a step's device time counts whole. Opt-in: the reference takes minutes."""
+    from prgpu import guide, hostscene, render
+
+    w, h, depth = args.c4_width, args.c4_height, 64
+    hs, ext = hostscene.build_large_scene(w, h, terrain_res=args.ls_terrain, cloud_res=args.ls_cloud)
+    desc = hs.desc()
+    t0 = time.perf_counter()
+    ref = render.render_ex(desc, w, h, args.c4_ref_spp, seed=999, max_depth=depth, ext=ext) / args.c4_ref_spp
+    ref_s = time.perf_counter() - t0
+
+    def relmse(img):
+        return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    def progress(step):
+        film = np.zeros((h, w, 3))
+        done, ms, trace = 0, 0.0, []
+        n = 1
+        while done < args.c4_max_spp:
+            ms += step(film, done, n)
+            done += n
+            e = relmse(film / done)
+            trace.append((done, ms, e))
+            if e <= args.c4_target:
+                break
+            n = max(1, done)
+        return trace
+
+    plain_ext = abi_copy_ext(ext, 0)
+
+    def plain_step(film, first, n):
+        _, st = render.render_ex(desc, w, h, n, first_sample=first, seed=1, max_depth=depth, ext=plain_ext, out=film,
+                                 stats=True)
+        return st.deviceMs
+
+    guide.set_options()
+    gext = abi_copy_ext(ext, render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET)
+
+    def guided_step(film, first, n):
+        st = render.render_batch([(desc, gext, dict(spp=n, first_sample=first, seed=1, max_depth=depth), film)],
+                                 config=render.batch_config(1 << 22, 256), stats=True)
+        gext.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
+        return st.deviceMs
+
+    tp, tg = progress(plain_step), progress(guided_step)
+    hit = lambda tr: tr[-1][1] if tr[-1][2] <= args.c4_target else None  # noqa: E731
+    out = {"workload": f"large outdoor scene, {w}x{h}, depth 64, reference {args.c4_ref_spp} spp plain ({ref_s:.0f} s)",
+           "target_relmse": args.c4_target, "plain": {"trace_spp_ms_relmse": tp, "ms_to_target": hit(tp)},
+           "guided_batched": {"trace_spp_ms_relmse": tg, "ms_to_target": hit(tg)}}
+    if hit(tp) and hit(tg):
+        out["guided_time_fraction"] = hit(tg) / hit(tp)
+    return out
+
+
 def abi_copy_ext(ext, flags: int):
     """A copy of a SceneExt with other guide flags (the arrays stay owned by the original)."""
     from prgpu import abi
@@ -383,10 +488,23 @@ def main():
                          "conditional graphs)")
     ap.add_argument("--batch-spp-div", type=int, default=1,
                     help="divide every render's spp (profiling captures only; the JSON says so)")
+    ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain comparison")
+    ap.add_argument("--guided-only", action="store_true",
+                    help="run only the guided-vs-plain comparison and print its JSON object (profiling captures)")
+    ap.add_argument("--gvp-res", type=int, default=128, help="guided-vs-plain image side (1024 = the full C3 size)")
+    ap.add_argument("--gvp-spp", type=int, default=256, help="plain samples per pixel of the equal-time comparison")
+    ap.add_argument("--gvp-ref-spp", type=int, default=65536, help="samples per pixel of the plain reference image")
     ap.add_argument("--large-scene", action="store_true",
                     help="also run the large outdoor scene (33.5M-triangle terrain, cloud grid, 4K film; opt-in: "
                          "about a minute of host scene build)")
     ap.add_argument("--large-scene-only", action="store_true", help="run only the large outdoor scene")
+    ap.add_argument("--c4-time-to-relmse", action="store_true",
+                    help="run only the large scene's time to relMSE, guided + batched vs plain (opt-in, minutes)")
+    ap.add_argument("--c4-width", type=int, default=480)
+    ap.add_argument("--c4-height", type=int, default=270)
+    ap.add_argument("--c4-ref-spp", type=int, default=16384)
+    ap.add_argument("--c4-target", type=float, default=0.01)
+    ap.add_argument("--c4-max-spp", type=int, default=4096)
     ap.add_argument("--ls-spp", type=int, default=4)
     ap.add_argument("--ls-steps", type=int, default=2)
     ap.add_argument("--ls-width", type=int, default=3840)
@@ -410,6 +528,12 @@ def main():
         return
     if args.large_scene_only:
         print(json.dumps(large_scene_bench(args, local)))
+        return
+    if args.guided_only:
+        print(json.dumps(guided_vs_plain_bench(args)))
+        return
+    if args.c4_time_to_relmse:
+        print(json.dumps(c4_time_to_relmse(args)))
         return
 
     import torch
@@ -514,6 +638,9 @@ def main():
     bt = None
     if world == 1 and not args.no_batch:
         bt = batch_bench(args, local, cpu=not args.no_cpu_baseline)
+    gvp = None
+    if world == 1 and not args.no_guided:
+        gvp = guided_vs_plain_bench(args)
     ls = None
     if world == 1 and args.large_scene:
         ls = large_scene_bench(args, local)
@@ -544,6 +671,7 @@ def main():
         "any_hit_mrays": N_RAYS / ((ms_per_step - closest_ms) * 1e3),
         "path_tracer": pt,
         "uneven_batch": bt,
+        "guided_vs_plain": gvp,
     }
     if ls is not None:
         line["large_scene"] = ls
