@@ -337,7 +337,7 @@ int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &
             // vertex uses the result).
             k_guide_features<true><<<L.gWide, 256, 0, st>>>(none, scenes, rs.P, cnt, cq, rs.capacity,
                                                            rs.guideFeat.as<__half>(), L.guideOpts.bands);
-            guide_infer_rows(st, device, rs.guideFeat.as<__half>(), cnt + kCntClass0 + kClassDiffuse, rs.capacity,
+            guide_infer_rows(st, device, rs.guideFeat.as<__half>(), cnt + kCntClass0 + kClassGuided, rs.capacity,
                              rs.guideOut.as<float>());
             launches += 1 + kGuideInferLaunches;
         }

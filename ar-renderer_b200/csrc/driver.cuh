@@ -11,17 +11,17 @@
 
 namespace prb {
 
-// Guide inputs for every path filed as diffuse: shading point, shading normal and outgoing
-// direction (the same quantities the shading kernel records for training), FP16 rows in the
-// order of the diffuse class queue.
+// Guide inputs for every path filed as guided (kClassGuided): shading point, shading normal and
+// outgoing direction (the same quantities the shading kernel records for training), FP16 rows in
+// the order of that class's queue.
 // kBatch: every path reads its own render's scene (and scene bounds).
 template <bool kBatch = false>
 __global__ void __launch_bounds__(256) k_guide_features(DevScene s0, const DevScene *scenes, Paths P,
                                                         const int *counters, const int *classQ, int classCap,
                                                         __half *feat, int bands) {
-    const int n = counters[kCntClass0 + kClassDiffuse];
+    const int n = counters[kCntClass0 + kClassGuided];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int j = classQ[size_t(kClassDiffuse) * classCap + i];
+        const int j = classQ[size_t(kClassGuided) * classCap + i];
         const DevScene &s = SceneOf<kBatch>::get(s0, scenes, kBatch ? path_render(P.meta[j].w) : 0);
         const float *bmin = s.root.box, *bmax = s.root.box + 3;
         float4 o4 = P.o[j], d4 = P.d[j], hit = P.hit[j];

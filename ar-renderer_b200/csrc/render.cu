@@ -222,11 +222,11 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                     if (timing) PRB_CUDA(cudaEventRecord(rs.ev[4 * b], st));
                     if (sph) k_extend<true><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
                     else k_extend<false><<<gExtend, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin);
-                    k_classify<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin, cq, rs.capacity);
+                    k_classify<false><<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, cnt, qin, cq, rs.capacity, guideMode);
                     if (guideMode & 1) {
                         k_guide_features<<<gShade, 256, 0, st>>>(scene, nullptr, rs.P, cnt, cq, rs.capacity,
                                                                  rs.guideFeat.as<__half>(), gopts.bands);
-                        guide_infer_rows(st, ds.device, rs.guideFeat.as<__half>(), cnt + kCntClass0 + kClassDiffuse,
+                        guide_infer_rows(st, ds.device, rs.guideFeat.as<__half>(), cnt + kCntClass0 + kClassGuided,
                                          rs.capacity, rs.guideOut.as<float>());
                         launches += 1 + kGuideInferLaunches;
                     }

@@ -47,7 +47,9 @@ enum ShadeClass : int {
     kClassDielectric = 3,  // smooth, rough or thin
     kClassOther = 4,       // interfaces, black and anything else
     kClassMedium = 5,      // the path is inside a medium (free flight first)
-    kClasses = 6
+    kClassGuided = 6,      // diffuse, at one of the first diffuse vertices of a path whose render
+                           // uses the path guide (its inference runs on this class's queue only)
+    kClasses = 7
 };
 
 // Image environment on the device: texels (sigmoid-polynomial spectra), and the 2D sampling

@@ -1120,8 +1120,10 @@ static __global__ void __launch_bounds__(256) k_raygen(DevScene s, Paths P, Chun
 // slots, so the shading kernel can walk the classes in order. The order within a class does not
 // matter: every path's update depends on its own state only.
 template <bool kBatch = false>
+// guideMode (single renders; batched renders read their scene's flags): diffuse vertices before a
+// path's kGuideVertices-th diffuse vertex are filed as kClassGuided when the render uses the guide.
 __global__ void __launch_bounds__(256) k_classify(DevScene s0, const DevScene *scenes, Paths P, int *counters,
-                                                  const int *queue, int *classQ, int classCap) {
+                                                  const int *queue, int *classQ, int classCap, int guideMode = 0) {
     __shared__ int hist[kClasses], base[kClasses];
     const int n = counters[kCntActive];
     for (int q0 = blockIdx.x * blockDim.x; q0 < n; q0 += gridDim.x * blockDim.x) {
@@ -1135,6 +1137,8 @@ __global__ void __launch_bounds__(256) k_classify(DevScene s0, const DevScene *s
             const int prim = __float_as_int(P.hit[j].w);
             const DevScene &s = SceneOf<kBatch>::get(s0, scenes, path_render(mt.w));
             c = mt.z >= 0 ? kClassMedium : (prim < 0 ? kClassMiss : int(__ldg(s.primClass + prim) & ~kTransparentBit));
+            const int gm = kBatch ? s.guideMode : guideMode;
+            if (c == kClassDiffuse && (gm & 3) && ((mt.w >> 2) & 7) < kGuideVertices) c = kClassGuided;
             rank = atomicAdd(&hist[c], 1);
         }
         __syncthreads();
@@ -1539,7 +1543,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     GuideMix gm;
                     // The guide is trained on, and applied at, the first kGuideVertices diffuse
                     // vertices of each path.
-                    const bool diffuseVertex = c == kClassDiffuse && m.type == prgpu::MatDiffuse;
+                    const bool diffuseVertex = c == kClassGuided && m.type == prgpu::MatDiffuse;
                     const bool inRange = diffuseVertex && gcount < kGuideVertices;
                     const bool guided = (gmode & 1) && inRange;
                     const int recIndex = gcount;

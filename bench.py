@@ -269,46 +269,60 @@ def batch_bench(args, device: int, cpu: bool):
 def guided_vs_plain_bench(args):
     """Equal-time relMSE, guided vs plain, on the guided-vs-plain scene (the box with its light
     behind an occluder with a 0.1-wide slit and 12 subsurface BK7 spheres; 4 hero wavelengths,
-    depth 32) at a reduced size (--gvp-res, default 128^2). The reference image is a 65,536-spp
-    plain render on the GPU. Plain renders --gvp-spp samples per pixel; the guided form starts from
-    fresh weights and trains online (one Adam step per 2^16 recorded samples) while it renders, for
-    as many samples per pixel as fit the plain render's device time (its own per-sample time,
-    training included, measured on a short run first). relMSE is the form of the reference's
-    tests/test_quality.cpp:241-248: mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2).
-    ratio = relMSE plain / relMSE guided (> 1: the guide wins at equal time)."""
+    depth 32) at a reduced size (--gvp-res, default 128^2), and on the box lit only indirectly (its
+    light facing the ceiling). The reference image is a --gvp-ref-spp plain render on the GPU.
+    Plain renders --gvp-spp samples per pixel; its device time is the budget. The guided form
+    starts from fresh weights, samples with the guide and trains it online (one Adam step per 2^16
+    recorded samples) for the first --gvp-train-frac of the budget, then samples with the trained
+    guide for the rest; every sample, those of the training phase included, is in its image.
+    Per-sample device times of both phases come from short runs beforehand (not in the images).
+    relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
+    channels of (x - ref)^2 / (ref^2 + 1e-2). ratio = relMSE plain / relMSE guided (> 1: the guide
+    wins at equal time)."""
     from prgpu import guide, hostscene, render, scenes
 
-    R, depth = args.gvp_res, 32
-    desc = hostscene.build_box_scene(scenes.slit_scene(seed=0, width=R, height=R, max_depth=depth)).desc()
-    t0 = time.perf_counter()
-    ref_spp = args.gvp_ref_spp
-    ref, rst = render.render_ex(desc, R, R, ref_spp, seed=777, max_depth=depth, stats=True)
-    ref /= ref_spp
+    R = args.gvp_res
+    out = {"metric": "equal-time relMSE ratio (plain / guided)", "unit": "x",
+           "guide_settings": guide.get_options()}
+    for name, s in (("slit_sss", scenes.slit_scene(seed=0, width=R, height=R, max_depth=32)),
+                    ("indirect", scenes.indirect_scene(seed=0, width=R, height=R, max_depth=32, subdiv=3))):
+        depth = s.max_depth
+        desc = hostscene.build_box_scene(s).desc()
+        t0 = time.perf_counter()
+        ref_spp = args.gvp_ref_spp
+        ref = render.render_ex(desc, R, R, ref_spp, seed=777, max_depth=depth) / ref_spp
+        ref_s = time.perf_counter() - t0
 
-    def relmse(img):
-        return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+        def relmse(img):
+            return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
-    spp = args.gvp_spp
-    plain, pst = render.render_ex(desc, R, R, spp, seed=11, max_depth=depth, stats=True)
-    plain_ms = pst.deviceMs
-    guide.set_options()
-    train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET, wavefront_paths=65536)
-    _, gst = render.render_ex(desc, R, R, 16, seed=12, max_depth=depth, ext=train, stats=True)
-    per_spp = gst.deviceMs / 16
-    gspp = max(1, int(plain_ms / per_spp))
-    train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET
-    guided, gst2 = render.render_ex(desc, R, R, gspp, seed=13, max_depth=depth, ext=train, stats=True)
-    ep, eg = relmse(plain / spp), relmse(guided / gspp)
-    # Equal sample count, for reference: the guide after that training, sampling only.
-    use = render.make_ext(guide=render.GUIDE_SAMPLE)
-    g_eq, _ = render.render_ex(desc, R, R, spp, seed=14, max_depth=depth, ext=use, stats=True)
-    return {"workload": f"guided vs plain: slit box with 12 subsurface BK7 spheres, {R}x{R}, depth {depth}, "
-                        f"4 hero wavelengths, reference {ref_spp} spp plain (GPU)",
-            "metric": "equal-time relMSE ratio (plain / guided)", "ratio": ep / eg, "unit": "x",
-            "plain": {"spp": spp, "device_ms": plain_ms, "relmse": ep},
-            "guided": {"spp": gspp, "device_ms": gst2.deviceMs, "relmse": eg, "training": "online, fresh weights"},
-            "equal_spp_ratio": ep / relmse(g_eq / spp), "reference_s": time.perf_counter() - t0,
-            "guide_settings": "defaults (selection cap 0.9, 8 lobes, 12 bands, lr 1e-3)"}
+        spp = args.gvp_spp
+        plain, pst = render.render_ex(desc, R, R, spp, seed=11, max_depth=depth, stats=True)
+        budget = pst.deviceMs
+        train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET,
+                                wavefront_paths=65536)
+        use = render.make_ext(guide=render.GUIDE_SAMPLE)
+        _, a = render.render_ex(desc, R, R, 16, seed=90, max_depth=depth, ext=train, stats=True)
+        _, b = render.render_ex(desc, R, R, 16, seed=91, max_depth=depth, ext=use, stats=True)
+        t_train, t_use = a.deviceMs / 16, b.deviceMs / 16
+        n_train = max(4, int(args.gvp_train_frac * budget / t_train))
+        n_use = max(0, int((budget - n_train * t_train) / t_use))
+        film, st1 = render.render_ex(desc, R, R, n_train, seed=13, max_depth=depth, ext=train, stats=True)
+        ms = st1.deviceMs
+        if n_use:
+            _, st2 = render.render_ex(desc, R, R, n_use, first_sample=n_train, seed=13, max_depth=depth, ext=use,
+                                      out=film, stats=True)
+            ms += st2.deviceMs
+        ep, eg = relmse(plain / spp), relmse(film / (n_train + n_use))
+        # Equal sample count, for reference: the trained guide sampling only.
+        g_eq, _ = render.render_ex(desc, R, R, spp, seed=14, max_depth=depth, ext=use, stats=True)
+        out[name] = {"workload": f"{R}x{R}, depth {depth}, 4 hero wavelengths, reference {ref_spp} spp plain "
+                                 f"({ref_s:.1f} s)",
+                     "ratio": ep / eg, "plain": {"spp": spp, "device_ms": budget, "relmse": ep},
+                     "guided": {"spp_training": n_train, "spp_trained": n_use, "device_ms": ms, "relmse": eg},
+                     "equal_spp_ratio": ep / relmse(g_eq / spp)}
+    out["ratio"] = out["slit_sss"]["ratio"]
+    return out
 
 
 def run_reference_arm(args, rank: int, world: int):
@@ -492,8 +506,10 @@ def main():
     ap.add_argument("--guided-only", action="store_true",
                     help="run only the guided-vs-plain comparison and print its JSON object (profiling captures)")
     ap.add_argument("--gvp-res", type=int, default=128, help="guided-vs-plain image side (1024 = the full C3 size)")
-    ap.add_argument("--gvp-spp", type=int, default=256, help="plain samples per pixel of the equal-time comparison")
+    ap.add_argument("--gvp-spp", type=int, default=1024, help="plain samples per pixel of the equal-time comparison")
     ap.add_argument("--gvp-ref-spp", type=int, default=65536, help="samples per pixel of the plain reference image")
+    ap.add_argument("--gvp-train-frac", type=float, default=0.3,
+                    help="share of the guided run's time budget spent training online")
     ap.add_argument("--large-scene", action="store_true",
                     help="also run the large outdoor scene (33.5M-triangle terrain, cloud grid, 4K film; opt-in: "
                          "about a minute of host scene build)")

@@ -35,22 +35,28 @@ def _cpu_seeds(rs, spp, seeds, depth):
 
 @pytest.mark.parametrize("mode", ["fixed", "online"])
 def test_guided_render_is_unbiased(gpu, oracle, mode):
-    """Box scene at 32 x 32: 16 guided renders of 256 spp against 16 reference renders; |z| < 4 on
-    >= 99.5% of values, mean luminance within 1.5%. 'online' trains the network during the render
-    (4,096-path wavefronts: 64 Adam steps per render)."""
+    """Box scene at 32 x 32 at the plain path tracer's gate bar: 16 guided renders of 1,024 spp
+    against 16 reference renders of 1,024 spp; |z| < 4 on >= 99.9% of values, mean luminance within
+    0.5% (its statistical error here is about 0.15%). 'fixed': random, badly placed lobes selected
+    often; 'online': the network trains during the render (4,096-path wavefronts). Both exercise
+    the one-sample MIS with the BSDF, NEE's MIS against the mixture pdf, and the Russian roulette
+    that tests the BSDF-sampling throughput at guided vertices."""
     w = h = 32
+    spp = 1024
     rs = oracle.RefScene(ru.scene_file("guided_box", seed=0, width=w, height=h))
     desc = rs.export()
     guide.set_weights(_weights(7))
     flags = render.GUIDE_SAMPLE | (render.GUIDE_TRAIN if mode == "online" else 0)
     ext = render.make_ext(guide=flags, wavefront_paths=4096 if mode == "online" else 0)
-    g = np.stack([render.render_ex(desc, w, h, 256, seed=1000 + k, max_depth=8, ext=ext) / 256 for k in range(16)])
-    c = _cpu_seeds(rs, 256, 16, 8)
+    g = np.stack([render.render_ex(desc, w, h, spp, seed=1000 + k, max_depth=8, ext=ext) / spp for k in range(16)])
+    oracle.set_threads(0)
+    c = _cpu_seeds(rs, spp, 16, 8)
     z = ru.z_scores(g, c)
     frac = np.mean(np.abs(z) < 4)
     yg, yc = g[..., 1].mean(), c[..., 1].mean()
-    assert frac >= 0.995, f"only {frac:.4f} of values within |z| < 4"
-    assert abs(yg / yc - 1) < 0.015, f"mean Y guided {yg} reference {yc}"
+    print(f"guided ({mode}) vs reference: frac {frac:.5f}, mean Y {yg:.6f} vs {yc:.6f} ({yg / yc - 1:+.3%})")
+    assert frac >= 0.999, f"only {frac:.5f} of values within |z| < 4"
+    assert abs(yg / yc - 1) < 0.005, f"mean Y guided {yg} reference {yc}"
     if mode == "online":
         assert not np.array_equal(guide.get_weights(), _weights(7))
 
