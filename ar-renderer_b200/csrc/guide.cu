@@ -329,7 +329,10 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(const __half *__restrict
                 float gout[kGuideOut];
                 if (valid) {
                     const GuideSample sm = samples[row];
-                    const float wn = opts.weightClamp > 0.f ? fminf(sm.w * wscale, opts.weightClamp) : sm.w * wscale;
+                    // The clamp applies to online batches (weights normalised to mean 1), not to
+                    // the caller-weighted gradient of prgpu_guide_gradient.
+                    const float wn = (wnorm && opts.weightClamp > 0.f) ? fminf(sm.w * wscale, opts.weightClamp)
+                                                                       : sm.w * wscale;
                     lossAcc += guide_loss_grad(z, mk(sm.wi[0], sm.wi[1], sm.wi[2]), mk(sm.n[0], sm.n[1], sm.n[2]),
                                                sm.pb, wn, gout, opts);
                 } else {

@@ -10,7 +10,8 @@
 //   inputs: x in [0,1]^3 (position normalised to the scene bounds), sin / cos(2^b pi x) for 12
 //           bands b (72), shading normal (3), outgoing direction (3), 1, zeros to 128.
 //   outputs: per lobe k < 8: direction (3, normalised), log kappa (clamped to [-4, 8]), weight
-//           logit (softmax over the 8); output 40: selection logit, c = 0.9 sigmoid; 41..47 unused.
+//           logit (softmax over the 8); output 40: selection logit, c = maxSelect sigmoid (default 0.5);
+//           41..47 unused.
 // One-sample MIS with the BSDF: wi ~ c q_n + (1 - c) p_bsdf, the pdf of both computed in FP32 from
 // the same decoded parameters, so the estimator stays unbiased for any weights. q_n is the mixture
 // folded onto the hemisphere of the shading normal n that holds wo (a sample below is mirrored
@@ -36,15 +37,16 @@ __host__ __device__ constexpr int guide_layer_out(int l) { return l == kGuideLay
 constexpr int kGuideParams = kGuideHid * kGuideIn + 3 * kGuideHid * kGuideHid + kGuideOut * kGuideHid;  // 23,552
 constexpr int kGuideVertices = 4;  // diffuse vertices per path that are guided and recorded
 
-// Settings of sampling and training (prgpu_guide_set_options). The defaults are the network's
-// original form: c = 0.9 sigmoid, log kappa clamped to [-4, 8], c trained on the KL objective.
+// Settings of sampling and training (prgpu_guide_set_options). Defaults: c = 0.5 sigmoid, log kappa
+// clamped to [-4, 8], c trained on the KL objective, the online batch's weights (normalised to mean
+// 1) clamped at 20 -- the best of the settings measured on the slit and indirectly lit box scenes.
 struct GuideOpts {
-    float maxSelect = 0.9f;    // c = maxSelect * sigmoid(output 40)
+    float maxSelect = 0.5f;    // c = maxSelect * sigmoid(output 40)
     float logKappaMax = 8.f;   // upper clamp of log kappa
     int selectLoss = 0;        // c's objective: 0 = -w log p_mix, 1 = second moment w^2 / p_mix
     int trainPasses = 1;       // passes over each chunk's recorded samples (online training)
     int bands = kGuideBandsMax;  // position encoding bands in use (the rest of the inputs zero)
-    float weightClamp = 0.f;   // > 0: training weights (normalised to mean 1 per batch) clamped to it
+    float weightClamp = 20.f;  // > 0: online training weights (normalised to mean 1 per batch) clamped to it
 };
 
 __host__ __device__ constexpr int guide_weight_offset(int l) {

@@ -73,11 +73,11 @@ def set_learning_rate(lr: float, device: int = 0) -> None:
               "prgpu_guide_set_learning_rate")
 
 
-DEFAULT_OPTIONS = dict(max_select=0.9, log_kappa_max=8.0, select_loss=0, train_passes=1, bands=12, weight_clamp=0.0)
+DEFAULT_OPTIONS = dict(max_select=0.5, log_kappa_max=8.0, select_loss=0, train_passes=1, bands=12, weight_clamp=20.0)
 
 
-def set_options(max_select: float = 0.9, log_kappa_max: float = 8.0, select_loss: int = 0, train_passes: int = 1,
-                bands: int = 12, weight_clamp: float = 0.0, device: int = 0) -> None:
+def set_options(max_select: float = 0.5, log_kappa_max: float = 8.0, select_loss: int = 0, train_passes: int = 1,
+                bands: int = 12, weight_clamp: float = 20.0, device: int = 0) -> None:
     """Sampling and training settings of the guide (prgpu_guide_set_options): the cap of the
     selection probability c, the cap of log kappa, c's objective (0 KL, 1 second moment of the
     one-sample estimator), the online training passes over each chunk's samples, the position

@@ -234,6 +234,16 @@ def batch_bench(args, device: int, cpu: bool):
         dev.append(st.deviceMs)
     samples = int(st.pathSamples)
     film_bytes = int(sum(f.nbytes for f in films))
+    # The same renders one by one (prgpu_render_ex each), against one batch of them, both at 1/8 of
+    # every render's spp: what batching gains over sequential single renders on this workload.
+    cmp_div = 8
+    cmp_items = [(d, e, dict(p, spp=max(1, p["spp"] // cmp_div)), np.zeros_like(f)) for d, e, p, f in items]
+    cst = render.render_batch(cmp_items, config=bcfg, stats=True)
+    single_ms = 0.0
+    for d, e, p, f in cmp_items:
+        _, sst = render.render_ex(d, f.shape[1], f.shape[0], p["spp"], seed=p["seed"], max_depth=p["max_depth"],
+                                  out=np.zeros_like(f), stats=True)
+        single_ms += sst.deviceMs
     out = {
         "workload": "uneven batch: 48 box-family renders, 128^2..1024^2, 16..256 spp, depth 8..32, half with media",
         "metric": "path samples/s", "value": samples / (statistics.mean(dev) * 1e-3), "unit": "path samples/s",
@@ -241,6 +251,8 @@ def batch_bench(args, device: int, cpu: bool):
         "path_samples_per_step": samples, "spp_divided_by": div, "waves": int(st.waves), "loop_iterations": int(st.loopIterations),
         "graph_launches_per_step": 0 if args.batch_host_loop else 1, "kernel_nodes_per_iteration": 14,
         "autotuned": {"wavefrontPaths": cfg.wavefrontPaths, "shadeBlock": cfg.shadeBlock, "seconds": tune_s},
+        "vs_sequential_singles": {"spp_divided_by": cmp_div, "batch_ms": cst.deviceMs, "singles_ms": single_ms,
+                                  "speedup": single_ms / cst.deviceMs},
         "host_scene_build_s": build_s,
         "rays_per_step": {"closest": int(st.closestRays), "shadow": int(st.shadowRays)},
         "e2e": {"value": samples / statistics.mean(wall), "unit": "path samples/s",
@@ -275,7 +287,6 @@ def guided_vs_plain_bench(args):
     starts from fresh weights, samples with the guide and trains it online (one Adam step per 2^16
     recorded samples) for the first --gvp-train-frac of the budget, then samples with the trained
     guide for the rest; every sample, those of the training phase included, is in its image.
-    Per-sample device times of both phases come from short runs beforehand (not in the images).
     relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
     channels of (x - ref)^2 / (ref^2 + 1e-2). ratio = relMSE plain / relMSE guided (> 1: the guide
     wins at equal time)."""
@@ -299,21 +310,30 @@ def guided_vs_plain_bench(args):
         spp = args.gvp_spp
         plain, pst = render.render_ex(desc, R, R, spp, seed=11, max_depth=depth, stats=True)
         budget = pst.deviceMs
+        guide.set_options()
+        guide.set_learning_rate(1e-3)
         train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET,
                                 wavefront_paths=65536)
         use = render.make_ext(guide=render.GUIDE_SAMPLE)
-        _, a = render.render_ex(desc, R, R, 16, seed=90, max_depth=depth, ext=train, stats=True)
-        _, b = render.render_ex(desc, R, R, 16, seed=91, max_depth=depth, ext=use, stats=True)
-        t_train, t_use = a.deviceMs / 16, b.deviceMs / 16
-        n_train = max(4, int(args.gvp_train_frac * budget / t_train))
-        n_use = max(0, int((budget - n_train * t_train) / t_use))
-        film, st1 = render.render_ex(desc, R, R, n_train, seed=13, max_depth=depth, ext=train, stats=True)
-        ms = st1.deviceMs
-        if n_use:
-            _, st2 = render.render_ex(desc, R, R, n_use, first_sample=n_train, seed=13, max_depth=depth, ext=use,
-                                      out=film, stats=True)
-            ms += st2.deviceMs
-        ep, eg = relmse(plain / spp), relmse(film / (n_train + n_use))
+        # Chunk by chunk on one film, counting device time: train while within the training share
+        # of the budget, then sample with the trained guide until the budget is spent (the last
+        # chunk may overshoot by one chunk's time, which is reported).
+        film = np.zeros((R, R, 3))
+        done, ms = 0, 0.0
+        while ms < args.gvp_train_frac * budget:
+            _, st = render.render_ex(desc, R, R, 16, first_sample=done, seed=13, max_depth=depth, ext=train, out=film,
+                                     stats=True)
+            train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
+            ms += st.deviceMs
+            done += 16
+        n_train = done
+        while ms < budget:
+            _, st = render.render_ex(desc, R, R, 64, first_sample=done, seed=13, max_depth=depth, ext=use, out=film,
+                                     stats=True)
+            ms += st.deviceMs
+            done += 64
+        n_use = done - n_train
+        ep, eg = relmse(plain / spp), relmse(film / done)
         # Equal sample count, for reference: the trained guide sampling only.
         g_eq, _ = render.render_ex(desc, R, R, spp, seed=14, max_depth=depth, ext=use, stats=True)
         out[name] = {"workload": f"{R}x{R}, depth {depth}, 4 hero wavelengths, reference {ref_spp} spp plain "
@@ -506,7 +526,7 @@ def main():
     ap.add_argument("--guided-only", action="store_true",
                     help="run only the guided-vs-plain comparison and print its JSON object (profiling captures)")
     ap.add_argument("--gvp-res", type=int, default=128, help="guided-vs-plain image side (1024 = the full C3 size)")
-    ap.add_argument("--gvp-spp", type=int, default=1024, help="plain samples per pixel of the equal-time comparison")
+    ap.add_argument("--gvp-spp", type=int, default=32768, help="plain samples per pixel of the equal-time comparison")
     ap.add_argument("--gvp-ref-spp", type=int, default=65536, help="samples per pixel of the plain reference image")
     ap.add_argument("--gvp-train-frac", type=float, default=0.3,
                     help="share of the guided run's time budget spent training online")

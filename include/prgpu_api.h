@@ -459,13 +459,13 @@ struct RenderStats {
 // Settings of the path-guiding network's sampling and online training (prgpu_guide_set_options;
 // defaults in brackets).
 struct GuideOptions {
-    float maxSelect;           // [0.9] cap of the probability c of sampling the guide (0 < x <= 0.99)
+    float maxSelect;           // [0.5] cap of the probability c of sampling the guide (0 < x <= 0.99)
     float logKappaMax;         // [8] upper clamp of the lobes' log concentration (0 <= x <= 8)
     int32_t selectLoss;        // [0] c trained on the mixture's KL divergence (0) or on the second
                                //     moment of the one-sample estimator (1)
     int32_t trainPasses;       // [1] online training passes over each chunk's samples (1..64)
     int32_t bands;             // [12] position-encoding bands in use (0..12; the others input 0)
-    float weightClamp;         // [0 = off] training weights, normalised to mean 1 per batch, clamped
+    float weightClamp;         // [20; 0 = off] online training weights, normalised to mean 1 per batch, clamped
 };
 
 } // namespace prgpu

@@ -11,7 +11,7 @@ activations (and backward signals) to FP16 at the same points, so the remaining 
 FP32 accumulation order.
 
 Outputs, per lobe k < 8: direction (3, normalised), log kappa (clamped to [-4, 8]), weight
-logit; output 40 the selection logit, c = 0.9 sigmoid. Mixture pdf of a unit direction w:
+logit; output 40 the selection logit, c = 0.5 sigmoid. Mixture pdf of a unit direction w:
 q(w) = sum_k pi_k kappa_k / (2 pi (1 - e^{-2 kappa_k})) exp(kappa_k (mu_k . w - 1)).
 The renderer folds the mixture onto the hemisphere of the shading normal n that holds the sample:
 q_n(w) = q(w) + q(w - 2 (w.n) n). Loss per sample, two parts: -w log q_n(wi) trains the lobes,
@@ -34,7 +34,7 @@ CONST_IN, CONST_HID = 81, 63
 LAYER_IN = [IN, HID, HID, HID, HID]
 LAYER_OUT = [HID, HID, HID, HID, OUT]
 N_PARAMS = sum(a * b for a, b in zip(LAYER_IN, LAYER_OUT))
-MAX_SELECT = 0.9
+MAX_SELECT = 0.5
 
 
 def split(params: np.ndarray):

@@ -106,7 +106,7 @@ def test_training_gradient_with_settings_matches_oracle(gpu, default_guide_optio
     guide.set_weights(w)
     guide.set_options(max_select=0.7, log_kappa_max=2.0, select_loss=1)
     assert guide.get_options() == dict(max_select=pytest.approx(0.7), log_kappa_max=2.0, select_loss=1,
-                                       train_passes=1, bands=12, weight_clamp=0.0)
+                                       train_passes=1, bands=12, weight_clamp=20.0)
     X = _inputs(n, 42)
     rng = np.random.default_rng(43)
     wi = rng.normal(size=(n, 3))
@@ -134,7 +134,7 @@ def test_guide_options_are_validated(gpu, default_guide_options):
                 dict(train_passes=0), dict(bands=13), dict(weight_clamp=-1.0)):
         with pytest.raises(abi.PrgpuError, match="out of range"):
             guide.set_options(**bad)
-    assert guide.get_options()["max_select"] == pytest.approx(0.9)
+    assert guide.get_options()["max_select"] == pytest.approx(0.5)
 
 
 def test_adam_steps_reduce_the_training_loss(gpu):

@@ -61,27 +61,53 @@ def test_guided_render_is_unbiased(gpu, oracle, mode):
         assert not np.array_equal(guide.get_weights(), _weights(7))
 
 
-def test_trained_guide_on_slit_scene_reports_its_gain(gpu):
-    """Slit scene (light only through a 0.1-wide slit, 12 subsurface spheres), 64 x 64, depth 16:
-    train the guide online over 16,384 spp (lr 1e-2), then compare 64-spp renders with and without
-    it against a 16,384-spp plain render, relMSE in the form of tests/test_quality.cpp:241-248.
-    The measured gain is printed; at this training budget the guided estimate is not yet better
-    than BSDF sampling (ratio about 0.9-0.96), so the test only bounds the loss (within 25%)."""
-    w = h = 64
-    hs = hostscene.build_box_scene(scenes.slit_scene(seed=0, width=w, height=h, subdiv=2))
-    desc = hs.desc()
-    ref = render.render_ex(desc, w, h, 16384, seed=77, max_depth=16) / 16384
-    guide.set_learning_rate(1e-2)
-    train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET, wavefront_paths=65536)
-    render.render_ex(desc, w, h, 16384, seed=5, max_depth=16, ext=train)
+def _gain(desc, w, depth, train_spp, seeds=12, spp=64):
+    """(relMSE plain, relMSE guided, device ms per render plain, guided) after training the guide
+    online from fresh weights over train_spp samples per pixel (65,536-path wavefronts, Adam lr
+    1e-3 as the guided-vs-plain configuration specifies); relMSE against an 8,192-spp plain render in
+    the form of tests/test_quality.cpp:241-248, averaged over `seeds` renders of `spp`."""
+    ref = render.render_ex(desc, w, w, 8192, seed=77, max_depth=depth) / 8192
+    guide.set_options()
     guide.set_learning_rate(1e-3)
+    train = render.make_ext(guide=render.GUIDE_SAMPLE | render.GUIDE_TRAIN | render.GUIDE_RESET, wavefront_paths=65536)
+    render.render_ex(desc, w, w, train_spp, seed=5, max_depth=depth, ext=train)
     use = render.make_ext(guide=render.GUIDE_SAMPLE)
 
-    def relmse(img):
-        return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+    def run(ext):
+        errs, ms = [], []
+        for k in range(seeds):
+            img, st = render.render_ex(desc, w, w, spp, seed=900 + k, max_depth=depth, ext=ext, stats=True)
+            errs.append(float(np.mean((img / spp - ref) ** 2 / (ref ** 2 + 1e-2))))
+            ms.append(st.deviceMs)
+        return float(np.mean(errs)), float(np.median(ms))
 
-    plain = np.mean([relmse(render.render_ex(desc, w, h, 64, seed=900 + k, max_depth=16) / 64) for k in range(8)])
-    guided = np.mean([relmse(render.render_ex(desc, w, h, 64, seed=900 + k, max_depth=16, ext=use) / 64)
-                      for k in range(8)])
-    print(f"slit scene relMSE at 64 spp: plain {plain:.4e}, guided {guided:.4e} (gain {plain / guided:.2f}x)")
-    assert guided < 1.25 * plain
+    (ep, tp), (eg, tg) = run(None), run(use)
+    return ep, eg, tp, tg
+
+
+def test_trained_guide_gains_on_the_indirectly_lit_box(gpu):
+    """The box-and-spheres scene lit only indirectly (its light faces the ceiling: all light reaches
+    the room by way of the bright patch above it), 128 x 128, depth 16: after 4,096 spp of online
+    training the guided renders' relMSE is at least 2x lower than BSDF sampling's at equal sample
+    count and at least 1.5x lower at equal device time of the renders (measured: 3.3x and 2.3x)."""
+    w, depth = 128, 16
+    desc = hostscene.build_box_scene(scenes.indirect_scene(seed=0, width=w, height=w, max_depth=depth, subdiv=2)).desc()
+    ep, eg, tp, tg = _gain(desc, w, depth, 4096)
+    print(f"indirect box: relMSE plain {ep:.4e} ({tp:.2f} ms), guided {eg:.4e} ({tg:.2f} ms): "
+          f"{ep / eg:.2f}x at equal spp, {ep * tp / (eg * tg):.2f}x at equal time")
+    assert ep / eg >= 2.0
+    assert ep * tp / (eg * tg) >= 1.5
+
+
+def test_trained_guide_on_slit_scene_reports_its_gain(gpu):
+    """The guided-vs-plain scene (light only through a 0.1-wide slit, 12 subsurface BK7 spheres),
+    128 x 128, depth 16: the trained guide lowers relMSE at equal sample count (measured 1.15x;
+    asserted > 1.05x). Most of this image's error is in the subsurface spheres' pixels (about 60 %,
+    which guiding at diffuse vertices does not reach), so at equal time the guided form's extra
+    cost per sample (inference per bounce, about 45 % here) outweighs the gain: the ratio is printed."""
+    w, depth = 128, 16
+    desc = hostscene.build_box_scene(scenes.slit_scene(seed=0, width=w, height=w, subdiv=2, max_depth=depth)).desc()
+    ep, eg, tp, tg = _gain(desc, w, depth, 4096)
+    print(f"slit scene: relMSE plain {ep:.4e} ({tp:.2f} ms), guided {eg:.4e} ({tg:.2f} ms): "
+          f"{ep / eg:.2f}x at equal spp, {ep * tp / (eg * tg):.2f}x at equal time")
+    assert ep / eg > 1.05
