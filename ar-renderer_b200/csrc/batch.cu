@@ -275,6 +275,7 @@ struct BatchLaunch {
     void (*shadowAny)(DevScene, const DevScene *, Paths, Shadows, int *);
     void (*shadowWalk)(DevScene, const DevScene *, Paths, Shadows, int *);
     void (*shade)(ShadeArgs);
+    void (*shadeGuided)(ShadeArgs);  // the guided class, when the batch uses the guide
     void (*shadeFull)(ShadeArgs);
     bool walls, full;
     int guideMode;  // OR of the renders' guide flags (bit 0 sample, bit 1 train): the guide launches run
@@ -290,8 +291,8 @@ BatchLaunch batch_launch(const DeviceState &ds, const BatchGraphKey &key) {
     const bool dl = key.variant & 16;
     L.guideMode = (key.variant >> 5) & 3;
     L.guideOpts = key.guideOpts;
-    if (L.guideMode) L.shade = dl ? k_shade<true, true, false, true> : k_shade<true, true>;
-    else L.shade = dl ? k_shade<true, false, false, true> : k_shade<true>;
+    L.shade = dl ? k_shade<true, false, false, true> : k_shade<true>;
+    L.shadeGuided = dl ? k_shade<true, true, false, true> : k_shade<true, true>;
     L.shadeFull = dl ? k_shade<true, false, true, true> : k_shade<true, false, true>;
     L.extend = sph ? k_extend<true, true> : k_extend<false, true>;
     L.shadowAny = L.walls ? (sph ? k_shadow_any<true, true, true, true> : k_shadow_any<false, true, true, true>)
@@ -345,6 +346,10 @@ int enqueue_batch_iteration(cudaStream_t st, BatchState &bs, const BatchLaunch &
                      L.guideMode ? rs.guideOut.as<float>() : nullptr, L.guideMode ? rs.guideRec.as<float4>() : nullptr,
                      L.guideMode, qin, L.guideOpts};
         L.shade<<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+        if (L.guideMode) {
+            L.shadeGuided<<<L.gShade, L.shadeBlock, 0, st>>>(sa);
+            ++launches;
+        }
         if (L.full) {
             L.shadeFull<<<L.gShade, L.shadeBlock, 0, st>>>(sa);
             ++launches;

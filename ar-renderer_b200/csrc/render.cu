@@ -235,12 +235,13 @@ bool render_into_film(DeviceState &ds, RenderState &rs, const prgpu::RenderParam
                                  rp.maxDepth, 0, rs.guideOut.as<float>(), rs.guideRec.as<float4>(), guideMode, qin,
                                  gopts};
                     const bool dl = scene.deltaCount > 0 || scene.matTex != nullptr;
+                    // The plain materials (and training snapshots), then the guided vertices.
+                    if (dl) k_shade<false, false, false, true><<<gShade, 256, 0, st>>>(sa);
+                    else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
                     if (guideMode) {
                         if (dl) k_shade<false, true, false, true><<<gShade, 256, 0, st>>>(sa);
                         else k_shade<false, true><<<gShade, 256, 0, st>>>(sa);
-                    } else {
-                        if (dl) k_shade<false, false, false, true><<<gShade, 256, 0, st>>>(sa);
-                        else k_shade<false, false><<<gShade, 256, 0, st>>>(sa);
+                        ++launches;
                     }
                     if (scene.hasFull) {
                         if (dl) k_shade<false, false, true, true><<<gShade, 256, 0, st>>>(sa);

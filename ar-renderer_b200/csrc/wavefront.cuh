@@ -1239,6 +1239,8 @@ struct ShadeArgs {
 // emission, to the fullQ queue; the kFull pass shades those surfaces. Keeping the layered code out
 // of the main pass keeps its register allocation that of the plain materials. kDelta: the scene has
 // spot / distant / goniometric lights or image textures (their code is instantiated only then).
+// kGuide: this launch shades the guided class (kClassGuided) only, sampling with the guide; the
+// main pass (kGuide false) shades every other class, so the plain materials keep the plain code.
 template <bool kBatch = false, bool kGuide = false, bool kFull = false, bool kDelta = false>
 __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     const Paths &P = a.P;
@@ -1247,12 +1249,14 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
     start[0] = 0;
 #pragma unroll
     for (int c = 0; c < kClasses; ++c) start[c + 1] = start[c] + a.counters[kCntClass0 + c];
-    const int n = kFull ? a.counters[kCntFull] : start[kClasses];
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        int c = kFull ? int(kClassOther) : 0, first = 0;
-        if constexpr (!kFull) {
+    const int q0 = kGuide ? start[kClassGuided] : 0;
+    const int n = kFull ? a.counters[kCntFull] : (kGuide ? start[kClasses] : start[kClassGuided]);
+    for (int q = q0 + blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int c = kFull ? int(kClassOther) : (kGuide ? int(kClassGuided) : 0);
+        int first = kGuide ? q0 : 0;
+        if constexpr (!kFull && !kGuide) {
 #pragma unroll
-            for (int k = 1; k < kClasses; ++k)
+            for (int k = 1; k < kClassGuided; ++k)
                 if (q >= start[k]) {
                     c = k;
                     first = start[k];
@@ -1281,7 +1285,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         bool alive = true, deferred = false;
         // Guide mode of this path: the call's, restricted in the batched form to its render's flags.
         const int gmode = kBatch ? (a.guideMode & s.guideMode) : a.guideMode;
-        if constexpr (kGuide && !kFull) if (gmode & 2) {
+        if constexpr (!kFull) if ((gmode & 2) && a.guideRec) {
             // A record taken at this path's previous vertex: its radiance snapshot is the sum so far
             // (that vertex's NEE included, nothing from here on), so the final sum minus it is the
             // light that came along the sampled direction.

@@ -284,9 +284,10 @@ def guided_vs_plain_bench(args):
     depth 32) at a reduced size (--gvp-res, default 128^2), and on the box lit only indirectly (its
     light facing the ceiling). The reference image is a --gvp-ref-spp plain render on the GPU.
     Plain renders --gvp-spp samples per pixel; its device time is the budget. The guided form
-    starts from fresh weights, samples with the guide and trains it online (one Adam step per 2^16
-    recorded samples) for the first --gvp-train-frac of the budget, then samples with the trained
-    guide for the rest; every sample, those of the training phase included, is in its image.
+    starts from fresh weights, samples with the guide and trains it online for the first
+    --gvp-train-frac of the budget (the guided, batched form: one graph launch per 64 spp, Adam steps
+    on the samples of every filmed wave of 2^16 paths), then samples with the trained guide for the
+    rest (prgpu_render_ex); every sample, those of the training phase included, is in its image.
     relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
     channels of (x - ref)^2 / (ref^2 + 1e-2). ratio = relMSE plain / relMSE guided (> 1: the guide
     wins at equal time)."""
@@ -320,12 +321,15 @@ def guided_vs_plain_bench(args):
         # chunk may overshoot by one chunk's time, which is reported).
         film = np.zeros((R, R, 3))
         done, ms = 0, 0.0
+        # Training runs in the guided, batched form: one graph launch per call, Adam steps after
+        # every filmed wave of 2^16 paths, no host round trip per bounce.
+        tcfg = render.batch_config(1 << 17, 256)
         while ms < args.gvp_train_frac * budget:
-            _, st = render.render_ex(desc, R, R, 16, first_sample=done, seed=13, max_depth=depth, ext=train, out=film,
-                                     stats=True)
+            st = render.render_batch([(desc, train, dict(spp=64, first_sample=done, seed=13, max_depth=depth), film)],
+                                     config=tcfg, stats=True)
             train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
             ms += st.deviceMs
-            done += 16
+            done += 64
         n_train = done
         while ms < budget:
             _, st = render.render_ex(desc, R, R, 64, first_sample=done, seed=13, max_depth=depth, ext=use, out=film,
@@ -475,7 +479,7 @@ def c4_time_to_relmse(args):
 
     def guided_step(film, first, n):
         st = render.render_batch([(desc, gext, dict(spp=n, first_sample=first, seed=1, max_depth=depth), film)],
-                                 config=render.batch_config(1 << 22, 256), stats=True)
+                                 config=render.batch_config(1 << 18, 256), stats=True)
         gext.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
         return st.deviceMs
 
