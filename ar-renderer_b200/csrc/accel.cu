@@ -10,18 +10,21 @@
 
 namespace prb {
 
-// Persistent warps: every lane that has no ray takes the next one from a global counter (one
-// atomic per warp and refill), then the lanes advance their traversals one node or leaf per
-// iteration. Incoherent rays end after very different numbers of steps; refilling keeps the
-// lanes of a warp busy instead of idling until the warp's longest ray ends.
+// Persistent warps: the lanes advance their traversals one node or leaf per iteration, and lanes
+// whose ray is done take the next rays from a global counter (one atomic per warp and refill).
+// Incoherent rays end after very different numbers of steps; refilling keeps the lanes of a warp
+// busy instead of idling until the warp's longest ray ends. A refill (ray load, reciprocal
+// direction, root-box test, and the finished rays' result stores) runs once kRefillLanes lanes of
+// the warp are idle, or none is busy.
+
 template <bool kAny, bool kWide>
-__global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ nodes,
-                                                       const LeafPrim *__restrict__ prims, RootInfo root,
-                                                       const float4 *__restrict__ rays, int64_t n,
-                                                       int32_t *__restrict__ primOut, float *__restrict__ tOut,
-                                                       float *__restrict__ b1Out, float *__restrict__ b2Out,
-                                                       int *__restrict__ status,
-                                                       unsigned long long *__restrict__ counter) {
+__global__ void __launch_bounds__(256, 4) k_trace_persist(const void *__restrict__ nodes,
+                                                          const LeafPrim *__restrict__ prims, RootInfo root,
+                                                          const float4 *__restrict__ rays, int64_t n,
+                                                          int32_t *__restrict__ primOut, float *__restrict__ tOut,
+                                                          float *__restrict__ b1Out, float *__restrict__ b2Out,
+                                                          int *__restrict__ status,
+                                                          unsigned long long *__restrict__ counter) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     int stackRef[kStackSize];
@@ -36,18 +39,33 @@ __global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ 
     s.sp = 0;
     s.tMax = 0.f;
     s.found = false;
+    s.hit.prim = -1;
     int64_t idx = 0;
-    bool active = false, exhausted = false, overflow = false;
+    // pending: this lane's last ray is finished and its result not yet stored.
+    bool active = false, exhausted = false, pending = false, overflow = false;
+    auto store = [&]() {
+        if (kAny) {
+            primOut[idx] = s.found ? 1 : 0;
+        } else {
+            primOut[idx] = s.found ? s.hit.prim : -1;
+            if (tOut) tOut[idx] = s.found ? s.hit.t : 0.f;
+            if (b1Out) b1Out[idx] = s.found ? s.hit.u : 0.f;
+            if (b2Out) b2Out[idx] = s.found ? s.hit.v : 0.f;
+        }
+    };
     while (true) {
-        unsigned need = __ballot_sync(full, !active && !exhausted);
-        if (need) {
+        const bool idle = !active && !exhausted;
+        const unsigned need = __ballot_sync(full, idle), busy = __ballot_sync(full, active);
+        if (need && (__popc(need) >= kRefillLanes || !busy)) {
             unsigned long long base = 0;
             if (lane == 0) base = atomicAdd(counter, (unsigned long long)__popc(need));
             base = __shfl_sync(full, base, 0);
-            if (!active && !exhausted) {
+            if (idle) {
+                if (pending) store();
                 idx = int64_t(base) + __popc(need & ((1u << lane) - 1u));
                 if (idx >= n) {
                     exhausted = true;
+                    pending = false;
                 } else {
                     float4 a = __ldcs(rays + 2 * idx), b = __ldcs(rays + 2 * idx + 1);
                     r = make_trace_ray(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z));
@@ -60,14 +78,8 @@ __global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ 
                              box_entry(r, root.box[0], root.box[1], root.box[2], root.box[3], root.box[4], root.box[5], &te) &&
                              te < s.tMax;
                     s.ref = root.ref;
-                    if (!active) {
-                        primOut[idx] = kAny ? 0 : -1;
-                        if (!kAny) {
-                            if (tOut) tOut[idx] = 0.f;
-                            if (b1Out) b1Out[idx] = 0.f;
-                            if (b2Out) b2Out[idx] = 0.f;
-                        }
-                    }
+                    // A ray that misses the root is done at once: a miss, stored at the next refill.
+                    pending = !active;
                 }
             }
         }
@@ -82,14 +94,7 @@ __global__ void __launch_bounds__(256) k_trace_persist(const void *__restrict__ 
         }
         if (done) {
             active = false;
-            if (kAny) {
-                primOut[idx] = s.found ? 1 : 0;
-            } else {
-                primOut[idx] = s.found ? s.hit.prim : -1;
-                if (tOut) tOut[idx] = s.found ? s.hit.t : 0.f;
-                if (b1Out) b1Out[idx] = s.found ? s.hit.u : 0.f;
-                if (b2Out) b2Out[idx] = s.found ? s.hit.v : 0.f;
-            }
+            pending = true;
         }
     }
     if (overflow) atomicOr(status, 1);

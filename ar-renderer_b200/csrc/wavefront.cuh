@@ -243,6 +243,18 @@ static __device__ Lobe make_lobe(const DevScene &s, const prgpu::Material &m, fl
     return l;
 }
 
+// make_lobe for a material known to be MatDiffuse (the guided shading class): the lobe kind is a
+// constant, so the code of the other kinds drops out of the kernels that use it.
+static __device__ __forceinline__ Lobe diffuse_lobe(const DevScene &s, const prgpu::Material &m, float u, float v,
+                                                    const Lambda &lam) {
+    Lobe l;
+    l.kind = kLobeDiffuse;
+    l.etaD = 1.f;
+    l.mf = Ggx{0.f, 0.f};
+    l.R = diffuse_albedo(s, m, u, v, lam);
+    return l;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Image textures (pr::ImageData::Lookup / ImageSpectrumTexture::Evaluate, texture.cpp:8-53) and the
 // albedo uplift through the RGB -> spectrum table (RGBToSpectrumTable, rgb2spec.cpp:278-305).
@@ -1150,12 +1162,14 @@ __global__ void __launch_bounds__(256) k_classify(DevScene s0, const DevScene *s
     }
 }
 
-// Closest hit for every queued path, by persistent warps whose finished lanes take the next
-// queue entry at once (see k_trace_persist in accel.cu): bounce rays are incoherent and end
-// after very different numbers of steps.
+// Closest hit for every queued path, by persistent warps whose idle lanes take the next queue
+// entries (see k_trace_persist in accel.cu): bounce rays are incoherent and end after very
+// different numbers of steps. A finished lane's hit is stored when it takes its next entry.
 template <bool kSpheres, bool kBatch = false>
-__global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *scenes, Paths P, int *counters,
-                                                const int *queue) {
+// 4 resident blocks (64 registers) for triangle scenes; the batched form would otherwise take 74
+// registers and 3 blocks. Scenes with spheres keep the double-precision sphere test unconstrained.
+__global__ void __launch_bounds__(256, kSpheres ? 1 : 4) k_extend(DevScene s0, const DevScene *scenes, Paths P,
+                                                                  int *counters, const int *queue) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n = counters[kCntActive];
@@ -1168,17 +1182,22 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
     st.sp = 0;
     st.tMax = kInf;
     st.found = false;
+    st.hit.prim = -1;
     int j = 0;
     const QNode *nodes = s0.qnodes;
     const LeafPrim *leaves = s0.leaves;
-    bool active = false, exhausted = n == 0, overflow = false;
+    bool active = false, exhausted = n == 0, pending = false, overflow = false;
     while (!__all_sync(full, exhausted)) {
-        unsigned need = __ballot_sync(full, !active && !exhausted);
-        if (need) {
+        const bool idle = !active && !exhausted;
+        const unsigned need = __ballot_sync(full, idle), busy = __ballot_sync(full, active);
+        if (need && (__popc(need) >= kRefillLanes || !busy)) {
             int base = 0;
             if (lane == 0) base = atomicAdd(counters + kCntExtendWork, __popc(need));
             base = __shfl_sync(full, base, 0);
-            if (!active && !exhausted) {
+            if (idle) {
+                if (pending)
+                    P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
+                pending = false;
                 int q = base + __popc(need & ((1u << lane) - 1u));
                 if (q >= n) {
                     exhausted = true;
@@ -1192,20 +1211,21 @@ __global__ void __launch_bounds__(256) k_extend(DevScene s0, const DevScene *sce
                     st.tMax = kInf;
                     st.sp = 0;
                     st.found = false;
-                    st.hit.prim = -1;
+                    st.hit = Hit{0.f, 0.f, 0.f, -1};
                     float te;
                     active = !s.root.empty &&
                              box_entry(r, s.root.box[0], s.root.box[1], s.root.box[2], s.root.box[3], s.root.box[4],
                                        s.root.box[5], &te) &&
                              te < kInf;
                     st.ref = s.root.ref;
-                    if (!active) P.hit[j] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+                    // A ray that misses the root: a miss (t, u, v 0), stored at the next refill.
+                    pending = !active;
                 }
             }
         }
         if (active && traverse4_step_st<false, kSpheres>(nodes, leaves, r, st, hs, &overflow)) {
             active = false;
-            P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
+            pending = true;
         }
     }
     if (overflow) atomicOr(counters + kCntStatus, kStatusStack);
@@ -1389,7 +1409,9 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
         // Participating medium along the segment: hero-driven free flight in homogeneous media
         // (medium.cpp:71-103, with the rPath pdf ratios of path-level spectral MIS), spectral
         // tracking in grid media (medium.cpp:232-285, wavelength-neutral: rPath unchanged).
-        if (!kFull && !handled && medium >= 0) {
+        // The guided class holds surface hits outside media on diffuse materials only (k_classify),
+        // so its launch (kGuide) compiles neither the medium, the escape nor the non-diffuse code.
+        if (!kFull && !kGuide && !handled && medium >= 0) {
             float tMax = found ? hit.x : kInf;
             int event = 0;  // 0: the segment is crossed, 1: real scattering at t, 2: the path ends
             float t = tMax, g = 0.f;
@@ -1460,7 +1482,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 }
             }
         }
-        if (!kFull && !handled && !found) {
+        if (!kFull && !kGuide && !handled && !found) {
             // Escaped: emission of every infinite light with MIS against the previous BSDF /
             // phase sample.
             if (s.envSpectrum >= 0) {
@@ -1498,7 +1520,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                 }
             }
             const prgpu::Material &m = s.mats[pr.material];
-            if (m.type == prgpu::MatInterface) {
+            if (!kGuide && m.type == prgpu::MatInterface) {
                 // Invisible medium boundary: switch media and continue straight on.
                 if (++crossings > 1000) {
                     alive = false;
@@ -1506,9 +1528,9 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                     medium = dot(d, sf.n) > 0.f ? pr.mediumOutside : pr.mediumInside;
                     o = offset_origin(sf.p, sf.n, d);
                 }
-            } else if (m.type == prgpu::MatBlack || (maxDepth > 0 && depth >= maxDepth)) {
+            } else if ((!kGuide && m.type == prgpu::MatBlack) || (maxDepth > 0 && depth >= maxDepth)) {
                 alive = false;
-            } else if (!kFull && full_material(m)) {
+            } else if (!kFull && !kGuide && full_material(m)) {
                 deferred = true;
             } else {
                 ++depth;
@@ -1541,7 +1563,7 @@ __global__ void __launch_bounds__(256, 2) k_shade(ShadeArgs a) {
                          isfinite(bs.f.v[0] + bs.f.v[1] + bs.f.v[2] + bs.f.v[3]);
                     misPdf = ok && proportional ? full_pdf(fb, wol, bs.wi) : bs.pdf;
                 } else {
-                Lobe lobe = make_lobe(s, m, sf.u, sf.v, lam);
+                Lobe lobe = kGuide ? diffuse_lobe(s, m, sf.u, sf.v, lam) : make_lobe(s, m, sf.u, sf.v, lam);
                 if constexpr (kDelta) textured_lobe(s, int(&m - s.mats), TexCtx{sf.p, sf.u, sf.v}, lam, &lobe);
                 if constexpr (kGuide) {
                     GuideMix gm;
@@ -1684,8 +1706,8 @@ __device__ __forceinline__ void shadow_accept(const DevScene &s, const Paths &P,
 // transparent to this query, an occluded segment is done, an unoccluded one that crossed no
 // interface stays in its starting medium, and the rest go to the walk queue (k_shadow_walk).
 template <bool kSpheres, bool kMedia, bool kBatch = false, bool kWalls = false>
-__global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene *scenes, Paths P, Shadows S,
-                                                    int *counters) {
+__global__ void __launch_bounds__(256, (kSpheres || kMedia || kWalls) ? 1 : 4)
+    k_shadow_any(DevScene s0, const DevScene *scenes, Paths P, Shadows S, int *counters) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int n = counters[kCntShadow];
@@ -1703,14 +1725,33 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
     const QNode *nodes = s0.qnodes;
     const LeafPrim *leaves = s0.leaves;
     const uint8_t *cls = s0.primClass;
-    bool active = false, exhausted = n == 0, overflow = false, toWalk = false;
+    // pending: this lane's segment is traced and its outcome (accept, walk or occluded) not yet
+    // applied; that happens when the lane takes its next entry (kRefillLanes).
+    bool active = false, exhausted = n == 0, pending = false, overflow = false;
     while (!__all_sync(full, exhausted)) {
-        unsigned need = __ballot_sync(full, !active && !exhausted);
-        if (need) {
+        const bool idle = !active && !exhausted;
+        const unsigned need = __ballot_sync(full, idle), busy = __ballot_sync(full, active);
+        if (need && (__popc(need) >= kRefillLanes || !busy)) {
+            bool toWalk = false;
+            if (idle && pending && !st.found) {
+                if (kWalls && st.crossed) toWalk = true;
+                else shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
+            }
+            pending = false;
+            if (kWalls) {
+                const unsigned m = __ballot_sync(full, toWalk);
+                if (m) {
+                    const int leader = __ffs(m) - 1;
+                    int wb = 0;
+                    if (lane == leader) wb = atomicAdd(counters + kCntWalk, __popc(m));
+                    wb = __shfl_sync(full, wb, leader);
+                    if (toWalk) S.walk[wb + __popc(m & ((1u << lane) - 1u))] = q;
+                }
+            }
             int base = 0;
             if (lane == 0) base = atomicAdd(counters + kCntShadowWork, __popc(need));
             base = __shfl_sync(full, base, 0);
-            if (!active && !exhausted) {
+            if (idle) {
                 q = base + __popc(need & ((1u << lane) - 1u));
                 if (q >= n) {
                     exhausted = true;
@@ -1732,27 +1773,14 @@ __global__ void __launch_bounds__(256) k_shadow_any(DevScene s0, const DevScene 
                                        s.root.box[5], &te) &&
                              te < st.tMax;
                     st.ref = s.root.ref;
-                    if (!active) shadow_accept<kMedia>(s, P, S, q);
+                    // A segment that misses the root box: unoccluded, accepted at the next refill.
+                    pending = !active;
                 }
             }
         }
         if (active && traverse4_step_st<true, kSpheres, kWalls>(nodes, leaves, r, st, hs, &overflow, cls)) {
             active = false;
-            if (!st.found) {
-                if (kWalls && st.crossed) toWalk = true;
-                else shadow_accept<kMedia>(SceneOf<kBatch>::get(s0, scenes, rid), P, S, q);
-            }
-        }
-        if (kWalls) {
-            const unsigned m = __ballot_sync(full, toWalk);
-            if (m) {
-                const int leader = __ffs(m) - 1;
-                int base = 0;
-                if (lane == leader) base = atomicAdd(counters + kCntWalk, __popc(m));
-                base = __shfl_sync(full, base, leader);
-                if (toWalk) S.walk[base + __popc(m & ((1u << lane) - 1u))] = q;
-                toWalk = false;
-            }
+            pending = true;
         }
     }
     if (overflow) atomicOr(counters + kCntStatus, kStatusStack);

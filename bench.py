@@ -41,18 +41,20 @@ N_TRIS = 1 << 20
 N_RAYS = 1 << 24
 METRIC = "path samples/s; equal-time relMSE guided vs plain (same B200); Mrays/s"
 
-# Per-ray work of the closest-hit pass on this workload with this library's SAH BVH (max 4
-# primitives per leaf), measured once with the oracle's counting traversal (oracle/restate.c) over
-# 2^18 of the benchmark rays: mean interior-node visits and triangle tests per ray.
-NODES_PER_RAY = 29.38
-TRIS_PER_RAY = 2.21
+# Per-ray work of the closest-hit pass on this workload: the reference's own BVH traversal
+# (pr::BVH::Intersect over the reference's tree), counted once with the oracle's counting traversal
+# (oracle/restate.c) over 2^18 of the benchmark rays by oracle/measure_trace_work.py: mean node
+# visits and triangle tests per ray. The device kernel, whatever tree it runs on, is credited with
+# this work.
+NODES_PER_RAY = 28.86
+TRIS_PER_RAY = 2.92
 # Algorithmic bytes per closest-hit ray: every visited node (32 B in the reference layout) and
 # every tested triangle (36 B) read once, the 32-byte ray read and an 8-byte hit written.
 BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
 # DRAM bytes per closest-hit launch: dram__bytes_read.sum + dram__bytes_write.sum of this kernel
 # in one ncu capture of a 2^22-ray launch of this workload (a full 2^24-ray launch is too large to
 # capture), scaled by the rays of a full launch. Not measured by this run; the JSON says so.
-NCU_TRAFFIC_PER_LAUNCH = (565.865472e6 + 46.270720e6) * 4
+NCU_TRAFFIC_PER_LAUNCH = (657.116672e6 + 41.239296e6) * 4
 # Plain path tracer (box scene, 256^2, depth 8): algorithmic bytes per path sample,
 # N_closest B_ray + N_shadow B_shadow + 24 B of film, with the reference traversal's per-ray node
 # and triangle counts on the rays the GPU traces for a seeded 2^16-path subset
@@ -286,7 +288,7 @@ def guided_vs_plain_bench(args):
     Plain renders --gvp-spp samples per pixel; its device time is the budget. The guided form
     starts from fresh weights, samples with the guide and trains it online for the first
     --gvp-train-frac of the budget (the guided, batched form: one graph launch per 64 spp, Adam steps
-    on the samples of every filmed wave of 2^16 paths), then samples with the trained guide for the
+    on the samples of every filmed wave of --gvp-train-wave / 2 paths), then samples with the trained guide for the
     rest (prgpu_render_ex); every sample, those of the training phase included, is in its image.
     relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
     channels of (x - ref)^2 / (ref^2 + 1e-2). ratio = relMSE plain / relMSE guided (> 1: the guide
@@ -322,8 +324,9 @@ def guided_vs_plain_bench(args):
         film = np.zeros((R, R, 3))
         done, ms = 0, 0.0
         # Training runs in the guided, batched form: one graph launch per call, Adam steps after
-        # every filmed wave of 2^16 paths, no host round trip per bounce.
-        tcfg = render.batch_config(1 << 17, 256)
+        # every filmed wave (--gvp-train-wave paths in flight, half of them per wave), no host
+        # round trip per bounce.
+        tcfg = render.batch_config(args.gvp_train_wave, 256)
         while ms < args.gvp_train_frac * budget:
             st = render.render_batch([(desc, train, dict(spp=64, first_sample=done, seed=13, max_depth=depth), film)],
                                      config=tcfg, stats=True)
@@ -479,7 +482,7 @@ def c4_time_to_relmse(args):
 
     def guided_step(film, first, n):
         st = render.render_batch([(desc, gext, dict(spp=n, first_sample=first, seed=1, max_depth=depth), film)],
-                                 config=render.batch_config(1 << 18, 256), stats=True)
+                                 config=render.batch_config(args.c4_wave, 256), stats=True)
         gext.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
         return st.deviceMs
 
@@ -534,6 +537,8 @@ def main():
     ap.add_argument("--gvp-ref-spp", type=int, default=65536, help="samples per pixel of the plain reference image")
     ap.add_argument("--gvp-train-frac", type=float, default=0.3,
                     help="share of the guided run's time budget spent training online")
+    ap.add_argument("--gvp-train-wave", type=int, default=1 << 22,
+                    help="paths in flight in the guided run's batched training calls (two waves of half)")
     ap.add_argument("--large-scene", action="store_true",
                     help="also run the large outdoor scene (33.5M-triangle terrain, cloud grid, 4K film; opt-in: "
                          "about a minute of host scene build)")
@@ -544,6 +549,8 @@ def main():
     ap.add_argument("--c4-height", type=int, default=270)
     ap.add_argument("--c4-ref-spp", type=int, default=16384)
     ap.add_argument("--c4-target", type=float, default=0.01)
+    ap.add_argument("--c4-wave", type=int, default=1 << 22,
+                    help="paths in flight in the guided, batched run (two waves of half)")
     ap.add_argument("--c4-max-spp", type=int, default=4096)
     ap.add_argument("--ls-spp", type=int, default=4)
     ap.add_argument("--ls-steps", type=int, default=2)
@@ -588,7 +595,7 @@ def main():
     from prgpu import abi
 
     verts, closest, anyhit, trace = make_inputs(rank)
-    nodes, order = trace.build_bvh_triangles(verts, max_leaf=4)
+    nodes, order = trace.build_bvh_triangles(verts, max_leaf=1)
     acc = trace.Accel(nodes, order, verts, device=local)
     lib = abi.gpu_lib()
 
@@ -693,7 +700,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
-                   "rays_per_pass": N_RAYS, "triangles": N_TRIS, "bvh": "own binned SAH, <=4 per leaf",
+                   "rays_per_pass": N_RAYS, "triangles": N_TRIS, "bvh": "own binned SAH, 1 triangle per leaf, collapsed 4-wide",
                    "l2": "inputs larger than L2 (1 GiB of rays per step)", "parallelism": f"replicas x{world}"},
         "e2e": None if e2e_value is None else
         {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(2 * N_RAYS * 32),

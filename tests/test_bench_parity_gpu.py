@@ -1,6 +1,6 @@
 """Parity on the configurations the benchmark times, not on neighbours of them.
 
-* Traversal: the benchmark traces with this library's own binned-SAH tree (<= 4 triangles per leaf)
+* Traversal: the benchmark traces with this library's own binned-SAH tree (one triangle per leaf)
   collapsed to the 4-wide layout, through the persistent device-pointer kernel on a caller stream.
   Here that exact path runs over the full 1,048,576-triangle soup on the first 2^21 of the
   benchmark's own 2^24 rays (same seeds, same generator call), against the reference's
@@ -46,7 +46,7 @@ def test_benchmarked_traversal_matches_reference(gpu, oracle):
     ro, _ = b.trace(workloads.rays_as_f8(anyhit), any_hit=True)
     b.close()
 
-    nodes, order = trace.build_bvh_triangles(verts, max_leaf=4)
+    nodes, order = trace.build_bvh_triangles(verts, max_leaf=1)
     acc = trace.Accel(nodes, order, verts)
     stream = torch.cuda.current_stream()
     dc = torch.from_numpy(closest.view(np.uint8)).cuda()
