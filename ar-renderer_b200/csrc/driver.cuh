@@ -35,10 +35,25 @@ __global__ void __launch_bounds__(256) k_guide_features(DevScene s0, const DevSc
 #pragma unroll
         for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
         guide_features_n(xn, sf.ns, -d, f, bands);
-        __half2 *dst = reinterpret_cast<__half2 *>(feat + size_t(i) * kGuideIn);
-#pragma unroll
-        for (int k = 0; k < kGuideIn / 2; ++k) dst[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
+        guide_store_features(feat + size_t(i) * kGuideIn, f);
     }
+}
+
+// Order in which the collection visits a chunk's paths: warp-sized groups of consecutive paths,
+// taken round-robin from kCollectSlices equal slices of the chunk (a transposition, so every path
+// is visited once; t runs over [0, collect_span(total)) and j >= total is skipped). Paths are
+// ordered sample-major, pixel-minor, and only the first `cap` samples are kept: visited in path
+// order, those would all come from the first pixels of the image (its top rows on a large film).
+constexpr int kCollectSlices = 1024;
+__host__ __device__ __forceinline__ int collect_span(int total) {
+    const int groups = (total + 31) >> 5;
+    return ((groups + kCollectSlices - 1) / kCollectSlices) * kCollectSlices * 32;
+}
+__device__ __forceinline__ int collect_path(int t, int total) {
+    const int groups = (total + 31) >> 5;
+    const int per = (groups + kCollectSlices - 1) / kCollectSlices;
+    const int g = t >> 5;
+    return (((g % kCollectSlices) * per + g / kCollectSlices) << 5) | (t & 31);
 }
 
 // After a chunk's film: every complete training record of the chunk's paths becomes a sample

@@ -523,17 +523,25 @@ __global__ void k_guide_prep(const GuideTrainRec *recs, const int *count, int of
     const int n = max(0, min(*count - offset, maxRows));
     recs += offset;
     if (blockIdx.x == 0 && threadIdx.x == 0) *rows = n;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const GuideTrainRec r = recs[i];
-        float f[kGuideIn];
+    // Every thread runs the same number of iterations (whole warps per iteration), so the weight
+    // sum is reduced per warp: one atomic per warp instead of one per row on a single address.
+    const int stride = gridDim.x * blockDim.x;
+    const int iters = (n + stride - 1) / stride;
+    for (int it = 0, i = blockIdx.x * blockDim.x + threadIdx.x; it < iters; ++it, i += stride) {
+        float w = 0.f;
+        if (i < n) {
+            const GuideTrainRec r = recs[i];
+            float f[kGuideIn];
 #pragma unroll
-        for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
-        guide_features_n(r.xn, mk(r.n[0], r.n[1], r.n[2]), mk(r.wo[0], r.wo[1], r.wo[2]), f, bands);
-        __half2 *dst = reinterpret_cast<__half2 *>(features + size_t(i) * kGuideIn);
+            for (int k = 0; k < kGuideIn; ++k) f[k] = 0.f;
+            guide_features_n(r.xn, mk(r.n[0], r.n[1], r.n[2]), mk(r.wo[0], r.wo[1], r.wo[2]), f, bands);
+            guide_store_features(features + size_t(i) * kGuideIn, f);
+            samples[i] = GuideSample{{r.wi[0], r.wi[1], r.wi[2]}, r.pb, r.w, {r.n[0], r.n[1], r.n[2]}};
+            w = r.w;
+        }
 #pragma unroll
-        for (int k = 0; k < kGuideIn / 2; ++k) dst[k] = __floats2half2_rn(f[2 * k], f[2 * k + 1]);
-        samples[i] = GuideSample{{r.wi[0], r.wi[1], r.wi[2]}, r.pb, r.w, {r.n[0], r.n[1], r.n[2]}};
-        atomicAdd(wsum, r.w);
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if ((threadIdx.x & 31) == 0 && w != 0.f) atomicAdd(wsum, w);
     }
 }
 

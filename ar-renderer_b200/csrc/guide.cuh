@@ -25,6 +25,10 @@
 // after which the lobes' gradient (proportional to c) vanishes.
 #pragma once
 
+#include <cuda_fp16.h>
+
+#include <cstring>
+
 #include "common.cuh"
 
 namespace prb {
@@ -75,6 +79,21 @@ __device__ __forceinline__ void guide_features(V3 x, V3 n, V3 wo, const float *b
     f[75] = n.x, f[76] = n.y, f[77] = n.z;
     f[78] = wo.x, f[79] = wo.y, f[80] = wo.z;
     f[kGuideConstIn] = 1.f;
+}
+
+// One row of FP16 features as 16-byte stores (8 features each): rows are 256 bytes apart, so
+// narrower stores would each fill only a few bytes of a memory sector.
+__device__ __forceinline__ void guide_store_features(__half *row, const float *f) {
+    int4 *dst = reinterpret_cast<int4 *>(row);
+#pragma unroll
+    for (int k = 0; k < kGuideIn / 8; ++k) {
+        __half2 h[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) h[e] = __floats2half2_rn(f[8 * k + 2 * e], f[8 * k + 2 * e + 1]);
+        int4 v;
+        memcpy(&v, h, sizeof(v));
+        dst[k] = v;
+    }
 }
 
 struct GuideMix {

@@ -17,8 +17,11 @@ namespace prb {
 
 __global__ void __launch_bounds__(256) k_guide_collect(Paths P, float4 *rec, int total, GuideTrainRec *out,
                                                        int *count, int cap) {
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += gridDim.x * blockDim.x)
-        guide_collect_path(P, rec, j, out, count, cap);
+    const int span = collect_span(total);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < span; t += gridDim.x * blockDim.x) {
+        const int j = collect_path(t, total);
+        if (j < total) guide_collect_path(P, rec, j, out, count, cap);
+    }
 }
 
 // Measurement tap: the closest-hit rays of queued paths in slots [0, paths), then (before the

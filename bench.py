@@ -213,7 +213,7 @@ def batch_bench(args, device: int, cpu: bool):
     copies in and out, scene residency checks, scheduling)."""
     from prgpu import hostscene, render, scenes
 
-    specs = scenes.uneven_batch(48)
+    specs = scenes.uneven_batch(48)[: max(1, min(48, args.batch_renders))]
     t0 = time.perf_counter()
     hosts = [hostscene.build_box_scene(s) for s in specs]
     build_s = time.perf_counter() - t0
@@ -222,7 +222,10 @@ def batch_bench(args, device: int, cpu: bool):
     items = [(h.desc(), None, dict(spp=max(1, s.spp // div), seed=1, max_depth=s.max_depth), f)
              for h, s, f in zip(hosts, specs, films)]
     t0 = time.perf_counter()
-    cfg = render.autotune_batch(items)
+    if args.batch_wave > 0:
+        cfg = render.batch_config(args.batch_wave, 256)
+    else:
+        cfg = render.autotune_batch(items)
     tune_s = time.perf_counter() - t0
     bcfg = render.batch_config(cfg.wavefrontPaths, cfg.shadeBlock, host_loop=args.batch_host_loop)
     for _ in range(args.batch_warmup):
@@ -247,12 +250,13 @@ def batch_bench(args, device: int, cpu: bool):
                                   out=np.zeros_like(f), stats=True)
         single_ms += sst.deviceMs
     out = {
-        "workload": "uneven batch: 48 box-family renders, 128^2..1024^2, 16..256 spp, depth 8..32, half with media",
+        "workload": f"uneven batch: {len(specs)} box-family renders, 128^2..1024^2, 16..256 spp, depth 8..32, half with media",
         "metric": "path samples/s", "value": samples / (statistics.mean(dev) * 1e-3), "unit": "path samples/s",
         "ms_per_step": statistics.mean(dev), "steps": args.batch_steps, "warmup": args.batch_warmup,
         "path_samples_per_step": samples, "spp_divided_by": div, "waves": int(st.waves), "loop_iterations": int(st.loopIterations),
         "graph_launches_per_step": 0 if args.batch_host_loop else 1, "kernel_nodes_per_iteration": 14,
-        "autotuned": {"wavefrontPaths": cfg.wavefrontPaths, "shadeBlock": cfg.shadeBlock, "seconds": tune_s},
+        "autotuned": {"wavefrontPaths": cfg.wavefrontPaths, "shadeBlock": cfg.shadeBlock, "seconds": tune_s,
+                      "fixed_by_flag": args.batch_wave > 0},
         "vs_sequential_singles": {"spp_divided_by": cmp_div, "batch_ms": cst.deviceMs, "singles_ms": single_ms,
                                   "speedup": single_ms / cst.deviceMs},
         "host_scene_build_s": build_s,
@@ -265,7 +269,7 @@ def batch_bench(args, device: int, cpu: bool):
 
         ref.set_threads(0)
         tot, secs = 0, 0.0
-        for k in (0, 1):
+        for k in range(min(2, len(specs))):
             s = specs[k]
             jp = os.path.join(tempfile.gettempdir(), "prb_bench", f"batch_{k}.prscene.json")
             rs = ref.RefScene(scenes.write_reference_json(s, jp))
@@ -287,7 +291,7 @@ def guided_vs_plain_bench(args):
     light facing the ceiling). The reference image is a --gvp-ref-spp plain render on the GPU.
     Plain renders --gvp-spp samples per pixel; its device time is the budget. The guided form
     starts from fresh weights, samples with the guide and trains it online for the first
-    --gvp-train-frac of the budget (the guided, batched form: one graph launch per 64 spp, Adam steps
+    --gvp-train-frac of the budget (the guided, batched form: one graph launch per 256 spp, Adam steps
     on the samples of every filmed wave of --gvp-train-wave / 2 paths), then samples with the trained guide for the
     rest (prgpu_render_ex); every sample, those of the training phase included, is in its image.
     relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
@@ -328,17 +332,22 @@ def guided_vs_plain_bench(args):
         # round trip per bounce.
         tcfg = render.batch_config(args.gvp_train_wave, 256)
         while ms < args.gvp_train_frac * budget:
-            st = render.render_batch([(desc, train, dict(spp=64, first_sample=done, seed=13, max_depth=depth), film)],
+            st = render.render_batch([(desc, train, dict(spp=256, first_sample=done, seed=13, max_depth=depth), film)],
                                      config=tcfg, stats=True)
             train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
             ms += st.deviceMs
-            done += 64
+            done += 256
         n_train = done
+        # Sampling with the trained guide: calls sized from the cost per sample measured so far, so
+        # that the last one ends close to the budget (chunks as large as plain rendering's).
+        per_spp = None
         while ms < budget:
-            _, st = render.render_ex(desc, R, R, 64, first_sample=done, seed=13, max_depth=depth, ext=use, out=film,
+            n = 64 if per_spp is None else max(8, min(8192, int((budget - ms) / per_spp) // 8 * 8))
+            _, st = render.render_ex(desc, R, R, n, first_sample=done, seed=13, max_depth=depth, ext=use, out=film,
                                      stats=True)
             ms += st.deviceMs
-            done += 64
+            done += n
+            per_spp = st.deviceMs / n
         n_use = done - n_train
         ep, eg = relmse(plain / spp), relmse(film / done)
         # Equal sample count, for reference: the trained guide sampling only.
@@ -529,6 +538,10 @@ def main():
                          "conditional graphs)")
     ap.add_argument("--batch-spp-div", type=int, default=1,
                     help="divide every render's spp (profiling captures only; the JSON says so)")
+    ap.add_argument("--batch-renders", type=int, default=48,
+                    help="render only the first K of the 48 batch scenes (profiling captures only; the JSON says so)")
+    ap.add_argument("--batch-wave", type=int, default=0,
+                    help="paths in flight instead of the autotuner's choice, shading blocks of 256 (profiling captures)")
     ap.add_argument("--no-guided", action="store_true", help="skip the guided-vs-plain comparison")
     ap.add_argument("--guided-only", action="store_true",
                     help="run only the guided-vs-plain comparison and print its JSON object (profiling captures)")
