@@ -179,11 +179,14 @@ bool make_accel(int deviceIndex, const prgpu::BVHNode *nodes, int32_t nodeCount,
 }
 
 // Host-buffer query: rays are copied in chunks on the copy stream while the previous chunk is
-// traced on the compute stream; results are copied back per chunk.
+// traced on the compute stream; results are copied back per chunk. The call is bound by the
+// host-to-device copy (32 B per ray in, 4-8 B out); chunks of 2^20 rays (32 MiB) keep the copy
+// engine busy while a chunk's trace and result copy (well under its copy time) overlap the next
+// chunk's copy, and keep the unoverlapped first copy and last trace of a call short.
 bool trace_host(prgpu_accel_t *a, const prgpu::Ray *rays, int64_t n, int anyHit, int32_t *primOut, float *tOut,
                 float *b1Out, float *b2Out, bool wide, std::string *err) {
     DeviceState &ds = device_state(a->device);
-    const int64_t chunk = int64_t(1) << 22;
+    const int64_t chunk = int64_t(1) << 20;
     int64_t cap = std::min<int64_t>(n, 2 * chunk);
     a->rays.ensure(size_t(std::max<int64_t>(cap, 1)) * sizeof(prgpu::Ray));
     a->prim.ensure(size_t(std::max<int64_t>(cap, 1)) * sizeof(int32_t));
