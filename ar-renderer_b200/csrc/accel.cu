@@ -46,6 +46,12 @@ __global__ void __launch_bounds__(256, 4) k_trace_persist(const void *__restrict
     auto store = [&]() {
         if (kAny) {
             primOut[idx] = s.found ? 1 : 0;
+        } else if (kWide) {
+            const Hit h = finish_hit<false>(prims, r, s);
+            primOut[idx] = h.prim;
+            if (tOut) tOut[idx] = h.t;
+            if (b1Out) b1Out[idx] = h.u;
+            if (b2Out) b2Out[idx] = h.v;
         } else {
             primOut[idx] = s.found ? s.hit.prim : -1;
             if (tOut) tOut[idx] = s.found ? s.hit.t : 0.f;
@@ -87,7 +93,8 @@ __global__ void __launch_bounds__(256, 4) k_trace_persist(const void *__restrict
         bool done = false;
         if (active) {
             if (kWide)
-                done = traverse4_step_st<kAny, false>(static_cast<const QNode *>(nodes), prims, r, s, hs, &overflow);
+                done = traverse4_step_st<kAny, false, false, true>(static_cast<const QNode *>(nodes), prims, r, s, hs,
+                                                                   &overflow);
             else
                 done = traverse_step<kAny, false>(static_cast<const WNode *>(nodes), prims, r, s, stackRef, stackT,
                                                   &overflow);

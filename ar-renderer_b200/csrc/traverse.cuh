@@ -421,7 +421,12 @@ struct HybridStack {
     __device__ __forceinline__ int node(int i) const { return i < kShort ? sh[i * kThreads].x : ref[i - kShort]; }
 };
 
-template <bool kAny, bool kSpheres, bool kSkipTransparent = false, class Stack>
+// kDeferUV (closest hit): a hit records only its leaf slot (s.hit.prim) and distance (s.tMax);
+// the caller repeats the winning primitive's test once at the end (finish_hit), which gives the
+// same t, u, v bit for bit. Fewer live registers in the loop let the slab planes be selected by
+// address as for any hit (ray-query benchmark, closest hit: 3,821 -> 3,926 Mrays/s; either change
+// alone was slower: 3,730 and 3,667).
+template <bool kAny, bool kSpheres, bool kSkipTransparent = false, bool kDeferUV = false, class Stack>
 __device__ __forceinline__ bool traverse4_step_st(const QNode *__restrict__ nodes, const LeafPrim *__restrict__ prims,
                                                   const TraceRay &r, TravState &s, Stack &stack, bool *overflow,
                                                   const uint8_t *__restrict__ cls = nullptr) {
@@ -430,13 +435,13 @@ __device__ __forceinline__ bool traverse4_step_st(const QNode *__restrict__ node
         float t0, t1, t2, t3;
         const float inf = __int_as_float(0x7f800000);
         int4 ch;
-        if constexpr (kAny) {
+        if constexpr (kAny || kDeferUV) {
             ch = __ldg(&n->child);
             if (!r.infInv) {
-                // Any hit: the near and far planes are chosen by address from the ray's octant (six
-                // loads, no per-child selects). Measured on the ray-query benchmark: any hit 5,314
-                // -> 5,689 Mrays/s; the closest-hit kernel ran slower this way (3,824 -> 3,667), so
-                // it keeps the loads of all six plane vectors below.
+                // The near and far planes chosen by address from the ray's octant (six loads, no
+                // per-child selects). Measured on the ray-query benchmark: any hit 5,314 -> 5,689
+                // Mrays/s; closest hit only together with kDeferUV (see above); the closest-hit
+                // form that keeps t, u, v live loads all six plane vectors below.
                 const char *nb = reinterpret_cast<const char *>(n);
                 const int ox = r.neg[0] ? 48 : 0, oy = r.neg[1] ? 48 : 0, oz = r.neg[2] ? 48 : 0;
                 const float4 nx = __ldg(reinterpret_cast<const float4 *>(nb + ox));
@@ -511,10 +516,14 @@ __device__ __forceinline__ bool traverse4_step_st(const QNode *__restrict__ node
                 s.found = true;
                 if (kAny) return true;
                 s.tMax = t;
-                s.hit.t = t;
-                s.hit.u = u;
-                s.hit.v = v;
-                s.hit.prim = __float_as_int(v0.w);
+                if constexpr (kDeferUV) {
+                    s.hit.prim = int(p - prims);
+                } else {
+                    s.hit.t = t;
+                    s.hit.u = u;
+                    s.hit.v = v;
+                    s.hit.prim = __float_as_int(v0.w);
+                }
             }
         }
     }
@@ -526,6 +535,23 @@ __device__ __forceinline__ bool traverse4_step_st(const QNode *__restrict__ node
         }
     }
     return true;
+}
+
+// The hit of a kDeferUV traversal: the winning leaf slot's test repeated (no tMax bound), which
+// reproduces the distance and barycentrics the traversal computed; prim = the original index.
+template <bool kSpheres>
+__device__ __forceinline__ Hit finish_hit(const LeafPrim *__restrict__ prims, const TraceRay &r, const TravState &s) {
+    Hit h{0.f, 0.f, 0.f, -1};
+    if (!s.found) return h;
+    const LeafPrim *p = prims + s.hit.prim;
+    const float4 v0 = __ldg(&p->v0), v1 = __ldg(&p->v1);
+    const float inf = __int_as_float(0x7f800000);
+    if (kSpheres && __float_as_int(v1.w) == 1)
+        hit_sphere(r, v0, v1, inf, &h.t);
+    else
+        hit_triangle(r, v0, v1, __ldg(&p->v2), inf, &h.t, &h.u, &h.v);
+    h.prim = __float_as_int(v0.w);
+    return h;
 }
 
 template <bool kAny, bool kSpheres, bool kSkipTransparent = false>

@@ -1195,8 +1195,10 @@ __global__ void __launch_bounds__(256, kSpheres ? 1 : 4) k_extend(DevScene s0, c
             if (lane == 0) base = atomicAdd(counters + kCntExtendWork, __popc(need));
             base = __shfl_sync(full, base, 0);
             if (idle) {
-                if (pending)
-                    P.hit[j] = make_float4(st.hit.t, st.hit.u, st.hit.v, __int_as_float(st.found ? st.hit.prim : -1));
+                if (pending) {
+                    const Hit h = finish_hit<kSpheres>(leaves, r, st);
+                    P.hit[j] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+                }
                 pending = false;
                 int q = base + __popc(need & ((1u << lane) - 1u));
                 if (q >= n) {
@@ -1223,7 +1225,7 @@ __global__ void __launch_bounds__(256, kSpheres ? 1 : 4) k_extend(DevScene s0, c
                 }
             }
         }
-        if (active && traverse4_step_st<false, kSpheres>(nodes, leaves, r, st, hs, &overflow)) {
+        if (active && traverse4_step_st<false, kSpheres, false, true>(nodes, leaves, r, st, hs, &overflow)) {
             active = false;
             pending = true;
         }
