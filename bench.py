@@ -54,7 +54,7 @@ BYTES_PER_RAY = 32 * NODES_PER_RAY + 36 * TRIS_PER_RAY + 32 + 8
 # DRAM bytes per closest-hit launch: dram__bytes_read.sum + dram__bytes_write.sum of this kernel
 # in one ncu capture of a 2^22-ray launch of this workload (a full 2^24-ray launch is too large to
 # capture), scaled by the rays of a full launch. Not measured by this run; the JSON says so.
-NCU_TRAFFIC_PER_LAUNCH = (657.116672e6 + 41.239296e6) * 4
+NCU_TRAFFIC_PER_LAUNCH = (664.852480e6 + 42.621440e6) * 4
 # Plain path tracer (box scene, 256^2, depth 8): algorithmic bytes per path sample,
 # N_closest B_ray + N_shadow B_shadow + 24 B of film, with the reference traversal's per-ray node
 # and triangle counts on the rays the GPU traces for a seeded 2^16-path subset
