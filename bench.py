@@ -119,6 +119,26 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(values, world: int, device: str = "cuda"):
+    """Element-wise maximum of this rank's timings over all ranks: a multi-GPU step takes as long as
+    its slowest rank. One all-reduce on the process group (NCCL for the GPUs, gloo in the CPU test)."""
+    vals = [float(v) for v in values]
+    if world <= 1:
+        return vals
+    import torch
+    import torch.distributed as dist
+
+    x = torch.tensor(vals, device=device, dtype=torch.float64)
+    dist.all_reduce(x, op=dist.ReduceOp.MAX)
+    return [float(v) for v in x.tolist()]
+
+
+def whole_job_mrays(world: int, rays_per_rank: int, seconds: float) -> float:
+    """Mrays/s of the whole job: every rank traces its own rays_per_rank in `seconds` (the maximum
+    over ranks), so the job's rate is world times one rank's rays over that time (weak scaling)."""
+    return world * rays_per_rank / seconds / 1e6
+
+
 def make_inputs(rank: int):
     from prgpu import trace, workloads
 
@@ -649,12 +669,9 @@ def main():
     launches = int(lib.prgpu_launch_count() - launches0)
     ms = t_start.elapsed_time(t_end)
     closest_ms = statistics.mean(a.elapsed_time(b) for a, b in evs)
-    if world > 1:
-        x = torch.tensor([ms, closest_ms], device="cuda")
-        dist.all_reduce(x, op=dist.ReduceOp.MAX)
-        ms, closest_ms = float(x[0]), float(x[1])
+    ms, closest_ms = max_over_ranks([ms, closest_ms], world)
     ms_per_step = ms / args.steps
-    value = world * 2 * N_RAYS / (ms_per_step * 1e3)  # Mrays/s, whole job
+    value = whole_job_mrays(world, 2 * N_RAYS, ms_per_step * 1e-3)
     assert acc.status() == 0, "traversal stack overflow"
 
     # End to end through the C ABI with pinned host buffers (the copies are inside the region).
@@ -676,11 +693,8 @@ def main():
             acc.trace_host(ha, hocc, None, True)
         barrier()
         e2e_s = (time.perf_counter() - t0) / e2e_steps
-        if world > 1:
-            x = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-            dist.all_reduce(x, op=dist.ReduceOp.MAX)
-            e2e_s = float(x[0])
-        e2e_value = world * 2 * N_RAYS / e2e_s / 1e6
+        (e2e_s,) = max_over_ranks([e2e_s], world)
+        e2e_value = whole_job_mrays(world, 2 * N_RAYS, e2e_s)
         np.testing.assert_array_equal(hprim, prim.cpu().numpy())
 
     peak, peak_kind = _peaks()
