@@ -29,12 +29,11 @@ N_TRIS = 1 << 20
 BENCH_RAYS = 1 << 24
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--rays", type=int, default=1 << 18)
-    args = ap.parse_args()
+def trace_work(rays_counted: int = 1 << 18) -> dict:
+    """Mean nodes visited and triangles tested per ray, closest-hit and any-hit passes, over the
+    reference's own tree on the first `rays_counted` rays of each benchmark pass."""
     verts = workloads.triangle_soup(N_TRIS, seed=1)
-    rays = workloads.rays_as_f8(workloads.soup_rays(BENCH_RAYS, seed=2)[: args.rays])
+    rays = workloads.rays_as_f8(workloads.soup_rays(BENCH_RAYS, seed=2)[:rays_counted])
     b = ref.SoupBVH(verts)
     nodes, order = b.export(abi.BVH_NODE)
     rp, rt, _, _, _ = b.trace(rays)
@@ -45,22 +44,32 @@ def main():
     nv = np.empty(n, np.int32)
     nt = np.empty(n, np.int32)
     lib = ref.restate_lib()
-    assert lib.rs_trace(ref._p(nodes), len(nodes), ref._p(order), ref._p(np.ascontiguousarray(verts)), ref._p(rays), n,
-                        0, ref._p(prim), ref._p(t), ref._p(nv), ref._p(nt)) == 0
+    vp = ref._p(np.ascontiguousarray(verts))
+    assert lib.rs_trace(ref._p(nodes), len(nodes), ref._p(order), vp, ref._p(rays), n, 0, ref._p(prim), ref._p(t),
+                        ref._p(nv), ref._p(nt)) == 0
     # The counting restatement answers as the reference build does.
     assert (prim == rp).all() and (t[rp >= 0].view(np.int32) == rt[rp >= 0].view(np.int32)).all()
-    nodes_per_ray, tris_per_ray = float(nv.mean()), float(nt.mean())
-    bytes_per_ray = 32 * nodes_per_ray + 36 * tris_per_ray + 32 + 8
-    print(f"reference BVH ({len(nodes)} nodes), {n} rays: {nodes_per_ray:.2f} nodes and {tris_per_ray:.2f} triangles "
-          f"per ray; {bytes_per_ray:.2f} algorithmic bytes per closest-hit ray")
-    # The any-hit pass (tMax uniform in [0, 2]): the same counts, 4 bytes of flag out.
-    arays = workloads.rays_as_f8(workloads.soup_rays(BENCH_RAYS, seed=3, any_hit=True)[: args.rays])
+    out = {"tree_nodes": len(nodes), "rays": n, "closest_nodes": float(nv.mean()), "closest_tris": float(nt.mean())}
+    # The any-hit pass (tMax uniform in [0, 2]).
+    arays = workloads.rays_as_f8(workloads.soup_rays(BENCH_RAYS, seed=3, any_hit=True)[:rays_counted])
     occ = np.empty(n, np.int32)
-    assert lib.rs_trace(ref._p(nodes), len(nodes), ref._p(order), ref._p(np.ascontiguousarray(verts)), ref._p(arays), n,
-                        1, ref._p(occ), None, ref._p(nv), ref._p(nt)) == 0
-    an, at = float(nv.mean()), float(nt.mean())
-    print(f"any hit: {an:.2f} nodes and {at:.2f} triangles per ray; {32 * an + 36 * at + 32 + 4:.2f} algorithmic bytes "
-          f"per any-hit ray ({occ.mean():.3f} of the rays occluded)")
+    assert lib.rs_trace(ref._p(nodes), len(nodes), ref._p(order), vp, ref._p(arays), n, 1, ref._p(occ), None,
+                        ref._p(nv), ref._p(nt)) == 0
+    out.update(any_nodes=float(nv.mean()), any_tris=float(nt.mean()), any_occluded=float(occ.mean()))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rays", type=int, default=1 << 18)
+    args = ap.parse_args()
+    w = trace_work(args.rays)
+    cb = 32 * w["closest_nodes"] + 36 * w["closest_tris"] + 32 + 8
+    ab = 32 * w["any_nodes"] + 36 * w["any_tris"] + 32 + 4
+    print(f"reference BVH ({w['tree_nodes']} nodes), {w['rays']} rays: {w['closest_nodes']:.2f} nodes and "
+          f"{w['closest_tris']:.2f} triangles per ray; {cb:.2f} algorithmic bytes per closest-hit ray")
+    print(f"any hit: {w['any_nodes']:.2f} nodes and {w['any_tris']:.2f} triangles per ray; {ab:.2f} algorithmic bytes "
+          f"per any-hit ray ({w['any_occluded']:.3f} of the rays occluded)")
 
 
 if __name__ == "__main__":
