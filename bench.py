@@ -310,10 +310,13 @@ def guided_vs_plain_bench(args):
     depth 32) at a reduced size (--gvp-res, default 128^2), and on the box lit only indirectly (its
     light facing the ceiling). The reference image is a --gvp-ref-spp plain render on the GPU.
     Plain renders --gvp-spp samples per pixel; its device time is the budget. The guided form
-    starts from fresh weights, samples with the guide and trains it online for the first
-    --gvp-train-frac of the budget (the guided, batched form: one graph launch per 256 spp, Adam steps
-    on the samples of every filmed wave of --gvp-train-wave / 2 paths), then samples with the trained guide for the
-    rest (prgpu_render_ex); every sample, those of the training phase included, is in its image.
+    starts from fresh weights, samples with the guide and trains it online for --gvp-train-frac of
+    the budget (default: all of it) in the guided, batched form (one graph launch per 256 spp, Adam
+    steps on the samples of every filmed wave of --gvp-train-wave / 2 paths), and samples with the
+    trained guide for the rest, if any (prgpu_render_ex); every sample is in its image. Training
+    throughout measured best (training share 0.3 / 0.6 / 1.0 of the budget: slit scene 0.89 /
+    0.90 / 0.91x, indirectly lit box 1.28 / 1.44 / 1.44x): a few Adam steps per wave cost little and
+    the guide keeps improving.
     relMSE is the form of the reference's tests/test_quality.cpp:241-248: mean over pixels and
     channels of (x - ref)^2 / (ref^2 + 1e-2). ratio = relMSE plain / relMSE guided (> 1: the guide
     wins at equal time)."""
@@ -568,7 +571,7 @@ def main():
     ap.add_argument("--gvp-res", type=int, default=128, help="guided-vs-plain image side (1024 = the full C3 size)")
     ap.add_argument("--gvp-spp", type=int, default=32768, help="plain samples per pixel of the equal-time comparison")
     ap.add_argument("--gvp-ref-spp", type=int, default=65536, help="samples per pixel of the plain reference image")
-    ap.add_argument("--gvp-train-frac", type=float, default=0.3,
+    ap.add_argument("--gvp-train-frac", type=float, default=1.0,
                     help="share of the guided run's time budget spent training online")
     ap.add_argument("--gvp-train-wave", type=int, default=1 << 22,
                     help="paths in flight in the guided run's batched training calls (two waves of half)")
