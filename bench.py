@@ -354,12 +354,16 @@ def guided_vs_plain_bench(args):
         # every filmed wave (--gvp-train-wave paths in flight, half of them per wave), no host
         # round trip per bounce.
         tcfg = render.batch_config(args.gvp_train_wave, 256)
+        # Calls of 256 spp, the last sized from the cost per sample so far to end near the budget.
+        per_spp = None
         while ms < args.gvp_train_frac * budget:
-            st = render.render_batch([(desc, train, dict(spp=256, first_sample=done, seed=13, max_depth=depth), film)],
+            n = 256 if per_spp is None else max(8, min(256, int((args.gvp_train_frac * budget - ms) / per_spp) // 8 * 8))
+            st = render.render_batch([(desc, train, dict(spp=n, first_sample=done, seed=13, max_depth=depth), film)],
                                      config=tcfg, stats=True)
             train.flags = render.GUIDE_SAMPLE | render.GUIDE_TRAIN
             ms += st.deviceMs
-            done += 256
+            done += n
+            per_spp = st.deviceMs / n
         n_train = done
         # Sampling with the trained guide: calls sized from the cost per sample measured so far, so
         # that the last one ends close to the budget (chunks as large as plain rendering's).
