@@ -119,6 +119,14 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def bench_config(world: int) -> dict:
+    """The workload both arms run (ours on the GPU, the reference's on the host cores): the same
+    triangles and rays per pass; each arm traverses its own BVH."""
+    return {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
+            "rays_per_pass": N_RAYS, "triangles": N_TRIS, "l2": "inputs larger than L2 (1 GiB of rays per step)",
+            "parallelism": f"replicas x{world}"}
+
+
 def max_over_ranks(values, world: int, device: str = "cuda"):
     """Element-wise maximum of this rank's timings over all ranks: a multi-GPU step takes as long as
     its slowest rank. One all-reduce on the process group (NCCL for the GPUs, gloo in the CPU test)."""
@@ -393,8 +401,9 @@ def run_reference_arm(args, rank: int, world: int):
         return
     from prgpu import workloads
 
+    # The whole workload of a step (2^24 + 2^24 rays, about 2 s on 16 host threads).
     verts = workloads.triangle_soup(N_TRIS, seed=1)
-    per = 1 << 21
+    per = N_RAYS
     closest = workloads.soup_rays(per, seed=2)
     anyhit = workloads.soup_rays(per, seed=3, any_hit=True)
     import ref
@@ -413,13 +422,13 @@ def run_reference_arm(args, rank: int, world: int):
     b.close()
     dt = sum(times)
     value = args.steps * 2 * per / dt / 1e6
-    sample = f"{per} closest-hit + {per} any-hit rays of the benchmark workload per step (reference BVH)"
+    sample = (f"{per} closest-hit + {per} any-hit rays of the benchmark workload per step: the reference's "
+              f"BVH::Intersect / IntersectP over its own BVH")
     line = {
         "metric": METRIC, "impl": "reference", "value": value, "unit": "Mrays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
-                   "reference_sample_rays_per_pass": per},
+        "config": bench_config(world), "bvh": "the reference's own pr::BVH",
         "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": ref.thread_count(), "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -733,9 +742,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "traversal microbenchmark: 2^24 rays vs 1,048,576-triangle soup, closest + any-hit",
-                   "rays_per_pass": N_RAYS, "triangles": N_TRIS, "bvh": "own binned SAH, 1 triangle per leaf, collapsed 4-wide",
-                   "l2": "inputs larger than L2 (1 GiB of rays per step)", "parallelism": f"replicas x{world}"},
+        "config": bench_config(world), "bvh": "own binned SAH, 1 triangle per leaf, collapsed 4-wide",
         "e2e": None if e2e_value is None else
         {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": int(2 * N_RAYS * 32),
          "d2h_bytes_per_step": int(N_RAYS * 8 + N_RAYS * 4)},
