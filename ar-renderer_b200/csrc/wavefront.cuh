@@ -456,6 +456,29 @@ static __device__ void textured_lobe(const DevScene &s, int mi, const TexCtx &c,
             }
             l->eta = e;
             l->k = k;
+        } else if (l->kind == kLobeConductor && s.mats[mi].eta < 0) {
+            // A reflectance-parameterised conductor whose reflectance is a texture (tree or image):
+            // the artist mapping of make_lobe on the looked-up value, eta 1 and k = 2 sqrt(r) /
+            // sqrt(1 - r) with r clamped to [0, 0.9999] (ConductorMaterial::MakeBxDF,
+            // material.cpp:90-96; not divided by a coat's IOR, as CoatedConductorMaterial,
+            // material.cpp:159-163).
+            const int tree = s.matTex[5 * mi + 1].w, img = s.matTex[5 * mi].x;
+            if (tree >= 0 || img >= 0) {
+                SS r;
+                if (tree >= 0) {
+                    r = spectrum_texture(s, tree, c, lam);
+                } else {
+                    float rgb[3];
+                    tex_rgb(s.textures[img], c.u, c.v, rgb);
+                    r = rgb_albedo(s, rgb[0], rgb[1], rgb[2], lam);
+                }
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float ri = clampf(r.v[i], 0.f, 0.9999f);
+                    l->eta.v[i] = 1.f;
+                    l->k.v[i] = 2.f * sqrtf(ri) / safe_sqrt(1.f - ri);
+                }
+            }
         }
         const int4 m2 = s.matTex[5 * mi + 2];
         if (m2.y < 0 && m2.z < 0) return;

@@ -325,7 +325,9 @@ struct TextureNode {
 };
 
 // Per SceneDesc material: the image texture of its reflectance (diffuse and coated diffuse
-// materials), of its tangent-space normal map and of its bump (height) map (any material;
+// materials, and the artist reflectance of conductors and coated conductors given by reflectance
+// rather than n and k: ConductorMaterial::MakeBxDF, material.cpp:90-96), of its tangent-space
+// normal map and of its bump (height) map (any material;
 // pr::NormalMapParams / BumpMapParams, material.h:30-41, applied as Material::PerturbShading,
 // material.cpp:16-60), -1 for none. A height map's texture carries the float texture's
 // multiplier in all three rgbScale components. The *Node fields name TextureNode trees instead

@@ -441,3 +441,54 @@ def test_textured_conductor_n_k_agree_with_reference(gpu, oracle):
     assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
     flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
     assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
+
+
+def test_textured_conductor_reflectance_agrees_with_reference(gpu, oracle):
+    """The artist reflectance of reflectance-parameterised conductors from texture trees
+    (ConductorMaterial::MakeBxDF, material.cpp:90-96): a rough conductor sphere whose reflectance is
+    a checker of two colours and a coated-conductor ground whose reflectance is a world-space noise
+    blend (not divided by the coat's IOR, material.cpp:159-163). The exported v4 materials carry
+    only the first checker colour or the average colour; the trees reach the module through
+    SceneExt. The same z statistics as above, and without the trees the images differ."""
+    w, h = 48, 32
+    d = os.path.join(tempfile.gettempdir(), "prb_scenes")
+    os.makedirs(d, exist_ok=True)
+    pfm = os.path.join(d, "unused_tex3.pfm")
+    _write_pfm(pfm, _texture())
+    doc = ru_outdoor_doc(w, h, pfm)
+    ra, rb = [0.95, 0.6, 0.2], [0.3, 0.5, 0.9]
+    doc["textures"] = {
+        "r_chk": {"type": "checker", "a": ra, "b": rb, "uv_scale": [4.0, 4.0]},
+        "r_nz": {"type": "noise", "a": ra, "b": rb, "frequency": 2.0, "octaves": 3},
+    }
+    doc["materials"] = {
+        "ground": {"type": "coated_conductor", "reflectance": {"texture": "r_nz"}, "roughness": 0.2,
+                   "coat_roughness": 0.1},
+        "red": {"type": "diffuse", "reflectance": [0.7, 0.2, 0.15]},
+        "tex_coat": {"type": "conductor", "reflectance": {"texture": "r_chk"}, "roughness": 0.3},
+    }
+    path = os.path.join(d, "textured_reflectance_conductor.prscene.json")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    sd, (ia, ib) = _with_albedo_spectra(rs, [ra, rb])
+    T = render.texture_node
+    nodes = [T(abi.TEX_CONSTANT, a=ia), T(abi.TEX_CONSTANT, a=ib), T(abi.TEX_CHECKER, a=0, b=1, uv_scale=(4.0, 4.0)),
+             T(abi.TEX_NOISE, frequency=2.0, octaves=3), T(abi.TEX_MIX, a=0, b=1, t=3)]
+    used = []
+    for o in doc["objects"]:
+        if o["material"] not in used:
+            used.append(o["material"])
+    slots = {"ground": {"reflectanceNode": 4}, "tex_coat": {"reflectanceNode": 2}}
+    ext = render.make_ext(material_textures=[slots.get(n, {}) for n in used], texture_nodes=nodes)
+    g = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6, ext=ext) / 256 for k in range(16)])
+    c = np.stack([rs.render(256, 2000 + k, 6)[0].astype(np.float64) / 256 for k in range(16)])
+    z = ru.z_scores(g, c)
+    frac = np.mean(np.abs(z) < 4)
+    mg, mc = g[..., 1].mean(axis=(1, 2)), c[..., 1].mean(axis=(1, 2))
+    se = np.sqrt(mg.var(ddof=1) / len(mg) + mc.var(ddof=1) / len(mc))
+    print(f"textured conductor reflectance: frac {frac:.4f}, mean Y gpu {mg.mean():.5f} cpu {mc.mean():.5f} se {se:.5f}")
+    assert frac >= 0.998, f"only {frac:.4f} of values within |z| < 4"
+    assert abs(mg.mean() - mc.mean()) < 4 * se, f"mean Y gpu {mg.mean()} cpu {mc.mean()} (se {se})"
+    flat = np.stack([render.render_ex(sd, w, h, 256, seed=1000 + k, max_depth=6) / 256 for k in range(4)])
+    assert np.mean(np.abs(ru.z_scores(flat, c[:4])) < 4) < 0.95
