@@ -70,6 +70,7 @@ static __device__ __noinline__ float indexed_density(const DevGrid &g, V3 p) {
 // Density at a medium-space point: 0 outside the bounds, trilinear between cell centres inside
 // (or the noise field's, or the index-space grid's).
 __device__ __forceinline__ float grid_density(const DevGrid &g, V3 p) {
+    if (g.boundless) return noise_field_density(g, p);
     if (!(p.x >= g.bmin[0] && p.x <= g.bmax[0] && p.y >= g.bmin[1] && p.y <= g.bmax[1] && p.z >= g.bmin[2] &&
           p.z <= g.bmax[2]))
         return 0.f;
@@ -99,6 +100,8 @@ __device__ __forceinline__ bool grid_clip(const DevGrid &g, V3 o, V3 d, float tM
              m[8] * d.x + m[9] * d.y + m[10] * d.z);
     *t0 = 0.f;
     *t1 = tMax;
+    // A field without bounds fills every finite segment (GridMedium::Clip, medium.cpp:182-188).
+    if (g.boundless) return isfinite(tMax);
     float oo[3] = {mo->x, mo->y, mo->z}, dd[3] = {md->x, md->y, md->z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {

@@ -156,13 +156,20 @@ bool validate(const prgpu::SceneDesc *sd, const prgpu::SceneExt *ext, std::strin
                 !std::isfinite(g.noiseThreshold) || !std::isfinite(g.noiseSharpness) || !std::isfinite(g.noiseOffset[0]) ||
                 !std::isfinite(g.noiseOffset[1]) || !std::isfinite(g.noiseOffset[2]))
                 return fail("bad noise medium parameters");
-            if (!(g.boundsMin.x < g.boundsMax.x && g.boundsMin.y < g.boundsMax.y && g.boundsMin.z < g.boundsMax.z))
-                return fail("noise media need non-empty bounds");
+            // Empty bounds (Bounds3f::IsEmpty, math.h:212: min > max on an axis) or a box of positive
+            // extent; a degenerate box would divide the falloff by zero.
+            const bool empty = g.boundsMin.x > g.boundsMax.x || g.boundsMin.y > g.boundsMax.y ||
+                               g.boundsMin.z > g.boundsMax.z;
+            if (!empty &&
+                !(g.boundsMin.x < g.boundsMax.x && g.boundsMin.y < g.boundsMax.y && g.boundsMin.z < g.boundsMax.z))
+                return fail("noise media need bounds of positive extent, or empty bounds");
         } else if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || int64_t(g.nx) * g.ny * g.nz > (int64_t(1) << 31) || !g.density) {
             return fail("bad grid medium dimensions or data");
         }
         if (!spec_ok(g.sigmaA, ns) || !spec_ok(g.sigmaS, ns)) return fail("grid medium spectrum index out of range");
-        if (!(g.boundsMin.x <= g.boundsMax.x && g.boundsMin.y <= g.boundsMax.y && g.boundsMin.z <= g.boundsMax.z))
+        // A noise field's bounds may be empty (min >= max on an axis): the field then has no bounds.
+        if (g.field != prgpu::GridNoise &&
+            !(g.boundsMin.x <= g.boundsMax.x && g.boundsMin.y <= g.boundsMax.y && g.boundsMin.z <= g.boundsMax.z))
             return fail("empty grid medium bounds");
     }
     if (!spec_ok(sd->envSpectrum, ns)) return fail("envSpectrum out of range");
@@ -658,14 +665,22 @@ bool upload_scene(DeviceState &ds, const prgpu::SceneDesc *sd, const prgpu::Scen
             dg.sigmaA = g.sigmaA;
             dg.sigmaS = g.sigmaS;
             dg.noise = g.field == prgpu::GridNoise ? 1 : 0;
+            dg.boundless = 0;
             if (dg.noise) {
-                // One macro cell over the bounds with the field's maximum density (1).
+                // One macro cell over the bounds with the field's maximum density (1). Empty bounds
+                // (Bounds3f::IsEmpty, math.h:212: min > max on an axis): no bounds at all, and no
+                // falloff (NoiseField::Density, medium.cpp:168-177); the zeroed box makes the
+                // macro-cell walk one cell over the whole segment.
+                if (g.boundsMin.x > g.boundsMax.x || g.boundsMin.y > g.boundsMax.y || g.boundsMin.z > g.boundsMax.z) {
+                    dg.boundless = 1;
+                    for (int a = 0; a < 3; ++a) dg.bmin[a] = dg.bmax[a] = 0.f;
+                }
                 dg.nx = dg.ny = dg.nz = 0;
                 dg.density = nullptr;
                 dg.maxDensity = std::max(1.f, std::isfinite(g.maxDensity) ? g.maxDensity : 1.f);
                 dg.mx = dg.my = dg.mz = 1;
                 dg.noiseOctaves = g.noiseOctaves;
-                dg.noiseFalloff = g.noiseFalloff ? 1 : 0;
+                dg.noiseFalloff = g.noiseFalloff && !dg.boundless ? 1 : 0;
                 dg.noiseFrequency = g.noiseFrequency;
                 dg.noiseThreshold = g.noiseThreshold;
                 dg.noiseSharpness = g.noiseSharpness;

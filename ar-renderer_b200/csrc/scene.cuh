@@ -29,8 +29,9 @@ struct DevGrid {
     // trilinear density anywhere in the cell (a one-voxel margin on every side).
     int mx, my, mz;
     const float *majorant;
-    // pr::NoiseField in place of the voxels (noise != 0).
-    int noise, noiseOctaves, noiseFalloff;
+    // pr::NoiseField in place of the voxels (noise != 0). boundless: a noise field with empty bounds,
+    // which fills every finite segment (medium.cpp:168-177, GridMedium::Clip, medium.cpp:182-188).
+    int noise, noiseOctaves, noiseFalloff, boundless;
     float noiseFrequency, noiseThreshold, noiseSharpness;
     float noiseOffset[3];
     // Index-space voxels (indexed != 0): voxel (x, y, z) at integer coordinate org + (x, y, z).

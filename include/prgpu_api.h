@@ -211,7 +211,9 @@ struct LightBVHNode {
 // field = GridNoise replaces the voxels by pr::NoiseField (medium.h:119-133, medium.cpp:168-177):
 // density = clamp((n - threshold) * sharpness, 0, 1) with n = 0.5 + 0.7 fBm((p + offset) *
 // frequency) of improved Perlin noise, faded by 1 - |2 (p - min) / (max - min) - 1|^2 when falloff
-// is set; 0 outside the (non-empty) bounds; the majorant is 1 unless maxDensity says more.
+// is set; 0 outside the bounds; the majorant is 1 unless maxDensity says more. Empty bounds
+// (boundsMin > boundsMax on an axis, as an unset pr::Bounds3f) mean no bounds: the field fills
+// every finite segment and has no falloff (GridMedium::Clip, medium.cpp:182-188).
 // field = GridIndexed takes the voxels of an index-space grid: a NanoVDB float grid densified by
 // the caller (pr::NanoVDBField, media/nanovdb_field.cpp:17-46). Medium space is then the grid's
 // index space (worldToMedium = the grid's world-to-index map after the medium's own transform);

@@ -158,3 +158,48 @@ def test_grid_medium_input_validation(gpu, oracle):
     with pytest.raises(abi.PrgpuError, match="(?i)medium"):
         render.render_ex(sd, w, h, 1)
     assert C.sizeof(abi.GridMediumDesc) == 160
+
+
+def test_boundless_noise_medium_matches_a_box_around_its_container(gpu, oracle):
+    """A noise field with empty bounds (pr::NoiseField over an empty box: medium.cpp:168-177 and
+    GridMedium::Clip, medium.cpp:182-188, which then fill every finite segment, without falloff).
+    The reference's scene loader never leaves a field unbounded (it fits the bounds to the enclosing
+    objects), so this compares two device renders: inside the smoke's closed interface box every
+    segment is finite and lies inside any box that contains the interface box, so the boundless
+    field must render bit for bit as the same field bounded by such a box (falloff off), which the
+    bounded-noise test above checks against the reference."""
+    import json
+
+    from prgpu import abi, media, render
+
+    w = h = 32
+    path, s = ru.grid_scene_file("noise_boundless_src", seed=0, width=w, height=h)
+    with open(path) as f:
+        doc = json.load(f)
+    params = {"frequency": 2.0, "octaves": 4, "threshold": 0.35, "sharpness": 3.0, "offset": [0.2, -0.1, 0.4]}
+    smoke = doc["media"]["smoke"]
+    smoke.pop("file")
+    smoke.pop("bounds", None)
+    smoke.update(type="noise", falloff="none", **params)
+    path = path.replace("noise_boundless_src", "noise_boundless")
+    with open(path, "w") as f:
+        json.dump(doc, f)
+    rs = oracle.RefScene(path)
+    (name, fitted), = rs.grid_media()  # the interface box, in medium space
+    assert name == "smoke" and (fitted[0] < fitted[1]).all(), fitted
+    sd, ext = ru.grid_scene_inputs(rs, s, noise=dict(params, falloff=False))
+    w2m = media.affine_inverse(s.grid["matrix"])
+    kw = dict(scale=s.grid["scale"], g=s.grid["g"], world_to_medium=w2m, falloff=False, **params)
+    na = sd.spectrumCount - 2  # the smoke's sigma_a and sigma_s, appended last
+    big = media.noise_desc(na, na + 1, np.stack([fitted[0] - 1.0, fitted[1] + 1.0]), **kw)
+    empty = media.noise_desc(na, na + 1, np.array([[np.inf] * 3, [-np.inf] * 3], np.float32), **kw)
+    images = []
+    for desc in (big, empty):
+        e = render.make_ext(grid_media=[desc])
+        images.append(np.stack([render.render_ex(sd, w, h, 64, seed=300 + k, max_depth=8, ext=e) for k in range(2)]))
+    assert images[0][..., 1].mean() > 0
+    np.testing.assert_array_equal(images[1], images[0])
+    # An empty field is not a box of zero extent: that is refused.
+    flat = media.noise_desc(na, na + 1, np.stack([fitted[0], fitted[0]]), **kw)
+    with pytest.raises(RuntimeError, match="positive extent"):
+        render.render_ex(sd, w, h, 1, seed=1, max_depth=8, ext=render.make_ext(grid_media=[flat]))
